@@ -1,0 +1,124 @@
+"""hacs_b200 -- host-side Python mirror of the B200-native exact modular matrix engine.
+
+The engine itself is libhme.so (CUDA C++ for sm_100a, C ABI in include/hme.h).
+This module mirrors the reference engine's operator names and argument meaning
+(drjanosch42/hacs 0.2.1, ``engine::kernels`` / ``engine::elim`` /
+``engine::ring2k`` / ``engine::ring3k``) over numpy host arrays, and offers
+device-pointer variants over torch CUDA tensors:
+
+  ``Engine.gemm(p, A, B, C=None, op=SET)``   engine::kernels::gemm<uint32_t> (Kernels.h:178-185)
+
+Every call goes to libhme; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from . import _lib
+from ._lib import HME_ADD as ADD, HME_SET as SET, HME_SUB as SUB, HmeError, check
+
+__all__ = ["Engine", "SET", "ADD", "SUB", "HmeError", "build", "limbs_for"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def build(verbose: bool = False) -> str:
+    """Compile libhme.so in-tree with nvcc for sm_100a; returns its path."""
+    out = None if verbose else subprocess.DEVNULL
+    subprocess.check_call(["make", "-j8", "-C", os.path.join(HERE, "csrc")], stdout=out)
+    return _lib.LIB_PATH
+
+
+def limbs_for(p: int) -> int:
+    """Unsigned 8-bit limbs per residue of Z/p: 1, 2, 3 or 4."""
+    return 1 if p <= 256 else 2 if p <= 65536 else 3 if p <= (1 << 24) else 4
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _p32(a: np.ndarray):
+    return a.ctypes.data_as(_lib.u32p)
+
+
+def _dev_ptr(t) -> int:
+    import torch
+
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("device entry points take CUDA torch tensors")
+    if t.element_size() != 4:
+        raise TypeError("device tensors must hold 32-bit words (torch.int32 or torch.uint32)")
+    if t.dim() != 2 or t.stride(1) != 1:
+        raise ValueError("device tensors must be 2-D with unit column stride")
+    return t.data_ptr()
+
+
+class Engine:
+    """One libhme context: a device, a stream and the device workspace."""
+
+    def __init__(self, device: int = 0):
+        self._lib = _lib.lib()
+        h = C.c_void_p()
+        check(self._lib.hme_ctx_create(device, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.hme_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - interpreter teardown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- context ------------------------------------------------------------
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(self._lib.hme_ctx_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def use_torch_stream(self) -> None:
+        """Run on torch's current CUDA stream (so torch and libhme order their work)."""
+        import torch
+
+        self.set_stream(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def sync(self) -> None:
+        check(self._lib.hme_ctx_sync(self._h))
+
+    @property
+    def launches(self) -> int:
+        return int(self._lib.hme_ctx_launches(self._h))
+
+    # ---- GEMM -------------------------------------------------------------------
+    def gemm(self, p: int, A, B, C=None, op: int = SET) -> np.ndarray:
+        """C op= A*B mod p on host arrays (engine::kernels::gemm<uint32_t>)."""
+        A, B = _u32(A), _u32(B)
+        m, k = A.shape
+        k2, n = B.shape
+        if k != k2:
+            raise ValueError("gemm: inner dimensions differ")
+        out = np.zeros((m, n), np.uint32) if C is None else _u32(C).copy()
+        check(self._lib.hme_gemm_u32(self._h, p, m, n, k, _p32(A), k, _p32(B), n, _p32(out), n, op))
+        return out
+
+    def gemm_dev(self, p: int, A, B, C, op: int = SET) -> None:
+        """C op= A*B mod p on CUDA tensors, asynchronous on the engine's stream."""
+        m, k = A.shape
+        n = B.shape[1]
+        if B.shape[0] != k or tuple(C.shape) != (m, n):
+            raise ValueError("gemm_dev: shape mismatch")
+        check(self._lib.hme_gemm_u32_dev(self._h, p, m, n, k, _dev_ptr(A), A.stride(0), _dev_ptr(B), B.stride(0),
+                                         _dev_ptr(C), C.stride(0), op))

@@ -1,0 +1,73 @@
+"""ctypes binding of libhme.so (the C ABI declared in include/hme.h).
+
+The library is built in-tree by ``hacs_b200.build()`` (nvcc, sm_100a).  There
+is no fallback: if libhme.so is missing or cannot be loaded, every entry point
+raises, so no result can silently come from anywhere but the CUDA library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhme.so")
+
+HME_OK = 0
+HME_EINVAL = -1
+HME_ECUDA = -2
+HME_ENOMEM = -3
+HME_ETIMEOUT = -4
+HME_EUNSUPPORTED = -5
+HME_ENOTINSPAN = -6
+
+HME_SET, HME_ADD, HME_SUB = 0, 1, 2
+
+u32p = C.POINTER(C.c_uint32)
+vp = C.c_void_p
+sz = C.c_size_t
+u32 = C.c_uint32
+
+# name -> (restype, argtypes); mirrors include/hme.h
+PROTOTYPES = {
+    "hme_ctx_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+    "hme_ctx_destroy": (C.c_int, [vp]),
+    "hme_ctx_set_stream": (C.c_int, [vp, vp]),
+    "hme_ctx_sync": (C.c_int, [vp]),
+    "hme_ctx_launches": (C.c_uint64, [vp]),
+    "hme_last_error": (C.c_char_p, []),
+    "hme_version": (C.c_char_p, []),
+    "hme_fnv1a_u32": (C.c_uint64, [u32p, u32, u32, sz]),
+    "hme_gemm_u32": (C.c_int, [vp, u32, u32, u32, u32, u32p, sz, u32p, sz, u32p, sz, C.c_int]),
+    "hme_gemm_u32_dev": (C.c_int, [vp, u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class HmeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"hme error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.exists(LIB_PATH):
+                    raise ImportError(f"libhme.so not built at {LIB_PATH}; run hacs_b200.build()")
+                L = C.CDLL(LIB_PATH)
+                for name, (res, args) in PROTOTYPES.items():
+                    f = getattr(L, name)
+                    f.restype = res
+                    f.argtypes = args
+                _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != HME_OK:
+        raise HmeError(rc, lib().hme_last_error().decode(errors="replace"))

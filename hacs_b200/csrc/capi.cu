@@ -1,0 +1,216 @@
+// The C ABI of libhme (include/hme.h): contexts, error plumbing, workspace and
+// the GEMM entry points.  No C++ exception crosses this boundary.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+
+#include "hme_internal.h"
+
+namespace hme {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+void* Workspace::get(int slot, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (size[slot] < bytes) {
+        if (ptr[slot]) HME_CUDA(cudaFree(ptr[slot]));
+        ptr[slot] = nullptr;
+        size[slot] = 0;
+        // grow with headroom so a sequence of slightly larger calls does not reallocate every time
+        const size_t want = bytes + bytes / 8;
+        HME_CUDA(cudaMalloc(&ptr[slot], want));
+        size[slot] = want;
+    }
+    return ptr[slot];
+}
+
+void Workspace::release() {
+    for (int s = 0; s < kSlots; ++s) {
+        if (ptr[s]) cudaFree(ptr[s]);
+        ptr[s] = nullptr;
+        size[s] = 0;
+    }
+}
+
+void bind(hme_ctx* ctx) { HME_CUDA(cudaSetDevice(ctx->device)); }
+
+void check_device_error(hme_ctx* ctx) {
+    HME_CUDA(cudaStreamSynchronize(ctx->stream));
+    int code = 0;
+    HME_CUDA(cudaMemcpy(&code, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (code != 0) {
+        const int zero = 0;
+        HME_CUDA(cudaMemcpy(ctx->d_err, &zero, sizeof(int), cudaMemcpyHostToDevice));
+        throw Error(HME_ETIMEOUT, "a bounded device-side wait ran out (device code " + std::to_string(code) +
+                                      "); the kernel returned early and its output is incomplete");
+    }
+}
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        return HME_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return HME_ENOMEM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return HME_EINVAL;
+    } catch (...) {
+        set_last_error("unknown exception");
+        return HME_EINVAL;
+    }
+}
+
+// RAII device buffer for the host-pointer entry points.
+struct DevBuf {
+    void* p = nullptr;
+    explicit DevBuf(size_t bytes) { HME_CUDA(cudaMalloc(&p, bytes ? bytes : 16)); }
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+const char* last_error_cstr() { return g_last_error.c_str(); }
+
+}  // namespace hme
+
+using namespace hme;
+
+extern "C" {
+
+const char* hme_last_error(void) { return last_error_cstr(); }
+
+const char* hme_version(void) { return "hme 0.1 (sm_100a)"; }
+
+int hme_ctx_create(int device, hme_ctx** out) {
+    return guard([&] {
+        HME_REQUIRE(out != nullptr, "hme_ctx_create: out is null");
+        *out = nullptr;
+        int count = 0;
+        HME_CUDA(cudaGetDeviceCount(&count));
+        HME_REQUIRE(device >= 0 && device < count, "hme_ctx_create: no such device");
+        cudaDeviceProp prop{};
+        HME_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major != 10 || prop.minor != 0)
+            throw Error(HME_EUNSUPPORTED, std::string("hme needs an sm_100 (B200) device; found ") + prop.name +
+                                              " sm_" + std::to_string(prop.major) + std::to_string(prop.minor));
+        auto* c = new hme_ctx();
+        c->device = device;
+        c->num_sms = prop.multiProcessorCount;
+        try {
+            HME_CUDA(cudaSetDevice(device));
+            HME_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+            c->stream = c->own_stream;
+            HME_CUDA(cudaMalloc(&c->d_err, sizeof(int)));
+            HME_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+        } catch (...) {
+            if (c->own_stream) cudaStreamDestroy(c->own_stream);
+            if (c->d_err) cudaFree(c->d_err);
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int hme_ctx_destroy(hme_ctx* ctx) {
+    return guard([&] {
+        if (!ctx) return;
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        ctx->ws.release();
+        if (ctx->d_err) cudaFree(ctx->d_err);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        delete ctx;
+    });
+}
+
+int hme_ctx_set_stream(hme_ctx* ctx, void* stream) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    });
+}
+
+int hme_ctx_sync(hme_ctx* ctx) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        bind(ctx);
+        check_device_error(ctx);
+    });
+}
+
+uint64_t hme_ctx_launches(const hme_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int hme_gemm_u32_dev(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A, size_t lda,
+                     const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        HME_REQUIRE(p >= 2, "gemm: modulus must be >= 2");
+        bind(ctx);
+        gemm_u32_device(ctx, make_mod(p), m, n, k, A, lda, B, ldb, C, ldc, op);
+    });
+}
+
+int hme_gemm_u32(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A, size_t lda,
+                 const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        HME_REQUIRE(p >= 2, "gemm: modulus must be >= 2");
+        HME_REQUIRE(op == HME_SET || op == HME_ADD || op == HME_SUB, "gemm: bad op");
+        if (m == 0 || n == 0) return;
+        HME_REQUIRE(C != nullptr && ldc >= n, "gemm: bad C");
+        HME_REQUIRE(k == 0 || (A && B && lda >= k && ldb >= n), "gemm: bad A/B");
+        bind(ctx);
+        // compact device copies (row-major, ld = cols)
+        DevBuf dA(sizeof(uint32_t) * static_cast<size_t>(m) * k), dB(sizeof(uint32_t) * static_cast<size_t>(k) * n),
+            dC(sizeof(uint32_t) * static_cast<size_t>(m) * n);
+        if (k) {
+            HME_CUDA(cudaMemcpy2DAsync(dA.p, sizeof(uint32_t) * k, A, sizeof(uint32_t) * lda, sizeof(uint32_t) * k, m,
+                                       cudaMemcpyHostToDevice, ctx->stream));
+            HME_CUDA(cudaMemcpy2DAsync(dB.p, sizeof(uint32_t) * n, B, sizeof(uint32_t) * ldb, sizeof(uint32_t) * n, k,
+                                       cudaMemcpyHostToDevice, ctx->stream));
+        }
+        if (op != HME_SET)
+            HME_CUDA(cudaMemcpy2DAsync(dC.p, sizeof(uint32_t) * n, C, sizeof(uint32_t) * ldc, sizeof(uint32_t) * n, m,
+                                       cudaMemcpyHostToDevice, ctx->stream));
+        gemm_u32_device(ctx, make_mod(p), m, n, k, dA.as<uint32_t>(), k, dB.as<uint32_t>(), n, dC.as<uint32_t>(), n,
+                        op);
+        HME_CUDA(cudaMemcpy2DAsync(C, sizeof(uint32_t) * ldc, dC.p, sizeof(uint32_t) * n, sizeof(uint32_t) * n, m,
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+        check_device_error(ctx);
+    });
+}
+
+}  // extern "C"
+
+extern "C" HME_API uint64_t hme_fnv1a_u32(const uint32_t* M, uint32_t rows, uint32_t cols, size_t ld) {
+    uint64_t h = 0xcbf29ce484222325ull;
+    auto feed = [&h](uint64_t v) {
+        for (int i = 0; i < 8; ++i) {
+            h ^= (v >> (8 * i)) & 0xffu;
+            h *= 0x100000001b3ull;
+        }
+    };
+    feed(rows);
+    feed(cols);
+    for (uint32_t i = 0; i < rows; ++i)
+        for (uint32_t j = 0; j < cols; ++j) feed(M[static_cast<size_t>(i) * ld + j]);
+    return h;
+}

@@ -1,0 +1,72 @@
+// Host-side internals shared by the translation units of libhme: the context,
+// error plumbing and the device workspace.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/hme.h"
+#include "hme_mod.h"
+
+namespace hme {
+
+// Thrown inside the library, turned into a status code at the C boundary.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+
+#define HME_CUDA(call)                                                                                  \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            throw ::hme::Error(e_ == cudaErrorMemoryAllocation ? HME_ENOMEM : HME_ECUDA,                \
+                               std::string(#call) + ": " + cudaGetErrorString(e_));                     \
+    } while (0)
+
+#define HME_REQUIRE(cond, msg)                                        \
+    do {                                                              \
+        if (!(cond)) throw ::hme::Error(HME_EINVAL, (msg));           \
+    } while (0)
+
+// Grow-only device scratch arena: one region per purpose ("slot") so that a
+// caller holding slot 0 (limb planes of A) can also hold slot 1 (planes of B).
+struct Workspace {
+    static constexpr int kSlots = 8;
+    void* ptr[kSlots] = {};
+    size_t size[kSlots] = {};
+    void* get(int slot, size_t bytes);
+    void release();
+};
+
+}  // namespace hme
+
+struct hme_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;      // active stream
+    cudaStream_t own_stream = nullptr;  // created by the context
+    int* d_err = nullptr;               // device error word written by bounded waits
+    uint64_t launches = 0;
+    hme::Workspace ws;
+};
+
+namespace hme {
+
+// Fails with HME_ETIMEOUT (and clears the word) when a kernel on this context
+// recorded a device-side wait that ran out.  Synchronises the stream.
+void check_device_error(hme_ctx* ctx);
+
+// Make the context's device current on the calling thread.
+void bind(hme_ctx* ctx);
+
+// ---- the limb GEMM (limb_gemm.cu) ------------------------------------------
+// C op= A*B mod p with device pointers, on ctx->stream.
+void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
+                     size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op);
+
+}  // namespace hme

@@ -1,0 +1,489 @@
+// The INT8-limb tcgen05 mod-p GEMM: C op= A*B mod p, u32 residues, p < 2^32.
+//
+// Reference semantics: engine::kernels::gemm<uint32_t> (src/ModArithmetic/
+// Kernels.h:178-185, Kernels.cpp:1418-1483) and its device twin
+// engine::cuda::gemm (src/Cuda/cuda_kernels.cu:195-299, 474-519): the exact sum
+// of k products reduced to the canonical residue, combined by Set/Add/Sub.
+//
+// Method.  Write a = sum_i a_i 256^i with unsigned bytes a_i (i < L).  Then
+//     A*B = sum_i a_i * B^(i)  (mod p),   B^(i) = 256^i * B mod p,
+// and with B^(i) = sum_j b^(i)_j 256^j:
+//     A*B = sum_j 256^j D_j (mod p),      D_j = sum_i a_i * b^(i)_j.
+// D_j is a plain u8 x u8 -> s32 GEMM over the virtual K' = L*K; for fixed
+// output columns the L matrices D_j sit side by side in one accumulator of
+// L*BN columns, so a CTA runs ONE integer GEMM of 128 x (L*BN) x (L*K) on the
+// tensor cores (tcgen05.mma kind::i8, M=128, N=L*BN, K=32 per instruction),
+// then recombines sum_j 256^j D_j in u64 and reduces once (Barrett, the
+// ModCtx<uint32_t>::reduce_u64 rule).  Exactness: every D_j is a sum of at
+// most L*K_chunk products below 255^2, and K is cut into chunks with
+// L * 255^2 * K_chunk < 2^31 (later chunks accumulate with Add).
+//
+// Layout in HBM (workspace): A limb planes [i][m][k] (L x M x Kp bytes) and
+// B planes [i][j][n][k] (L x L x N x Kp bytes), K contiguous (K-major for both
+// tensor-core operands), Kp = K rounded up to 16 bytes for TMA strides.
+//
+// Kernel: persistent, one CTA per SM, 6 warps: warp 0 issues TMA loads
+// (128-byte swizzle, no multicast), warp 1 owns tensor memory and issues the
+// MMAs, warps 2-5 drain the double-buffered accumulator (2 x L*BN columns of
+// TMEM) into C while the next tile's MMAs run.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "hme_internal.h"
+#include "hme_ptx.cuh"
+
+namespace hme {
+namespace {
+
+constexpr int kBM = 128;     // UMMA M (rows of C per tile, one TMEM lane each)
+constexpr int kBK = 128;     // bytes of K per pipeline stage: one 128-byte swizzle row
+constexpr int kThreads = 192;
+
+template <int L, int BN>
+struct Cfg {
+    static constexpr int UN = L * BN;  // UMMA N: L accumulators of BN columns
+    static_assert(UN % 16 == 0 && UN >= 16 && UN <= 256, "UMMA N must be a multiple of 16 in [16, 256]");
+    static_assert(BN % 16 == 0, "the epilogue drains 16 columns at a time");
+    static constexpr int A_BYTES = kBM * kBK;
+    static constexpr int B_BYTES = UN * kBK;
+    static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+    static constexpr int STAGES = UN > 128 ? 4 : UN > 64 ? 6 : 8;
+    static constexpr int ACC_STRIDE = UN <= 32 ? 32 : UN <= 64 ? 64 : UN <= 128 ? 128 : 256;
+    static constexpr int TMEM_COLS = 2 * ACC_STRIDE;
+    static constexpr int BAR_BYTES = 256;
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + BAR_BYTES;
+    static constexpr uint32_t IDESC = idesc_u8(kBM, UN);
+    static_assert((2 * STAGES + 5) * 8 + 8 <= BAR_BYTES, "barrier area too small");
+};
+
+struct GemmArgs {
+    uint32_t* C;
+    uint64_t ldc;
+    int M, N;
+    int k_begin;  // first k of this chunk (multiple of kBK)
+    int kblocks;  // k-blocks of kBK bytes in this chunk
+    int op;
+    uint32_t p;
+    uint64_t barrett;
+    int tiles_m, tiles_n, group_m;
+    int* err;
+};
+
+__device__ __forceinline__ void tile_coords(int tile, const GemmArgs& g, int& tm, int& tn) {
+    // Grouped raster: group_m tile-rows share the B tiles they stream, so a
+    // wave of CTAs re-reads each K-slice of A and B from L2, not HBM.
+    const int per_group = g.group_m * g.tiles_n;
+    const int grp = tile / per_group;
+    const int first_m = grp * g.group_m;
+    const int gm = min(g.tiles_m - first_m, g.group_m);
+    const int local = tile - grp * per_group;
+    tm = first_m + local % gm;
+    tn = local / gm;
+}
+
+// Time-bounded wait that ignores the abort flag: used while tearing down, to
+// let in-flight copies and MMAs land before shared / tensor memory is released.
+__device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity, int* err) {
+    int never = 0;
+    mbar_wait(bar, parity, &never, err, DERR_WAIT_DRAIN);
+}
+
+template <int L, int BN>
+__global__ void __launch_bounds__(kThreads, 1)
+    limb_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     const GemmArgs g) {
+    using CF = Cfg<L, BN>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + CF::STAGES * CF::A_BYTES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + CF::STAGES * CF::STAGE_BYTES);
+    uint64_t* empty = full + CF::STAGES;
+    uint64_t* acc_full = empty + CF::STAGES;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int total_tiles = g.tiles_m * g.tiles_n;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < CF::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 128);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+        fence_proxy_async_smem();
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, CF::TMEM_COLS);
+        tmem_relinquish();
+    }
+    if (warp == 0 && lane == 0) {
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            int it = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; ok && tile < total_tiles; tile += gridDim.x) {
+                int tm, tn;
+                tile_coords(tile, g, tm, tn);
+                for (int i = 0; ok && i < L; ++i) {
+                    for (int kb = 0; kb < g.kblocks; ++kb, ++it) {
+                        const int s = it % CF::STAGES;
+                        const uint32_t ph = (it / CF::STAGES) & 1;
+                        if (!mbar_wait(&empty[s], ph ^ 1, abort_flag, g.err, DERR_WAIT_EMPTY)) {
+                            ok = false;
+                            break;
+                        }
+                        mbar_arrive_expect_tx(&full[s], CF::STAGE_BYTES);
+                        const int kx = g.k_begin + kb * kBK;
+                        tma_load_3d(sA + s * CF::A_BYTES, &tmA, &full[s], kx, tm * kBM, i);
+                        tma_load_4d(sB + s * CF::B_BYTES, &tmB, &full[s], kx, tn * BN, 0, i);
+                    }
+                }
+            }
+            if (!ok) {
+                // let every copy issued into shared memory land before the CTA exits
+                for (int t = max(0, it - CF::STAGES); t < it; ++t)
+                    drain_wait(&full[t % CF::STAGES], (t / CF::STAGES) & 1, g.err);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            int it = 0, lt = 0;
+            bool ok = true, issued_any = false;
+            for (int tile = blockIdx.x; ok && tile < total_tiles; tile += gridDim.x, ++lt) {
+                const int a = lt & 1;
+                const uint32_t aph = (lt >> 1) & 1;
+                if (!mbar_wait(&acc_empty[a], aph ^ 1, abort_flag, g.err, DERR_WAIT_ACCUM_FREE)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem_base + a * CF::ACC_STRIDE;
+                for (int i = 0; ok && i < L; ++i) {
+                    for (int kb = 0; kb < g.kblocks; ++kb, ++it) {
+                        const int s = it % CF::STAGES;
+                        const uint32_t ph = (it / CF::STAGES) & 1;
+                        if (!mbar_wait(&full[s], ph, abort_flag, g.err, DERR_WAIT_FULL)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint64_t adesc = smem_desc_k128(smem_u32(sA + s * CF::A_BYTES));
+                        const uint64_t bdesc = smem_desc_k128(smem_u32(sB + s * CF::B_BYTES));
+#pragma unroll
+                        for (int kk = 0; kk < kBK / 32; ++kk) {
+                            // +32 bytes along K inside the swizzle atom = +2 in the 16-byte address field
+                            mma_u8(d, adesc + 2 * kk, bdesc + 2 * kk, CF::IDESC, (i | kb | kk) != 0);
+                        }
+                        issued_any = true;
+                        mma_commit(&empty[s]);
+                    }
+                }
+                if (ok) mma_commit(&acc_full[a]);
+            }
+            if (!ok && issued_any) {
+                mma_commit(drain);
+                drain_wait(drain, 0, g.err);
+            }
+        }
+    } else {
+        // ---------------- epilogue: TMEM -> registers -> C ----------------
+        const int q = warp & 3;  // the TMEM lane quarter this warp may read
+        const uint32_t lane_base = static_cast<uint32_t>(q * 32) << 16;
+        const bool vec_ok = ((reinterpret_cast<uintptr_t>(g.C) & 15) == 0) && ((g.ldc & 3) == 0);
+        int lt = 0;
+        for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++lt) {
+            const int a = lt & 1;
+            const uint32_t aph = (lt >> 1) & 1;
+            if (!mbar_wait(&acc_full[a], aph, abort_flag, g.err, DERR_WAIT_ACCUM)) break;
+            tc_fence_after();
+            int tm, tn;
+            tile_coords(tile, g, tm, tn);
+            const int row = tm * kBM + q * 32 + lane;
+            const bool row_ok = row < g.M;
+            uint32_t* crow = g.C + static_cast<size_t>(row_ok ? row : 0) * g.ldc;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                uint32_t v[L][16];
+#pragma unroll
+                for (int j = 0; j < L; ++j)
+                    tmem_ld16(tmem_base + lane_base + a * CF::ACC_STRIDE + j * BN + c0, v[j]);
+                tmem_wait_ld();
+                const int col0 = tn * BN + c0;
+                if (!row_ok || col0 >= g.N) continue;
+                uint32_t r[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    uint64_t s = v[0][e];
+                    if (L > 1) s += static_cast<uint64_t>(v[L > 1 ? 1 : 0][e]) << 8;
+                    if (L > 2) s += static_cast<uint64_t>(v[L > 2 ? 2 : 0][e]) << 16;
+                    if (L > 3) s += static_cast<uint64_t>(v[L > 3 ? 3 : 0][e]) << 24;
+                    r[e] = reduce_u64(s, g.p, g.barrett);
+                }
+                uint32_t* dst = crow + col0;
+                if (vec_ok && col0 + 16 <= g.N) {
+                    uint4* d4 = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+                    for (int w = 0; w < 4; ++w) {
+                        uint4 o = make_uint4(r[4 * w], r[4 * w + 1], r[4 * w + 2], r[4 * w + 3]);
+                        if (g.op != HME_SET) {
+                            const uint4 c = d4[w];
+                            if (g.op == HME_ADD) {
+                                o.x = mod_add(c.x, o.x, g.p); o.y = mod_add(c.y, o.y, g.p);
+                                o.z = mod_add(c.z, o.z, g.p); o.w = mod_add(c.w, o.w, g.p);
+                            } else {
+                                o.x = mod_sub(c.x, o.x, g.p); o.y = mod_sub(c.y, o.y, g.p);
+                                o.z = mod_sub(c.z, o.z, g.p); o.w = mod_sub(c.w, o.w, g.p);
+                            }
+                        }
+                        d4[w] = o;
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        if (col0 + e >= g.N) break;
+                        uint32_t o = r[e];
+                        if (g.op == HME_ADD) o = mod_add(dst[e], o, g.p);
+                        else if (g.op == HME_SUB) o = mod_sub(dst[e], o, g.p);
+                        dst[e] = o;
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&acc_empty[a]);
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, CF::TMEM_COLS);
+    }
+}
+
+// ---- limb split ------------------------------------------------------------------
+// planes[i][m][k] = byte i of A[m][k]; k in [K, Kp) zero.  16 k per thread.
+template <int L>
+__global__ void split_a_kernel(const uint32_t* __restrict__ A, uint64_t lda, int M, int K, int Kp,
+                               uint8_t* __restrict__ planes) {
+    const int kch = Kp >> 4;
+    const size_t total = static_cast<size_t>(M) * kch;
+    const size_t plane = static_cast<size_t>(M) * Kp;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int row = static_cast<int>(idx / kch);
+        const int k0 = static_cast<int>(idx - static_cast<size_t>(row) * kch) << 4;
+        const uint32_t* src = A + static_cast<size_t>(row) * lda + k0;
+        uint32_t w[L][4];
+#pragma unroll
+        for (int j = 0; j < L; ++j) w[j][0] = w[j][1] = w[j][2] = w[j][3] = 0;
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            const uint32_t x = (k0 + e < K) ? __ldg(src + e) : 0u;
+#pragma unroll
+            for (int j = 0; j < L; ++j) w[j][e >> 2] |= ((x >> (8 * j)) & 0xffu) << (8 * (e & 3));
+        }
+        uint8_t* dst = planes + static_cast<size_t>(row) * Kp + k0;
+#pragma unroll
+        for (int j = 0; j < L; ++j)
+            *reinterpret_cast<uint4*>(dst + j * plane) = make_uint4(w[j][0], w[j][1], w[j][2], w[j][3]);
+    }
+}
+
+// planes[i][j][n][k] = byte j of (256^i * B[k][n] mod p): B transposed to
+// K-major through shared memory, 64 k x 32 n per block, 8 k per thread.
+template <int L>
+__global__ void __launch_bounds__(256) split_b_kernel(const uint32_t* __restrict__ B, uint64_t ldb, int K, int N,
+                                                      int Kp, uint32_t p, uint64_t barrett,
+                                                      uint8_t* __restrict__ planes) {
+    __shared__ uint32_t tile[64][33];
+    const int k0 = blockIdx.x * 64, n0 = blockIdx.y * 32;
+    for (int t = threadIdx.x; t < 64 * 32; t += 256) {
+        const int kk = t >> 5, nn = t & 31;
+        const int k = k0 + kk, n = n0 + nn;
+        tile[kk][nn] = (k < K && n < N) ? __ldg(B + static_cast<size_t>(k) * ldb + n) : 0u;
+    }
+    __syncthreads();
+    const int nn = threadIdx.x >> 3, kc = threadIdx.x & 7;
+    const int n = n0 + nn, kb = k0 + kc * 8;
+    if (n >= N || kb >= Kp) return;
+    uint32_t out[L][L][2];
+#pragma unroll
+    for (int i = 0; i < L; ++i)
+#pragma unroll
+        for (int j = 0; j < L; ++j) out[i][j][0] = out[i][j][1] = 0;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        uint32_t v = tile[kc * 8 + e][nn];
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+            if (i) v = reduce_u64(static_cast<uint64_t>(v) << 8, p, barrett);
+#pragma unroll
+            for (int j = 0; j < L; ++j) out[i][j][e >> 2] |= ((v >> (8 * j)) & 0xffu) << (8 * (e & 3));
+        }
+    }
+    const size_t plane = static_cast<size_t>(N) * Kp;
+#pragma unroll
+    for (int i = 0; i < L; ++i)
+#pragma unroll
+        for (int j = 0; j < L; ++j)
+            *reinterpret_cast<uint2*>(planes + (i * L + j) * plane + static_cast<size_t>(n) * Kp + kb) =
+                make_uint2(out[i][j][0], out[i][j][1]);
+}
+
+// ---- host side ---------------------------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    if (!fn) throw Error(HME_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    return fn;
+}
+
+void encode_u8(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
+               const cuuint32_t* box) {
+    cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, rank, base, dims, strides, box, estr,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(HME_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")");
+}
+
+template <int L, int BN>
+void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, int Kp,
+                 uint8_t* planesA, uint8_t* planesB, uint32_t* C, size_t ldc, int op) {
+    using CF = Cfg<L, BN>;
+    static std::once_flag attr_once;
+    std::call_once(attr_once, [] {
+        cudaFuncSetAttribute(limb_gemm_kernel<L, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM);
+    });
+    CUtensorMap tmA, tmB;
+    {
+        const cuuint64_t dims[3] = {k, m, static_cast<cuuint64_t>(L)};
+        const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * m};
+        const cuuint32_t box[3] = {kBK, kBM, 1};
+        encode_u8(&tmA, planesA, 3, dims, strides, box);
+    }
+    {
+        const cuuint64_t dims[4] = {k, n, static_cast<cuuint64_t>(L), static_cast<cuuint64_t>(L)};
+        const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * n,
+                                       static_cast<cuuint64_t>(Kp) * n * L};
+        const cuuint32_t box[4] = {kBK, BN, static_cast<cuuint32_t>(L), 1};
+        encode_u8(&tmB, planesB, 4, dims, strides, box);
+    }
+    GemmArgs g{};
+    g.C = C;
+    g.ldc = ldc;
+    g.M = static_cast<int>(m);
+    g.N = static_cast<int>(n);
+    g.p = mp.p;
+    g.barrett = mp.barrett;
+    g.tiles_m = static_cast<int>((m + kBM - 1) / kBM);
+    g.tiles_n = static_cast<int>((n + BN - 1) / BN);
+    g.group_m = 16;
+    g.err = ctx->d_err;
+    const int total = g.tiles_m * g.tiles_n;
+    const int grid = std::min(total, ctx->num_sms);
+    const uint32_t chunk = limb_k_chunk(L);
+    for (uint32_t kb0 = 0; kb0 < k; kb0 += chunk) {
+        const uint32_t kc = std::min(chunk, k - kb0);
+        g.k_begin = static_cast<int>(kb0);
+        g.kblocks = static_cast<int>((kc + kBK - 1) / kBK);
+        g.op = kb0 == 0 ? op : (op == HME_SET ? HME_ADD : op);
+        limb_gemm_kernel<L, BN><<<grid, kThreads, CF::SMEM, ctx->stream>>>(tmA, tmB, g);
+        HME_CUDA(cudaGetLastError());
+        ++ctx->launches;
+    }
+}
+
+__global__ void fill_zero_kernel(uint32_t* C, uint64_t ldc, int m, int n) {
+    const size_t total = static_cast<size_t>(m) * n;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        C[(i / n) * ldc + (i % n)] = 0;
+}
+
+}  // namespace
+
+void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
+                     size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op) {
+    HME_REQUIRE(op == HME_SET || op == HME_ADD || op == HME_SUB, "gemm: op must be HME_SET, HME_ADD or HME_SUB");
+    HME_REQUIRE(mp.p >= 2, "gemm: modulus must be >= 2");
+    HME_REQUIRE(m < (1u << 30) && n < (1u << 30) && k < (1u << 30), "gemm: dimension too large");
+    if (m == 0 || n == 0) return;
+    HME_REQUIRE(ldc >= n, "gemm: ldc < n");
+    if (k == 0) {
+        if (op == HME_SET) {
+            fill_zero_kernel<<<std::min<size_t>(1024, (static_cast<size_t>(m) * n + 255) / 256), 256, 0,
+                               ctx->stream>>>(C, ldc, m, n);
+            HME_CUDA(cudaGetLastError());
+            ++ctx->launches;
+        }
+        return;
+    }
+    HME_REQUIRE(A && B && C, "gemm: null pointer");
+    HME_REQUIRE(lda >= k && ldb >= n, "gemm: leading dimension too small");
+    const int L = static_cast<int>(mp.limbs);
+    const int Kp = static_cast<int>((k + 15) / 16 * 16);
+    uint8_t* pa = static_cast<uint8_t*>(ctx->ws.get(0, static_cast<size_t>(L) * m * Kp));
+    uint8_t* pb = static_cast<uint8_t*>(ctx->ws.get(1, static_cast<size_t>(L) * L * n * Kp));
+
+    {
+        const size_t work = static_cast<size_t>(m) * (Kp / 16);
+        const int grid = static_cast<int>(std::min<size_t>((work + 255) / 256, static_cast<size_t>(ctx->num_sms) * 16));
+        const dim3 gb((Kp + 63) / 64, (n + 31) / 32);
+        switch (L) {
+            case 1: split_a_kernel<1><<<grid, 256, 0, ctx->stream>>>(A, lda, m, k, Kp, pa);
+                    split_b_kernel<1><<<gb, 256, 0, ctx->stream>>>(B, ldb, k, n, Kp, mp.p, mp.barrett, pb); break;
+            case 2: split_a_kernel<2><<<grid, 256, 0, ctx->stream>>>(A, lda, m, k, Kp, pa);
+                    split_b_kernel<2><<<gb, 256, 0, ctx->stream>>>(B, ldb, k, n, Kp, mp.p, mp.barrett, pb); break;
+            case 3: split_a_kernel<3><<<grid, 256, 0, ctx->stream>>>(A, lda, m, k, Kp, pa);
+                    split_b_kernel<3><<<gb, 256, 0, ctx->stream>>>(B, ldb, k, n, Kp, mp.p, mp.barrett, pb); break;
+            default: split_a_kernel<4><<<grid, 256, 0, ctx->stream>>>(A, lda, m, k, Kp, pa);
+                    split_b_kernel<4><<<gb, 256, 0, ctx->stream>>>(B, ldb, k, n, Kp, mp.p, mp.barrett, pb); break;
+        }
+        HME_CUDA(cudaGetLastError());
+        ctx->launches += 2;
+    }
+    switch (L) {
+        case 1: launch_gemm<1, 256>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
+        case 2: launch_gemm<2, 128>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
+        case 3: launch_gemm<3, 80>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
+        default: launch_gemm<4, 64>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
+    }
+}
+
+}  // namespace hme

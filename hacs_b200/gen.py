@@ -1,0 +1,65 @@
+"""Seeded input generators of the reference's benchmarks, vectorised.
+
+splitmix64 / SeedFor / RandomEntries / EngineMatrixImpl follow
+src/ModArithmetic/PerformanceSmokeValidation.cpp:64-88 and :329-337 of the
+reference; the FNV-1a-64 matrix checksum follows :104-120 and
+src/ModArithmetic/Fnv.h.  Element i of a splitmix64 stream seeded with s is
+mix(s + (i + 1) * gamma), so a whole matrix is one vectorised expression.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+GAMMA = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+MASK64 = (1 << 64) - 1
+
+
+def seed_for(r: int, c: int, ell: int, salt: int) -> int:
+    s = 0xC0FFEE123456789 ^ salt
+    s = (s * 0x100000001B3 + r) & MASK64
+    s = (s * 0x100000001B3 + c) & MASK64
+    s = (s * 0x100000001B3 + ell) & MASK64
+    return s
+
+
+def splitmix_stream(seed: int, count: int, start: int = 0) -> np.ndarray:
+    """Outputs start .. start+count-1 of splitmix64 seeded with `seed`."""
+    with np.errstate(over="ignore"):
+        i = np.arange(start + 1, start + count + 1, dtype=np.uint64)
+        z = np.uint64(seed) + i * GAMMA
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+def random_entries(count: int, ell: int, seed: int) -> np.ndarray:
+    out = np.empty(count, dtype=np.uint32)
+    step = 1 << 24
+    for s0 in range(0, count, step):
+        n = min(step, count - s0)
+        out[s0:s0 + n] = (splitmix_stream(seed, n, s0) % np.uint64(ell)).astype(np.uint32)
+    return out
+
+
+def engine_matrix(rows: int, cols: int, ell: int, salt: int) -> np.ndarray:
+    """EngineMatrixImpl(rows, cols, ell, salt)."""
+    return random_entries(rows * cols, ell, seed_for(rows, cols, ell, salt)).reshape(rows, cols)
+
+
+def ranked_factors(rows: int, cols: int, rank: int, ell: int):
+    """The two factors of RankedMatrix(rows, cols, rank, ell) (salts 0x21 / 0x22,
+    PerformanceSmokeValidation.cpp:144-160); the matrix is their product mod ell."""
+    L = random_entries(rows * rank, ell, seed_for(rows, rank, ell, 0x21)).reshape(rows, rank)
+    R = random_entries(rank * cols, ell, seed_for(rank, cols, ell, 0x22)).reshape(rank, cols)
+    return L, R
+
+
+def fnv_matrix(M: np.ndarray) -> int:
+    """FNV-1a-64 over (rows, cols, entries), each fed as a 64-bit word, low byte
+    first: the reference micro-bench checksum (computed by libhme on the host)."""
+    from . import _lib
+    import ctypes as C
+    M = np.ascontiguousarray(M, dtype=np.uint32)
+    return int(_lib.lib().hme_fnv1a_u32(M.ctypes.data_as(C.POINTER(C.c_uint32)), M.shape[0], M.shape[1], M.shape[1]))

@@ -1,0 +1,97 @@
+/* hme -- a B200-native (sm_100a) exact modular matrix engine.  C ABI.
+ *
+ * Drop-in device layer for the matrix engine of drjanosch42/hacs 0.2.1.  Each
+ * entry point names the reference interface it replaces (file:line in the
+ * reference tree); INTEGRATION.md shows the C++ shim that installs these
+ * behind the reference's own seams (the device RREF hook, the micro-bench GPU
+ * hooks, the tape's device kernels, the Z/2^k and Z/3^k Smith / Howell calls).
+ *
+ * Conventions (the reference's, ENGINE_API.md Sec. 1-5):
+ *   - matrices are row-major uint32 with an explicit leading dimension in
+ *     elements; every residue is canonical, in [0, p);
+ *   - moduli: 2 <= p < 2^32 (fields: p prime; rings: p = ell^k);
+ *   - op: HME_SET (C = A*B), HME_ADD (C += A*B), HME_SUB (C -= A*B), mod p;
+ *   - every call returns HME_OK (0) or a negative HME_E* code; the message of
+ *     the last failure on the calling thread is hme_last_error().  No C++
+ *     exception crosses this boundary;
+ *   - "_dev" entry points take device pointers and are asynchronous on the
+ *     context's stream; the others take host pointers, copy in, compute and
+ *     copy out, and return when the result is in host memory;
+ *   - one context per thread at a time (the reference's "one driver thread per
+ *     backend", ENGINE_API.md:1332-1333); different contexts are independent.
+ */
+#ifndef HME_H
+#define HME_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define HME_API __attribute__((visibility("default")))
+#else
+#define HME_API
+#endif
+
+#define HME_OK 0
+#define HME_EINVAL (-1)       /* contract violation (shape, modulus, alignment, op) */
+#define HME_ECUDA (-2)        /* CUDA runtime / driver error */
+#define HME_ENOMEM (-3)       /* device memory exhausted */
+#define HME_ETIMEOUT (-4)     /* a bounded device-side wait ran out (kernel returned early) */
+#define HME_EUNSUPPORTED (-5) /* no sm_100 device, or a case outside the supported range */
+#define HME_ENOTINSPAN (-6)   /* solve: a right-hand side is not in the column span */
+
+#define HME_SET 0
+#define HME_ADD 1
+#define HME_SUB 2
+
+typedef struct hme_ctx hme_ctx;
+
+/* ---- context ---------------------------------------------------------------
+ * Replaces engine::cuda::CudaCtx (src/Cuda/CudaCtx.h:51-256): device choice,
+ * stream, device workspace (grown on demand and reused), device error word. */
+HME_API int hme_ctx_create(int device, hme_ctx **out);
+HME_API int hme_ctx_destroy(hme_ctx *ctx);
+/* Use a caller-owned cudaStream_t (NULL restores the context's own stream). */
+HME_API int hme_ctx_set_stream(hme_ctx *ctx, void *cuda_stream);
+/* Wait for the context's stream; reports a device-side timeout as HME_ETIMEOUT. */
+HME_API int hme_ctx_sync(hme_ctx *ctx);
+/* Kernel launches issued by this library on the context so far (a counter). */
+HME_API uint64_t hme_ctx_launches(const hme_ctx *ctx);
+HME_API const char *hme_last_error(void);
+/* Library version string. */
+HME_API const char *hme_version(void);
+
+/* ---- dense mod-p GEMM ------------------------------------------------------
+ * C op= A*B mod p; A m x k, B k x n, C m x n.  The INT8-limb tcgen05 GEMM:
+ * each residue splits into L unsigned bytes (L = 1 for p <= 2^8, 2 for
+ * p <= 2^16, 3 for p <= 2^24, 4 otherwise), the limb products run on the
+ * tensor cores with exact int32 accumulation over K chunks with
+ * L * 255 * 255 * K_chunk < 2^31, and the epilogue recombines and reduces.
+ * Bit-exact with engine::kernels::gemm<uint32_t>.
+ *
+ * hme_gemm_u32: host pointers.  Replaces the GPU micro-bench hook
+ *   micro::GpuHooks::gemm (src/ModArithmetic/PerformanceSmokeValidation.h:158-165,
+ *   installed at src/Cuda/CudaBench.cpp:339) and serves the CPU entry
+ *   engine::kernels::gemm<uint32_t> (src/ModArithmetic/Kernels.h:178-185).
+ * hme_gemm_u32_dev: device pointers, asynchronous.  Replaces
+ *   engine::cuda::gemm / schur_update (src/Cuda/CudaKernels.h:120-140,
+ *   cuda_kernels.cu:815) as called by the tape's DeviceBackend
+ *   (src/Engine/DeviceBackend.cpp:391-604). */
+HME_API int hme_gemm_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A, size_t lda,
+                 const uint32_t *B, size_t ldb, uint32_t *C, size_t ldc, int op);
+HME_API int hme_gemm_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A,
+                     size_t lda, const uint32_t *B, size_t ldb, uint32_t *C, size_t ldc, int op);
+
+/* FNV-1a-64 of a host matrix over (rows, cols, entries), each fed as a 64-bit
+ * word, low byte first: the checksum the reference's micro bench prints and
+ * compares across backends (src/ModArithmetic/PerformanceSmokeValidation.cpp:
+ * 104-120, src/ModArithmetic/Fnv.h). */
+HME_API uint64_t hme_fnv1a_u32(const uint32_t *M, uint32_t rows, uint32_t cols, size_t ld);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HME_H */
