@@ -1,0 +1,440 @@
+#!/usr/bin/env python
+"""Headline benchmark of the B200-native exact modular matrix engine.
+
+Workload (one "step"): the mod-p GEMM C = A*B mod p of the reference's
+micro bench, `--bench micro gemm 1024 1024 65521`: A, B 1024 x 1024 uint32
+from the reference's seeded splitmix64 generator (EngineMatrix salts
+0x01 / 0x02), p = 65521, on the INT8-limb tcgen05 GEMM.  Metric: Tops/s with
+ops = 2*m*n*k (one modular multiply-add = 2 ops).  Inputs (4 MiB each) fit L2,
+so L2 is flushed (a 256 MiB write) before every timed step.
+
+The JSON line also carries: the dominant kernel's roofline (INT8 tensor ops
+L^2 * 2mnk per launch over its CUDA-event time, against the measured peak),
+the reference CPU engine timed on this host (cpu_baseline), the end-to-end
+rate through the public host-pointer API (pinned host buffers, H2D + D2H
+inside the timed region), SM clocks sampled during the timed region, and the
+8192^3 GEMM at p = 65521 (2 limbs) and p = 2^31 - 19 (4 limbs) next to the
+reference's own CUDA-core GEMM (the plain method) on the same buffers.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl hme|reference]
+
+Under torchrun (N > 1) every rank runs its own replica of the step (GEMMs
+shard by independent output tiles / jobs; no collective is needed): value =
+all ranks' ops / max-over-ranks time, scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P_HEAD = 65521
+N_HEAD = 1024
+METRIC = "mod-p GEMM Tops/s (C = A*B mod p, bit-exact)"
+UNIT = "Tops/s"
+L2_FLUSH_BYTES = 256 << 20
+PEAK_FALLBACK_BF16_TFLOPS = 1590.0
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"bf16_tflops": PEAK_FALLBACK_BF16_TFLOPS, "hbm_gbs": 6650.0}, "fallback"
+
+
+def profile_traffic(name: str):
+    """dram bytes per launch recorded in the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.15)
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        time.sleep(0.15)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_gemm_rate(p: int, n: int, budget_s: float = 10.0, min_reps: int = 3):
+    """The reference's CPU engine (oracle/_ref, kernels::gemm<uint32_t> over row
+    blocks on all host threads) on the headline GEMM; falls back to the
+    oracle's C port (one thread) when the reference library is not built."""
+    import oracle as O
+    from hacs_b200 import gen
+
+    A = gen.engine_matrix(n, n, p, 0x01)
+    B = gen.engine_matrix(n, n, p, 0x02)
+    if O.ref_available():
+        thr = host_threads()
+        kind = "reference"
+        fn = lambda: O.ref_gemm(p, A, B, threads=thr)  # noqa: E731
+        sample_n = n
+    else:
+        thr = 1
+        kind = "port"
+        sample_n = 256
+        A, B = A[:sample_n, :sample_n].copy(), B[:sample_n, :sample_n].copy()
+        fn = lambda: O.gemm(p, A, B)  # noqa: E731
+    fn()  # warm
+    reps, t0 = 0, time.perf_counter()
+    while reps < min_reps or time.perf_counter() - t0 < budget_s:
+        fn()
+        reps += 1
+    dt = time.perf_counter() - t0
+    ops = 2.0 * sample_n ** 3 * reps
+    return {"value": ops / dt / 1e12, "unit": UNIT, "cores": thr, "kind": kind,
+            "sample": f"{reps} x GEMM {sample_n}^3 p={p} (EngineMatrix salts 1/2), {dt:.1f} s"}
+
+
+def run_reference(args):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    import oracle as O
+    from hacs_b200 import gen
+
+    p, n = P_HEAD, N_HEAD
+    A = gen.engine_matrix(n, n, p, 0x01)
+    B = gen.engine_matrix(n, n, p, 0x02)
+    if O.ref_available():
+        thr, kind = host_threads(), "reference"
+        step = lambda: O.ref_gemm(p, A, B, threads=thr)  # noqa: E731
+    else:
+        thr, kind = 1, "port"
+        step = lambda: O.gemm(p, A, B)  # noqa: E731
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        C_ = step()
+    dt = time.perf_counter() - t0
+    ok = gen.fnv_matrix(C_) == 0x572E8347446366C6
+    val = 2.0 * n ** 3 * args.steps / dt / 1e12
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (reference splitmix64 EngineMatrix)",
+        "config": {"workload": f"GEMM {n}^3 p={p} (config 1)", "m": n, "n": n, "k": n, "p": p,
+                   "checksum_ok": ok},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": thr, "kind": kind,
+                         "sample": f"{args.steps} x GEMM {n}^3 p={p} on {thr} host threads"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def load_plain():
+    path = os.path.join(ROOT, "baseline", "_ref", "libplain.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    L.plain_gemm_u32_dev.restype = C.c_int
+    L.plain_gemm_u32_dev.argtypes = [C.c_uint32] * 4 + [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                                        C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]
+    L.plain_last_error.restype = C.c_char_p
+    return L
+
+
+def time_device(fn, steps, warmup, flush=None):
+    """Sum of per-step CUDA-event times (ms) on torch's current stream."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(steps):
+        if flush is not None:
+            flush()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        total += a.elapsed_time(b)
+    return total
+
+
+def big_gemm(eng, plain, p, n, steps=5, warmup=3):
+    """8192^3-class GEMM: inputs resident (256 MiB each, larger than L2)."""
+    import torch
+
+    from hacs_b200 import limbs_for
+
+    g = torch.Generator(device="cuda").manual_seed(p)
+    A = torch.randint(0, p, (n, n), dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
+    B = torch.randint(0, p, (n, n), dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
+    Cm = torch.empty((n, n), dtype=torch.int32, device="cuda")
+    eng.set_timing(True)
+    eng.timing_reset()
+    ms = time_device(lambda: eng.gemm_dev(p, A, B, Cm), steps, warmup)
+    kms, kl = eng.kernel_time("limb_gemm")
+    eng.set_timing(False)
+    L = limbs_for(p)
+    out = {"p": p, "n": n, "limbs": L, "tops": 2.0 * n ** 3 * steps / ms / 1e9, "ms": ms / steps,
+           "kernel_ms": kms / max(1, kl), "int8_tops_kernel": L * L * 2.0 * n ** 3 / (kms / max(1, kl)) / 1e9}
+    if plain is not None:
+        Cp = torch.empty_like(Cm)
+        st = torch.cuda.current_stream().cuda_stream
+
+        def run_plain():
+            rc = plain.plain_gemm_u32_dev(p, n, n, n, A.data_ptr(), n, B.data_ptr(), n, Cp.data_ptr(), n, 0, st)
+            if rc != 0:
+                raise RuntimeError(plain.plain_last_error().decode())
+
+        pms = time_device(run_plain, 2, 1)
+        out["plain_gpu_tops"] = 2.0 * n ** 3 * 2 / pms / 1e9
+        out["plain_gpu_ms"] = pms / 2
+        out["speedup_vs_plain"] = out["tops"] / out["plain_gpu_tops"]
+        out["bit_exact_vs_plain"] = bool(torch.equal(Cm, Cp))
+    return out
+
+
+def run_case(args):
+    """One kernel configuration for an ncu capture (prints a short JSON, not a bench line)."""
+    import torch
+
+    import hacs_b200
+
+    kind, n, p = args.case.split(":")
+    n, p = int(n), int(p)
+    assert kind == "gemm"
+    torch.cuda.set_stream(torch.cuda.Stream())
+    eng = hacs_b200.Engine(0)
+    eng.use_torch_stream()
+    g = torch.Generator(device="cuda").manual_seed(1)
+    A = torch.randint(0, p, (n, n), dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
+    B = torch.randint(0, p, (n, n), dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
+    Cm = torch.empty((n, n), dtype=torch.int32, device="cuda")
+    ms = time_device(lambda: eng.gemm_dev(p, A, B, Cm), max(1, args.steps), args.warmup)
+    eng.sync()
+    print(json.dumps({"case": args.case, "ms_per_gemm": ms / max(1, args.steps),
+                      "tops": 2.0 * n ** 3 * max(1, args.steps) / ms / 1e9}), flush=True)
+    eng.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="hme", choices=["hme", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the 8192^3 and plain-method lines")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--case", default=None,
+                    help="profiling case instead of the bench line: gemm:<n>:<p> runs W + K GEMMs of n^3 mod p")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.case:
+        return run_case(args)
+    args.warmup = max(3, args.warmup)
+
+    ws, rank, local = dist_setup()
+    import torch
+
+    import hacs_b200
+    from hacs_b200 import gen, limbs_for
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)  # torch's events and the library's kernels share one stream
+    eng = hacs_b200.Engine(local)
+    eng.use_torch_stream()
+
+    p, n = P_HEAD, N_HEAD
+    A_h = gen.engine_matrix(n, n, p, 0x01)
+    B_h = gen.engine_matrix(n, n, p, 0x02)
+    A = torch.from_numpy(A_h.view(np.int32)).cuda()
+    B = torch.from_numpy(B_h.view(np.int32)).cuda()
+    Cm = torch.empty((n, n), dtype=torch.int32, device="cuda")
+    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+
+    def flush():
+        flush_buf.fill_(1)
+
+    # ---- device-resident timed region ----
+    eng.gemm_dev(p, A, B, Cm)
+    torch.cuda.synchronize()
+    ok = gen.fnv_matrix(Cm.cpu().numpy().view(np.uint32)) == 0x572E8347446366C6
+    for _ in range(args.warmup):
+        flush()
+        eng.gemm_dev(p, A, B, Cm)
+    eng.set_timing(True)
+    eng.timing_reset()
+    l0 = eng.launches
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        total_ms = time_device(lambda: eng.gemm_dev(p, A, B, Cm), args.steps, 0, flush=flush)
+        torch.cuda.synchronize()
+    barrier(ws)
+    launches = eng.launches - l0
+    kms, kl = eng.kernel_time("limb_gemm")
+    sp, _ = eng.kernel_time("limb_split")
+    eng.set_timing(False)
+    t_max = max_over_ranks(total_ms, ws)
+    ops = 2.0 * n ** 3
+    value = ops * args.steps * ws / (t_max / 1e3) / 1e12
+
+    # ---- end to end through the host-pointer API (pinned buffers) ----
+    A_pin = torch.from_numpy(A_h.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    B_pin = torch.from_numpy(B_h.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    C_pin = torch.empty((n, n), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    for _ in range(3):
+        eng.gemm(p, A_pin, B_pin, out=C_pin)
+    barrier(ws)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush()
+        torch.cuda.synchronize()
+        eng.gemm(p, A_pin, B_pin, out=C_pin)
+    e2e_s = time.perf_counter() - t0
+    barrier(ws)
+    e2e_s = max_over_ranks(e2e_s, ws)
+    e2e_ok = gen.fnv_matrix(C_pin) == 0x572E8347446366C6
+
+    pk, pk_src = peaks()
+    int8_peak = 2.0 * float(pk["bf16_tflops"])
+    L = limbs_for(p)
+    k_avg_ms = kms / max(1, kl)
+    achieved = L * L * ops / (k_avg_ms / 1e3) / 1e12
+    roof = {"kernel": "limb_gemm", "bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS",
+            "frac": achieved / int8_peak, "traffic": profile_traffic("limb_gemm_1024_p65521.md"),
+            "peak_source": f"2 x {pk_src} bf16 dense TFLOP/s (INT8 dense rate = 2 x bf16 on B200)",
+            "algorithmic_ops_per_launch": L * L * ops, "kernel_ms": k_avg_ms,
+            "limb_split_ms": sp / max(1, args.steps)}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 residues (u8 limbs x u8 -> s32 tensor-core accumulation)",
+        "data": "synthetic (reference splitmix64 EngineMatrix, salts 0x01/0x02)",
+        "config": {"workload": f"GEMM {n}^3 p={p} (config 1: --bench micro gemm {n} {n} {p})", "m": n, "n": n,
+                   "k": n, "p": p, "limbs": L, "parallelism": f"replicas x{ws}", "l2": "flushed before every step",
+                   "checksum_ok": bool(ok)},
+        "e2e": {"value": ops * args.steps * ws / e2e_s / 1e12, "unit": UNIT, "h2d_bytes_per_step": 8 * n * n,
+                "d2h_bytes_per_step": 4 * n * n, "api": "hme_gemm_u32 (host pointers, pinned)",
+                "checksum_ok": bool(e2e_ok)},
+        "gpu_launches": launches,
+        "roofline": roof,
+    }
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_gemm_rate(p, n)
+    line["clocks"] = clk.summary()
+    if not args.no_extras:
+        plain = load_plain()
+        ext = {}
+        for pp in (65521, 2147483629):
+            ext[f"gemm_8192_p{pp}"] = big_gemm(eng, plain, pp, 8192)
+        line["extras"] = ext
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

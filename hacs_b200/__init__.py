@@ -87,7 +87,11 @@ class Engine:
 
     # ---- context ------------------------------------------------------------
     def set_stream(self, stream_ptr: int | None) -> None:
+        """Run on a cudaStream_t handle (0 / None = the CUDA legacy default stream)."""
         check(self._lib.hme_ctx_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def use_own_stream(self) -> None:
+        check(self._lib.hme_ctx_set_stream(self._h, self._lib.hme_ctx_own_stream(self._h)))
 
     def use_torch_stream(self) -> None:
         """Run on torch's current CUDA stream (so torch and libhme order their work)."""
@@ -102,15 +106,36 @@ class Engine:
     def launches(self) -> int:
         return int(self._lib.hme_ctx_launches(self._h))
 
+    def set_timing(self, on: bool) -> None:
+        check(self._lib.hme_ctx_set_timing(self._h, 1 if on else 0))
+
+    def kernel_time(self, name: str | None = None) -> tuple[float, int]:
+        """(total ms, launches) of one kernel name since the last timing reset."""
+        ms, cnt = C.c_double(), C.c_uint64()
+        check(self._lib.hme_ctx_kernel_time(self._h, name.encode() if name else None, C.byref(ms), C.byref(cnt)))
+        return ms.value, cnt.value
+
+    def timing_reset(self) -> None:
+        check(self._lib.hme_ctx_timing_reset(self._h))
+
     # ---- GEMM -------------------------------------------------------------------
-    def gemm(self, p: int, A, B, C=None, op: int = SET) -> np.ndarray:
-        """C op= A*B mod p on host arrays (engine::kernels::gemm<uint32_t>)."""
+    def gemm(self, p: int, A, B, C=None, op: int = SET, out: np.ndarray | None = None) -> np.ndarray:
+        """C op= A*B mod p on host arrays (engine::kernels::gemm<uint32_t>).
+
+        Returns a new array unless `out` (a C-contiguous uint32 m x n array,
+        e.g. a pinned buffer) is given; for Add / Sub `out` starts as C."""
         A, B = _u32(A), _u32(B)
         m, k = A.shape
         k2, n = B.shape
         if k != k2:
             raise ValueError("gemm: inner dimensions differ")
-        out = np.zeros((m, n), np.uint32) if C is None else _u32(C).copy()
+        if out is None:
+            out = np.zeros((m, n), np.uint32) if C is None else _u32(C).copy()
+        else:
+            if out.dtype != np.uint32 or out.shape != (m, n) or not out.flags.c_contiguous:
+                raise ValueError("gemm: out must be a C-contiguous uint32 m x n array")
+            if C is not None and op != SET:
+                out[...] = C
         check(self._lib.hme_gemm_u32(self._h, p, m, n, k, _p32(A), k, _p32(B), n, _p32(out), n, op))
         return out
 

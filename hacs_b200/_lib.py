@@ -33,8 +33,12 @@ PROTOTYPES = {
     "hme_ctx_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
     "hme_ctx_destroy": (C.c_int, [vp]),
     "hme_ctx_set_stream": (C.c_int, [vp, vp]),
+    "hme_ctx_own_stream": (vp, [vp]),
     "hme_ctx_sync": (C.c_int, [vp]),
     "hme_ctx_launches": (C.c_uint64, [vp]),
+    "hme_ctx_set_timing": (C.c_int, [vp, C.c_int]),
+    "hme_ctx_kernel_time": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    "hme_ctx_timing_reset": (C.c_int, [vp]),
     "hme_last_error": (C.c_char_p, []),
     "hme_version": (C.c_char_p, []),
     "hme_fnv1a_u32": (C.c_uint64, [u32p, u32, u32, sz]),

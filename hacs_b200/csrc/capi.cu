@@ -37,6 +37,30 @@ void Workspace::release() {
     }
 }
 
+cudaEvent_t KernelTimer::take() {
+    if (!pool.empty()) {
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    HME_CUDA(cudaEventCreate(&e));
+    return e;
+}
+void KernelTimer::begin(const char* name, cudaStream_t s) {
+    Rec r{name, take(), take()};
+    HME_CUDA(cudaEventRecord(r.a, s));
+    recs.push_back(r);
+}
+void KernelTimer::end(cudaStream_t s) { HME_CUDA(cudaEventRecord(recs.back().b, s)); }
+void KernelTimer::clear() {
+    for (auto& r : recs) {
+        pool.push_back(r.a);
+        pool.push_back(r.b);
+    }
+    recs.clear();
+}
+
 void bind(hme_ctx* ctx) { HME_CUDA(cudaSetDevice(ctx->device)); }
 
 void check_device_error(hme_ctx* ctx) {
@@ -71,20 +95,6 @@ int guard(F&& f) {
     }
 }
 
-// RAII device buffer for the host-pointer entry points.
-struct DevBuf {
-    void* p = nullptr;
-    explicit DevBuf(size_t bytes) { HME_CUDA(cudaMalloc(&p, bytes ? bytes : 16)); }
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-    template <class T>
-    T* as() const {
-        return static_cast<T*>(p);
-    }
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-};
 
 const char* last_error_cstr() { return g_last_error.c_str(); }
 
@@ -135,6 +145,8 @@ int hme_ctx_destroy(hme_ctx* ctx) {
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
         ctx->ws.release();
+        ctx->timer.clear();
+        for (cudaEvent_t e : ctx->timer.pool) cudaEventDestroy(e);
         if (ctx->d_err) cudaFree(ctx->d_err);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         delete ctx;
@@ -144,9 +156,11 @@ int hme_ctx_destroy(hme_ctx* ctx) {
 int hme_ctx_set_stream(hme_ctx* ctx, void* stream) {
     return guard([&] {
         HME_REQUIRE(ctx != nullptr, "null context");
-        ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+        ctx->stream = static_cast<cudaStream_t>(stream);
     });
 }
+
+void* hme_ctx_own_stream(const hme_ctx* ctx) { return ctx ? static_cast<void*>(ctx->own_stream) : nullptr; }
 
 int hme_ctx_sync(hme_ctx* ctx) {
     return guard([&] {
@@ -157,6 +171,41 @@ int hme_ctx_sync(hme_ctx* ctx) {
 }
 
 uint64_t hme_ctx_launches(const hme_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int hme_ctx_set_timing(hme_ctx* ctx, int on) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        ctx->timer.on = on != 0;
+    });
+}
+
+int hme_ctx_kernel_time(hme_ctx* ctx, const char* name, double* total_ms, uint64_t* count) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr && total_ms && count, "hme_ctx_kernel_time: null argument");
+        bind(ctx);
+        HME_CUDA(cudaStreamSynchronize(ctx->stream));
+        double t = 0.0;
+        uint64_t c = 0;
+        for (auto& r : ctx->timer.recs) {
+            if (name && std::strcmp(name, r.name) != 0) continue;
+            float ms = 0.f;
+            HME_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+            t += ms;
+            ++c;
+        }
+        *total_ms = t;
+        *count = c;
+    });
+}
+
+int hme_ctx_timing_reset(hme_ctx* ctx) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        bind(ctx);
+        HME_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->timer.clear();
+    });
+}
 
 int hme_gemm_u32_dev(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A, size_t lda,
                      const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op) {
@@ -178,21 +227,21 @@ int hme_gemm_u32(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, c
         HME_REQUIRE(C != nullptr && ldc >= n, "gemm: bad C");
         HME_REQUIRE(k == 0 || (A && B && lda >= k && ldb >= n), "gemm: bad A/B");
         bind(ctx);
-        // compact device copies (row-major, ld = cols)
-        DevBuf dA(sizeof(uint32_t) * static_cast<size_t>(m) * k), dB(sizeof(uint32_t) * static_cast<size_t>(k) * n),
-            dC(sizeof(uint32_t) * static_cast<size_t>(m) * n);
+        // compact device copies (row-major, ld = cols) in the context's staging slots
+        uint32_t* dA = static_cast<uint32_t*>(ctx->ws.get(kSlotStageA, sizeof(uint32_t) * static_cast<size_t>(m) * k));
+        uint32_t* dB = static_cast<uint32_t*>(ctx->ws.get(kSlotStageB, sizeof(uint32_t) * static_cast<size_t>(k) * n));
+        uint32_t* dC = static_cast<uint32_t*>(ctx->ws.get(kSlotStageC, sizeof(uint32_t) * static_cast<size_t>(m) * n));
         if (k) {
-            HME_CUDA(cudaMemcpy2DAsync(dA.p, sizeof(uint32_t) * k, A, sizeof(uint32_t) * lda, sizeof(uint32_t) * k, m,
+            HME_CUDA(cudaMemcpy2DAsync(dA, sizeof(uint32_t) * k, A, sizeof(uint32_t) * lda, sizeof(uint32_t) * k, m,
                                        cudaMemcpyHostToDevice, ctx->stream));
-            HME_CUDA(cudaMemcpy2DAsync(dB.p, sizeof(uint32_t) * n, B, sizeof(uint32_t) * ldb, sizeof(uint32_t) * n, k,
+            HME_CUDA(cudaMemcpy2DAsync(dB, sizeof(uint32_t) * n, B, sizeof(uint32_t) * ldb, sizeof(uint32_t) * n, k,
                                        cudaMemcpyHostToDevice, ctx->stream));
         }
         if (op != HME_SET)
-            HME_CUDA(cudaMemcpy2DAsync(dC.p, sizeof(uint32_t) * n, C, sizeof(uint32_t) * ldc, sizeof(uint32_t) * n, m,
+            HME_CUDA(cudaMemcpy2DAsync(dC, sizeof(uint32_t) * n, C, sizeof(uint32_t) * ldc, sizeof(uint32_t) * n, m,
                                        cudaMemcpyHostToDevice, ctx->stream));
-        gemm_u32_device(ctx, make_mod(p), m, n, k, dA.as<uint32_t>(), k, dB.as<uint32_t>(), n, dC.as<uint32_t>(), n,
-                        op);
-        HME_CUDA(cudaMemcpy2DAsync(C, sizeof(uint32_t) * ldc, dC.p, sizeof(uint32_t) * n, sizeof(uint32_t) * n, m,
+        gemm_u32_device(ctx, make_mod(p), m, n, k, dA, k, dB, n, dC, n, op);
+        HME_CUDA(cudaMemcpy2DAsync(C, sizeof(uint32_t) * ldc, dC, sizeof(uint32_t) * n, sizeof(uint32_t) * n, m,
                                    cudaMemcpyDeviceToHost, ctx->stream));
         check_device_error(ctx);
     });

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/hme.h"
 #include "hme_mod.h"
@@ -35,14 +36,44 @@ void set_last_error(const std::string& msg);
 
 // Grow-only device scratch arena: one region per purpose ("slot") so that a
 // caller holding slot 0 (limb planes of A) can also hold slot 1 (planes of B).
+enum WorkspaceSlot : int {
+    kSlotPlanesA = 0,  // limb planes of the left GEMM operand
+    kSlotPlanesB = 1,  // limb planes of 256^i * right operand
+    kSlotStageA = 2,   // device copies made by the host-pointer entry points
+    kSlotStageB = 3,
+    kSlotStageC = 4,
+    kSlotElim0 = 5,    // elimination / ring drivers
+    kSlotElim1 = 6,
+    kSlotElim2 = 7,
+};
+
 struct Workspace {
-    static constexpr int kSlots = 8;
+    static constexpr int kSlots = 12;
     void* ptr[kSlots] = {};
     size_t size[kSlots] = {};
     void* get(int slot, size_t bytes);
     void release();
 };
 
+}  // namespace hme
+
+namespace hme {
+// Optional per-kernel CUDA-event timing (bench / profiling use): when enabled,
+// every launch of a named kernel is bracketed by two events on the launching
+// stream; hme_ctx_kernel_time() sums the elapsed times per name.
+struct KernelTimer {
+    bool on = false;
+    struct Rec {
+        const char* name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t take();
+    void begin(const char* name, cudaStream_t s);
+    void end(cudaStream_t s);
+    void clear();
+};
 }  // namespace hme
 
 struct hme_ctx {
@@ -53,7 +84,17 @@ struct hme_ctx {
     int* d_err = nullptr;               // device error word written by bounded waits
     uint64_t launches = 0;
     hme::Workspace ws;
+    hme::KernelTimer timer;
 };
+
+// Bracket one kernel launch with timing events when the context's timer is on.
+#define HME_TIMED(ctx, name, ...)                                   \
+    do {                                                            \
+        if ((ctx)->timer.on) (ctx)->timer.begin(name, (ctx)->stream); \
+        __VA_ARGS__;                                                \
+        if ((ctx)->timer.on) (ctx)->timer.end((ctx)->stream);       \
+        ++(ctx)->launches;                                          \
+    } while (0)
 
 namespace hme {
 

@@ -285,52 +285,71 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-// ---- limb split ------------------------------------------------------------------
-// planes[i][m][k] = byte i of A[m][k]; k in [K, Kp) zero.  16 k per thread.
+// ---- limb split (one launch for both operands) ------------------------------------
+// Blocks [0, a_blocks): A planes[i][m][k] = byte i of A[m][k], 16 k per thread
+// (four 16-byte loads when A rows are 16-byte aligned).  Blocks [a_blocks, ..):
+// B planes[i][j][n][k] = byte j of (256^i * B[k][n] mod p), B transposed to
+// K-major through shared memory, 64 k x 32 n per block, 8 k per thread.
+// k in [K, Kp) is written as zero in both.
+struct SplitArgs {
+    const uint32_t* A;
+    uint64_t lda;
+    const uint32_t* B;
+    uint64_t ldb;
+    int M, N, K, Kp;
+    uint32_t p;
+    uint64_t barrett;
+    uint8_t* planesA;
+    uint8_t* planesB;
+    int a_blocks;        // blocks of the A part
+    int b_blocks_k;      // B part: blocks along k (64 k each)
+    bool a_vec;          // A rows 16-byte aligned: vector loads
+};
+
 template <int L>
-__global__ void split_a_kernel(const uint32_t* __restrict__ A, uint64_t lda, int M, int K, int Kp,
-                               uint8_t* __restrict__ planes) {
-    const int kch = Kp >> 4;
-    const size_t total = static_cast<size_t>(M) * kch;
-    const size_t plane = static_cast<size_t>(M) * Kp;
-    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
-         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+__device__ __forceinline__ void split_a_part(const SplitArgs& s, int block) {
+    const int kch = s.Kp >> 4;
+    const size_t total = static_cast<size_t>(s.M) * kch;
+    const size_t plane = static_cast<size_t>(s.M) * s.Kp;
+    for (size_t idx = static_cast<size_t>(block) * blockDim.x + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(s.a_blocks) * blockDim.x) {
         const int row = static_cast<int>(idx / kch);
         const int k0 = static_cast<int>(idx - static_cast<size_t>(row) * kch) << 4;
-        const uint32_t* src = A + static_cast<size_t>(row) * lda + k0;
-        uint32_t w[L][4];
+        const uint32_t* src = s.A + static_cast<size_t>(row) * s.lda + k0;
+        uint32_t x[16];
+        if (s.a_vec && k0 + 16 <= s.K) {
 #pragma unroll
-        for (int j = 0; j < L; ++j) w[j][0] = w[j][1] = w[j][2] = w[j][3] = 0;
+            for (int q = 0; q < 4; ++q) {
+                const uint4 v = __ldg(reinterpret_cast<const uint4*>(src) + q);
+                x[4 * q] = v.x; x[4 * q + 1] = v.y; x[4 * q + 2] = v.z; x[4 * q + 3] = v.w;
+            }
+        } else {
 #pragma unroll
-        for (int e = 0; e < 16; ++e) {
-            const uint32_t x = (k0 + e < K) ? __ldg(src + e) : 0u;
-#pragma unroll
-            for (int j = 0; j < L; ++j) w[j][e >> 2] |= ((x >> (8 * j)) & 0xffu) << (8 * (e & 3));
+            for (int e = 0; e < 16; ++e) x[e] = (k0 + e < s.K) ? __ldg(src + e) : 0u;
         }
-        uint8_t* dst = planes + static_cast<size_t>(row) * Kp + k0;
+        uint8_t* dst = s.planesA + static_cast<size_t>(row) * s.Kp + k0;
 #pragma unroll
-        for (int j = 0; j < L; ++j)
-            *reinterpret_cast<uint4*>(dst + j * plane) = make_uint4(w[j][0], w[j][1], w[j][2], w[j][3]);
+        for (int j = 0; j < L; ++j) {
+            uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int e = 0; e < 16; ++e) w[e >> 2] |= ((x[e] >> (8 * j)) & 0xffu) << (8 * (e & 3));
+            *reinterpret_cast<uint4*>(dst + j * plane) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
     }
 }
 
-// planes[i][j][n][k] = byte j of (256^i * B[k][n] mod p): B transposed to
-// K-major through shared memory, 64 k x 32 n per block, 8 k per thread.
 template <int L>
-__global__ void __launch_bounds__(256) split_b_kernel(const uint32_t* __restrict__ B, uint64_t ldb, int K, int N,
-                                                      int Kp, uint32_t p, uint64_t barrett,
-                                                      uint8_t* __restrict__ planes) {
-    __shared__ uint32_t tile[64][33];
-    const int k0 = blockIdx.x * 64, n0 = blockIdx.y * 32;
+__device__ __forceinline__ void split_b_part(const SplitArgs& s, int block, uint32_t (*tile)[33]) {
+    const int k0 = (block % s.b_blocks_k) * 64, n0 = (block / s.b_blocks_k) * 32;
     for (int t = threadIdx.x; t < 64 * 32; t += 256) {
         const int kk = t >> 5, nn = t & 31;
         const int k = k0 + kk, n = n0 + nn;
-        tile[kk][nn] = (k < K && n < N) ? __ldg(B + static_cast<size_t>(k) * ldb + n) : 0u;
+        tile[kk][nn] = (k < s.K && n < s.N) ? __ldg(s.B + static_cast<size_t>(k) * s.ldb + n) : 0u;
     }
     __syncthreads();
     const int nn = threadIdx.x >> 3, kc = threadIdx.x & 7;
     const int n = n0 + nn, kb = k0 + kc * 8;
-    if (n >= N || kb >= Kp) return;
+    if (n >= s.N || kb >= s.Kp) return;
     uint32_t out[L][L][2];
 #pragma unroll
     for (int i = 0; i < L; ++i)
@@ -341,18 +360,27 @@ __global__ void __launch_bounds__(256) split_b_kernel(const uint32_t* __restrict
         uint32_t v = tile[kc * 8 + e][nn];
 #pragma unroll
         for (int i = 0; i < L; ++i) {
-            if (i) v = reduce_u64(static_cast<uint64_t>(v) << 8, p, barrett);
+            if (i) v = reduce_u64(static_cast<uint64_t>(v) << 8, s.p, s.barrett);
 #pragma unroll
             for (int j = 0; j < L; ++j) out[i][j][e >> 2] |= ((v >> (8 * j)) & 0xffu) << (8 * (e & 3));
         }
     }
-    const size_t plane = static_cast<size_t>(N) * Kp;
+    const size_t plane = static_cast<size_t>(s.N) * s.Kp;
 #pragma unroll
     for (int i = 0; i < L; ++i)
 #pragma unroll
         for (int j = 0; j < L; ++j)
-            *reinterpret_cast<uint2*>(planes + (i * L + j) * plane + static_cast<size_t>(n) * Kp + kb) =
+            *reinterpret_cast<uint2*>(s.planesB + (i * L + j) * plane + static_cast<size_t>(n) * s.Kp + kb) =
                 make_uint2(out[i][j][0], out[i][j][1]);
+}
+
+template <int L>
+__global__ void __launch_bounds__(256) limb_split_kernel(const SplitArgs s) {
+    __shared__ uint32_t tile[64][33];
+    if (static_cast<int>(blockIdx.x) < s.a_blocks)
+        split_a_part<L>(s, blockIdx.x);
+    else
+        split_b_part<L>(s, blockIdx.x - s.a_blocks, tile);
 }
 
 // ---- host side ---------------------------------------------------------------------
@@ -423,9 +451,8 @@ void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint
         g.k_begin = static_cast<int>(kb0);
         g.kblocks = static_cast<int>((kc + kBK - 1) / kBK);
         g.op = kb0 == 0 ? op : (op == HME_SET ? HME_ADD : op);
-        limb_gemm_kernel<L, BN><<<grid, kThreads, CF::SMEM, ctx->stream>>>(tmA, tmB, g);
+        HME_TIMED(ctx, "limb_gemm", limb_gemm_kernel<L, BN><<<grid, kThreads, CF::SMEM, ctx->stream>>>(tmA, tmB, g));
         HME_CUDA(cudaGetLastError());
-        ++ctx->launches;
     }
 }
 
@@ -447,10 +474,10 @@ void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, 
     HME_REQUIRE(ldc >= n, "gemm: ldc < n");
     if (k == 0) {
         if (op == HME_SET) {
-            fill_zero_kernel<<<std::min<size_t>(1024, (static_cast<size_t>(m) * n + 255) / 256), 256, 0,
-                               ctx->stream>>>(C, ldc, m, n);
+            HME_TIMED(ctx, "fill_zero",
+                      fill_zero_kernel<<<std::min<size_t>(1024, (static_cast<size_t>(m) * n + 255) / 256), 256, 0,
+                                         ctx->stream>>>(C, ldc, m, n));
             HME_CUDA(cudaGetLastError());
-            ++ctx->launches;
         }
         return;
     }
@@ -458,31 +485,42 @@ void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, 
     HME_REQUIRE(lda >= k && ldb >= n, "gemm: leading dimension too small");
     const int L = static_cast<int>(mp.limbs);
     const int Kp = static_cast<int>((k + 15) / 16 * 16);
-    uint8_t* pa = static_cast<uint8_t*>(ctx->ws.get(0, static_cast<size_t>(L) * m * Kp));
-    uint8_t* pb = static_cast<uint8_t*>(ctx->ws.get(1, static_cast<size_t>(L) * L * n * Kp));
+    uint8_t* pa = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesA, static_cast<size_t>(L) * m * Kp));
+    uint8_t* pb = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesB, static_cast<size_t>(L) * L * n * Kp));
 
     {
+        SplitArgs sa{};
+        sa.A = A; sa.lda = lda; sa.B = B; sa.ldb = ldb;
+        sa.M = static_cast<int>(m); sa.N = static_cast<int>(n); sa.K = static_cast<int>(k); sa.Kp = Kp;
+        sa.p = mp.p; sa.barrett = mp.barrett;
+        sa.planesA = pa; sa.planesB = pb;
         const size_t work = static_cast<size_t>(m) * (Kp / 16);
-        const int grid = static_cast<int>(std::min<size_t>((work + 255) / 256, static_cast<size_t>(ctx->num_sms) * 16));
-        const dim3 gb((Kp + 63) / 64, (n + 31) / 32);
+        sa.a_blocks = static_cast<int>(std::min<size_t>((work + 255) / 256, static_cast<size_t>(ctx->num_sms) * 8));
+        sa.b_blocks_k = (Kp + 63) / 64;
+        sa.a_vec = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && ((lda & 3) == 0);
+        const int grid = sa.a_blocks + sa.b_blocks_k * static_cast<int>((n + 31) / 32);
         switch (L) {
-            case 1: split_a_kernel<1><<<grid, 256, 0, ctx->stream>>>(A, lda, m, k, Kp, pa);
-                    split_b_kernel<1><<<gb, 256, 0, ctx->stream>>>(B, ldb, k, n, Kp, mp.p, mp.barrett, pb); break;
-            case 2: split_a_kernel<2><<<grid, 256, 0, ctx->stream>>>(A, lda, m, k, Kp, pa);
-                    split_b_kernel<2><<<gb, 256, 0, ctx->stream>>>(B, ldb, k, n, Kp, mp.p, mp.barrett, pb); break;
-            case 3: split_a_kernel<3><<<grid, 256, 0, ctx->stream>>>(A, lda, m, k, Kp, pa);
-                    split_b_kernel<3><<<gb, 256, 0, ctx->stream>>>(B, ldb, k, n, Kp, mp.p, mp.barrett, pb); break;
-            default: split_a_kernel<4><<<grid, 256, 0, ctx->stream>>>(A, lda, m, k, Kp, pa);
-                    split_b_kernel<4><<<gb, 256, 0, ctx->stream>>>(B, ldb, k, n, Kp, mp.p, mp.barrett, pb); break;
+            case 1: HME_TIMED(ctx, "limb_split", limb_split_kernel<1><<<grid, 256, 0, ctx->stream>>>(sa)); break;
+            case 2: HME_TIMED(ctx, "limb_split", limb_split_kernel<2><<<grid, 256, 0, ctx->stream>>>(sa)); break;
+            case 3: HME_TIMED(ctx, "limb_split", limb_split_kernel<3><<<grid, 256, 0, ctx->stream>>>(sa)); break;
+            default: HME_TIMED(ctx, "limb_split", limb_split_kernel<4><<<grid, 256, 0, ctx->stream>>>(sa)); break;
         }
         HME_CUDA(cudaGetLastError());
-        ctx->launches += 2;
     }
+    // Wide tiles (L*BN = 256 columns of TMEM per accumulator) unless that leaves
+    // SMs idle; then half-width tiles, which double the tile count.
+    const uint32_t tiles_m = (m + kBM - 1) / kBM;
+    auto tiles_for = [&](uint32_t bn) { return static_cast<size_t>(tiles_m) * ((n + bn - 1) / bn); };
+    const bool narrow = 4 * tiles_for(256 / L > 64 ? 256 / L : 64) < 3 * static_cast<size_t>(ctx->num_sms);
     switch (L) {
-        case 1: launch_gemm<1, 256>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
-        case 2: launch_gemm<2, 128>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
-        case 3: launch_gemm<3, 80>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
-        default: launch_gemm<4, 64>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
+        case 1: if (narrow) launch_gemm<1, 128>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op);
+                else launch_gemm<1, 256>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
+        case 2: if (narrow) launch_gemm<2, 64>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op);
+                else launch_gemm<2, 128>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
+        case 3: if (narrow) launch_gemm<3, 32>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op);
+                else launch_gemm<3, 80>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
+        default: if (narrow) launch_gemm<4, 32>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op);
+                else launch_gemm<4, 64>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
     }
 }
 

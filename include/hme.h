@@ -54,12 +54,22 @@ typedef struct hme_ctx hme_ctx;
  * stream, device workspace (grown on demand and reused), device error word. */
 HME_API int hme_ctx_create(int device, hme_ctx **out);
 HME_API int hme_ctx_destroy(hme_ctx *ctx);
-/* Use a caller-owned cudaStream_t (NULL restores the context's own stream). */
+/* Run the context's work on a caller-owned cudaStream_t (NULL = the CUDA
+ * legacy default stream); hme_ctx_own_stream() is the stream the context
+ * created and uses until this is called. */
 HME_API int hme_ctx_set_stream(hme_ctx *ctx, void *cuda_stream);
+HME_API void *hme_ctx_own_stream(const hme_ctx *ctx);
 /* Wait for the context's stream; reports a device-side timeout as HME_ETIMEOUT. */
 HME_API int hme_ctx_sync(hme_ctx *ctx);
 /* Kernel launches issued by this library on the context so far (a counter). */
 HME_API uint64_t hme_ctx_launches(const hme_ctx *ctx);
+/* Per-kernel CUDA-event timing on the context's stream (bench / profiling
+ * use): while on, each kernel launch is bracketed by two events;
+ * hme_ctx_kernel_time sums the elapsed milliseconds and the launch count of
+ * one kernel name ("limb_gemm", "split_a", "split_b", ...; NULL = all). */
+HME_API int hme_ctx_set_timing(hme_ctx *ctx, int on);
+HME_API int hme_ctx_kernel_time(hme_ctx *ctx, const char *name, double *total_ms, uint64_t *count);
+HME_API int hme_ctx_timing_reset(hme_ctx *ctx);
 HME_API const char *hme_last_error(void);
 /* Library version string. */
 HME_API const char *hme_version(void);

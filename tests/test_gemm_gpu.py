@@ -60,3 +60,34 @@ def test_gemm_config1_checksum(engine):
     want = O.gemm(p, A, B)
     assert np.array_equal(got, want)
     assert gen.fnv_matrix(got) == 0x572E8347446366C6
+
+
+@pytest.mark.parametrize("p", [251, 65521, 16777213, 2147483629])
+def test_gemm_wide_tiles(engine, p):
+    # enough output tiles that the wide-tile variant (L*BN = 256) is chosen
+    rng = np.random.default_rng(p % 97)
+    m, n, k = 2048, 2304, 160
+    A, B, C0 = _rand(rng, (m, k), p), _rand(rng, (k, n), p), _rand(rng, (m, n), p)
+    assert np.array_equal(engine.gemm(p, A, B, C0, SUB), O.gemm(p, A, B, C0, SUB))
+
+
+def test_gemm_device_pointers_strided(engine):
+    """hme_gemm_u32_dev on torch CUDA tensors with padded leading dimensions."""
+    import torch
+
+    p = 2147483629
+    rng = np.random.default_rng(3)
+    m, n, k = 300, 200, 500
+    A, B, C0 = _rand(rng, (m, k), p), _rand(rng, (k, n), p), _rand(rng, (m, n), p)
+    dA = torch.zeros((m, k + 7), dtype=torch.int32, device="cuda")
+    dB = torch.zeros((k, n + 3), dtype=torch.int32, device="cuda")
+    dC = torch.zeros((m, n + 5), dtype=torch.int32, device="cuda")
+    dA[:, :k] = torch.from_numpy(A.view(np.int32))
+    dB[:, :n] = torch.from_numpy(B.view(np.int32))
+    dC[:, :n] = torch.from_numpy(C0.view(np.int32))
+    engine.use_torch_stream()
+    engine.gemm_dev(p, dA[:, :k], dB[:, :n], dC[:, :n], ADD)
+    engine.sync()
+    got = dC[:, :n].cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, O.gemm(p, A, B, C0, ADD))
+    assert np.all(dC[:, n:].cpu().numpy() == 0)  # padding untouched
