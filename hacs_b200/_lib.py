@@ -44,6 +44,7 @@ PROTOTYPES = {
     "hme_fnv1a_u32": (C.c_uint64, [u32p, u32, u32, sz]),
     "hme_gemm_u32": (C.c_int, [vp, u32, u32, u32, u32, u32p, sz, u32p, sz, u32p, sz, C.c_int]),
     "hme_gemm_u32_dev": (C.c_int, [vp, u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int]),
+    "hme_gemm_u32_dev_noalloc": (C.c_int, [u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int, vp]),
 }
 
 _lib = None

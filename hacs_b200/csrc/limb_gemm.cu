@@ -525,3 +525,205 @@ void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, 
 }
 
 }  // namespace hme
+
+// ---- allocation-free GEMM entry point ---------------------------------------------
+//
+// Some callers cannot allocate device memory at the point where they need a
+// GEMM: a plugin running inside another runtime that owns the whole device
+// budget and forbids allocations after start-up, or a latency-critical path
+// where cudaMalloc / cudaFree would synchronise the device.  For them,
+// hme_gemm_u32_dev_noalloc runs the same limb-split and limb-GEMM kernels as
+// hme_gemm_u32_dev, with the limb planes in a fixed scratch array that lives
+// in this library's device image (held by every GPU that loads the library,
+// until the process exits), and with no context.  It never calls cudaMalloc,
+// cudaFree or any allocating routine.
+//
+// Limits and sharing: the planes of one call (L*m*Kp + L*L*n*Kp bytes, each
+// rounded up to 256, Kp = k rounded up to 16) must fit the 32 MiB array, else
+// the call fails with HME_EINVAL before launching anything.  Every call on a
+// device shares the one array and leaves its planes behind; each call writes
+// all plane bytes it reads before reading them, and clears the device error
+// word it uses at its start.  Calls that overlap on the GPU (on different
+// streams, or from several host threads at once) race on the array and give
+// wrong results: serialise them.
+namespace hme {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+static __device__ int g_noalloc_err;
+
+struct NoAllocDevice {
+    bool ready = false;
+    uint8_t* scratch = nullptr;  // device address of g_noalloc_scratch on this device
+    int* err = nullptr;          // device address of g_noalloc_err on this device
+    int num_sms = 0;
+};
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+
+template <int L, int BN>
+void noalloc_smem_attr() {
+    HME_CUDA(cudaFuncSetAttribute(limb_gemm_kernel<L, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  Cfg<L, BN>::SMEM));
+}
+
+// Once per device, with that device current: resolve the device addresses of
+// the scratch array and the error word (the host-side names of __device__
+// variables are not device addresses) and set the kernels' shared-memory limit.
+const NoAllocDevice& noalloc_setup(int dev) {
+    HME_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, "hme_gemm_u32_dev_noalloc: device id out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (d.ready) return d;
+    void* ptr = nullptr;
+    HME_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    d.scratch = static_cast<uint8_t*>(ptr);
+    ptr = nullptr;
+    HME_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_err));
+    d.err = static_cast<int*>(ptr);
+    HME_CUDA(cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, dev));
+    noalloc_smem_attr<1, 128>(); noalloc_smem_attr<1, 256>();
+    noalloc_smem_attr<2, 64>();  noalloc_smem_attr<2, 128>();
+    noalloc_smem_attr<3, 32>();  noalloc_smem_attr<3, 80>();
+    noalloc_smem_attr<4, 32>();  noalloc_smem_attr<4, 64>();
+    d.ready = true;
+    return d;
+}
+
+template <int L, int BN>
+void noalloc_gemm(const NoAllocDevice& d, cudaStream_t st, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k,
+                  int Kp, uint8_t* pa, uint8_t* pb, uint32_t* C, size_t ldc, int op) {
+    using CF = Cfg<L, BN>;
+    CUtensorMap tmA, tmB;
+    {
+        const cuuint64_t dims[3] = {k, m, static_cast<cuuint64_t>(L)};
+        const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * m};
+        const cuuint32_t box[3] = {kBK, kBM, 1};
+        encode_u8(&tmA, pa, 3, dims, strides, box);
+    }
+    {
+        const cuuint64_t dims[4] = {k, n, static_cast<cuuint64_t>(L), static_cast<cuuint64_t>(L)};
+        const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * n,
+                                       static_cast<cuuint64_t>(Kp) * n * L};
+        const cuuint32_t box[4] = {kBK, BN, static_cast<cuuint32_t>(L), 1};
+        encode_u8(&tmB, pb, 4, dims, strides, box);
+    }
+    GemmArgs g{};
+    g.C = C;
+    g.ldc = ldc;
+    g.M = static_cast<int>(m);
+    g.N = static_cast<int>(n);
+    g.p = mp.p;
+    g.barrett = mp.barrett;
+    g.tiles_m = static_cast<int>((m + kBM - 1) / kBM);
+    g.tiles_n = static_cast<int>((n + BN - 1) / BN);
+    g.group_m = 16;
+    g.err = d.err;
+    const int grid = std::min(g.tiles_m * g.tiles_n, d.num_sms);
+    const uint32_t chunk = limb_k_chunk(L);
+    for (uint32_t kb0 = 0; kb0 < k; kb0 += chunk) {
+        const uint32_t kc = std::min(chunk, k - kb0);
+        g.k_begin = static_cast<int>(kb0);
+        g.kblocks = static_cast<int>((kc + kBK - 1) / kBK);
+        g.op = kb0 == 0 ? op : (op == HME_SET ? HME_ADD : op);
+        limb_gemm_kernel<L, BN><<<grid, kThreads, CF::SMEM, st>>>(tmA, tmB, g);
+        HME_CUDA(cudaGetLastError());
+    }
+}
+
+size_t round256(size_t x) { return (x + 255) / 256 * 256; }
+
+}  // namespace
+}  // namespace hme
+
+extern "C" HME_API int hme_gemm_u32_dev_noalloc(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
+                                                size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc,
+                                                int op, void* cuda_stream) {
+    using namespace hme;
+    try {
+        HME_REQUIRE(op == HME_SET || op == HME_ADD || op == HME_SUB, "gemm: op must be HME_SET, HME_ADD or HME_SUB");
+        HME_REQUIRE(p >= 2, "gemm: modulus must be >= 2");
+        HME_REQUIRE(m < (1u << 30) && n < (1u << 30) && k < (1u << 30), "gemm: dimension too large");
+        const ModParams mp = make_mod(p);
+        const int L = static_cast<int>(mp.limbs);
+        const size_t Kp = (static_cast<size_t>(k) + 15) / 16 * 16;
+        const size_t bytes_a = round256(static_cast<size_t>(L) * m * Kp);
+        const size_t need = bytes_a + round256(static_cast<size_t>(L) * L * n * Kp);
+        if (need > kNoAllocScratchBytes)
+            throw Error(HME_EINVAL, "hme_gemm_u32_dev_noalloc: this GEMM needs " + std::to_string(need) +
+                                        " bytes of limb planes; the allocation-free entry point holds " +
+                                        std::to_string(kNoAllocScratchBytes) +
+                                        " (32 MiB). Use hme_gemm_u32_dev for larger products.");
+        if (m == 0 || n == 0) return HME_OK;
+        HME_REQUIRE(C != nullptr && ldc >= n, "gemm: bad C");
+        HME_REQUIRE(k == 0 || (A && B && lda >= k && ldb >= n), "gemm: bad A/B");
+        int dev = 0;
+        HME_CUDA(cudaGetDevice(&dev));
+        const NoAllocDevice& d = noalloc_setup(dev);
+        cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+        HME_CUDA(cudaMemsetAsync(d.err, 0, sizeof(int), st));
+        if (k == 0) {
+            if (op == HME_SET)
+                fill_zero_kernel<<<std::min<size_t>(1024, (static_cast<size_t>(m) * n + 255) / 256), 256, 0, st>>>(
+                    C, ldc, m, n);
+            HME_CUDA(cudaGetLastError());
+            HME_CUDA(cudaStreamSynchronize(st));
+            return HME_OK;
+        }
+        uint8_t* pa = d.scratch;
+        uint8_t* pb = d.scratch + bytes_a;
+        SplitArgs sa{};
+        sa.A = A; sa.lda = lda; sa.B = B; sa.ldb = ldb;
+        sa.M = static_cast<int>(m); sa.N = static_cast<int>(n); sa.K = static_cast<int>(k);
+        sa.Kp = static_cast<int>(Kp);
+        sa.p = mp.p; sa.barrett = mp.barrett;
+        sa.planesA = pa; sa.planesB = pb;
+        const size_t work = static_cast<size_t>(m) * (Kp / 16);
+        sa.a_blocks = static_cast<int>(std::min<size_t>((work + 255) / 256, static_cast<size_t>(d.num_sms) * 8));
+        sa.b_blocks_k = static_cast<int>((Kp + 63) / 64);
+        sa.a_vec = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && ((lda & 3) == 0);
+        const int grid = sa.a_blocks + sa.b_blocks_k * static_cast<int>((n + 31) / 32);
+        const uint32_t tiles_m = (m + kBM - 1) / kBM;
+        auto tiles_for = [&](uint32_t bn) { return static_cast<size_t>(tiles_m) * ((n + bn - 1) / bn); };
+        const bool narrow = 4 * tiles_for(256 / L > 64 ? 256 / L : 64) < 3 * static_cast<size_t>(d.num_sms);
+        const int kpi = static_cast<int>(Kp);
+        switch (L) {
+            case 1:
+                limb_split_kernel<1><<<grid, 256, 0, st>>>(sa);
+                if (narrow) noalloc_gemm<1, 128>(d, st, mp, m, n, k, kpi, pa, pb, C, ldc, op);
+                else noalloc_gemm<1, 256>(d, st, mp, m, n, k, kpi, pa, pb, C, ldc, op);
+                break;
+            case 2:
+                limb_split_kernel<2><<<grid, 256, 0, st>>>(sa);
+                if (narrow) noalloc_gemm<2, 64>(d, st, mp, m, n, k, kpi, pa, pb, C, ldc, op);
+                else noalloc_gemm<2, 128>(d, st, mp, m, n, k, kpi, pa, pb, C, ldc, op);
+                break;
+            case 3:
+                limb_split_kernel<3><<<grid, 256, 0, st>>>(sa);
+                if (narrow) noalloc_gemm<3, 32>(d, st, mp, m, n, k, kpi, pa, pb, C, ldc, op);
+                else noalloc_gemm<3, 80>(d, st, mp, m, n, k, kpi, pa, pb, C, ldc, op);
+                break;
+            default:
+                limb_split_kernel<4><<<grid, 256, 0, st>>>(sa);
+                if (narrow) noalloc_gemm<4, 32>(d, st, mp, m, n, k, kpi, pa, pb, C, ldc, op);
+                else noalloc_gemm<4, 64>(d, st, mp, m, n, k, kpi, pa, pb, C, ldc, op);
+                break;
+        }
+        HME_CUDA(cudaGetLastError());
+        HME_CUDA(cudaStreamSynchronize(st));
+        int code = 0;
+        HME_CUDA(cudaMemcpyFromSymbol(&code, g_noalloc_err, sizeof(int)));
+        if (code != 0)
+            throw Error(HME_ETIMEOUT, "hme_gemm_u32_dev_noalloc: a bounded device-side wait ran out (device code " +
+                                          std::to_string(code) + "); C is incomplete");
+        return HME_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return HME_EINVAL;
+    }
+}

@@ -95,6 +95,25 @@ HME_API int hme_gemm_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint3
 HME_API int hme_gemm_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A,
                      size_t lda, const uint32_t *B, size_t ldb, uint32_t *C, size_t ldc, int op);
 
+/* The GEMM above (same kernels, same result bits) for callers that cannot
+ * allocate device memory when they call it -- a plugin inside another runtime
+ * that owns the device-memory budget, or a latency-critical path where
+ * cudaMalloc / cudaFree would synchronise the device.  It takes no context
+ * and allocates nothing: the limb planes live in a 32 MiB scratch array
+ * compiled into the library (every GPU that loads the library holds it until
+ * the process exits).  It runs on the calling thread's current device, on
+ * `cuda_stream` (NULL = the legacy default stream), and returns when C is
+ * final.  The planes of one call, L*m*Kp + L*L*n*Kp bytes (each rounded up
+ * to 256; Kp = k rounded up to 16; L limbs as above), must fit 32 MiB, else
+ * HME_EINVAL before anything runs.  The first call on a device does that
+ * device's set-up (scratch address lookup, kernel attributes); make it
+ * before any stream capture.  All calls share the one scratch array: calls
+ * that overlap on the GPU race and give wrong results, so serialise them.
+ * No counterpart in the reference: an addition of this library. */
+HME_API int hme_gemm_u32_dev_noalloc(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A, size_t lda,
+                                     const uint32_t *B, size_t ldb, uint32_t *C, size_t ldc, int op,
+                                     void *cuda_stream);
+
 /* FNV-1a-64 of a host matrix over (rows, cols, entries), each fed as a 64-bit
  * word, low byte first: the checksum the reference's micro bench prints and
  * compares across backends (src/ModArithmetic/PerformanceSmokeValidation.cpp:
