@@ -63,3 +63,52 @@ def fnv_matrix(M: np.ndarray) -> int:
     import ctypes as C
     M = np.ascontiguousarray(M, dtype=np.uint32)
     return int(_lib.lib().hme_fnv1a_u32(M.ctypes.data_as(C.POINTER(C.c_uint32)), M.shape[0], M.shape[1], M.shape[1]))
+
+
+def planted_udv(n: int, ell: int, k: int, salt: int = 0x33, ops: int = 64):
+    """Config-3 input: M = U * D * V mod ell^k, n x n.
+
+    U and V are each the product of `ops` seeded elementary row operations
+    row_i += c * row_j (i != j, c uniform in [-5, 5]) applied to the identity,
+    so both are unimodular; D = diag(ell^e_i) with e_i ~ Geometric(1/2) on
+    {0, 1, ...} truncated at k (e_i = k gives a zero diagonal entry).  Returns
+    (M, e) with M uint32 canonical in [0, ell^k).  The Smith valuations of M
+    over Z/ell^k are exactly sorted({e_i : e_i < k}).  All arithmetic is mod
+    ell^k, which is the exact integer product reduced mod ell^k.
+    """
+    q = ell ** k
+    st = seed_for(n, n, q, salt)
+    stream = splitmix_stream(st, 3 * 2 * ops + n)
+    pos = 0
+
+    def nxt():
+        nonlocal pos
+        v = int(stream[pos])
+        pos += 1
+        return v
+
+    e = []
+    for _ in range(n):
+        w = nxt()
+        tz = (w & -w).bit_length() - 1 if w else 64
+        e.append(min(tz, k))
+    mats = []
+    for _ in range(2):
+        T = np.eye(n, dtype=np.int64)
+        for _ in range(ops):
+            i = nxt() % n
+            j = nxt() % (n - 1)
+            if j >= i:
+                j += 1
+            c = int(nxt() % 11) - 5
+            T[i] = (T[i] + c * T[j]) % q
+        mats.append(T)
+    U, V = mats
+    d = np.array([pow(ell, x, q) if x < k else 0 for x in e], dtype=np.int64)
+    UD = (U * d[None, :]) % q
+    # exact product mod q in int64: entries < q <= 2^31, so chunk K to keep sums < 2^63
+    M = np.zeros((n, n), dtype=np.int64)
+    step = max(1, (1 << 62) // (q * q))
+    for k0 in range(0, n, step):
+        M = (M + UD[:, k0:k0 + step] @ V[k0:k0 + step]) % q
+    return M.astype(np.uint32), np.array(e, dtype=np.uint32)
