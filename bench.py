@@ -320,7 +320,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the 8192^3 and plain-method lines")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--case", default=None,
-                    help="profiling case instead of the bench line: gemm:<n>:<p> runs W + K GEMMs of n^3 mod p")
+                    help="profiling case instead of the bench line: gemm:<n>:<p> runs W + K GEMMs of n^3 "
+                         "mod p; rref:<n>:<rank>:<p> runs W + K device RREFs of a rank-deficient n x n matrix")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

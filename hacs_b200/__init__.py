@@ -7,6 +7,12 @@ This module mirrors the reference engine's operator names and argument meaning
 device-pointer variants over torch CUDA tensors:
 
   ``Engine.gemm(p, A, B, C=None, op=SET)``   engine::kernels::gemm<uint32_t> (Kernels.h:178-185)
+  ``Engine.rref(p, A)``                      engine::elim::rref (DenseElim.h:153-158)
+  ``Engine.column_rank_profile(p, A)``       engine::elim::column_rank_profile (DenseElim.h:160-169)
+  ``Engine.det(p, A)``                       determinant mod p (no reference entry point)
+  ``Engine.kernel_basis(p, A)``              engine::elim::kernel_basis of rref(A) (DenseElim.h:171-179)
+  ``Engine.inverse(p, A)``                   engine::elim::inverse (DenseElim.h:186-189)
+  ``Engine.solve_multi_rhs(p, B, Y)``        engine::elim::solve_multi_rhs (DenseElim.h:191-197)
 
 Every call goes to libhme; there is no CPU fallback.
 """
@@ -147,3 +153,81 @@ class Engine:
             raise ValueError("gemm_dev: shape mismatch")
         check(self._lib.hme_gemm_u32_dev(self._h, p, m, n, k, _dev_ptr(A), A.stride(0), _dev_ptr(B), B.stride(0),
                                          _dev_ptr(C), C.stride(0), op))
+
+    # ---- elimination over F_p ------------------------------------------------------
+    def set_elim_options(self, panel: int = 0, rows_per_cta: int = 0, panel_ctas: int = 0, back_block: int = 0):
+        check(self._lib.hme_ctx_set_elim_options(self._h, panel, rows_per_cta, panel_ctas, back_block))
+
+    def rref(self, p: int, A):
+        """(RREF(A), pivot columns): the reference's elim::rref result."""
+        R = _u32(A).copy()
+        m, n = R.shape
+        piv = np.zeros(max(1, min(m, n)), np.uint32)
+        rank = C.c_uint32()
+        check(self._lib.hme_rref_u32(self._h, p, m, n, _p32(R), n, _p32(piv), C.byref(rank)))
+        return R, piv[: rank.value].copy()
+
+    def column_rank_profile(self, p: int, A) -> np.ndarray:
+        A = _u32(A)
+        m, n = A.shape
+        piv = np.zeros(max(1, min(m, n)), np.uint32)
+        rank = C.c_uint32()
+        check(self._lib.hme_rank_profile_u32(self._h, p, m, n, _p32(A), n, _p32(piv), C.byref(rank)))
+        return piv[: rank.value].copy()
+
+    def rank(self, p: int, A) -> int:
+        return len(self.column_rank_profile(p, A))
+
+    def det(self, p: int, A) -> int:
+        A = _u32(A)
+        n = A.shape[0]
+        if A.shape != (n, n):
+            raise ValueError("det: square matrix required")
+        d = C.c_uint32()
+        check(self._lib.hme_det_u32(self._h, p, n, _p32(A), n, C.byref(d)))
+        return d.value
+
+    def rref_det(self, p: int, A):
+        """(RREF, pivots, det) of a square matrix from one factorisation."""
+        R = _u32(A).copy()
+        n = R.shape[0]
+        piv = np.zeros(max(1, n), np.uint32)
+        rank, d = C.c_uint32(), C.c_uint32()
+        check(self._lib.hme_rref_det_u32(self._h, p, n, _p32(R), n, _p32(piv), C.byref(rank), C.byref(d)))
+        return R, piv[: rank.value].copy(), d.value
+
+    def kernel_basis(self, p: int, A) -> np.ndarray:
+        A = _u32(A)
+        m, n = A.shape
+        K = np.zeros((max(1, n), n), np.uint32)
+        f = C.c_uint32()
+        check(self._lib.hme_kernel_basis_u32(self._h, p, m, n, _p32(A), n, _p32(K), n, C.byref(f)))
+        return K[: f.value].copy()
+
+    def inverse(self, p: int, A):
+        A = _u32(A)
+        n = A.shape[0]
+        X = np.zeros((n, n), np.uint32)
+        ok = C.c_int()
+        check(self._lib.hme_inverse_u32(self._h, p, n, _p32(A), n, _p32(X), n, C.byref(ok)))
+        return X if ok.value else None
+
+    def solve_multi_rhs(self, p: int, B, Y):
+        """X with B X = Y (nb x ny), or None when some column of Y is outside span(B)."""
+        B, Y = _u32(B), _u32(Y)
+        m, nb = B.shape
+        ny = Y.shape[1]
+        X = np.zeros((max(1, nb), max(1, ny)), np.uint32)
+        rc = self._lib.hme_solve_u32(self._h, p, m, nb, ny, _p32(B), nb, _p32(Y), ny, _p32(X), max(1, ny))
+        if rc == _lib.HME_ENOTINSPAN:
+            return None
+        check(rc)
+        return X[:nb, :ny].copy()
+
+    def rref_dev(self, p: int, A):
+        """In-place RREF of a CUDA tensor (m x n, int32/uint32 words); returns the pivots."""
+        m, n = A.shape
+        piv = np.zeros(max(1, min(m, n)), np.uint32)
+        rank = C.c_uint32()
+        check(self._lib.hme_rref_u32_dev(self._h, p, m, n, _dev_ptr(A), A.stride(0), _p32(piv), C.byref(rank)))
+        return piv[: rank.value].copy()

@@ -42,6 +42,15 @@ PROTOTYPES = {
     "hme_last_error": (C.c_char_p, []),
     "hme_version": (C.c_char_p, []),
     "hme_fnv1a_u32": (C.c_uint64, [u32p, u32, u32, sz]),
+    "hme_rref_u32": (C.c_int, [vp, u32, u32, u32, u32p, sz, u32p, u32p]),
+    "hme_rref_u32_dev": (C.c_int, [vp, u32, u32, u32, vp, sz, u32p, u32p]),
+    "hme_rank_profile_u32": (C.c_int, [vp, u32, u32, u32, u32p, sz, u32p, u32p]),
+    "hme_det_u32": (C.c_int, [vp, u32, u32, u32p, sz, u32p]),
+    "hme_rref_det_u32": (C.c_int, [vp, u32, u32, u32p, sz, u32p, u32p, u32p]),
+    "hme_kernel_basis_u32": (C.c_int, [vp, u32, u32, u32, u32p, sz, u32p, sz, u32p]),
+    "hme_inverse_u32": (C.c_int, [vp, u32, u32, u32p, sz, u32p, sz, C.POINTER(C.c_int)]),
+    "hme_solve_u32": (C.c_int, [vp, u32, u32, u32, u32, u32p, sz, u32p, sz, u32p, sz]),
+    "hme_ctx_set_elim_options": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "hme_gemm_u32": (C.c_int, [vp, u32, u32, u32, u32, u32p, sz, u32p, sz, u32p, sz, C.c_int]),
     "hme_gemm_u32_dev": (C.c_int, [vp, u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int]),
     "hme_gemm_u32_dev_noalloc": (C.c_int, [u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int, vp]),

@@ -75,25 +75,6 @@ void check_device_error(hme_ctx* ctx) {
     }
 }
 
-template <class F>
-int guard(F&& f) {
-    try {
-        f();
-        return HME_OK;
-    } catch (const Error& e) {
-        set_last_error(e.what());
-        return e.code;
-    } catch (const std::bad_alloc&) {
-        set_last_error("host allocation failed");
-        return HME_ENOMEM;
-    } catch (const std::exception& e) {
-        set_last_error(e.what());
-        return HME_EINVAL;
-    } catch (...) {
-        set_last_error("unknown exception");
-        return HME_EINVAL;
-    }
-}
 
 
 const char* last_error_cstr() { return g_last_error.c_str(); }

@@ -1,0 +1,571 @@
+// Device-resident elimination over F_p, p < 2^32 prime: RREF, rank, column
+// rank profile, determinant (and, built on them, kernel basis, inverse, solve).
+//
+// Reference semantics: engine::elim::rref / column_rank_profile
+// (src/ModArithmetic/DenseElim.h:153-169; Plu factor / trailing_update / to_rref
+// DenseElim.cpp:323-560, rref :921).  RREF(A) is unique (leading 1, zero rows
+// at the bottom) and its pivot columns are the column rank profile, so the pivot
+// ROW choice cannot show in the output; this driver takes the reference's rule
+// anyway (leftmost column with a non-zero in the Schur complement, topmost such
+// row) because it is also the cheapest to find in parallel (a min over rows).
+//
+// Blocked right-looking LU, panels of `bw` columns:
+//   1. panel_factor_kernel: one cooperative launch factors A[r0:m, c0:c0+bw)
+//      with one bounded grid barrier per column.  Pivot rows are not swapped
+//      during the panel; they leave the active set.  Each CTA owns a slice of
+//      rows; before every barrier each CTA publishes its topmost candidate row
+//      for the next column (values into a parity-double-buffered slot, index
+//      by atomicMin), so after the barrier every CTA knows the pivot row and
+//      has its values without a second barrier.  Multipliers are stored in the
+//      pivot columns of the active rows (packed L).
+//   2. the panel's pivot rows move to rows r0 .. r0+k-1 in pivot order (columns
+//      >= c0; columns left of the panel of non-U rows hold dead multipliers).
+//   3. U12 = L11^-1 A12: L11 inverted in shared memory, then one limb GEMM.
+//   4. A22 -= L21 * U12: the INT8-limb tcgen05 GEMM (Sub), K = k pivots.
+// Then RREF = U1^-1 U on the free columns only (the pivot columns of the RREF
+// are the identity): every diagonal block of U1 is inverted in shared memory
+// (one launch), and the blocked backward substitution is two limb GEMMs per
+// block (X_B = U_BB^-1 W_B, then W_above -= U_above,B X_B).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "hme_elim.h"
+#include "hme_internal.h"
+#include "hme_ptx.cuh"
+
+namespace hme {
+namespace {
+
+constexpr int kPanelThreads = 256;
+constexpr int kPanelWarps = kPanelThreads / 32;
+constexpr int kMaxPanel = 128;
+constexpr int kNoRow = 0x7f7f7f7f;  // piv_slot sentinel (memset 0x7f): larger than any row index
+
+// a^(p-2) mod p: the inverse of a unit of F_p (p prime) by Fermat's little
+// theorem, square-and-multiply with Barrett products (no divisions).
+__device__ __forceinline__ uint32_t inv_fermat(uint32_t a, uint32_t p, uint64_t barrett) {
+    uint32_t e = p - 2, r = 1 % p, b = a;
+    while (e) {
+        if (e & 1) r = mod_mul(r, b, p, barrett);
+        b = mod_mul(b, b, p, barrett);
+        e >>= 1;
+    }
+    return r;
+}
+
+struct PanelArgs {
+    uint32_t* A;
+    uint64_t ld;
+    int m;
+    int c0, bw;  // panel columns [c0, c0 + bw)
+    int r0;      // first active row
+    uint32_t p;
+    uint64_t barrett;
+    int* piv_slot;       // [bw], kNoRow on entry: topmost candidate row per column
+    uint32_t* cand;      // [2][grid][kMaxPanel]: candidate row values, by column parity
+    int* pivot_rows;     // [bw] out
+    int* pivot_cols;     // [bw] out
+    int* k_out;          // out: pivots found
+    unsigned* bar;       // [2]: arrival count, generation
+    int* err;
+};
+
+// Bounded grid-wide barrier for a cooperative launch (all CTAs co-resident).
+// Returns false on timeout or when another CTA already gave up.
+__device__ bool grid_barrier(unsigned* bar, int* err, int* s_flag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = bar + 1;
+        volatile int* verr = err;
+        const unsigned g = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        int ok = 1;
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const uint64_t t0 = global_timer_ns();
+            uint32_t spin = 0;
+            while (*vgen == g) {
+                if ((++spin & 63u) == 0) {
+                    if (*verr != 0) { ok = 0; break; }
+                    if (global_timer_ns() - t0 > HME_WAIT_LIMIT_NS) {
+                        atomicCAS(err, 0, DERR_GRID_BARRIER);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        __threadfence();
+        *s_flag = ok;
+    }
+    __syncthreads();
+    return *s_flag != 0;
+}
+
+__global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const PanelArgs a) {
+    __shared__ uint32_t s_prow[kMaxPanel];
+    __shared__ int s_cand;
+    __shared__ int s_flag;
+    __shared__ int s_piv;
+    __shared__ uint32_t s_inv;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int active_rows = a.m - a.r0;
+    const int rpc = (active_rows + gridDim.x - 1) / gridDim.x;
+    const int row_begin = a.r0 + blockIdx.x * rpc;
+    const int row_end = min(a.m, row_begin + rpc);
+    const int cend = a.c0 + a.bw;
+    uint32_t* cand_base = a.cand;
+    const size_t cand_stride = static_cast<size_t>(gridDim.x) * kMaxPanel;
+
+    // Rows of this CTA that became pivots are excluded by a per-row flag kept in
+    // the pivot_rows list: a CTA owns at most rpc rows, so it tracks its own
+    // pivots in shared memory.
+    __shared__ int s_mine[kMaxPanel];
+    __shared__ int s_nmine;
+    if (threadIdx.x == 0) s_nmine = 0;
+    __syncthreads();
+    auto is_pivot_row = [&](int i) {
+        for (int t = 0; t < s_nmine; ++t)
+            if (s_mine[t] == i) return true;
+        return false;
+    };
+
+    auto find_candidate = [&](int c) {
+        if (threadIdx.x == 0) s_cand = kNoRow;
+        __syncthreads();
+        if (c < cend) {
+            for (int i = row_begin + threadIdx.x; i < row_end; i += blockDim.x) {
+                if (a.A[static_cast<size_t>(i) * a.ld + c] != 0 && !is_pivot_row(i)) atomicMin(&s_cand, i);
+            }
+        }
+        __syncthreads();
+        if (c < cend && s_cand != kNoRow) {
+            const uint32_t* src = a.A + static_cast<size_t>(s_cand) * a.ld;
+            uint32_t* dst = cand_base + static_cast<size_t>(c & 1) * cand_stride + static_cast<size_t>(blockIdx.x) * kMaxPanel;
+            for (int j = c + threadIdx.x; j < cend; j += blockDim.x) dst[j - a.c0] = src[j];
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                atomicMin(&a.piv_slot[c - a.c0], s_cand);
+            }
+        }
+    };
+
+    find_candidate(a.c0);
+    int k = 0;
+    for (int c = a.c0; c < cend; ++c) {
+        if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+        if (threadIdx.x == 0) s_piv = *reinterpret_cast<volatile int*>(&a.piv_slot[c - a.c0]);
+        __syncthreads();
+        const int prow = s_piv;
+        if (prow == kNoRow) {
+            // column c is not a pivot column: every active row is zero there
+            find_candidate(c + 1);
+            continue;
+        }
+        const int owner = (prow - a.r0) / rpc;
+        const uint32_t* src = cand_base + static_cast<size_t>(c & 1) * cand_stride + static_cast<size_t>(owner) * kMaxPanel;
+        for (int j = c + threadIdx.x; j < cend; j += blockDim.x)
+            s_prow[j - a.c0] = *reinterpret_cast<const volatile uint32_t*>(&src[j - a.c0]);
+        if (threadIdx.x == 0) {
+            if (prow >= row_begin && prow < row_end) s_mine[s_nmine++] = prow;
+            if (blockIdx.x == 0) {
+                a.pivot_rows[k] = prow;
+                a.pivot_cols[k] = c;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_inv = inv_fermat(s_prow[c - a.c0], a.p, a.barrett);
+        __syncthreads();
+        const uint32_t inv = s_inv;
+        ++k;
+        // eliminate column c from this CTA's active rows: warp per row, lanes over columns
+        for (int i = row_begin + warp; i < row_end; i += kPanelWarps) {
+            if (i == prow || is_pivot_row(i)) continue;
+            uint32_t* row = a.A + static_cast<size_t>(i) * a.ld;
+            const uint32_t x = row[c];
+            if (x == 0) continue;
+            const uint32_t l = mod_mul(x, inv, a.p, a.barrett);
+            for (int j = c + 1 + lane; j < cend; j += 32) {
+                const uint32_t t = mod_mul(l, s_prow[j - a.c0], a.p, a.barrett);
+                row[j] = mod_sub(row[j], t, a.p);
+            }
+            __syncwarp();
+            if (lane == 0) row[c] = l;
+        }
+        __syncthreads();
+        find_candidate(c + 1);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.k_out = k;
+}
+
+// ---- row permutation of columns [c0, n) for rows [r0, m) -------------------------
+// tmp[i'][j'] = A[perm[i']][c0 + j']
+__global__ void gather_rows_kernel(const uint32_t* __restrict__ A, uint64_t ld, const int* __restrict__ perm,
+                                   int rows, int c0, int cols, uint32_t* __restrict__ tmp) {
+    const size_t total = static_cast<size_t>(rows) * cols;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int i = static_cast<int>(idx / cols), j = static_cast<int>(idx % cols);
+        tmp[idx] = A[static_cast<size_t>(perm[i]) * ld + c0 + j];
+    }
+}
+__global__ void scatter_rows_kernel(uint32_t* __restrict__ A, uint64_t ld, int r0, int rows, int c0, int cols,
+                                    const uint32_t* __restrict__ tmp) {
+    const size_t total = static_cast<size_t>(rows) * cols;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int i = static_cast<int>(idx / cols), j = static_cast<int>(idx % cols);
+        A[static_cast<size_t>(r0 + i) * ld + c0 + j] = tmp[idx];
+    }
+}
+
+// dst[i][t] = A[row0 + i][cols[t]]  (rows x k, ld k)
+__global__ void gather_cols_kernel(const uint32_t* __restrict__ A, uint64_t ld, int row0, int rows,
+                                   const int* __restrict__ cols, int k, uint32_t* __restrict__ dst) {
+    const size_t total = static_cast<size_t>(rows) * k;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int i = static_cast<int>(idx / k), t = static_cast<int>(idx % k);
+        dst[idx] = A[static_cast<size_t>(row0 + i) * ld + cols[t]];
+    }
+}
+
+// Inverses of triangular diagonal blocks, one CTA per block.  Block b covers
+// rows [row0 + b*bb, row0 + b*bb + nb) of A and the pivot columns
+// pcols[b*bb ..]: T(t, s) = A[row0 + b*bb + t][pcols[b*bb + s]].
+//   UPPER: T upper triangular with non-zero diagonal (the U1 blocks of the RREF)
+//   !UPPER: T unit lower triangular, strictly-lower part read (the L11 of a panel)
+// out + b*bb*bb receives T^-1 (nb x nb, row-major, ld nb).  Thread j solves
+// T x = e_j for column j of the inverse by substitution in shared memory.
+template <bool UPPER>
+__global__ void tri_inv_kernel(const uint32_t* __restrict__ A, uint64_t ld, int row0, const int* __restrict__ pcols,
+                               int total, int bb, uint32_t p, uint64_t barrett, uint32_t kmax,
+                               uint32_t* __restrict__ out) {
+    extern __shared__ uint32_t smem_ti[];
+    const int i0 = blockIdx.x * bb;
+    const int nb = min(bb, total - i0);
+    uint32_t* T = smem_ti;             // nb x nb
+    uint32_t* X = smem_ti + nb * nb;   // nb x nb, column j owned by thread j
+    uint32_t* dinv = X + nb * nb;      // nb
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+        const int t = idx / nb, s = idx % nb;
+        const bool keep = UPPER ? (s > t) : (s < t);
+        T[idx] = keep ? A[static_cast<size_t>(row0 + i0 + t) * ld + pcols[i0 + s]] : 0u;
+        X[idx] = 0;
+    }
+    for (int t = threadIdx.x; t < nb; t += blockDim.x)
+        dinv[t] = UPPER ? inv_fermat(A[static_cast<size_t>(row0 + i0 + t) * ld + pcols[i0 + t]], p, barrett) : 1u % p;
+    __syncthreads();
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        if (UPPER) {
+            X[j * nb + j] = dinv[j];
+            for (int t = j - 1; t >= 0; --t) {
+                uint64_t acc = 0;
+                uint32_t cnt = 0, sum = 0;
+                for (int s = t + 1; s <= j; ++s) {
+                    acc += static_cast<uint64_t>(T[t * nb + s]) * X[s * nb + j];
+                    if (++cnt == kmax) { sum = mod_add(sum, reduce_u64(acc, p, barrett), p); acc = 0; cnt = 0; }
+                }
+                sum = mod_add(sum, reduce_u64(acc, p, barrett), p);
+                X[t * nb + j] = mod_mul(sum == 0 ? 0u : p - sum, dinv[t], p, barrett);
+            }
+        } else {
+            X[j * nb + j] = 1u % p;
+            for (int t = j + 1; t < nb; ++t) {
+                uint64_t acc = 0;
+                uint32_t cnt = 0, sum = 0;
+                for (int s = j; s < t; ++s) {
+                    acc += static_cast<uint64_t>(T[t * nb + s]) * X[s * nb + j];
+                    if (++cnt == kmax) { sum = mod_add(sum, reduce_u64(acc, p, barrett), p); acc = 0; cnt = 0; }
+                }
+                sum = mod_add(sum, reduce_u64(acc, p, barrett), p);
+                X[t * nb + j] = sum == 0 ? 0u : p - sum;
+            }
+        }
+    }
+    __syncthreads();
+    uint32_t* o = out + static_cast<size_t>(blockIdx.x) * bb * bb;
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) o[idx] = X[idx];
+}
+
+// R (m x n, ld ldr): rows < rank: identity at the pivot columns, X at the free
+// columns; rows >= rank: zero.
+__global__ void assemble_rref_kernel(uint32_t* __restrict__ R, uint64_t ldr, int m, int n, int rank,
+                                     const int* __restrict__ colmap, const uint32_t* __restrict__ X, int f) {
+    // colmap[j] >= 0: pivot index of pivot column j; colmap[j] = -1 - t: free column number t
+    const size_t total = static_cast<size_t>(m) * n;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int i = static_cast<int>(idx / n), j = static_cast<int>(idx % n);
+        uint32_t v = 0;
+        if (i < rank) {
+            const int cm = colmap[j];
+            v = cm >= 0 ? (cm == i ? 1u : 0u) : X[static_cast<size_t>(i) * f + (-1 - cm)];
+        }
+        R[static_cast<size_t>(i) * ldr + j] = v;
+    }
+}
+
+// diag[t] = A[t][pivots[t]]
+__global__ void gather_diag_kernel(const uint32_t* __restrict__ A, uint64_t ld, const int* __restrict__ piv, int rank,
+                                   uint32_t* __restrict__ diag) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < rank; t += gridDim.x * blockDim.x)
+        diag[t] = A[static_cast<size_t>(t) * ld + piv[t]];
+}
+
+uint32_t kmax_for(uint32_t p) {
+    const uint64_t d = static_cast<uint64_t>(p - 1) * (p - 1);
+    uint64_t km = d == 0 ? 1024 : (~0ull) / d;
+    return static_cast<uint32_t>(std::min<uint64_t>(km, 1024));
+}
+
+int grid_1d(size_t work, int sms) {
+    return static_cast<int>(std::max<size_t>(1, std::min<size_t>((work + 255) / 256, static_cast<size_t>(sms) * 8)));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld, int m, int n, bool want_rref,
+                       uint32_t* R, size_t ldr, const ElimOptions& opt) {
+    HME_REQUIRE(m >= 0 && n >= 0, "elim: negative shape");
+    ElimResult res;
+    res.sign_negative = false;
+    if (m == 0 || n == 0) {
+        if (want_rref && m > 0 && n > 0) HME_CUDA(cudaMemsetAsync(R, 0, 1, ctx->stream));
+        return res;
+    }
+    const int bw = std::max(1, std::min<int>(opt.panel > 0 ? opt.panel : 64, kMaxPanel));
+    const uint32_t p = mp.p;
+
+    static std::once_flag attr_once;
+    std::call_once(attr_once, [] {
+        const int smem2 = sizeof(uint32_t) * (2 * kMaxPanel * kMaxPanel + kMaxPanel);
+        cudaFuncSetAttribute(tri_inv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
+        cudaFuncSetAttribute(tri_inv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
+    });
+
+    // device scratch
+    int max_grid = 0;
+    {
+        int per_sm = 0;
+        HME_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_factor_kernel, kPanelThreads, 0));
+        max_grid = std::max(1, per_sm) * ctx->num_sms;
+    }
+    const int grid_cap = std::min(max_grid, opt.panel_ctas > 0 ? opt.panel_ctas : ctx->num_sms);
+    struct Scratch {
+        int piv_slot[kMaxPanel];
+        int pivot_rows[kMaxPanel];
+        int pivot_cols[kMaxPanel];
+        int k;
+        unsigned bar[2];
+    };
+    const size_t cand_bytes = sizeof(uint32_t) * 2 * static_cast<size_t>(grid_cap) * kMaxPanel;
+    const size_t perm_bytes = sizeof(int) * static_cast<size_t>(m);
+    uint8_t* base = static_cast<uint8_t*>(ctx->ws.get(kSlotElim0, sizeof(Scratch) + 256 + cand_bytes + perm_bytes + 256));
+    Scratch* d_s = reinterpret_cast<Scratch*>(base);
+    uint32_t* d_cand = reinterpret_cast<uint32_t*>(base + (sizeof(Scratch) + 255) / 256 * 256);
+    int* d_perm = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(d_cand) + cand_bytes);
+    HME_CUDA(cudaMemsetAsync(d_s->bar, 0, sizeof(unsigned) * 2, ctx->stream));
+
+    std::vector<int> pivots;
+    pivots.reserve(std::min(m, n));
+    std::vector<int> perm_host;
+    int r0 = 0;
+    Scratch h_s;
+    for (int c0 = 0; c0 < n && r0 < m; c0 += bw) {
+        const int w = std::min(bw, n - c0);
+        HME_CUDA(cudaMemsetAsync(d_s->piv_slot, 0x7f, sizeof(int) * kMaxPanel, ctx->stream));  // > any row
+        PanelArgs pa{};
+        pa.A = A;
+        pa.ld = ld;
+        pa.m = m;
+        pa.c0 = c0;
+        pa.bw = w;
+        pa.r0 = r0;
+        pa.p = p;
+        pa.barrett = mp.barrett;
+        pa.piv_slot = d_s->piv_slot;
+        pa.cand = d_cand;
+        pa.pivot_rows = d_s->pivot_rows;
+        pa.pivot_cols = d_s->pivot_cols;
+        pa.k_out = &d_s->k;
+        pa.bar = d_s->bar;
+        pa.err = ctx->d_err;
+        const int rows = m - r0;
+        const int rpc = std::max(1, opt.rows_per_cta > 0 ? opt.rows_per_cta : 32);
+        const int want_grid = std::max(1, std::min(grid_cap, (rows + rpc - 1) / rpc));
+        void* args[] = {&pa};
+        HME_TIMED(ctx, "panel_factor",
+                  HME_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(panel_factor_kernel), want_grid,
+                                                       kPanelThreads, args, 0, ctx->stream)));
+        HME_CUDA(cudaMemcpyAsync(&h_s, d_s, sizeof(Scratch), cudaMemcpyDeviceToHost, ctx->stream));
+        check_device_error(ctx);  // synchronises
+        const int k = h_s.k;
+        if (k == 0) continue;
+        for (int t = 0; t < k; ++t) pivots.push_back(h_s.pivot_cols[t]);
+
+        // (2) pivot rows first, in pivot order, the other active rows after them in order
+        perm_host.assign(rows, 0);
+        {
+            std::vector<char> is_piv(rows, 0);
+            for (int t = 0; t < k; ++t) {
+                perm_host[t] = h_s.pivot_rows[t];
+                is_piv[h_s.pivot_rows[t] - r0] = 1;
+            }
+            int q = k;
+            for (int i = 0; i < rows; ++i)
+                if (!is_piv[i]) perm_host[q++] = r0 + i;
+            // permutation parity: inversions of the sequence (rows relative to r0)
+            long long inv = 0;
+            std::vector<int> bit(rows + 1, 0);
+            for (int t = rows - 1; t >= 0; --t) {
+                int x = perm_host[t] - r0 + 1;
+                for (int y = x - 1; y > 0; y -= y & -y) inv += bit[y];
+                for (int y = x; y <= rows; y += y & -y) bit[y] += 1;
+            }
+            if (inv & 1) res.sign_negative = !res.sign_negative;
+        }
+        bool identity = true;
+        for (int i = 0; i < rows && identity; ++i) identity = perm_host[i] == r0 + i;
+        const int cols_right = n - c0;
+        if (!identity) {
+            HME_CUDA(cudaMemcpyAsync(d_perm, perm_host.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, ctx->stream));
+            uint32_t* tmp = static_cast<uint32_t*>(ctx->ws.get(kSlotElim1, sizeof(uint32_t) * static_cast<size_t>(rows) * cols_right));
+            const int g = grid_1d(static_cast<size_t>(rows) * cols_right, ctx->num_sms);
+            HME_TIMED(ctx, "row_permute", gather_rows_kernel<<<g, 256, 0, ctx->stream>>>(A, ld, d_perm, rows, c0, cols_right, tmp));
+            HME_TIMED(ctx, "row_permute", scatter_rows_kernel<<<g, 256, 0, ctx->stream>>>(A, ld, r0, rows, c0, cols_right, tmp));
+            HME_CUDA(cudaGetLastError());
+        }
+        // pivot columns of this panel, on the device (reuse the pivot_cols slot)
+        const int c1 = c0 + w;
+        const int trail = n - c1;
+        const int below = m - r0 - k;
+        if (trail > 0) {
+            // (3) U12 = L11^-1 A12: invert the unit-lower k x k L11 in shared memory,
+            //     then one limb GEMM into a scratch buffer, copied back over A12
+            if (k > 1) {
+                uint32_t* Linv = static_cast<uint32_t*>(ctx->ws.get(kSlotElim5, sizeof(uint32_t) * kMaxPanel * kMaxPanel));
+                const size_t sm = sizeof(uint32_t) * (2 * static_cast<size_t>(k) * k + k);
+                HME_TIMED(ctx, "tri_inv", tri_inv_kernel<false><<<1, 128, sm, ctx->stream>>>(
+                                              A, ld, r0, d_s->pivot_cols, k, k, p, mp.barrett, kmax_for(p), Linv));
+                HME_CUDA(cudaGetLastError());
+                uint32_t* T = static_cast<uint32_t*>(ctx->ws.get(kSlotElim6, sizeof(uint32_t) * static_cast<size_t>(k) * trail));
+                gemm_u32_device(ctx, mp, k, trail, k, Linv, k, A + static_cast<size_t>(r0) * ld + c1, ld, T, trail,
+                                HME_SET);
+                HME_CUDA(cudaMemcpy2DAsync(A + static_cast<size_t>(r0) * ld + c1, sizeof(uint32_t) * ld, T,
+                                           sizeof(uint32_t) * trail, sizeof(uint32_t) * trail, k,
+                                           cudaMemcpyDeviceToDevice, ctx->stream));
+            }
+            // (4) A22 -= L21 * U12
+            if (below > 0) {
+                uint32_t* L21 = static_cast<uint32_t*>(ctx->ws.get(kSlotElim2, sizeof(uint32_t) * static_cast<size_t>(below) * k));
+                HME_TIMED(ctx, "gather_cols",
+                          gather_cols_kernel<<<grid_1d(static_cast<size_t>(below) * k, ctx->num_sms), 256, 0, ctx->stream>>>(
+                              A, ld, r0 + k, below, d_s->pivot_cols, k, L21));
+                HME_CUDA(cudaGetLastError());
+                gemm_u32_device(ctx, mp, below, trail, k, L21, k, A + static_cast<size_t>(r0) * ld + c1, ld,
+                                A + static_cast<size_t>(r0 + k) * ld + c1, ld, HME_SUB);
+            }
+        }
+        r0 += k;
+    }
+    res.rank = r0;
+    res.pivots = pivots;
+
+    // determinant factors: the U diagonal
+    if (opt.want_diag && res.rank > 0) {
+        int* d_pv = static_cast<int*>(ctx->ws.get(kSlotElim3, sizeof(int) * (2 * static_cast<size_t>(n) + 16)));
+        uint32_t* d_diag = reinterpret_cast<uint32_t*>(d_pv + n);
+        HME_CUDA(cudaMemcpyAsync(d_pv, pivots.data(), sizeof(int) * res.rank, cudaMemcpyHostToDevice, ctx->stream));
+        HME_TIMED(ctx, "gather_diag", gather_diag_kernel<<<grid_1d(res.rank, ctx->num_sms), 256, 0, ctx->stream>>>(
+                                          A, ld, d_pv, res.rank, d_diag));
+        HME_CUDA(cudaGetLastError());
+        res.diag.resize(res.rank);
+        HME_CUDA(cudaMemcpyAsync(res.diag.data(), d_diag, sizeof(uint32_t) * res.rank, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        HME_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    if (!want_rref) return res;
+
+    // ---- RREF = U1^-1 U on the free columns ------------------------------------------
+    const int rank = res.rank;
+    const int f = n - rank;
+    std::vector<int> colmap(n);
+    std::vector<int> free_cols;
+    {
+        std::vector<char> isp(n, 0);
+        for (int t = 0; t < rank; ++t) {
+            isp[pivots[t]] = 1;
+            colmap[pivots[t]] = t;
+        }
+        for (int j = 0; j < n; ++j)
+            if (!isp[j]) {
+                colmap[j] = -1 - static_cast<int>(free_cols.size());
+                free_cols.push_back(j);
+            }
+    }
+    int* d_cols = static_cast<int*>(ctx->ws.get(kSlotElim3, sizeof(int) * (2 * static_cast<size_t>(n) + 16)));
+    int* d_piv = d_cols + n;  // pivots, then free columns at d_cols
+    uint32_t* X = nullptr;
+    if (rank > 0) {
+        HME_CUDA(cudaMemcpyAsync(d_piv, pivots.data(), sizeof(int) * rank, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    if (rank > 0 && f > 0) {
+        HME_CUDA(cudaMemcpyAsync(d_cols, free_cols.data(), sizeof(int) * f, cudaMemcpyHostToDevice, ctx->stream));
+        X = static_cast<uint32_t*>(ctx->ws.get(kSlotElim1, sizeof(uint32_t) * static_cast<size_t>(rank) * f));
+        HME_TIMED(ctx, "gather_cols",
+                  gather_cols_kernel<<<grid_1d(static_cast<size_t>(rank) * f, ctx->num_sms), 256, 0, ctx->stream>>>(
+                      A, ld, 0, rank, d_cols, f, X));
+        HME_CUDA(cudaGetLastError());
+        const int bb = std::max(16, std::min(opt.back_block > 0 ? opt.back_block : 128, 128));
+        const int nblk = (rank + bb - 1) / bb;
+        // all diagonal blocks of U1 inverted at once, one CTA each
+        uint32_t* Uinv = static_cast<uint32_t*>(ctx->ws.get(kSlotElim5, sizeof(uint32_t) * static_cast<size_t>(nblk) * bb * bb));
+        {
+            const size_t sm = sizeof(uint32_t) * (2 * static_cast<size_t>(bb) * bb + bb);
+            HME_TIMED(ctx, "tri_inv", tri_inv_kernel<true><<<nblk, 128, sm, ctx->stream>>>(
+                                          A, ld, 0, d_piv, rank, bb, p, mp.barrett, kmax_for(p), Uinv));
+            HME_CUDA(cudaGetLastError());
+        }
+        // W (rank x f) in X's slot; the solution accumulates in Xs
+        uint32_t* Xs = static_cast<uint32_t*>(ctx->ws.get(kSlotElim6, sizeof(uint32_t) * static_cast<size_t>(rank) * f));
+        for (int blk = nblk - 1; blk >= 0; --blk) {
+            const int i0 = blk * bb, nb = std::min(bb, rank - i0);
+            // X_B = U_BB^-1 W_B
+            gemm_u32_device(ctx, mp, nb, f, nb, Uinv + static_cast<size_t>(blk) * bb * bb, nb,
+                            X + static_cast<size_t>(i0) * f, f, Xs + static_cast<size_t>(i0) * f, f, HME_SET);
+            if (i0 > 0) {
+                // W[0:i0] -= U1[0:i0, block pivots] * X_B
+                uint32_t* Ub = static_cast<uint32_t*>(ctx->ws.get(kSlotElim2, sizeof(uint32_t) * static_cast<size_t>(i0) * nb));
+                HME_TIMED(ctx, "gather_cols",
+                          gather_cols_kernel<<<grid_1d(static_cast<size_t>(i0) * nb, ctx->num_sms), 256, 0, ctx->stream>>>(
+                              A, ld, 0, i0, d_piv + i0, nb, Ub));
+                HME_CUDA(cudaGetLastError());
+                gemm_u32_device(ctx, mp, i0, f, nb, Ub, nb, Xs + static_cast<size_t>(i0) * f, f, X, f, HME_SUB);
+            }
+        }
+        X = Xs;
+    }
+    int* d_colmap = static_cast<int*>(ctx->ws.get(kSlotElim4, sizeof(int) * (static_cast<size_t>(n) + 16)));
+    HME_CUDA(cudaMemcpyAsync(d_colmap, colmap.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));
+    HME_TIMED(ctx, "assemble_rref",
+              assemble_rref_kernel<<<grid_1d(static_cast<size_t>(m) * n, ctx->num_sms), 256, 0, ctx->stream>>>(
+                  R, ldr, m, n, rank, d_colmap, X, std::max(f, 1)));
+    HME_CUDA(cudaGetLastError());
+    HME_CUDA(cudaStreamSynchronize(ctx->stream));
+    return res;
+}
+
+}  // namespace hme

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <new>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -45,6 +46,10 @@ enum WorkspaceSlot : int {
     kSlotElim0 = 5,    // elimination / ring drivers
     kSlotElim1 = 6,
     kSlotElim2 = 7,
+    kSlotElim3 = 8,
+    kSlotElim4 = 9,
+    kSlotElim5 = 10,
+    kSlotElim6 = 11,
 };
 
 struct Workspace {
@@ -58,6 +63,15 @@ struct Workspace {
 }  // namespace hme
 
 namespace hme {
+// Tunables of the device elimination (elim.cu); none of them changes a value.
+struct ElimOptions {
+    int panel = 64;         // LU panel width (columns, <= 128)
+    int rows_per_cta = 32;  // active rows per CTA of the cooperative panel kernel
+    int panel_ctas = 0;     // cap on the panel kernel's grid (0 = one CTA per SM)
+    int back_block = 128;   // block of the RREF backward substitution
+    bool want_diag = false; // return the U diagonal (determinant)
+};
+
 // Optional per-kernel CUDA-event timing (bench / profiling use): when enabled,
 // every launch of a named kernel is bracketed by two events on the launching
 // stream; hme_ctx_kernel_time() sums the elapsed times per name.
@@ -85,6 +99,7 @@ struct hme_ctx {
     uint64_t launches = 0;
     hme::Workspace ws;
     hme::KernelTimer timer;
+    hme::ElimOptions elim;
 };
 
 // Bracket one kernel launch with timing events when the context's timer is on.
@@ -104,6 +119,30 @@ void check_device_error(hme_ctx* ctx);
 
 // Make the context's device current on the calling thread.
 void bind(hme_ctx* ctx);
+
+// Run f, turning every exception into a status code and hme_last_error().
+template <class F>
+inline int guard(F&& f) {
+    try {
+        f();
+        return HME_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return HME_ENOMEM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return HME_EINVAL;
+    } catch (...) {
+        set_last_error("unknown exception");
+        return HME_EINVAL;
+    }
+}
+
+// Deterministic primality for 32-bit moduli (Miller-Rabin, bases 2, 7, 61).
+bool is_prime_u32(uint32_t p);
 
 // ---- the limb GEMM (limb_gemm.cu) ------------------------------------------
 // C op= A*B mod p with device pointers, on ctx->stream.

@@ -25,6 +25,7 @@ enum DeviceErr : int {
     DERR_WAIT_ACCUM_FREE = 4, // MMA issuer waited too long for a drained accumulator
     DERR_WAIT_DRAIN = 5,      // tear-down wait for in-flight copies / MMAs ran out
     DERR_TMEM_ADDR = 6,       // tensor-memory allocation returned an unusable address
+    DERR_GRID_BARRIER = 7,    // a cooperative kernel's grid barrier waited too long
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

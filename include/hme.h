@@ -95,6 +95,58 @@ HME_API int hme_gemm_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint3
 HME_API int hme_gemm_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A,
                      size_t lda, const uint32_t *B, size_t ldb, uint32_t *C, size_t ldc, int op);
 
+/* ---- elimination over F_p (p prime, p < 2^32) --------------------------------
+ * Device-resident blocked LU: a cooperative panel kernel (pivot = leftmost
+ * column with a non-zero in the Schur complement, topmost such row), row
+ * permutation, unit-lower TRSM and the limb GEMM for every trailing update;
+ * RREF = U1^-1 U by a blocked backward substitution on the free columns.  The
+ * RREF, pivots, rank and determinant are unique, so every output equals the
+ * reference's bit for bit.  A composite p is refused with HME_EINVAL (the
+ * reference's field-only rule, ENGINE_API.md Sec. 13.3).
+ *
+ * hme_rref_u32: in-place RREF of a host matrix (leading 1, zero rows at the
+ *   bottom), pivot columns ascending into pivots[] (min(m, n) entries), rank.
+ *   Replaces elim::DeviceRrefHook with want_rref = true
+ *   (src/ModArithmetic/DenseElim.h:121-123, installed at src/Engine/TapeElim.cpp:250;
+ *   the reference's own hook, cuda::imma_rref, serves p <= 127 only) and
+ *   serves elim::rref (DenseElim.h:153-158, DenseElim.cpp:921).
+ * hme_rref_u32_dev: the same on a device matrix (in place).
+ * hme_rank_profile_u32: pivots and rank only; A untouched.  Replaces the hook's
+ *   want_rref = false arm and elim::column_rank_profile (DenseElim.h:160-169).
+ * hme_det_u32: det(A) mod p of a square matrix (sign of the row permutation
+ *   times the product of the U diagonal; 0 when singular).  The reference has
+ *   no determinant entry point; this is the restatement of its PLU
+ *   (DenseElim.cpp:323-560).
+ * hme_rref_det_u32: RREF, pivots, rank and determinant of a square matrix in
+ *   one factorisation.
+ * hme_kernel_basis_u32: the (n - rank) x n kernel basis of A, one row per free
+ *   column ascending (1 there, -R[i][free] at pivot i): elim::kernel_basis of
+ *   the RREF (DenseElim.h:171-179).  K needs n rows of capacity.
+ * hme_inverse_u32: A^-1 through RREF([A | I]); *invertible = 0 when singular
+ *   (elim::inverse, DenseElim.h:186-189).
+ * hme_solve_u32: X (nb x ny) with B X = Y through RREF([B | Y]); column t of X
+ *   is the reference's result[t] (elim::solve_multi_rhs, DenseElim.h:191-197);
+ *   HME_ENOTINSPAN when a column of Y is outside the span of B's columns.
+ * hme_ctx_set_elim_options: panel width (<= 128), rows per CTA of the panel
+ *   kernel, cap on its grid, block of the backward substitution (0 = default).
+ *   Tuning only: no option changes a value. */
+HME_API int hme_rref_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t *A, size_t lda,
+                         uint32_t *pivots, uint32_t *rank);
+HME_API int hme_rref_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t *A, size_t lda,
+                             uint32_t *pivots, uint32_t *rank);
+HME_API int hme_rank_profile_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, const uint32_t *A, size_t lda,
+                                 uint32_t *pivots, uint32_t *rank);
+HME_API int hme_det_u32(hme_ctx *ctx, uint32_t p, uint32_t n, const uint32_t *A, size_t lda, uint32_t *det);
+HME_API int hme_rref_det_u32(hme_ctx *ctx, uint32_t p, uint32_t n, uint32_t *A, size_t lda, uint32_t *pivots,
+                             uint32_t *rank, uint32_t *det);
+HME_API int hme_kernel_basis_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, const uint32_t *A, size_t lda,
+                                 uint32_t *K, size_t ldk, uint32_t *nullity);
+HME_API int hme_inverse_u32(hme_ctx *ctx, uint32_t p, uint32_t n, const uint32_t *A, size_t lda, uint32_t *Ainv,
+                            size_t ldi, int *invertible);
+HME_API int hme_solve_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t nb, uint32_t ny, const uint32_t *B,
+                          size_t ldb, const uint32_t *Y, size_t ldy, uint32_t *X, size_t ldx);
+HME_API int hme_ctx_set_elim_options(hme_ctx *ctx, int panel, int rows_per_cta, int panel_ctas, int back_block);
+
 /* The GEMM above (same kernels, same result bits) for callers that cannot
  * allocate device memory when they call it -- a plugin inside another runtime
  * that owns the device-memory budget, or a latency-critical path where

@@ -70,6 +70,31 @@ def main():
                   "sigma": [int(x) for x in sig], "planted_e": [int(x) for x in e]})
     out["ring"] = h
 
+    # full-size configurations: config 2 (RankedMatrix 4096 x 4096, rank 3900, p = 2^31 - 19) and
+    # config 3 (planted U*D*V 2048 x 2048, Howell over Z/2^16 and Smith over Z/3^10)
+    if os.environ.get("GOLDEN_FULL", "1") == "1":
+        p = 2147483629
+        L, R = gen.ranked_factors(4096, 4096, 3900, p)
+        A = O.ref_gemm(p, L, R, threads=8)
+        Rr, piv = O.ref_rref(p, A)
+        out["config2"] = {"p": p, "m": 4096, "n": 4096, "rank_target": 3900, "input_fnv": fnv(A),
+                          "rank": int(len(piv)), "pivots_fnv": fnv(piv.reshape(1, -1)), "rref_fnv": fnv(Rr),
+                          "det": 0}
+        c3 = {}
+        for (ell, k) in [(2, 16), (3, 10)]:
+            M, e = gen.planted_udv(2048, ell, k, 0x33)
+            if ell == 2:
+                H, hp, hv = O.ref_howell_2k(k, M, threads=8)
+                sig = O.ref_smith_2k(k, M, threads=8)
+            else:
+                H, hp, hv = O.ref_howell_3k(k, M, threads=8)
+                sig = O.ref_smith_3k(k, M, threads=8)
+            c3[f"{ell}^{k}"] = {"ell": ell, "k": k, "n": 2048, "salt": 0x33, "input_fnv": fnv(M),
+                                "h": int(len(hp)), "howell_fnv": fnv(H), "pivots_fnv": fnv(hp.reshape(1, -1)),
+                                "pivot_v_fnv": fnv(hv.reshape(1, -1)), "sigma": [int(x) for x in sig],
+                                "planted_e_fnv": fnv(e.reshape(1, -1))}
+        out["config3"] = c3
+
     # known answers (ENGINE_API.md Sec. 13.5 and HeckeReductionValidation's Z/4 arms)
     H, piv, pv = O.ref_elim_howell(2, 2, np.array([[2, 1]], np.uint32))
     H2, piv2, pv2 = O.ref_elim_howell(2, 2, np.array([[2], [1]], np.uint32))
