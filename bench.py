@@ -293,8 +293,25 @@ def run_case(args):
 
     import hacs_b200
 
-    kind, n, p = args.case.split(":")
-    n, p = int(n), int(p)
+    parts = args.case.split(":")
+    kind = parts[0]
+    if kind == "rref":
+        # rref:<n>:<rank>:<p>: the config-2 family (RankedMatrix factors, device-resident elimination)
+        from hacs_b200 import gen
+
+        n, r, p = int(parts[1]), int(parts[2]), int(parts[3])
+        eng = hacs_b200.Engine(0)
+        L, R = gen.ranked_factors(n, n, r, p)
+        A = eng.gemm(p, L, R)
+        t0 = time.perf_counter()
+        for _ in range(max(1, args.warmup + args.steps)):
+            Rr, piv, d = eng.rref_det(p, A)
+        dt = (time.perf_counter() - t0) / max(1, args.warmup + args.steps)
+        print(json.dumps({"case": args.case, "rank": int(len(piv)), "det": int(d), "s_per_rref": dt,
+                          "rref_fnv": hex(gen.fnv_matrix(Rr))}), flush=True)
+        eng.close()
+        return 0
+    n, p = int(parts[1]), int(parts[2])
     assert kind == "gemm"
     torch.cuda.set_stream(torch.cuda.Stream())
     eng = hacs_b200.Engine(0)

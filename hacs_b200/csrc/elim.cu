@@ -44,6 +44,7 @@ namespace {
 constexpr int kPanelThreads = 256;
 constexpr int kPanelWarps = kPanelThreads / 32;
 constexpr int kMaxPanel = 128;
+constexpr int kPanelSmemMax = 160 * 1024;  // largest shared-memory row slice of the panel kernel
 constexpr int kNoRow = 0x7f7f7f7f;  // piv_slot sentinel (memset 0x7f): larger than any row index
 
 // a^(p-2) mod p: the inverse of a unit of F_p (p prime) by Fermat's little
@@ -111,12 +112,19 @@ __device__ bool grid_barrier(unsigned* bar, int* err, int* s_flag) {
     return *s_flag != 0;
 }
 
-__global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const PanelArgs a) {
+// One cooperative launch per panel.  With smem_rows, every CTA copies its
+// slice of the panel (rpc rows x bw columns) into shared memory first and
+// writes it back at the end, so the per-column work never leaves the SM; the
+// global-memory mode (slices too large for shared memory) works in place.
+__global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const PanelArgs a, int smem_rows) {
+    extern __shared__ uint32_t s_slice[];
     __shared__ uint32_t s_prow[kMaxPanel];
     __shared__ int s_cand;
     __shared__ int s_flag;
     __shared__ int s_piv;
     __shared__ uint32_t s_inv;
+    __shared__ int s_mine[kMaxPanel];
+    __shared__ int s_nmine;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int active_rows = a.m - a.r0;
@@ -124,14 +132,20 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
     const int row_begin = a.r0 + blockIdx.x * rpc;
     const int row_end = min(a.m, row_begin + rpc);
     const int cend = a.c0 + a.bw;
-    uint32_t* cand_base = a.cand;
     const size_t cand_stride = static_cast<size_t>(gridDim.x) * kMaxPanel;
 
-    // Rows of this CTA that became pivots are excluded by a per-row flag kept in
-    // the pivot_rows list: a CTA owns at most rpc rows, so it tracks its own
-    // pivots in shared memory.
-    __shared__ int s_mine[kMaxPanel];
-    __shared__ int s_nmine;
+    // row i of the panel, indexed by absolute column c in [c0, cend)
+    auto rowp = [&](int i) -> uint32_t* {
+        return smem_rows ? s_slice + static_cast<size_t>(i - row_begin) * a.bw - a.c0
+                         : a.A + static_cast<size_t>(i) * a.ld;
+    };
+    if (smem_rows) {
+        for (int i = row_begin + warp; i < row_end; i += kPanelWarps) {
+            const uint32_t* src = a.A + static_cast<size_t>(i) * a.ld;
+            uint32_t* dst = rowp(i);
+            for (int j = a.c0 + lane; j < cend; j += 32) dst[j] = src[j];
+        }
+    }
     if (threadIdx.x == 0) s_nmine = 0;
     __syncthreads();
     auto is_pivot_row = [&](int i) {
@@ -140,18 +154,19 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
         return false;
     };
 
+    // Publish this CTA's topmost active row with a non-zero in column c: its
+    // values (columns [c, cend)) into the parity slot, its index by atomicMin.
     auto find_candidate = [&](int c) {
         if (threadIdx.x == 0) s_cand = kNoRow;
         __syncthreads();
         if (c < cend) {
-            for (int i = row_begin + threadIdx.x; i < row_end; i += blockDim.x) {
-                if (a.A[static_cast<size_t>(i) * a.ld + c] != 0 && !is_pivot_row(i)) atomicMin(&s_cand, i);
-            }
+            for (int i = row_begin + threadIdx.x; i < row_end; i += blockDim.x)
+                if (rowp(i)[c] != 0 && !is_pivot_row(i)) atomicMin(&s_cand, i);
         }
         __syncthreads();
         if (c < cend && s_cand != kNoRow) {
-            const uint32_t* src = a.A + static_cast<size_t>(s_cand) * a.ld;
-            uint32_t* dst = cand_base + static_cast<size_t>(c & 1) * cand_stride + static_cast<size_t>(blockIdx.x) * kMaxPanel;
+            const uint32_t* src = rowp(s_cand);
+            uint32_t* dst = a.cand + static_cast<size_t>(c & 1) * cand_stride + static_cast<size_t>(blockIdx.x) * kMaxPanel;
             for (int j = c + threadIdx.x; j < cend; j += blockDim.x) dst[j - a.c0] = src[j];
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -163,8 +178,12 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
 
     find_candidate(a.c0);
     int k = 0;
+    bool ok = true;
     for (int c = a.c0; c < cend; ++c) {
-        if (!grid_barrier(a.bar, a.err, &s_flag)) return;
+        if (!grid_barrier(a.bar, a.err, &s_flag)) {
+            ok = false;
+            break;
+        }
         if (threadIdx.x == 0) s_piv = *reinterpret_cast<volatile int*>(&a.piv_slot[c - a.c0]);
         __syncthreads();
         const int prow = s_piv;
@@ -174,7 +193,7 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
             continue;
         }
         const int owner = (prow - a.r0) / rpc;
-        const uint32_t* src = cand_base + static_cast<size_t>(c & 1) * cand_stride + static_cast<size_t>(owner) * kMaxPanel;
+        const uint32_t* src = a.cand + static_cast<size_t>(c & 1) * cand_stride + static_cast<size_t>(owner) * kMaxPanel;
         for (int j = c + threadIdx.x; j < cend; j += blockDim.x)
             s_prow[j - a.c0] = *reinterpret_cast<const volatile uint32_t*>(&src[j - a.c0]);
         if (threadIdx.x == 0) {
@@ -192,7 +211,7 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
         // eliminate column c from this CTA's active rows: warp per row, lanes over columns
         for (int i = row_begin + warp; i < row_end; i += kPanelWarps) {
             if (i == prow || is_pivot_row(i)) continue;
-            uint32_t* row = a.A + static_cast<size_t>(i) * a.ld;
+            uint32_t* row = rowp(i);
             const uint32_t x = row[c];
             if (x == 0) continue;
             const uint32_t l = mod_mul(x, inv, a.p, a.barrett);
@@ -206,7 +225,15 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
         __syncthreads();
         find_candidate(c + 1);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) *a.k_out = k;
+    if (smem_rows) {
+        __syncthreads();
+        for (int i = row_begin + warp; i < row_end; i += kPanelWarps) {
+            uint32_t* dst = a.A + static_cast<size_t>(i) * a.ld;
+            const uint32_t* srow = rowp(i);
+            for (int j = a.c0 + lane; j < cend; j += 32) dst[j] = srow[j];
+        }
+    }
+    if (ok && blockIdx.x == 0 && threadIdx.x == 0) *a.k_out = k;
 }
 
 // ---- row permutation of columns [c0, n) for rows [r0, m) -------------------------
@@ -351,19 +378,14 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
 
     static std::once_flag attr_once;
     std::call_once(attr_once, [] {
+        cudaFuncSetAttribute(panel_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax);
         const int smem2 = sizeof(uint32_t) * (2 * kMaxPanel * kMaxPanel + kMaxPanel);
         cudaFuncSetAttribute(tri_inv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
         cudaFuncSetAttribute(tri_inv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
     });
 
     // device scratch
-    int max_grid = 0;
-    {
-        int per_sm = 0;
-        HME_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_factor_kernel, kPanelThreads, 0));
-        max_grid = std::max(1, per_sm) * ctx->num_sms;
-    }
-    const int grid_cap = std::min(max_grid, opt.panel_ctas > 0 ? opt.panel_ctas : ctx->num_sms);
+    const int grid_cap = std::max(1, std::min(ctx->num_sms, opt.panel_ctas > 0 ? opt.panel_ctas : ctx->num_sms));
     struct Scratch {
         int piv_slot[kMaxPanel];
         int pivot_rows[kMaxPanel];
@@ -404,12 +426,16 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         pa.bar = d_s->bar;
         pa.err = ctx->d_err;
         const int rows = m - r0;
-        const int rpc = std::max(1, opt.rows_per_cta > 0 ? opt.rows_per_cta : 32);
-        const int want_grid = std::max(1, std::min(grid_cap, (rows + rpc - 1) / rpc));
-        void* args[] = {&pa};
+        const int rpc_want = std::max(1, opt.rows_per_cta > 0 ? opt.rows_per_cta : 32);
+        const int want_grid = std::max(1, std::min(grid_cap, (rows + rpc_want - 1) / rpc_want));
+        const int rpc = (rows + want_grid - 1) / want_grid;
+        const size_t slice_bytes = sizeof(uint32_t) * static_cast<size_t>(rpc) * w;
+        int smem_rows = slice_bytes <= kPanelSmemMax ? 1 : 0;
+        const size_t dyn = smem_rows ? slice_bytes : 0;
+        void* args[] = {&pa, &smem_rows};
         HME_TIMED(ctx, "panel_factor",
                   HME_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(panel_factor_kernel), want_grid,
-                                                       kPanelThreads, args, 0, ctx->stream)));
+                                                       kPanelThreads, args, dyn, ctx->stream)));
         HME_CUDA(cudaMemcpyAsync(&h_s, d_s, sizeof(Scratch), cudaMemcpyDeviceToHost, ctx->stream));
         check_device_error(ctx);  // synchronises
         const int k = h_s.k;

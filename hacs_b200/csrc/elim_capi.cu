@@ -81,10 +81,16 @@ __global__ void kernel_basis_fill_kernel(const uint32_t* __restrict__ R, uint64_
 
 ElimOptions& opts(hme_ctx* ctx) { return ctx->elim; }
 
-// Device copy of a host matrix (rows x cols, ld) into workspace slot `slot`, compact (ld = cols).
-uint32_t* upload(hme_ctx* ctx, int slot, const uint32_t* H, size_t ldh, uint32_t rows, uint32_t cols,
-                 size_t extra_cols = 0) {
-    const size_t w = cols + extra_cols;
+// Working leading dimension of a device matrix with `cols` columns: a multiple
+// of 4 (16-byte rows for vector access) that is not a power-of-two multiple of
+// the row size, so the rows a warp touches together spread over the memory
+// partitions instead of camping on one.
+size_t padded_ld(size_t cols) { return (cols + 15) / 16 * 16 + 16; }
+
+// Device copy of a host matrix (rows x cols, ld) into workspace slot `slot`,
+// with the padded leading dimension padded_ld(cols).
+uint32_t* upload(hme_ctx* ctx, int slot, const uint32_t* H, size_t ldh, uint32_t rows, uint32_t cols) {
+    const size_t w = padded_ld(cols);
     uint32_t* d = static_cast<uint32_t*>(ctx->ws.get(slot, sizeof(uint32_t) * std::max<size_t>(1, rows * w)));
     if (rows && cols)
         HME_CUDA(cudaMemcpy2DAsync(d, sizeof(uint32_t) * w, H, sizeof(uint32_t) * ldh, sizeof(uint32_t) * cols, rows,
@@ -149,9 +155,10 @@ int hme_rref_u32(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t* A, 
         *rank = 0;
         if (m == 0 || n == 0) return;
         uint32_t* d = upload(ctx, kSlotStageA, A, lda, m, n);
+        const size_t dl = padded_ld(n);
         ElimOptions o = opts(ctx);
-        const ElimResult r = elim_device(ctx, make_mod(p), d, n, m, n, true, d, n, o);
-        HME_CUDA(cudaMemcpy2DAsync(A, sizeof(uint32_t) * lda, d, sizeof(uint32_t) * n, sizeof(uint32_t) * n, m,
+        const ElimResult r = elim_device(ctx, make_mod(p), d, dl, m, n, true, d, dl, o);
+        HME_CUDA(cudaMemcpy2DAsync(A, sizeof(uint32_t) * lda, d, sizeof(uint32_t) * dl, sizeof(uint32_t) * n, m,
                                    cudaMemcpyDeviceToHost, ctx->stream));
         check_device_error(ctx);
         *rank = r.rank;
@@ -171,7 +178,7 @@ int hme_rank_profile_u32(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, const
         if (m == 0 || n == 0) return;
         uint32_t* d = upload(ctx, kSlotStageA, A, lda, m, n);
         ElimOptions o = opts(ctx);
-        const ElimResult r = elim_device(ctx, make_mod(p), d, n, m, n, false, nullptr, 0, o);
+        const ElimResult r = elim_device(ctx, make_mod(p), d, padded_ld(n), m, n, false, nullptr, 0, o);
         check_device_error(ctx);
         *rank = r.rank;
         if (pivots)
@@ -192,7 +199,7 @@ int hme_det_u32(hme_ctx* ctx, uint32_t p, uint32_t n, const uint32_t* A, size_t 
         uint32_t* d = upload(ctx, kSlotStageA, A, lda, n, n);
         ElimOptions o = opts(ctx);
         o.want_diag = true;
-        const ElimResult r = elim_device(ctx, make_mod(p), d, n, n, n, false, nullptr, 0, o);
+        const ElimResult r = elim_device(ctx, make_mod(p), d, padded_ld(n), n, n, false, nullptr, 0, o);
         check_device_error(ctx);
         *det = det_from(r, n, p);
     });
@@ -209,10 +216,11 @@ int hme_rref_det_u32(hme_ctx* ctx, uint32_t p, uint32_t n, uint32_t* A, size_t l
         if (n == 0) return;
         HME_REQUIRE(A && lda >= n, "bad A");
         uint32_t* d = upload(ctx, kSlotStageA, A, lda, n, n);
+        const size_t dl = padded_ld(n);
         ElimOptions o = opts(ctx);
         o.want_diag = true;
-        const ElimResult r = elim_device(ctx, make_mod(p), d, n, n, n, true, d, n, o);
-        HME_CUDA(cudaMemcpy2DAsync(A, sizeof(uint32_t) * lda, d, sizeof(uint32_t) * n, sizeof(uint32_t) * n, n,
+        const ElimResult r = elim_device(ctx, make_mod(p), d, dl, n, n, true, d, dl, o);
+        HME_CUDA(cudaMemcpy2DAsync(A, sizeof(uint32_t) * lda, d, sizeof(uint32_t) * dl, sizeof(uint32_t) * n, n,
                                    cudaMemcpyDeviceToHost, ctx->stream));
         check_device_error(ctx);
         *rank = r.rank;
@@ -238,7 +246,7 @@ int hme_kernel_basis_u32(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, const
             HME_REQUIRE(A && lda >= n, "bad A");
             d = upload(ctx, kSlotStageA, A, lda, m, n);
             ElimOptions o = opts(ctx);
-            const ElimResult r = elim_device(ctx, make_mod(p), d, n, m, n, true, d, n, o);
+            const ElimResult r = elim_device(ctx, make_mod(p), d, padded_ld(n), m, n, true, d, padded_ld(n), o);
             piv = r.pivots;
             rank = r.rank;
         }
@@ -260,12 +268,12 @@ int hme_kernel_basis_u32(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, const
         HME_CUDA(cudaMemcpyAsync(d_idx + rank, freec.data(), sizeof(int) * f, cudaMemcpyHostToDevice, ctx->stream));
         uint32_t* dK = static_cast<uint32_t*>(ctx->ws.get(kSlotStageC, sizeof(uint32_t) * static_cast<size_t>(f) * n));
         HME_TIMED(ctx, "kernel_basis", kernel_basis_kernel<<<grid_for(static_cast<size_t>(f) * n, ctx->num_sms), 256, 0,
-                                                             ctx->stream>>>(d, n, n, rank, d_idx, d_idx + rank, f, p,
-                                                                            dK, n));
+                                                             ctx->stream>>>(d, padded_ld(n), n, rank, d_idx, d_idx + rank,
+                                                                            f, p, dK, n));
         if (rank)
             HME_TIMED(ctx, "kernel_basis",
                       kernel_basis_fill_kernel<<<grid_for(static_cast<size_t>(f) * rank, ctx->num_sms), 256, 0,
-                                                 ctx->stream>>>(d, n, rank, d_idx, d_idx + rank, f, p, dK, n));
+                                                 ctx->stream>>>(d, padded_ld(n), rank, d_idx, d_idx + rank, f, p, dK, n));
         HME_CUDA(cudaGetLastError());
         HME_CUDA(cudaMemcpy2DAsync(K, sizeof(uint32_t) * ldk, dK, sizeof(uint32_t) * n, sizeof(uint32_t) * n, f,
                                    cudaMemcpyDeviceToHost, ctx->stream));
@@ -293,13 +301,14 @@ int hme_inverse_u32(hme_ctx* ctx, uint32_t p, uint32_t n, const uint32_t* A, siz
             aug[i * w + n + i] = 1 % p;
         }
         uint32_t* d = upload(ctx, kSlotStageA, aug.data(), w, n, static_cast<uint32_t>(w));
+        const size_t dl = padded_ld(w);
         ElimOptions o = opts(ctx);
-        const ElimResult r = elim_device(ctx, make_mod(p), d, w, n, static_cast<int>(w), true, d, w, o);
+        const ElimResult r = elim_device(ctx, make_mod(p), d, dl, n, static_cast<int>(w), true, d, dl, o);
         check_device_error(ctx);
         bool ok = r.rank == static_cast<int>(n);
         for (int t = 0; ok && t < r.rank; ++t) ok = r.pivots[t] == t;
         if (!ok) return;
-        HME_CUDA(cudaMemcpy2DAsync(Ainv, sizeof(uint32_t) * ldi, d + n, sizeof(uint32_t) * w, sizeof(uint32_t) * n, n,
+        HME_CUDA(cudaMemcpy2DAsync(Ainv, sizeof(uint32_t) * ldi, d + n, sizeof(uint32_t) * dl, sizeof(uint32_t) * n, n,
                                    cudaMemcpyDeviceToHost, ctx->stream));
         check_device_error(ctx);
         *invertible = 1;
@@ -324,15 +333,17 @@ int hme_solve_u32(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t nb, uint32_t ny
         std::vector<uint32_t> Xh(static_cast<size_t>(nb) * ny, 0);
         if (m > 0) {
             uint32_t* d = upload(ctx, kSlotStageA, aug.data(), w, m, static_cast<uint32_t>(w));
+            const size_t dl = padded_ld(w);
             ElimOptions o = opts(ctx);
-            const ElimResult r = elim_device(ctx, make_mod(p), d, w, m, static_cast<int>(w), true, d, w, o);
+            const ElimResult r = elim_device(ctx, make_mod(p), d, dl, m, static_cast<int>(w), true, d, dl, o);
             for (int t = 0; t < r.rank; ++t)
                 if (r.pivots[t] >= static_cast<int>(nb))
                     throw Error(HME_ENOTINSPAN, "solve: right-hand side " + std::to_string(r.pivots[t] - nb) +
                                                     " is not in the column span of B");
             std::vector<uint32_t> R(static_cast<size_t>(r.rank) * w);
             if (r.rank)
-                HME_CUDA(cudaMemcpyAsync(R.data(), d, sizeof(uint32_t) * R.size(), cudaMemcpyDeviceToHost, ctx->stream));
+                HME_CUDA(cudaMemcpy2DAsync(R.data(), sizeof(uint32_t) * w, d, sizeof(uint32_t) * dl, sizeof(uint32_t) * w,
+                                           r.rank, cudaMemcpyDeviceToHost, ctx->stream));
             check_device_error(ctx);
             for (int t = 0; t < r.rank; ++t)
                 std::memcpy(&Xh[static_cast<size_t>(r.pivots[t]) * ny], &R[t * w + nb], sizeof(uint32_t) * ny);

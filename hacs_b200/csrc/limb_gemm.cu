@@ -54,7 +54,8 @@ struct Cfg {
     static constexpr int ACC_STRIDE = UN <= 32 ? 32 : UN <= 64 ? 64 : UN <= 128 ? 128 : 256;
     static constexpr int TMEM_COLS = 2 * ACC_STRIDE;
     static constexpr int BAR_BYTES = 256;
-    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + BAR_BYTES;
+    static constexpr int EPI_BYTES = 4 * 32 * 17 * 4;  // per-warp 32 x 16 staging chunk (+1 column of padding)
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + BAR_BYTES + EPI_BYTES;
     static constexpr uint32_t IDESC = idesc_u8(kBM, UN);
     static_assert((2 * STAGES + 5) * 8 + 8 <= BAR_BYTES, "barrier area too small");
 };
@@ -107,6 +108,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t* drain = acc_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    uint32_t* epi_stage = reinterpret_cast<uint32_t*>(smem + CF::STAGES * CF::STAGE_BYTES + CF::BAR_BYTES);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -210,10 +212,15 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
     } else {
-        // ---------------- epilogue: TMEM -> registers -> C ----------------
+        // ---------------- epilogue: TMEM -> registers -> shared -> C ----------------
+        // Each thread owns one accumulator row (its TMEM lane); the reduced
+        // 16-column chunk goes through a per-warp shared-memory stage so that
+        // C is read and written along rows: two rows x 64 contiguous bytes
+        // per warp instruction instead of 32 rows x 16 bytes.
         const int q = warp & 3;  // the TMEM lane quarter this warp may read
         const uint32_t lane_base = static_cast<uint32_t>(q * 32) << 16;
-        const bool vec_ok = ((reinterpret_cast<uintptr_t>(g.C) & 15) == 0) && ((g.ldc & 3) == 0);
+        uint32_t (*stage)[17] = reinterpret_cast<uint32_t (*)[17]>(epi_stage + (warp - 2) * 32 * 17);
+        const int half = lane >> 4, col_in = lane & 15;
         int lt = 0;
         for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++lt) {
             const int a = lt & 1;
@@ -222,9 +229,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_fence_after();
             int tm, tn;
             tile_coords(tile, g, tm, tn);
-            const int row = tm * kBM + q * 32 + lane;
-            const bool row_ok = row < g.M;
-            uint32_t* crow = g.C + static_cast<size_t>(row_ok ? row : 0) * g.ldc;
+            const int row0 = tm * kBM + q * 32;
 #pragma unroll 1
             for (int c0 = 0; c0 < BN; c0 += 16) {
                 uint32_t v[L][16];
@@ -232,45 +237,29 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int j = 0; j < L; ++j)
                     tmem_ld16(tmem_base + lane_base + a * CF::ACC_STRIDE + j * BN + c0, v[j]);
                 tmem_wait_ld();
-                const int col0 = tn * BN + c0;
-                if (!row_ok || col0 >= g.N) continue;
-                uint32_t r[16];
 #pragma unroll
                 for (int e = 0; e < 16; ++e) {
                     uint64_t s = v[0][e];
                     if (L > 1) s += static_cast<uint64_t>(v[L > 1 ? 1 : 0][e]) << 8;
                     if (L > 2) s += static_cast<uint64_t>(v[L > 2 ? 2 : 0][e]) << 16;
                     if (L > 3) s += static_cast<uint64_t>(v[L > 3 ? 3 : 0][e]) << 24;
-                    r[e] = reduce_u64(s, g.p, g.barrett);
+                    stage[lane][e] = reduce_u64(s, g.p, g.barrett);
                 }
-                uint32_t* dst = crow + col0;
-                if (vec_ok && col0 + 16 <= g.N) {
-                    uint4* d4 = reinterpret_cast<uint4*>(dst);
-#pragma unroll
-                    for (int w = 0; w < 4; ++w) {
-                        uint4 o = make_uint4(r[4 * w], r[4 * w + 1], r[4 * w + 2], r[4 * w + 3]);
-                        if (g.op != HME_SET) {
-                            const uint4 c = d4[w];
-                            if (g.op == HME_ADD) {
-                                o.x = mod_add(c.x, o.x, g.p); o.y = mod_add(c.y, o.y, g.p);
-                                o.z = mod_add(c.z, o.z, g.p); o.w = mod_add(c.w, o.w, g.p);
-                            } else {
-                                o.x = mod_sub(c.x, o.x, g.p); o.y = mod_sub(c.y, o.y, g.p);
-                                o.z = mod_sub(c.z, o.z, g.p); o.w = mod_sub(c.w, o.w, g.p);
-                            }
-                        }
-                        d4[w] = o;
-                    }
-                } else {
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        if (col0 + e >= g.N) break;
-                        uint32_t o = r[e];
-                        if (g.op == HME_ADD) o = mod_add(dst[e], o, g.p);
-                        else if (g.op == HME_SUB) o = mod_sub(dst[e], o, g.p);
-                        dst[e] = o;
+                __syncwarp();
+                const int col = tn * BN + c0 + col_in;
+                if (col < g.N) {
+#pragma unroll 4
+                    for (int rr = half; rr < 32; rr += 2) {
+                        const int row = row0 + rr;
+                        if (row >= g.M) break;
+                        uint32_t* dst = g.C + static_cast<size_t>(row) * g.ldc + col;
+                        uint32_t o = stage[rr][col_in];
+                        if (g.op == HME_ADD) o = mod_add(*dst, o, g.p);
+                        else if (g.op == HME_SUB) o = mod_sub(*dst, o, g.p);
+                        *dst = o;
                     }
                 }
+                __syncwarp();
             }
             tc_fence_before();
             mbar_arrive(&acc_empty[a]);
@@ -420,13 +409,14 @@ void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint
     });
     CUtensorMap tmA, tmB;
     {
-        const cuuint64_t dims[3] = {k, m, static_cast<cuuint64_t>(L)};
+        const cuuint64_t dims[3] = {static_cast<cuuint64_t>(Kp), m, static_cast<cuuint64_t>(L)};
         const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * m};
         const cuuint32_t box[3] = {kBK, kBM, 1};
         encode_u8(&tmA, planesA, 3, dims, strides, box);
     }
     {
-        const cuuint64_t dims[4] = {k, n, static_cast<cuuint64_t>(L), static_cast<cuuint64_t>(L)};
+        const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), n, static_cast<cuuint64_t>(L),
+                                    static_cast<cuuint64_t>(L)};
         const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * n,
                                        static_cast<cuuint64_t>(Kp) * n * L};
         const cuuint32_t box[4] = {kBK, BN, static_cast<cuuint32_t>(L), 1};
@@ -484,7 +474,9 @@ void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, 
     HME_REQUIRE(A && B && C, "gemm: null pointer");
     HME_REQUIRE(lda >= k && ldb >= n, "gemm: leading dimension too small");
     const int L = static_cast<int>(mp.limbs);
-    const int Kp = static_cast<int>((k + 15) / 16 * 16);
+    // K padded to whole 128-byte k-blocks (the split kernel writes the pad as
+    // zeros), so no TMA box ever reaches past the planes' K extent
+    const int Kp = static_cast<int>((k + kBK - 1) / kBK * kBK);
     uint8_t* pa = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesA, static_cast<size_t>(L) * m * Kp));
     uint8_t* pb = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesB, static_cast<size_t>(L) * L * n * Kp));
 
