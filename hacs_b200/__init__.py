@@ -13,6 +13,8 @@ device-pointer variants over torch CUDA tensors:
   ``Engine.kernel_basis(p, A)``              engine::elim::kernel_basis of rref(A) (DenseElim.h:171-179)
   ``Engine.inverse(p, A)``                   engine::elim::inverse (DenseElim.h:186-189)
   ``Engine.solve_multi_rhs(p, B, Y)``        engine::elim::solve_multi_rhs (DenseElim.h:191-197)
+  ``Engine.howell(ell, k, A)``               elim::howell / ring2k::howell / ring3k::howell (ENGINE_API.md Sec. 13.5)
+  ``Engine.smith(ell, k, A)``                ring2k::smith / ring3k::smith valuations (Ring2k.h:702, Ring3k.h:100)
 
 Every call goes to libhme; there is no CPU fallback.
 """
@@ -231,3 +233,29 @@ class Engine:
         rank = C.c_uint32()
         check(self._lib.hme_rref_u32_dev(self._h, p, m, n, _dev_ptr(A), A.stride(0), _p32(piv), C.byref(rank)))
         return piv[: rank.value].copy()
+
+    # ---- Z/ell^k --------------------------------------------------------------------------
+    def howell(self, ell: int, k: int, A):
+        """(H, pivots, pivot_v): the Howell form of rowspan(A) over Z/ell^k."""
+        A = _u32(A)
+        m, n = A.shape
+        H = np.zeros((max(1, n), max(1, n)), np.uint32)
+        piv = np.zeros(max(1, n), np.uint32)
+        pv = np.zeros(max(1, n), np.uint32)
+        h = C.c_uint32()
+        check(self._lib.hme_howell_u32(self._h, ell, k, m, n, _p32(A), max(1, n), _p32(H), max(1, n), _p32(piv),
+                                       _p32(pv), C.byref(h)))
+        return H[: h.value, :n].copy(), piv[: h.value].copy(), pv[: h.value].copy()
+
+    def smith(self, ell: int, k: int, A) -> np.ndarray:
+        """Smith valuations sigma (ascending, each < k) of A over Z/ell^k."""
+        A = _u32(A)
+        m, n = A.shape
+        s = np.zeros(max(1, min(m, n)), np.uint32)
+        cnt = C.c_uint32()
+        check(self._lib.hme_smith_u32(self._h, ell, k, m, n, _p32(A), max(1, n), _p32(s), C.byref(cnt)))
+        return s[: cnt.value].copy()
+
+    def invariant_factors(self, ell: int, k: int, A) -> np.ndarray:
+        """elim::invariant_factors: the exponents k - sigma, descending."""
+        return np.sort(k - self.smith(ell, k, A).astype(np.int64))[::-1].astype(np.uint32)

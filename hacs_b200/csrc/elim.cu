@@ -45,7 +45,7 @@ constexpr int kPanelThreads = 256;
 constexpr int kPanelWarps = kPanelThreads / 32;
 constexpr int kMaxPanel = 128;
 constexpr int kPanelSmemMax = 160 * 1024;  // largest shared-memory row slice of the panel kernel
-constexpr int kNoRow = 0x7f7f7f7f;  // piv_slot sentinel (memset 0x7f): larger than any row index
+constexpr unsigned long long kNoKey = 0x7f7f7f7f7f7f7f7full;  // piv_slot sentinel (memset 0x7f)
 
 // a^(p-2) mod p: the inverse of a unit of F_p (p prime) by Fermat's little
 // theorem, square-and-multiply with Barrett products (no divisions).
@@ -59,15 +59,55 @@ __device__ __forceinline__ uint32_t inv_fermat(uint32_t a, uint32_t p, uint64_t 
     return r;
 }
 
+// b^e mod p by square-and-multiply with Barrett products.
+__device__ __forceinline__ uint32_t pow_mod(uint32_t b, uint32_t e, uint32_t p, uint64_t barrett) {
+    uint32_t r = 1 % p;
+    while (e) {
+        if (e & 1) r = mod_mul(r, b, p, barrett);
+        b = mod_mul(b, b, p, barrett);
+        e >>= 1;
+    }
+    return r;
+}
+
+// The ring Z/q, q = ell^k (k = 1: the field F_ell), as the elimination sees it.
+struct Ring {
+    uint32_t q;          // modulus
+    uint64_t barrett;    // floor(2^64 / q)
+    uint32_t ell, k;
+    uint32_t unit_exp;   // phi(q) - 1: u^unit_exp is the inverse of a unit u
+    uint32_t max_v;      // pivots of valuation <= max_v only (0: unit pivots)
+    uint32_t pw[32];     // ell^0 .. ell^k
+};
+
+// ell-adic valuation of x != 0, capped at cap + 1 (enough to reject a candidate).
+__device__ __forceinline__ uint32_t valuation(uint32_t x, const Ring& R, uint32_t cap) {
+    if (R.ell == 2) return min(static_cast<uint32_t>(__ffs(x) - 1), cap + 1);
+    uint32_t v = 0;
+    while (v <= cap && x % R.ell == 0) {
+        x /= R.ell;
+        ++v;
+    }
+    return v;
+}
+
+// Pivot key of an entry: (valuation << 32 | row), or kNoKey when x is zero or
+// its valuation exceeds the ring's max_v.
+__device__ __forceinline__ unsigned long long pivot_key(uint32_t x, int row, const Ring& R) {
+    if (x == 0) return kNoKey;
+    const uint32_t v = R.k == 1 ? 0u : R.max_v == 0 ? (x % R.ell == 0 ? 1u : 0u) : valuation(x, R, R.max_v);
+    if (v > R.max_v) return kNoKey;
+    return (static_cast<unsigned long long>(v) << 32) | static_cast<unsigned>(row);
+}
+
 struct PanelArgs {
     uint32_t* A;
     uint64_t ld;
     int m;
     int c0, bw;  // panel columns [c0, c0 + bw)
     int r0;      // first active row
-    uint32_t p;
-    uint64_t barrett;
-    int* piv_slot;       // [bw], kNoRow on entry: topmost candidate row per column
+    Ring R;
+    unsigned long long* piv_slot;  // [bw], kNoKey on entry: smallest (valuation, row) key per column
     uint32_t* cand;      // [2][grid][kMaxPanel]: candidate row values, by column parity
     int* pivot_rows;     // [bw] out
     int* pivot_cols;     // [bw] out
@@ -119,10 +159,10 @@ __device__ bool grid_barrier(unsigned* bar, int* err, int* s_flag) {
 __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const PanelArgs a, int smem_rows) {
     extern __shared__ uint32_t s_slice[];
     __shared__ uint32_t s_prow[kMaxPanel];
-    __shared__ int s_cand;
+    __shared__ unsigned long long s_cand;
     __shared__ int s_flag;
-    __shared__ int s_piv;
-    __shared__ uint32_t s_inv;
+    __shared__ unsigned long long s_piv;
+    __shared__ uint32_t s_inv, s_div;
     __shared__ int s_mine[kMaxPanel];
     __shared__ int s_nmine;
 
@@ -157,15 +197,17 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
     // Publish this CTA's topmost active row with a non-zero in column c: its
     // values (columns [c, cend)) into the parity slot, its index by atomicMin.
     auto find_candidate = [&](int c) {
-        if (threadIdx.x == 0) s_cand = kNoRow;
+        if (threadIdx.x == 0) s_cand = kNoKey;
         __syncthreads();
         if (c < cend) {
-            for (int i = row_begin + threadIdx.x; i < row_end; i += blockDim.x)
-                if (rowp(i)[c] != 0 && !is_pivot_row(i)) atomicMin(&s_cand, i);
+            for (int i = row_begin + threadIdx.x; i < row_end; i += blockDim.x) {
+                const unsigned long long key = pivot_key(rowp(i)[c], i, a.R);
+                if (key != kNoKey && !is_pivot_row(i)) atomicMin(&s_cand, key);
+            }
         }
         __syncthreads();
-        if (c < cend && s_cand != kNoRow) {
-            const uint32_t* src = rowp(s_cand);
+        if (c < cend && s_cand != kNoKey) {
+            const uint32_t* src = rowp(static_cast<int>(s_cand & 0xffffffffu));
             uint32_t* dst = a.cand + static_cast<size_t>(c & 1) * cand_stride + static_cast<size_t>(blockIdx.x) * kMaxPanel;
             for (int j = c + threadIdx.x; j < cend; j += blockDim.x) dst[j - a.c0] = src[j];
             __syncthreads();
@@ -184,14 +226,16 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
             ok = false;
             break;
         }
-        if (threadIdx.x == 0) s_piv = *reinterpret_cast<volatile int*>(&a.piv_slot[c - a.c0]);
+        if (threadIdx.x == 0) s_piv = *reinterpret_cast<volatile unsigned long long*>(&a.piv_slot[c - a.c0]);
         __syncthreads();
-        const int prow = s_piv;
-        if (prow == kNoRow) {
+        const unsigned long long pkey = s_piv;
+        if (pkey == kNoKey) {
             // column c is not a pivot column: every active row is zero there
             find_candidate(c + 1);
             continue;
         }
+        const int prow = static_cast<int>(pkey & 0xffffffffu);
+        const uint32_t pv = static_cast<uint32_t>(pkey >> 32);
         const int owner = (prow - a.r0) / rpc;
         const uint32_t* src = a.cand + static_cast<size_t>(c & 1) * cand_stride + static_cast<size_t>(owner) * kMaxPanel;
         for (int j = c + threadIdx.x; j < cend; j += blockDim.x)
@@ -204,9 +248,15 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) s_inv = inv_fermat(s_prow[c - a.c0], a.p, a.barrett);
+        if (threadIdx.x == 0) {
+            // pivot x = ell^v * u: multipliers are (x_i / ell^v) * u^-1
+            const uint32_t x = s_prow[c - a.c0];
+            const uint32_t div = a.R.pw[pv];
+            s_div = div;
+            s_inv = pow_mod(x / div, a.R.unit_exp, a.R.q, a.R.barrett);
+        }
         __syncthreads();
-        const uint32_t inv = s_inv;
+        const uint32_t inv = s_inv, div = s_div;
         ++k;
         // eliminate column c from this CTA's active rows: warp per row, lanes over columns
         for (int i = row_begin + warp; i < row_end; i += kPanelWarps) {
@@ -214,10 +264,10 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
             uint32_t* row = rowp(i);
             const uint32_t x = row[c];
             if (x == 0) continue;
-            const uint32_t l = mod_mul(x, inv, a.p, a.barrett);
+            const uint32_t l = mod_mul(div == 1 ? x : x / div, inv, a.R.q, a.R.barrett);
             for (int j = c + 1 + lane; j < cend; j += 32) {
-                const uint32_t t = mod_mul(l, s_prow[j - a.c0], a.p, a.barrett);
-                row[j] = mod_sub(row[j], t, a.p);
+                const uint32_t t = mod_mul(l, s_prow[j - a.c0], a.R.q, a.R.barrett);
+                row[j] = mod_sub(row[j], t, a.R.q);
             }
             __syncwarp();
             if (lane == 0) row[c] = l;
@@ -365,8 +415,9 @@ int grid_1d(size_t work, int sms) {
 
 // ---------------------------------------------------------------------------------
 ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld, int m, int n, bool want_rref,
-                       uint32_t* R, size_t ldr, const ElimOptions& opt) {
+                       uint32_t* R, size_t ldr, const ElimOptions& opt, const RingSpec* ring) {
     HME_REQUIRE(m >= 0 && n >= 0, "elim: negative shape");
+    HME_REQUIRE(!(want_rref && ring && ring->k > 1), "elim: the RREF is a field-only object");
     ElimResult res;
     res.sign_negative = false;
     if (m == 0 || n == 0) {
@@ -375,6 +426,24 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     }
     const int bw = std::max(1, std::min<int>(opt.panel > 0 ? opt.panel : 64, kMaxPanel));
     const uint32_t p = mp.p;
+    // the ring: F_p by default, Z/ell^k with a pivot valuation bound when given
+    Ring rg{};
+    rg.q = p;
+    rg.barrett = mp.barrett;
+    rg.ell = ring ? ring->ell : p;
+    rg.k = ring ? ring->k : 1;
+    rg.max_v = ring ? ring->max_v : 0;
+    {
+        uint64_t pw = 1;
+        for (uint32_t v = 0; v <= rg.k && v < 32; ++v) {
+            rg.pw[v] = static_cast<uint32_t>(pw);
+            pw *= rg.ell;
+        }
+        HME_REQUIRE(static_cast<uint64_t>(rg.pw[rg.k]) == p || rg.k == 1, "elim: modulus is not ell^k");
+        // phi(ell^k) - 1 = ell^(k-1) (ell - 1) - 1
+        rg.unit_exp = static_cast<uint32_t>(static_cast<uint64_t>(rg.pw[rg.k - 1]) * (rg.ell - 1) - 1);
+    }
+    const int lu_cols = ring && ring->lu_cols > 0 ? std::min(ring->lu_cols, n) : n;
 
     static std::once_flag attr_once;
     std::call_once(attr_once, [] {
@@ -387,7 +456,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     // device scratch
     const int grid_cap = std::max(1, std::min(ctx->num_sms, opt.panel_ctas > 0 ? opt.panel_ctas : ctx->num_sms));
     struct Scratch {
-        int piv_slot[kMaxPanel];
+        unsigned long long piv_slot[kMaxPanel];
         int pivot_rows[kMaxPanel];
         int pivot_cols[kMaxPanel];
         int k;
@@ -406,9 +475,9 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     std::vector<int> perm_host;
     int r0 = 0;
     Scratch h_s;
-    for (int c0 = 0; c0 < n && r0 < m; c0 += bw) {
-        const int w = std::min(bw, n - c0);
-        HME_CUDA(cudaMemsetAsync(d_s->piv_slot, 0x7f, sizeof(int) * kMaxPanel, ctx->stream));  // > any row
+    for (int c0 = 0; c0 < lu_cols && r0 < m; c0 += bw) {
+        const int w = std::min(bw, lu_cols - c0);
+        HME_CUDA(cudaMemsetAsync(d_s->piv_slot, 0x7f, sizeof(unsigned long long) * kMaxPanel, ctx->stream));
         PanelArgs pa{};
         pa.A = A;
         pa.ld = ld;
@@ -416,8 +485,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         pa.c0 = c0;
         pa.bw = w;
         pa.r0 = r0;
-        pa.p = p;
-        pa.barrett = mp.barrett;
+        pa.R = rg;
         pa.piv_slot = d_s->piv_slot;
         pa.cand = d_cand;
         pa.pivot_rows = d_s->pivot_rows;

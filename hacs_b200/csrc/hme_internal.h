@@ -50,10 +50,20 @@ enum WorkspaceSlot : int {
     kSlotElim4 = 9,
     kSlotElim5 = 10,
     kSlotElim6 = 11,
+    kSlotRing0 = 12,   // Howell / Smith drivers
+    kSlotRing1 = 13,
+    kSlotRing2 = 14,
+    kSlotRing3 = 15,
+    kSlotRing4 = 16,
+    kSlotRing5 = 17,
+    kSlotJobs0 = 18,   // batched job stream
+    kSlotJobs1 = 19,
+    kSlotJobs2 = 20,
+    kSlotJobs3 = 21,
 };
 
 struct Workspace {
-    static constexpr int kSlots = 12;
+    static constexpr int kSlots = 24;
     void* ptr[kSlots] = {};
     size_t size[kSlots] = {};
     void* get(int slot, size_t bytes);

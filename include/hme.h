@@ -147,6 +147,27 @@ HME_API int hme_solve_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t nb, uin
                           size_t ldb, const uint32_t *Y, size_t ldy, uint32_t *X, size_t ldx);
 HME_API int hme_ctx_set_elim_options(hme_ctx *ctx, int panel, int rows_per_cta, int panel_ctas, int back_block);
 
+/* ---- Howell and Smith forms over Z/ell^k (ell prime, ell^k < 2^32) ----------
+ * Input canonical in [0, ell^k) (else HME_EINVAL, the reference's entry check).
+ *
+ * hme_howell_u32: the Howell form of rowspan(A) (ENGINE_API.md Sec. 13.5): h
+ *   rows (h <= n, possibly > m), leading columns strictly increasing, row i
+ *   leading with exactly ell^pivot_v[i], entries above each pivot reduced into
+ *   [0, ell^v).  H needs n rows of capacity (ldh >= n).  Replaces
+ *   elim::howell (src/ModArithmetic/DenseElim.h:248-249), ring2k::howell
+ *   (src/ModArithmetic/Binary/Ring2k.h:960-969, the Z/2^k device-ops table
+ *   ring2k::device::Ops of Binary/Ring2kDevice.h:64-83 serves its LU) and
+ *   ring3k::howell (Binary/Ring3k.h:101, host-only in the reference).
+ * hme_smith_u32: the Smith valuations sigma (ascending, each < k; the
+ *   non-zero Smith diagonal entries ell^sigma), count <= min(m, n).  Replaces
+ *   ring2k::smith (Ring2k.h:702) and ring3k::smith (Ring3k.h:100; host-only in
+ *   the reference); elim::invariant_factors (DenseElim.h:613-617) is
+ *   {k - sigma} descending. */
+HME_API int hme_howell_u32(hme_ctx *ctx, uint32_t ell, uint32_t k, uint32_t m, uint32_t n, const uint32_t *A,
+                           size_t lda, uint32_t *H, size_t ldh, uint32_t *pivots, uint32_t *pivot_v, uint32_t *h);
+HME_API int hme_smith_u32(hme_ctx *ctx, uint32_t ell, uint32_t k, uint32_t m, uint32_t n, const uint32_t *A,
+                          size_t lda, uint32_t *sigma, uint32_t *count);
+
 /* The GEMM above (same kernels, same result bits) for callers that cannot
  * allocate device memory when they call it -- a plugin inside another runtime
  * that owns the device-memory budget, or a latency-critical path where
