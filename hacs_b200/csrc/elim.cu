@@ -47,27 +47,38 @@ constexpr int kMaxPanel = 128;
 constexpr int kPanelSmemMax = 160 * 1024;  // largest shared-memory row slice of the panel kernel
 constexpr unsigned long long kNoKey = 0x7f7f7f7f7f7f7f7full;  // piv_slot sentinel (memset 0x7f)
 
-// a^(p-2) mod p: the inverse of a unit of F_p (p prime) by Fermat's little
-// theorem, square-and-multiply with Barrett products (no divisions).
-__device__ __forceinline__ uint32_t inv_fermat(uint32_t a, uint32_t p, uint64_t barrett) {
-    uint32_t e = p - 2, r = 1 % p, b = a;
-    while (e) {
-        if (e & 1) r = mod_mul(r, b, p, barrett);
-        b = mod_mul(b, b, p, barrett);
-        e >>= 1;
-    }
-    return r;
-}
 
-// b^e mod p by square-and-multiply with Barrett products.
-__device__ __forceinline__ uint32_t pow_mod(uint32_t b, uint32_t e, uint32_t p, uint64_t barrett) {
-    uint32_t r = 1 % p;
-    while (e) {
-        if (e & 1) r = mod_mul(r, b, p, barrett);
-        b = mod_mul(b, b, p, barrett);
-        e >>= 1;
+// Inverse of a unit u of Z/q, q = ell^k, without divisions on the slow path:
+//   ell = 2: Newton's iteration x <- x (2 - u x) in native 32-bit wraparound
+//            (each step doubles the correct low bits), then reduced mod 2^k;
+//   k > 1:   the inverse mod ell (binary extended gcd) lifted by the same
+//            iteration mod q (Hensel), doubling the ell-adic precision;
+//   k = 1:   the binary extended gcd mod the odd prime q.
+__device__ __forceinline__ uint32_t inv_binary_xgcd(uint32_t u, uint32_t q) {
+    // invariant: x1 * u == a (mod q), x2 * u == b (mod q), q odd.  Bounded:
+    // each pass shrinks a + b by at least one bit position or a subtraction,
+    // so 128 passes cover 32-bit operands; a non-unit (gcd > 1) returns 0.
+    if (u == 0) return 0;
+    uint32_t a = u, b = q, x1 = 1, x2 = 0;
+    for (int guard_it = 0; a != 1 && b != 1; ++guard_it) {
+        if (a == 0 || b == 0 || guard_it > 128) return 0;
+        while ((a & 1) == 0) {
+            a >>= 1;
+            x1 = (x1 & 1) ? static_cast<uint32_t>((static_cast<uint64_t>(x1) + q) >> 1) : x1 >> 1;
+        }
+        while ((b & 1) == 0) {
+            b >>= 1;
+            x2 = (x2 & 1) ? static_cast<uint32_t>((static_cast<uint64_t>(x2) + q) >> 1) : x2 >> 1;
+        }
+        if (a >= b) {
+            a -= b;
+            x1 = x1 >= x2 ? x1 - x2 : static_cast<uint32_t>(static_cast<uint64_t>(x1) + q - x2);
+        } else {
+            b -= a;
+            x2 = x2 >= x1 ? x2 - x1 : static_cast<uint32_t>(static_cast<uint64_t>(x2) + q - x1);
+        }
     }
-    return r;
+    return a == 1 ? x1 : x2;
 }
 
 // The ring Z/q, q = ell^k (k = 1: the field F_ell), as the elimination sees it.
@@ -79,6 +90,21 @@ struct Ring {
     uint32_t max_v;      // pivots of valuation <= max_v only (0: unit pivots)
     uint32_t pw[32];     // ell^0 .. ell^k
 };
+
+__device__ __forceinline__ uint32_t unit_inverse(uint32_t u, const Ring& R) {
+    if (R.ell == 2) {
+        uint32_t x = u;  // correct to 3 bits for odd u
+        for (int i = 0; i < 5; ++i) x *= 2u - u * x;
+        return R.k >= 32 ? x : (x & (R.q - 1));
+    }
+    if (R.k == 1) return inv_binary_xgcd(u % R.q, R.q);
+    uint32_t x = inv_binary_xgcd(u % R.ell, R.ell);  // inverse mod ell
+    for (uint32_t prec = 1; prec < R.k; prec *= 2) {
+        const uint32_t ux = mod_mul(u, x, R.q, R.barrett);
+        x = mod_mul(x, mod_sub(2u % R.q, ux, R.q), R.q, R.barrett);
+    }
+    return x;
+}
 
 // ell-adic valuation of x != 0, capped at cap + 1 (enough to reject a candidate).
 __device__ __forceinline__ uint32_t valuation(uint32_t x, const Ring& R, uint32_t cap) {
@@ -163,8 +189,6 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
     __shared__ int s_flag;
     __shared__ unsigned long long s_piv;
     __shared__ uint32_t s_inv, s_div;
-    __shared__ int s_mine[kMaxPanel];
-    __shared__ int s_nmine;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int active_rows = a.m - a.r0;
@@ -186,25 +210,18 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
             for (int j = a.c0 + lane; j < cend; j += 32) dst[j] = src[j];
         }
     }
-    if (threadIdx.x == 0) s_nmine = 0;
+    // per-row multiplier of the current column, and per-row flag: the row
+    // became a pivot row of this panel
+    uint32_t* s_l = s_slice + (smem_rows ? static_cast<size_t>(rpc) * a.bw : 0);
+    unsigned char* s_isp = reinterpret_cast<unsigned char*>(s_l + rpc);
+    for (int i = threadIdx.x; i < rpc; i += blockDim.x) s_isp[i] = 0;
     __syncthreads();
-    auto is_pivot_row = [&](int i) {
-        for (int t = 0; t < s_nmine; ++t)
-            if (s_mine[t] == i) return true;
-        return false;
-    };
+    auto is_pivot_row = [&](int i) { return s_isp[i - row_begin] != 0; };
 
-    // Publish this CTA's topmost active row with a non-zero in column c: its
-    // values (columns [c, cend)) into the parity slot, its index by atomicMin.
-    auto find_candidate = [&](int c) {
-        if (threadIdx.x == 0) s_cand = kNoKey;
-        __syncthreads();
-        if (c < cend) {
-            for (int i = row_begin + threadIdx.x; i < row_end; i += blockDim.x) {
-                const unsigned long long key = pivot_key(rowp(i)[c], i, a.R);
-                if (key != kNoKey && !is_pivot_row(i)) atomicMin(&s_cand, key);
-            }
-        }
+    // Publish this CTA's best pivot candidate for column c (smallest
+    // (valuation, row) key, already in s_cand): the row's values of columns
+    // [c, cend) into the parity slot, the key by atomicMin.
+    auto publish_candidate = [&](int c) {
         __syncthreads();
         if (c < cend && s_cand != kNoKey) {
             const uint32_t* src = rowp(static_cast<int>(s_cand & 0xffffffffu));
@@ -216,6 +233,17 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
                 atomicMin(&a.piv_slot[c - a.c0], s_cand);
             }
         }
+    };
+    auto find_candidate = [&](int c) {
+        if (threadIdx.x == 0) s_cand = kNoKey;
+        __syncthreads();
+        if (c < cend) {
+            for (int i = row_begin + threadIdx.x; i < row_end; i += blockDim.x) {
+                const unsigned long long key = pivot_key(rowp(i)[c], i, a.R);
+                if (key != kNoKey && !is_pivot_row(i)) atomicMin(&s_cand, key);
+            }
+        }
+        publish_candidate(c);
     };
 
     find_candidate(a.c0);
@@ -241,7 +269,7 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
         for (int j = c + threadIdx.x; j < cend; j += blockDim.x)
             s_prow[j - a.c0] = *reinterpret_cast<const volatile uint32_t*>(&src[j - a.c0]);
         if (threadIdx.x == 0) {
-            if (prow >= row_begin && prow < row_end) s_mine[s_nmine++] = prow;
+            if (prow >= row_begin && prow < row_end) s_isp[prow - row_begin] = 1;
             if (blockIdx.x == 0) {
                 a.pivot_rows[k] = prow;
                 a.pivot_cols[k] = c;
@@ -253,27 +281,52 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
             const uint32_t x = s_prow[c - a.c0];
             const uint32_t div = a.R.pw[pv];
             s_div = div;
-            s_inv = pow_mod(x / div, a.R.unit_exp, a.R.q, a.R.barrett);
+            s_inv = unit_inverse(x / div, a.R);
         }
         __syncthreads();
         const uint32_t inv = s_inv, div = s_div;
         ++k;
-        // eliminate column c from this CTA's active rows: warp per row, lanes over columns
-        for (int i = row_begin + warp; i < row_end; i += kPanelWarps) {
-            if (i == prow || is_pivot_row(i)) continue;
-            uint32_t* row = rowp(i);
-            const uint32_t x = row[c];
-            if (x == 0) continue;
-            const uint32_t l = mod_mul(div == 1 ? x : x / div, inv, a.R.q, a.R.barrett);
-            for (int j = c + 1 + lane; j < cend; j += 32) {
-                const uint32_t t = mod_mul(l, s_prow[j - a.c0], a.R.q, a.R.barrett);
-                row[j] = mod_sub(row[j], t, a.R.q);
+        // eliminate column c from this CTA's active rows in two phases:
+        // (1) one thread per row: multiplier l = (x / ell^v) * u^-1, stored in
+        //     the pivot column (packed L); (2) all threads over the (row,
+        //     column > c) elements, l * pivot row subtracted; the elements of
+        //     column c + 1 feed the next column's pivot candidate on the way.
+        const int nloc = row_end - row_begin;
+        if (threadIdx.x == 0) s_cand = kNoKey;
+        for (int li = threadIdx.x; li < nloc; li += blockDim.x) {
+            const int i = row_begin + li;
+            uint32_t l = 0;
+            if (i != prow && !is_pivot_row(i)) {
+                uint32_t* row = rowp(i);
+                const uint32_t x = row[c];
+                if (x != 0) {
+                    l = mod_mul(div == 1 ? x : x / div, inv, a.R.q, a.R.barrett);
+                    row[c] = l;
+                }
             }
-            __syncwarp();
-            if (lane == 0) row[c] = l;
+            s_l[li] = l;
         }
         __syncthreads();
-        find_candidate(c + 1);
+        const int width = cend - c - 1;
+        if (width > 0) {
+            const int total = nloc * width;
+            for (int e = threadIdx.x; e < total; e += blockDim.x) {
+                const int li = e / width, j = c + 1 + (e - li * width);
+                const int i = row_begin + li;
+                uint32_t* row = rowp(i);
+                uint32_t y = row[j];
+                const uint32_t l = s_l[li];
+                if (l != 0) {
+                    y = mod_sub(y, mod_mul(l, s_prow[j - a.c0], a.R.q, a.R.barrett), a.R.q);
+                    row[j] = y;
+                }
+                if (j == c + 1 && i != prow && !is_pivot_row(i)) {
+                    const unsigned long long key = pivot_key(y, i, a.R);
+                    if (key != kNoKey) atomicMin(&s_cand, key);
+                }
+            }
+        }
+        publish_candidate(c + 1);
     }
     if (smem_rows) {
         __syncthreads();
@@ -342,33 +395,31 @@ __global__ void tri_inv_kernel(const uint32_t* __restrict__ A, uint64_t ld, int 
         X[idx] = 0;
     }
     for (int t = threadIdx.x; t < nb; t += blockDim.x)
-        dinv[t] = UPPER ? inv_fermat(A[static_cast<size_t>(row0 + i0 + t) * ld + pcols[i0 + t]], p, barrett) : 1u % p;
+        dinv[t] = UPPER ? inv_binary_xgcd(A[static_cast<size_t>(row0 + i0 + t) * ld + pcols[i0 + t]], p) : 1u % p;
     __syncthreads();
-    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
-        if (UPPER) {
-            X[j * nb + j] = dinv[j];
-            for (int t = j - 1; t >= 0; --t) {
-                uint64_t acc = 0;
-                uint32_t cnt = 0, sum = 0;
-                for (int s = t + 1; s <= j; ++s) {
-                    acc += static_cast<uint64_t>(T[t * nb + s]) * X[s * nb + j];
-                    if (++cnt == kmax) { sum = mod_add(sum, reduce_u64(acc, p, barrett), p); acc = 0; cnt = 0; }
-                }
-                sum = mod_add(sum, reduce_u64(acc, p, barrett), p);
-                X[t * nb + j] = mod_mul(sum == 0 ? 0u : p - sum, dinv[t], p, barrett);
+    // one warp per column of the inverse; the dot product of each
+    // substitution step is split over the lanes and summed by shuffles
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    (void)kmax;
+    for (int j = warp; j < nb; j += nw) {
+        if (lane == 0) X[j * nb + j] = dinv[j];
+        __syncwarp();
+        const int tb = UPPER ? j - 1 : j + 1;
+        const int te = UPPER ? -1 : nb;
+        const int dt = UPPER ? -1 : 1;
+        for (int t = tb; t != te; t += dt) {
+            // UPPER: sum_{s=t+1..j} T[t][s] x_s ; LOWER: sum_{s=j..t-1} T[t][s] x_s
+            const int s0 = UPPER ? t + 1 : j, s1 = UPPER ? j : t - 1;
+            uint32_t part = 0;
+            for (int s2 = s0 + lane; s2 <= s1; s2 += 32)
+                part = mod_add(part, mod_mul(T[t * nb + s2], X[s2 * nb + j], p, barrett), p);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) part = mod_add(part, __shfl_xor_sync(0xffffffffu, part, off), p);
+            if (lane == 0) {
+                const uint32_t neg = part == 0 ? 0u : p - part;
+                X[t * nb + j] = UPPER ? mod_mul(neg, dinv[t], p, barrett) : neg;
             }
-        } else {
-            X[j * nb + j] = 1u % p;
-            for (int t = j + 1; t < nb; ++t) {
-                uint64_t acc = 0;
-                uint32_t cnt = 0, sum = 0;
-                for (int s = j; s < t; ++s) {
-                    acc += static_cast<uint64_t>(T[t * nb + s]) * X[s * nb + j];
-                    if (++cnt == kmax) { sum = mod_add(sum, reduce_u64(acc, p, barrett), p); acc = 0; cnt = 0; }
-                }
-                sum = mod_add(sum, reduce_u64(acc, p, barrett), p);
-                X[t * nb + j] = sum == 0 ? 0u : p - sum;
-            }
+            __syncwarp();
         }
     }
     __syncthreads();
@@ -498,8 +549,9 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         const int want_grid = std::max(1, std::min(grid_cap, (rows + rpc_want - 1) / rpc_want));
         const int rpc = (rows + want_grid - 1) / want_grid;
         const size_t slice_bytes = sizeof(uint32_t) * static_cast<size_t>(rpc) * w;
-        int smem_rows = slice_bytes <= kPanelSmemMax ? 1 : 0;
-        const size_t dyn = smem_rows ? slice_bytes : 0;
+        const size_t extra = 5 * static_cast<size_t>(rpc) + 16;  // multipliers + pivot flags
+        int smem_rows = slice_bytes + extra <= kPanelSmemMax ? 1 : 0;
+        const size_t dyn = (smem_rows ? slice_bytes : 0) + extra;
         void* args[] = {&pa, &smem_rows};
         HME_TIMED(ctx, "panel_factor",
                   HME_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(panel_factor_kernel), want_grid,
@@ -552,7 +604,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             if (k > 1) {
                 uint32_t* Linv = static_cast<uint32_t*>(ctx->ws.get(kSlotElim5, sizeof(uint32_t) * kMaxPanel * kMaxPanel));
                 const size_t sm = sizeof(uint32_t) * (2 * static_cast<size_t>(k) * k + k);
-                HME_TIMED(ctx, "tri_inv", tri_inv_kernel<false><<<1, 128, sm, ctx->stream>>>(
+                HME_TIMED(ctx, "tri_inv", tri_inv_kernel<false><<<1, 1024, sm, ctx->stream>>>(
                                               A, ld, r0, d_s->pivot_cols, k, k, p, mp.barrett, kmax_for(p), Linv));
                 HME_CUDA(cudaGetLastError());
                 uint32_t* T = static_cast<uint32_t*>(ctx->ws.get(kSlotElim6, sizeof(uint32_t) * static_cast<size_t>(k) * trail));
@@ -629,7 +681,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         uint32_t* Uinv = static_cast<uint32_t*>(ctx->ws.get(kSlotElim5, sizeof(uint32_t) * static_cast<size_t>(nblk) * bb * bb));
         {
             const size_t sm = sizeof(uint32_t) * (2 * static_cast<size_t>(bb) * bb + bb);
-            HME_TIMED(ctx, "tri_inv", tri_inv_kernel<true><<<nblk, 128, sm, ctx->stream>>>(
+            HME_TIMED(ctx, "tri_inv", tri_inv_kernel<true><<<nblk, 1024, sm, ctx->stream>>>(
                                           A, ld, 0, d_piv, rank, bb, p, mp.barrett, kmax_for(p), Uinv));
             HME_CUDA(cudaGetLastError());
         }
