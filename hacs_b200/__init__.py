@@ -259,3 +259,42 @@ class Engine:
     def invariant_factors(self, ell: int, k: int, A) -> np.ndarray:
         """elim::invariant_factors: the exponents k - sigma, descending."""
         return np.sort(k - self.smith(ell, k, A).astype(np.int64))[::-1].astype(np.uint32)
+
+    # ---- batched job stream -----------------------------------------------------------------
+    @staticmethod
+    def _jobs(jobs):
+        arr = (_lib.HmeJob * max(1, len(jobs)))()
+        for t, j in enumerate(jobs):
+            A, B, Cm, p = j["A"], j["B"], j["C"], j["p"]
+            m, n = Cm.shape
+            k = A.shape[1] if A is not None else 0
+            arr[t] = _lib.HmeJob(p, m, n, k, A.data_ptr() if A is not None else None, A.stride(0) if A is not None else 0,
+                                 B.data_ptr() if B is not None else None, B.stride(0) if B is not None else 0,
+                                 Cm.data_ptr(), Cm.stride(0))
+        return arr
+
+    def batch_gemm_dev(self, jobs) -> None:
+        """Every C_j = A_j B_j mod p_j (jobs: dicts with CUDA tensors A, B, C and p)."""
+        arr = self._jobs(jobs)
+        check(self._lib.hme_batch_gemm_u32_dev(self._h, len(jobs), arr))
+
+    def batch_rank_dev(self, jobs) -> np.ndarray:
+        """rank of each C_j over F_{p_j} (destroys C_j)."""
+        arr = self._jobs(jobs)
+        ranks = np.zeros(max(1, len(jobs)), np.uint32)
+        check(self._lib.hme_batch_rank_u32_dev(self._h, len(jobs), arr, _p32(ranks)))
+        return ranks[: len(jobs)].copy()
+
+    def batch_gemm_rank_dev(self, jobs) -> np.ndarray:
+        arr = self._jobs(jobs)
+        ranks = np.zeros(max(1, len(jobs)), np.uint32)
+        check(self._lib.hme_batch_gemm_rank_u32_dev(self._h, len(jobs), arr, _p32(ranks)))
+        return ranks[: len(jobs)].copy()
+
+    def gen_jobs_dev(self, specs) -> None:
+        """Fill CUDA tensors with the seeded job-stream matrices: specs are
+        (tensor, p, family, seed) tuples."""
+        arr = (_lib.HmeGenSpec * max(1, len(specs)))()
+        for t, (T, p, fam, seed) in enumerate(specs):
+            arr[t] = _lib.HmeGenSpec(T.data_ptr(), T.stride(0), T.shape[0], T.shape[1], p, fam, int(seed))
+        check(self._lib.hme_gen_jobs_u32_dev(self._h, len(specs), arr))

@@ -58,6 +58,27 @@ PROTOTYPES = {
     "hme_gemm_u32_dev_noalloc": (C.c_int, [u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int, vp]),
 }
 
+
+
+class HmeJob(C.Structure):
+    """struct hme_job (include/hme.h)."""
+    _fields_ = [("p", u32), ("m", u32), ("n", u32), ("k", u32), ("A", vp), ("lda", sz), ("B", vp), ("ldb", sz),
+                ("C", vp), ("ldc", sz)]
+
+
+class HmeGenSpec(C.Structure):
+    """struct hme_gen_spec (include/hme.h)."""
+    _fields_ = [("dst", vp), ("ld", sz), ("rows", u32), ("cols", u32), ("p", u32), ("family", C.c_int),
+                ("seed", C.c_uint64)]
+
+
+PROTOTYPES.update({
+    "hme_batch_gemm_u32_dev": (C.c_int, [vp, u32, C.POINTER(HmeJob)]),
+    "hme_batch_rank_u32_dev": (C.c_int, [vp, u32, C.POINTER(HmeJob), u32p]),
+    "hme_batch_gemm_rank_u32_dev": (C.c_int, [vp, u32, C.POINTER(HmeJob), u32p]),
+    "hme_gen_jobs_u32_dev": (C.c_int, [vp, u32, C.POINTER(HmeGenSpec)]),
+})
+
 _lib = None
 _lock = threading.Lock()
 

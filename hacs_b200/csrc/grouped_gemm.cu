@@ -1,0 +1,387 @@
+// Grouped INT8-limb GEMM: many independent mod-p products of different shapes
+// (C_j op= A_j * B_j mod p, one modulus per launch) in ONE persistent tcgen05
+// launch, plus one launch that splits every operand into limb planes.
+//
+// The per-problem table lives in device memory: the TMA descriptors of each
+// problem's planes (CUtensorMap objects in global memory), C, ldc, the shape
+// and the op.  A CTA walks global tile indices; a binary search over the tile
+// prefix finds the problem of each tile.  Warp roles, pipeline, tensor-memory
+// double buffer and epilogue are those of limb_gemm_kernel.  This is the
+// batched path the reference lacks: its GemmBatch (src/Cuda/CudaKernels.h:
+// 141-185, cuda_kernels.cu:831-946) runs one launch per SAME-shape batch, so
+// uneven shapes each cost a launch.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "hme_grouped.h"
+#include "hme_internal.h"
+#include "hme_limb.cuh"
+#include "hme_ptx.cuh"
+
+namespace hme {
+namespace {
+
+using namespace limb;
+
+struct GroupedProblem {
+    const CUtensorMap* tmA;  // limb planes of A_j: dims {Kp, M, L}
+    const CUtensorMap* tmB;  // limb planes of 256^i B_j: dims {Kp, N, L, L}
+    uint32_t* C;
+    uint64_t ldc;
+    int M, N;
+    int kblocks;
+    int op;
+    int tiles_n;
+    int tile_begin;
+    int pad[2];
+};
+
+__device__ __forceinline__ int find_problem(const GroupedProblem* __restrict__ probs, int nprob, int tile) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (probs[mid].tile_begin <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void grouped_drain(uint64_t* bar, uint32_t parity, int* err) {
+    int never = 0;
+    mbar_wait(bar, parity, &never, err, DERR_WAIT_DRAIN);
+}
+
+template <int L, int BN>
+__global__ void __launch_bounds__(kThreads, 1)
+    grouped_limb_gemm_kernel(const GroupedProblem* __restrict__ probs, int nprob, int total_tiles, uint32_t p,
+                             uint64_t barrett, int* err) {
+    using CF = Cfg<L, BN>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + CF::STAGES * CF::A_BYTES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + CF::STAGES * CF::STAGE_BYTES);
+    uint64_t* empty = full + CF::STAGES;
+    uint64_t* acc_full = empty + CF::STAGES;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    uint32_t* epi_stage = reinterpret_cast<uint32_t*>(smem + CF::STAGES * CF::STAGE_BYTES + CF::BAR_BYTES);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < CF::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 128);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+        fence_proxy_async_smem();
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, CF::TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int it = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; ok && tile < total_tiles; tile += gridDim.x) {
+                const int pi = find_problem(probs, nprob, tile);
+                const GroupedProblem& P = probs[pi];
+                const int local = tile - P.tile_begin;
+                const int tm = local / P.tiles_n, tn = local - tm * P.tiles_n;
+                for (int i = 0; ok && i < L; ++i) {
+                    for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
+                        const int s = it % CF::STAGES;
+                        const uint32_t ph = (it / CF::STAGES) & 1;
+                        if (!mbar_wait(&empty[s], ph ^ 1, abort_flag, err, DERR_WAIT_EMPTY)) {
+                            ok = false;
+                            break;
+                        }
+                        mbar_arrive_expect_tx(&full[s], CF::STAGE_BYTES);
+                        tma_load_3d(sA + s * CF::A_BYTES, P.tmA, &full[s], kb * kBK, tm * kBM, i);
+                        tma_load_4d(sB + s * CF::B_BYTES, P.tmB, &full[s], kb * kBK, tn * BN, 0, i);
+                    }
+                }
+            }
+            if (!ok)
+                for (int t = max(0, it - CF::STAGES); t < it; ++t)
+                    grouped_drain(&full[t % CF::STAGES], (t / CF::STAGES) & 1, err);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int it = 0, lt = 0;
+            bool ok = true, issued_any = false;
+            for (int tile = blockIdx.x; ok && tile < total_tiles; tile += gridDim.x, ++lt) {
+                const int kblocks = probs[find_problem(probs, nprob, tile)].kblocks;
+                const int a = lt & 1;
+                const uint32_t aph = (lt >> 1) & 1;
+                if (!mbar_wait(&acc_empty[a], aph ^ 1, abort_flag, err, DERR_WAIT_ACCUM_FREE)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem_base + a * CF::ACC_STRIDE;
+                for (int i = 0; ok && i < L; ++i) {
+                    for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                        const int s = it % CF::STAGES;
+                        const uint32_t ph = (it / CF::STAGES) & 1;
+                        if (!mbar_wait(&full[s], ph, abort_flag, err, DERR_WAIT_FULL)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint64_t adesc = smem_desc_k128(smem_u32(sA + s * CF::A_BYTES));
+                        const uint64_t bdesc = smem_desc_k128(smem_u32(sB + s * CF::B_BYTES));
+#pragma unroll
+                        for (int kk = 0; kk < kBK / 32; ++kk)
+                            mma_u8(d, adesc + 2 * kk, bdesc + 2 * kk, CF::IDESC, (i | kb | kk) != 0);
+                        issued_any = true;
+                        mma_commit(&empty[s]);
+                    }
+                }
+                if (ok) mma_commit(&acc_full[a]);
+            }
+            if (!ok && issued_any) {
+                mma_commit(drain);
+                grouped_drain(drain, 0, err);
+            }
+        }
+    } else {
+        const int q = warp & 3;
+        const uint32_t lane_base = static_cast<uint32_t>(q * 32) << 16;
+        uint32_t (*stage)[17] = reinterpret_cast<uint32_t (*)[17]>(epi_stage + (warp - 2) * 32 * 17);
+        const int half = lane >> 4, col_in = lane & 15;
+        int lt = 0;
+        for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++lt) {
+            const int a = lt & 1;
+            const uint32_t aph = (lt >> 1) & 1;
+            if (!mbar_wait(&acc_full[a], aph, abort_flag, err, DERR_WAIT_ACCUM)) break;
+            tc_fence_after();
+            const GroupedProblem& P = probs[find_problem(probs, nprob, tile)];
+            const int local = tile - P.tile_begin;
+            const int tm = local / P.tiles_n, tn = local - tm * P.tiles_n;
+            const int row0 = tm * kBM + q * 32;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                uint32_t v[L][16];
+#pragma unroll
+                for (int j = 0; j < L; ++j)
+                    tmem_ld16(tmem_base + lane_base + a * CF::ACC_STRIDE + j * BN + c0, v[j]);
+                tmem_wait_ld();
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    uint64_t s = v[0][e];
+                    if (L > 1) s += static_cast<uint64_t>(v[L > 1 ? 1 : 0][e]) << 8;
+                    if (L > 2) s += static_cast<uint64_t>(v[L > 2 ? 2 : 0][e]) << 16;
+                    if (L > 3) s += static_cast<uint64_t>(v[L > 3 ? 3 : 0][e]) << 24;
+                    stage[lane][e] = reduce_u64(s, p, barrett);
+                }
+                __syncwarp();
+                const int col = tn * BN + c0 + col_in;
+                if (col < P.N) {
+#pragma unroll 4
+                    for (int rr = half; rr < 32; rr += 2) {
+                        const int row = row0 + rr;
+                        if (row >= P.M) break;
+                        uint32_t* dst = P.C + static_cast<size_t>(row) * P.ldc + col;
+                        uint32_t o = stage[rr][col_in];
+                        if (P.op == HME_ADD) o = mod_add(*dst, o, p);
+                        else if (P.op == HME_SUB) o = mod_sub(*dst, o, p);
+                        *dst = o;
+                    }
+                }
+                __syncwarp();
+            }
+            tc_fence_before();
+            mbar_arrive(&acc_empty[a]);
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, CF::TMEM_COLS);
+    }
+}
+
+// One launch splits every problem's operands into limb planes.
+struct GroupedSplitJob {
+    SplitArgs s;
+    int b_blocks;     // blocks of the B part
+    int block_begin;  // prefix over all jobs (A part then B part)
+};
+
+template <int L>
+__global__ void __launch_bounds__(256) grouped_split_kernel(const GroupedSplitJob* __restrict__ jobs, int njobs) {
+    __shared__ uint32_t tile[64][33];
+    int lo = 0, hi = njobs - 1;
+    const int b = blockIdx.x;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].block_begin <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const GroupedSplitJob& J = jobs[lo];
+    const int local = b - J.block_begin;
+    if (local < J.s.a_blocks)
+        split_a_part<L>(J.s, local);
+    else
+        split_b_part<L>(J.s, local - J.s.a_blocks, tile);
+}
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+template <int L, int BN>
+void launch_grouped(hme_ctx* ctx, const ModParams& mp, const GroupedProblem* d_probs, int nprob, int total_tiles) {
+    using CF = Cfg<L, BN>;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(grouped_limb_gemm_kernel<L, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM);
+    });
+    const int grid = std::min(total_tiles, ctx->num_sms);
+    HME_TIMED(ctx, "grouped_gemm", grouped_limb_gemm_kernel<L, BN><<<grid, kThreads, CF::SMEM, ctx->stream>>>(
+                                       d_probs, nprob, total_tiles, mp.p, mp.barrett, ctx->d_err));
+    HME_CUDA(cudaGetLastError());
+}
+
+template <int L>
+void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs_in) {
+    std::vector<GemmJob> jobs;
+    jobs.reserve(jobs_in.size());
+    for (const GemmJob& j : jobs_in) {
+        if (j.M == 0 || j.N == 0) continue;
+        HME_REQUIRE(j.K > 0 && j.K <= limb_k_chunk(L), "grouped gemm: K must be in [1, the exact-accumulation chunk]");
+        jobs.push_back(j);
+    }
+    if (jobs.empty()) return;
+    const int nj = static_cast<int>(jobs.size());
+    // tile width: wide (L*BN close to 256) unless the whole group leaves SMs idle
+    constexpr int BNw = L == 1 ? 256 : L == 2 ? 128 : L == 3 ? 80 : 64;
+    constexpr int BNn = L == 1 ? 128 : L == 2 ? 64 : 32;
+    size_t tiles_wide = 0;
+    for (const GemmJob& j : jobs) tiles_wide += static_cast<size_t>((j.M + kBM - 1) / kBM) * ((j.N + BNw - 1) / BNw);
+    const bool narrow = tiles_wide < static_cast<size_t>(ctx->num_sms);
+    const int BN = narrow ? BNn : BNw;
+
+    // plane layout and split table
+    std::vector<GroupedSplitJob> split(nj);
+    std::vector<size_t> offA(nj), offB(nj);
+    size_t bytes = 0;
+    int blocks = 0;
+    for (int t = 0; t < nj; ++t) {
+        const GemmJob& j = jobs[t];
+        const int Kp = static_cast<int>((j.K + kBK - 1) / kBK * kBK);
+        offA[t] = bytes;
+        bytes += align256(static_cast<size_t>(L) * j.M * Kp);
+        offB[t] = bytes;
+        bytes += align256(static_cast<size_t>(L) * L * j.N * Kp);
+        SplitArgs& s = split[t].s;
+        s = SplitArgs{};
+        s.A = j.A;
+        s.lda = j.lda;
+        s.B = j.B;
+        s.ldb = j.ldb;
+        s.M = static_cast<int>(j.M);
+        s.N = static_cast<int>(j.N);
+        s.K = static_cast<int>(j.K);
+        s.Kp = Kp;
+        s.p = mp.p;
+        s.barrett = mp.barrett;
+        const size_t work = static_cast<size_t>(j.M) * (Kp / 16);
+        s.a_blocks = static_cast<int>(std::max<size_t>(1, std::min<size_t>((work + 255) / 256, 64)));
+        s.b_blocks_k = (Kp + 63) / 64;
+        s.a_vec = ((reinterpret_cast<uintptr_t>(j.A) & 15) == 0) && ((j.lda & 3) == 0);
+        split[t].b_blocks = s.b_blocks_k * static_cast<int>((j.N + 31) / 32);
+        split[t].block_begin = blocks;
+        blocks += s.a_blocks + split[t].b_blocks;
+    }
+    uint8_t* planes = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs0, bytes));
+    for (int t = 0; t < nj; ++t) {
+        split[t].s.planesA = planes + offA[t];
+        split[t].s.planesB = planes + offB[t];
+    }
+    // tensor maps (64-byte aligned objects) and the problem table, one upload each
+    const size_t maps_bytes = sizeof(CUtensorMap) * 2 * static_cast<size_t>(nj);
+    const size_t probs_bytes = sizeof(GroupedProblem) * static_cast<size_t>(nj);
+    const size_t split_bytes = sizeof(GroupedSplitJob) * static_cast<size_t>(nj);
+    uint8_t* tables = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs1, align256(maps_bytes) + align256(probs_bytes) +
+                                                                         align256(split_bytes)));
+    CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(tables);
+    GroupedProblem* d_probs = reinterpret_cast<GroupedProblem*>(tables + align256(maps_bytes));
+    GroupedSplitJob* d_split = reinterpret_cast<GroupedSplitJob*>(tables + align256(maps_bytes) + align256(probs_bytes));
+    std::vector<CUtensorMap> maps(2 * static_cast<size_t>(nj));
+    std::vector<GroupedProblem> probs(nj);
+    int tiles = 0;
+    for (int t = 0; t < nj; ++t) {
+        const GemmJob& j = jobs[t];
+        const int Kp = split[t].s.Kp;
+        {
+            const cuuint64_t dims[3] = {static_cast<cuuint64_t>(Kp), j.M, static_cast<cuuint64_t>(L)};
+            const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * j.M};
+            const cuuint32_t box[3] = {kBK, kBM, 1};
+            encode_tma_u8(&maps[2 * t], split[t].s.planesA, 3, dims, strides, box);
+        }
+        {
+            const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), j.N, static_cast<cuuint64_t>(L),
+                                        static_cast<cuuint64_t>(L)};
+            const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * j.N,
+                                           static_cast<cuuint64_t>(Kp) * j.N * L};
+            const cuuint32_t box[4] = {kBK, static_cast<cuuint32_t>(BN), static_cast<cuuint32_t>(L), 1};
+            encode_tma_u8(&maps[2 * t + 1], split[t].s.planesB, 4, dims, strides, box);
+        }
+        GroupedProblem& P = probs[t];
+        P.tmA = d_maps + 2 * t;
+        P.tmB = d_maps + 2 * t + 1;
+        P.C = j.C;
+        P.ldc = j.ldc;
+        P.M = static_cast<int>(j.M);
+        P.N = static_cast<int>(j.N);
+        P.kblocks = Kp / kBK;
+        P.op = j.op;
+        P.tiles_n = static_cast<int>((j.N + BN - 1) / BN);
+        P.tile_begin = tiles;
+        tiles += static_cast<int>((j.M + kBM - 1) / kBM) * P.tiles_n;
+    }
+    HME_CUDA(cudaMemcpyAsync(d_maps, maps.data(), maps_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    HME_CUDA(cudaMemcpyAsync(d_probs, probs.data(), probs_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    HME_CUDA(cudaMemcpyAsync(d_split, split.data(), split_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    HME_TIMED(ctx, "grouped_split", grouped_split_kernel<L><<<blocks, 256, 0, ctx->stream>>>(d_split, nj));
+    HME_CUDA(cudaGetLastError());
+    if (narrow) launch_grouped<L, BNn>(ctx, mp, d_probs, nj, tiles);
+    else launch_grouped<L, BNw>(ctx, mp, d_probs, nj, tiles);
+    // the host tables must outlive the asynchronous uploads
+    HME_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace
+
+void grouped_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs) {
+    switch (mp.limbs) {
+        case 1: run_grouped<1>(ctx, mp, jobs); break;
+        case 2: run_grouped<2>(ctx, mp, jobs); break;
+        case 3: run_grouped<3>(ctx, mp, jobs); break;
+        default: run_grouped<4>(ctx, mp, jobs); break;
+    }
+}
+
+}  // namespace hme

@@ -60,10 +60,16 @@ enum WorkspaceSlot : int {
     kSlotJobs1 = 19,
     kSlotJobs2 = 20,
     kSlotJobs3 = 21,
+    kSlotJobs4 = 22,
+    kSlotJobs5 = 23,
+    kSlotJobs6 = 24,
+    kSlotJobs7 = 25,
+    kSlotSched0 = 26,  // scheduler / autotuner
+    kSlotSched1 = 27,
 };
 
 struct Workspace {
-    static constexpr int kSlots = 24;
+    static constexpr int kSlots = 32;
     void* ptr[kSlots] = {};
     size_t size[kSlots] = {};
     void* get(int slot, size_t bytes);

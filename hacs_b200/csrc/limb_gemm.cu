@@ -33,32 +33,13 @@
 #include <mutex>
 
 #include "hme_internal.h"
+#include "hme_limb.cuh"
 #include "hme_ptx.cuh"
 
 namespace hme {
 namespace {
 
-constexpr int kBM = 128;     // UMMA M (rows of C per tile, one TMEM lane each)
-constexpr int kBK = 128;     // bytes of K per pipeline stage: one 128-byte swizzle row
-constexpr int kThreads = 192;
-
-template <int L, int BN>
-struct Cfg {
-    static constexpr int UN = L * BN;  // UMMA N: L accumulators of BN columns
-    static_assert(UN % 16 == 0 && UN >= 16 && UN <= 256, "UMMA N must be a multiple of 16 in [16, 256]");
-    static_assert(BN % 16 == 0, "the epilogue drains 16 columns at a time");
-    static constexpr int A_BYTES = kBM * kBK;
-    static constexpr int B_BYTES = UN * kBK;
-    static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-    static constexpr int STAGES = UN > 128 ? 4 : UN > 64 ? 6 : 8;
-    static constexpr int ACC_STRIDE = UN <= 32 ? 32 : UN <= 64 ? 64 : UN <= 128 ? 128 : 256;
-    static constexpr int TMEM_COLS = 2 * ACC_STRIDE;
-    static constexpr int BAR_BYTES = 256;
-    static constexpr int EPI_BYTES = 4 * 32 * 17 * 4;  // per-warp 32 x 16 staging chunk (+1 column of padding)
-    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + BAR_BYTES + EPI_BYTES;
-    static constexpr uint32_t IDESC = idesc_u8(kBM, UN);
-    static_assert((2 * STAGES + 5) * 8 + 8 <= BAR_BYTES, "barrier area too small");
-};
+using namespace limb;
 
 struct GemmArgs {
     uint32_t* C;
@@ -274,95 +255,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-// ---- limb split (one launch for both operands) ------------------------------------
-// Blocks [0, a_blocks): A planes[i][m][k] = byte i of A[m][k], 16 k per thread
-// (four 16-byte loads when A rows are 16-byte aligned).  Blocks [a_blocks, ..):
-// B planes[i][j][n][k] = byte j of (256^i * B[k][n] mod p), B transposed to
-// K-major through shared memory, 64 k x 32 n per block, 8 k per thread.
-// k in [K, Kp) is written as zero in both.
-struct SplitArgs {
-    const uint32_t* A;
-    uint64_t lda;
-    const uint32_t* B;
-    uint64_t ldb;
-    int M, N, K, Kp;
-    uint32_t p;
-    uint64_t barrett;
-    uint8_t* planesA;
-    uint8_t* planesB;
-    int a_blocks;        // blocks of the A part
-    int b_blocks_k;      // B part: blocks along k (64 k each)
-    bool a_vec;          // A rows 16-byte aligned: vector loads
-};
-
-template <int L>
-__device__ __forceinline__ void split_a_part(const SplitArgs& s, int block) {
-    const int kch = s.Kp >> 4;
-    const size_t total = static_cast<size_t>(s.M) * kch;
-    const size_t plane = static_cast<size_t>(s.M) * s.Kp;
-    for (size_t idx = static_cast<size_t>(block) * blockDim.x + threadIdx.x; idx < total;
-         idx += static_cast<size_t>(s.a_blocks) * blockDim.x) {
-        const int row = static_cast<int>(idx / kch);
-        const int k0 = static_cast<int>(idx - static_cast<size_t>(row) * kch) << 4;
-        const uint32_t* src = s.A + static_cast<size_t>(row) * s.lda + k0;
-        uint32_t x[16];
-        if (s.a_vec && k0 + 16 <= s.K) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint4 v = __ldg(reinterpret_cast<const uint4*>(src) + q);
-                x[4 * q] = v.x; x[4 * q + 1] = v.y; x[4 * q + 2] = v.z; x[4 * q + 3] = v.w;
-            }
-        } else {
-#pragma unroll
-            for (int e = 0; e < 16; ++e) x[e] = (k0 + e < s.K) ? __ldg(src + e) : 0u;
-        }
-        uint8_t* dst = s.planesA + static_cast<size_t>(row) * s.Kp + k0;
-#pragma unroll
-        for (int j = 0; j < L; ++j) {
-            uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-            for (int e = 0; e < 16; ++e) w[e >> 2] |= ((x[e] >> (8 * j)) & 0xffu) << (8 * (e & 3));
-            *reinterpret_cast<uint4*>(dst + j * plane) = make_uint4(w[0], w[1], w[2], w[3]);
-        }
-    }
-}
-
-template <int L>
-__device__ __forceinline__ void split_b_part(const SplitArgs& s, int block, uint32_t (*tile)[33]) {
-    const int k0 = (block % s.b_blocks_k) * 64, n0 = (block / s.b_blocks_k) * 32;
-    for (int t = threadIdx.x; t < 64 * 32; t += 256) {
-        const int kk = t >> 5, nn = t & 31;
-        const int k = k0 + kk, n = n0 + nn;
-        tile[kk][nn] = (k < s.K && n < s.N) ? __ldg(s.B + static_cast<size_t>(k) * s.ldb + n) : 0u;
-    }
-    __syncthreads();
-    const int nn = threadIdx.x >> 3, kc = threadIdx.x & 7;
-    const int n = n0 + nn, kb = k0 + kc * 8;
-    if (n >= s.N || kb >= s.Kp) return;
-    uint32_t out[L][L][2];
-#pragma unroll
-    for (int i = 0; i < L; ++i)
-#pragma unroll
-        for (int j = 0; j < L; ++j) out[i][j][0] = out[i][j][1] = 0;
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-        uint32_t v = tile[kc * 8 + e][nn];
-#pragma unroll
-        for (int i = 0; i < L; ++i) {
-            if (i) v = reduce_u64(static_cast<uint64_t>(v) << 8, s.p, s.barrett);
-#pragma unroll
-            for (int j = 0; j < L; ++j) out[i][j][e >> 2] |= ((v >> (8 * j)) & 0xffu) << (8 * (e & 3));
-        }
-    }
-    const size_t plane = static_cast<size_t>(s.N) * s.Kp;
-#pragma unroll
-    for (int i = 0; i < L; ++i)
-#pragma unroll
-        for (int j = 0; j < L; ++j)
-            *reinterpret_cast<uint2*>(s.planesB + (i * L + j) * plane + static_cast<size_t>(n) * s.Kp + kb) =
-                make_uint2(out[i][j][0], out[i][j][1]);
-}
-
 template <int L>
 __global__ void __launch_bounds__(256) limb_split_kernel(const SplitArgs s) {
     __shared__ uint32_t tile[64][33];
@@ -454,6 +346,11 @@ __global__ void fill_zero_kernel(uint32_t* C, uint64_t ldc, int m, int n) {
 }
 
 }  // namespace
+
+void encode_tma_u8(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
+                   const cuuint32_t* box) {
+    encode_u8(map, base, rank, dims, strides, box);
+}
 
 void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
                      size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op) {

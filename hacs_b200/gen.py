@@ -112,3 +112,51 @@ def planted_udv(n: int, ell: int, k: int, salt: int = 0x33, ops: int = 64):
     for k0 in range(0, n, step):
         M = (M + UD[:, k0:k0 + step] @ V[k0:k0 + step]) % q
     return M.astype(np.uint32), np.array(e, dtype=np.uint32)
+
+
+P_JOBS = (65521, 2147483629)
+
+
+def _mix(z):
+    with np.errstate(over="ignore"):
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+def job_stream(n_jobs: int, salt: int = 0x44):
+    """The batched job stream (config 4): per job j, side s = round(16 * 64^u)
+    with u uniform in [0, 1) (sides log-uniform in [16, 1024]), family j % 2
+    (0 banded sparse boundary-like, 1 dense Hecke-like), modulus p from a
+    seeded coin over {65521, 2^31 - 19}, and the splitmix64 seeds of A and B.
+    Returns numpy arrays (s, family, p, seed_a, seed_b)."""
+    j = np.arange(n_jobs, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        base = (np.uint64(0xC0FFEE123456789 ^ salt) * np.uint64(0x100000001B3) + j)
+        base = base * np.uint64(0x100000001B3) * np.uint64(0x100000001B3)
+        z0 = _mix(base + np.uint64(1) * GAMMA)
+        z1 = _mix(base + np.uint64(2) * GAMMA)
+    u = (z0 >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+    s = np.clip(np.rint(16.0 * np.power(64.0, u)), 16, 1024).astype(np.int64)
+    fam = (j % np.uint64(2)).astype(np.int64)
+    p = np.where((z1 & np.uint64(1)) == 0, P_JOBS[0], P_JOBS[1]).astype(np.int64)
+    seed_a = np.array([seed_for(int(i), 0, int(q), 0x45) for i, q in zip(range(n_jobs), p)], dtype=np.uint64)
+    seed_b = np.array([seed_for(int(i), 1, int(q), 0x45) for i, q in zip(range(n_jobs), p)], dtype=np.uint64)
+    return s, fam, p, seed_a, seed_b
+
+
+def job_matrix(rows: int, cols: int, p: int, family: int, seed: int) -> np.ndarray:
+    """Host twin of the device generator (hme_gen_jobs_u32_dev): element (r, c)
+    is output r*cols + c of splitmix64(seed); family 1 dense uniform mod p,
+    family 0 banded (|r - c| <= 8) with 5 % density and values in [-3, 3]."""
+    z = splitmix_stream(int(seed), rows * cols)
+    if family == 1:
+        return (z % np.uint64(p)).astype(np.uint32).reshape(rows, cols)
+    r = np.arange(rows)[:, None]
+    c = np.arange(cols)[None, :]
+    band = (np.abs(r - c) <= 8).reshape(-1)
+    hit = band & ((z % np.uint64(100)) < np.uint64(5))
+    w = ((z >> np.uint64(32)) % np.uint64(7)).astype(np.int64) - 3
+    v = np.where(w < 0, p + w, w)
+    out = np.where(hit, v, 0).astype(np.uint32)
+    return out.reshape(rows, cols)

@@ -168,6 +168,45 @@ HME_API int hme_howell_u32(hme_ctx *ctx, uint32_t ell, uint32_t k, uint32_t m, u
 HME_API int hme_smith_u32(hme_ctx *ctx, uint32_t ell, uint32_t k, uint32_t m, uint32_t n, const uint32_t *A,
                           size_t lda, uint32_t *sigma, uint32_t *count);
 
+/* ---- batched job stream ------------------------------------------------------
+ * A job is C = A*B mod p (A m x k, B k x n, device pointers) and/or the rank
+ * of C over F_p.  Thousands of uneven jobs run as one launch per phase: the
+ * GEMMs in one grouped persistent tcgen05 launch per modulus (the reference's
+ * GemmBatch, src/Cuda/CudaKernels.h:141-185, needs equal shapes), the ranks
+ * as rounds of a batched blocked LU (one CTA per job per panel, one grouped
+ * limb GEMM for every job's trailing update).  No reference caller uses the
+ * batch API yet; it serves the tape's BATCHED_GEMM node
+ * (src/Engine/DeviceBackend.cpp:416-439, 551-559) and per-job rank queries
+ * (elim::column_rank_profile, DenseElim.h:160-169).
+ * hme_batch_gemm_u32_dev: every C_j = A_j B_j mod p_j.
+ * hme_batch_rank_u32_dev: ranks[j] = rank of C_j (m x n) over F_{p_j} (p_j
+ *   prime); destroys C_j.
+ * hme_batch_gemm_rank_u32_dev: both, in that order.
+ * hme_gen_jobs_u32_dev: the seeded synthetic job-stream matrices on the
+ *   device (family 0: banded sparse, |i - j| <= 8, 5 % density, values in
+ *   [-3, 3] mod p; family 1: dense uniform mod p); element (r, c) is output
+ *   r*cols + c of splitmix64(seed). */
+typedef struct hme_job {
+    uint32_t p, m, n, k;
+    const uint32_t *A;
+    size_t lda;
+    const uint32_t *B;
+    size_t ldb;
+    uint32_t *C;
+    size_t ldc;
+} hme_job;
+typedef struct hme_gen_spec {
+    uint32_t *dst;
+    size_t ld;
+    uint32_t rows, cols, p;
+    int family;
+    uint64_t seed;
+} hme_gen_spec;
+HME_API int hme_batch_gemm_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs);
+HME_API int hme_batch_rank_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, uint32_t *ranks);
+HME_API int hme_batch_gemm_rank_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, uint32_t *ranks);
+HME_API int hme_gen_jobs_u32_dev(hme_ctx *ctx, uint32_t nmat, const hme_gen_spec *specs);
+
 /* The GEMM above (same kernels, same result bits) for callers that cannot
  * allocate device memory when they call it -- a plugin inside another runtime
  * that owns the device-memory budget, or a latency-critical path where
