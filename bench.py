@@ -287,6 +287,129 @@ def big_gemm(eng, plain, p, n, steps=5, warmup=3):
     return out
 
 
+def _golden():
+    path = os.path.join(ROOT, "tests", "golden", "golden.json")
+    return json.load(open(path)) if os.path.exists(path) else {}
+
+
+def extra_rref(eng, reps=3):
+    """Config 2: RREF + rank + det of RankedMatrix(4096, 4096, 3900, 2^31 - 19), device-resident."""
+    import torch
+
+    from hacs_b200 import gen
+
+    g = _golden().get("config2", {})
+    p, n, r = 2147483629, 4096, 3900
+    L, R = gen.ranked_factors(n, n, r, p)
+    A0 = torch.empty((n, n), dtype=torch.int32, device="cuda")
+    eng.gemm_dev(p, torch.from_numpy(L.view(np.int32)).cuda(), torch.from_numpy(R.view(np.int32)).cuda(), A0)
+    eng.sync()
+    A = torch.empty_like(A0)
+    times = []
+    for _ in range(reps + 1):
+        A.copy_(A0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        piv = eng.rref_dev(p, A)
+        times.append(time.perf_counter() - t0)
+    t = min(times[1:])
+    ok = gen.fnv_matrix(A.cpu().numpy().view(np.uint32)) == int(g.get("rref_fnv", "0x0"), 16)
+    work = n * n * r - (n + n) * r * r / 2 + r ** 3 / 3 + r * r * (n - r) / 2
+    return {"workload": "RREF/rank/det 4096^2 rank 3900 p=2^31-19 (config 2)", "ms": t * 1e3, "rank": int(len(piv)),
+            "modmac_per_s": work / t, "checksum_ok_vs_reference": bool(ok)}
+
+
+def extra_ring(eng, reps=3):
+    """Config 3: Howell over Z/2^16 and Smith over Z/3^10 of planted 2048^2 U*D*V."""
+    from hacs_b200 import gen
+
+    g = _golden().get("config3", {})
+    out = {}
+    for (ell, k, kind) in [(2, 16, "howell"), (3, 10, "smith"), (2, 16, "smith"), (3, 10, "howell")]:
+        M, e = gen.planted_udv(2048, ell, k, 0x33)
+        fn = (lambda: eng.howell(ell, k, M)) if kind == "howell" else (lambda: eng.smith(ell, k, M))
+        fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            res = fn()
+            ts.append(time.perf_counter() - t0)
+        c = g.get(f"{ell}^{k}", {})
+        if kind == "howell":
+            ok = gen.fnv_matrix(res[0]) == int(c.get("howell_fnv", "0x0"), 16)
+        else:
+            ok = list(res) == c.get("sigma")
+        out[f"{kind}_2048_{ell}^{k}"] = {"ms": min(ts) * 1e3, "bit_exact_vs_reference": bool(ok),
+                                        "api": "host pointers (H2D + D2H inside)"}
+    return out
+
+
+def extra_jobstream(eng, plain, n_jobs=10000, sample=500):
+    """Config 4: the 10,000-job stream (GEMM + rank per job, sides 16..1024), batched,
+    next to one-launch-per-job plain dispatch (the reference's CUDA-core GEMM plus a
+    per-job device rank) on the first `sample` jobs."""
+    import ctypes as C_
+
+    import torch
+
+    import hacs_b200
+    from hacs_b200 import gen
+
+    s, fam, p, sa, sb = gen.job_stream(n_jobs)
+    tot = int((s * s).sum())
+    bufA = torch.empty(tot, dtype=torch.int32, device="cuda")
+    bufB, bufC = torch.empty_like(bufA), torch.empty_like(bufA)
+    jobs, specs, off = [], [], 0
+    for j in range(n_jobs):
+        n = int(s[j])
+        A, B, Cm = (b[off:off + n * n].view(n, n) for b in (bufA, bufB, bufC))
+        off += n * n
+        jobs.append({"p": int(p[j]), "A": A, "B": B, "C": Cm})
+        specs += [(A, int(p[j]), int(fam[j]), int(sa[j])), (B, int(p[j]), int(fam[j]), int(sb[j]))]
+    eng.gen_jobs_dev(specs)
+    arr = eng._jobs(jobs)
+
+    def batched(nj, a):
+        ranks = np.zeros(nj, np.uint32)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hacs_b200.check(eng._lib.hme_batch_gemm_rank_u32_dev(eng._h, nj, a, ranks.ctypes.data_as(C_.POINTER(C_.c_uint32))))
+        return time.perf_counter() - t0, ranks
+
+    batched(n_jobs, arr)  # warm: workspace growth, module load
+    eng.gen_jobs_dev(specs)
+    t_all, ranks = batched(n_jobs, arr)
+    out = {"workload": f"{n_jobs} jobs GEMM + rank mod p in {{65521, 2^31-19}}, sides log-uniform 16..1024 (config 4)",
+           "jobs_per_s": n_jobs / t_all, "s": t_all, "modmac_gemm": float((s.astype(np.float64) ** 3).sum())}
+    eng.gen_jobs_dev(specs)
+    sub = eng._jobs(jobs[:sample])
+    t_b, r_b = batched(sample, sub)
+    out["sample_jobs"] = sample
+    out["sample_batched_jobs_per_s"] = sample / t_b
+    if plain is not None:
+        eng.gen_jobs_dev(specs[: 2 * sample])
+        eng.use_torch_stream()
+        st = torch.cuda.current_stream().cuda_stream
+        r2 = np.zeros(sample, np.uint32)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for j in range(sample):
+            jb = jobs[j]
+            n = jb["C"].shape[0]
+            if plain.plain_gemm_u32_dev(jb["p"], n, n, n, jb["A"].data_ptr(), n, jb["B"].data_ptr(), n,
+                                        jb["C"].data_ptr(), n, 0, st) != 0:
+                raise RuntimeError(plain.plain_last_error().decode())
+            rr = np.zeros(1, np.uint32)
+            hacs_b200.check(eng._lib.hme_batch_rank_u32_dev(eng._h, 1, eng._jobs([jb]),
+                                                            rr.ctypes.data_as(C_.POINTER(C_.c_uint32))))
+            r2[j] = rr[0]
+        t_p = time.perf_counter() - t0
+        out["sample_plain_dispatch_jobs_per_s"] = sample / t_p
+        out["speedup_vs_plain_dispatch"] = t_p / t_b
+        out["ranks_equal"] = bool((r2 == r_b).all() and (r_b == ranks[:sample]).all())
+    return out
+
+
 def run_case(args):
     """One kernel configuration for an ncu capture (prints a short JSON, not a bench line)."""
     import torch
@@ -443,6 +566,10 @@ def main():
         ext = {}
         for pp in (65521, 2147483629):
             ext[f"gemm_8192_p{pp}"] = big_gemm(eng, plain, pp, 8192)
+        eng.use_own_stream()
+        ext["rref_config2"] = extra_rref(eng)
+        ext.update(extra_ring(eng))
+        ext["jobstream_config4"] = extra_jobstream(eng, plain)
         line["extras"] = ext
     if rank == 0:
         print(json.dumps(line), flush=True)

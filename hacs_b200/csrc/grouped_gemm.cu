@@ -27,9 +27,13 @@ namespace {
 
 using namespace limb;
 
+// Problems with the same padded K share one stacked plane tensor per operand
+// (their rows / columns at offsets a_row0 / b_col0); tiles that run past a
+// problem's rows or columns read a neighbour's planes, which only reach
+// accumulator rows and columns the epilogue does not store.
 struct GroupedProblem {
-    const CUtensorMap* tmA;  // limb planes of A_j: dims {Kp, M, L}
-    const CUtensorMap* tmB;  // limb planes of 256^i B_j: dims {Kp, N, L, L}
+    const CUtensorMap* tmA;  // stacked limb planes of the A operands: dims {Kp, rows, L}
+    const CUtensorMap* tmB;  // stacked limb planes of 256^i B: dims {Kp, cols, L, L}
     uint32_t* C;
     uint64_t ldc;
     int M, N;
@@ -37,7 +41,7 @@ struct GroupedProblem {
     int op;
     int tiles_n;
     int tile_begin;
-    int pad[2];
+    int a_row0, b_col0;
 };
 
 __device__ __forceinline__ int find_problem(const GroupedProblem* __restrict__ probs, int nprob, int tile) {
@@ -117,8 +121,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                             break;
                         }
                         mbar_arrive_expect_tx(&full[s], CF::STAGE_BYTES);
-                        tma_load_3d(sA + s * CF::A_BYTES, P.tmA, &full[s], kb * kBK, tm * kBM, i);
-                        tma_load_4d(sB + s * CF::B_BYTES, P.tmB, &full[s], kb * kBK, tn * BN, 0, i);
+                        tma_load_3d(sA + s * CF::A_BYTES, P.tmA, &full[s], kb * kBK, P.a_row0 + tm * kBM, i);
+                        tma_load_4d(sB + s * CF::B_BYTES, P.tmB, &full[s], kb * kBK, P.b_col0 + tn * BN, 0, i);
                     }
                 }
             }
@@ -198,15 +202,24 @@ __global__ void __launch_bounds__(kThreads, 1)
                 __syncwarp();
                 const int col = tn * BN + c0 + col_in;
                 if (col < P.N) {
-#pragma unroll 4
-                    for (int rr = half; rr < 32; rr += 2) {
-                        const int row = row0 + rr;
-                        if (row >= P.M) break;
-                        uint32_t* dst = P.C + static_cast<size_t>(row) * P.ldc + col;
+                    // all 16 rows' C values in flight at once, then combine and store
+                    const int rlim = min(32, P.M - row0);
+                    uint32_t old[16];
+                    if (P.op != HME_SET) {
+#pragma unroll
+                        for (int t = 0; t < 16; ++t) {
+                            const int rr = half + 2 * t;
+                            old[t] = rr < rlim ? P.C[static_cast<size_t>(row0 + rr) * P.ldc + col] : 0u;
+                        }
+                    }
+#pragma unroll
+                    for (int t = 0; t < 16; ++t) {
+                        const int rr = half + 2 * t;
+                        if (rr >= rlim) break;
                         uint32_t o = stage[rr][col_in];
-                        if (P.op == HME_ADD) o = mod_add(*dst, o, p);
-                        else if (P.op == HME_SUB) o = mod_sub(*dst, o, p);
-                        *dst = o;
+                        if (P.op == HME_ADD) o = mod_add(old[t], o, p);
+                        else if (P.op == HME_SUB) o = mod_sub(old[t], o, p);
+                        P.C[static_cast<size_t>(row0 + rr) * P.ldc + col] = o;
                     }
                 }
                 __syncwarp();
@@ -283,18 +296,45 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
     const bool narrow = tiles_wide < static_cast<size_t>(ctx->num_sms);
     const int BN = narrow ? BNn : BNw;
 
-    // plane layout and split table
-    std::vector<GroupedSplitJob> split(nj);
-    std::vector<size_t> offA(nj), offB(nj);
+    // plane layout: problems bucketed by padded K; per bucket one stacked tensor
+    // for the A planes (rows of all problems) and one for the B planes
+    std::vector<int> kp_of(nj), bucket_of(nj);
+    std::vector<int> bucket_kp;
+    for (int t = 0; t < nj; ++t) {
+        kp_of[t] = static_cast<int>((jobs[t].K + kBK - 1) / kBK * kBK);
+        auto it = std::find(bucket_kp.begin(), bucket_kp.end(), kp_of[t]);
+        if (it == bucket_kp.end()) {
+            bucket_of[t] = static_cast<int>(bucket_kp.size());
+            bucket_kp.push_back(kp_of[t]);
+        } else {
+            bucket_of[t] = static_cast<int>(it - bucket_kp.begin());
+        }
+    }
+    const int nb = static_cast<int>(bucket_kp.size());
+    std::vector<size_t> b_rows(nb, 0), b_cols(nb, 0);
+    std::vector<int> row0(nj), col0(nj);
+    for (int t = 0; t < nj; ++t) {
+        row0[t] = static_cast<int>(b_rows[bucket_of[t]]);
+        col0[t] = static_cast<int>(b_cols[bucket_of[t]]);
+        b_rows[bucket_of[t]] += jobs[t].M;
+        b_cols[bucket_of[t]] += jobs[t].N;
+    }
+    std::vector<size_t> offA(nb), offB(nb);
     size_t bytes = 0;
+    for (int b = 0; b < nb; ++b) {
+        offA[b] = bytes;
+        bytes += align256(static_cast<size_t>(L) * b_rows[b] * bucket_kp[b]);
+        offB[b] = bytes;
+        bytes += align256(static_cast<size_t>(L) * L * b_cols[b] * bucket_kp[b]);
+    }
+    HME_REQUIRE(static_cast<double>(bytes) < 1.0e11, "grouped gemm: plane tensors too large");
+    uint8_t* planes = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs0, bytes));
+    std::vector<GroupedSplitJob> split(nj);
     int blocks = 0;
     for (int t = 0; t < nj; ++t) {
         const GemmJob& j = jobs[t];
-        const int Kp = static_cast<int>((j.K + kBK - 1) / kBK * kBK);
-        offA[t] = bytes;
-        bytes += align256(static_cast<size_t>(L) * j.M * Kp);
-        offB[t] = bytes;
-        bytes += align256(static_cast<size_t>(L) * L * j.N * Kp);
+        const int b = bucket_of[t];
+        const int Kp = kp_of[t];
         SplitArgs& s = split[t].s;
         s = SplitArgs{};
         s.A = j.A;
@@ -307,6 +347,10 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
         s.Kp = Kp;
         s.p = mp.p;
         s.barrett = mp.barrett;
+        s.planesA = planes + offA[b] + static_cast<size_t>(row0[t]) * Kp;
+        s.planesB = planes + offB[b] + static_cast<size_t>(col0[t]) * Kp;
+        s.a_plane = static_cast<uint64_t>(b_rows[b]) * Kp;
+        s.b_plane = static_cast<uint64_t>(b_cols[b]) * Kp;
         const size_t work = static_cast<size_t>(j.M) * (Kp / 16);
         s.a_blocks = static_cast<int>(std::max<size_t>(1, std::min<size_t>((work + 255) / 256, 64)));
         s.b_blocks_k = (Kp + 63) / 64;
@@ -315,13 +359,8 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
         split[t].block_begin = blocks;
         blocks += s.a_blocks + split[t].b_blocks;
     }
-    uint8_t* planes = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs0, bytes));
-    for (int t = 0; t < nj; ++t) {
-        split[t].s.planesA = planes + offA[t];
-        split[t].s.planesB = planes + offB[t];
-    }
-    // tensor maps (64-byte aligned objects) and the problem table, one upload each
-    const size_t maps_bytes = sizeof(CUtensorMap) * 2 * static_cast<size_t>(nj);
+    // tensor maps (64-byte aligned objects, two per bucket) and the problem table
+    const size_t maps_bytes = sizeof(CUtensorMap) * 2 * static_cast<size_t>(nb);
     const size_t probs_bytes = sizeof(GroupedProblem) * static_cast<size_t>(nj);
     const size_t split_bytes = sizeof(GroupedSplitJob) * static_cast<size_t>(nj);
     uint8_t* tables = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs1, align256(maps_bytes) + align256(probs_bytes) +
@@ -329,37 +368,39 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
     CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(tables);
     GroupedProblem* d_probs = reinterpret_cast<GroupedProblem*>(tables + align256(maps_bytes));
     GroupedSplitJob* d_split = reinterpret_cast<GroupedSplitJob*>(tables + align256(maps_bytes) + align256(probs_bytes));
-    std::vector<CUtensorMap> maps(2 * static_cast<size_t>(nj));
+    std::vector<CUtensorMap> maps(2 * static_cast<size_t>(nb));
+    for (int b = 0; b < nb; ++b) {
+        const cuuint64_t Kp = static_cast<cuuint64_t>(bucket_kp[b]);
+        {
+            const cuuint64_t dims[3] = {Kp, b_rows[b], static_cast<cuuint64_t>(L)};
+            const cuuint64_t strides[2] = {Kp, Kp * b_rows[b]};
+            const cuuint32_t box[3] = {kBK, kBM, 1};
+            encode_tma_u8(&maps[2 * b], planes + offA[b], 3, dims, strides, box);
+        }
+        {
+            const cuuint64_t dims[4] = {Kp, b_cols[b], static_cast<cuuint64_t>(L), static_cast<cuuint64_t>(L)};
+            const cuuint64_t strides[3] = {Kp, Kp * b_cols[b], Kp * b_cols[b] * L};
+            const cuuint32_t box[4] = {kBK, static_cast<cuuint32_t>(BN), static_cast<cuuint32_t>(L), 1};
+            encode_tma_u8(&maps[2 * b + 1], planes + offB[b], 4, dims, strides, box);
+        }
+    }
     std::vector<GroupedProblem> probs(nj);
     int tiles = 0;
     for (int t = 0; t < nj; ++t) {
         const GemmJob& j = jobs[t];
-        const int Kp = split[t].s.Kp;
-        {
-            const cuuint64_t dims[3] = {static_cast<cuuint64_t>(Kp), j.M, static_cast<cuuint64_t>(L)};
-            const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * j.M};
-            const cuuint32_t box[3] = {kBK, kBM, 1};
-            encode_tma_u8(&maps[2 * t], split[t].s.planesA, 3, dims, strides, box);
-        }
-        {
-            const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), j.N, static_cast<cuuint64_t>(L),
-                                        static_cast<cuuint64_t>(L)};
-            const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * j.N,
-                                           static_cast<cuuint64_t>(Kp) * j.N * L};
-            const cuuint32_t box[4] = {kBK, static_cast<cuuint32_t>(BN), static_cast<cuuint32_t>(L), 1};
-            encode_tma_u8(&maps[2 * t + 1], split[t].s.planesB, 4, dims, strides, box);
-        }
         GroupedProblem& P = probs[t];
-        P.tmA = d_maps + 2 * t;
-        P.tmB = d_maps + 2 * t + 1;
+        P.tmA = d_maps + 2 * bucket_of[t];
+        P.tmB = d_maps + 2 * bucket_of[t] + 1;
         P.C = j.C;
         P.ldc = j.ldc;
         P.M = static_cast<int>(j.M);
         P.N = static_cast<int>(j.N);
-        P.kblocks = Kp / kBK;
+        P.kblocks = kp_of[t] / kBK;
         P.op = j.op;
         P.tiles_n = static_cast<int>((j.N + BN - 1) / BN);
         P.tile_begin = tiles;
+        P.a_row0 = row0[t];
+        P.b_col0 = col0[t];
         tiles += static_cast<int>((j.M + kBM - 1) / kBM) * P.tiles_n;
     }
     HME_CUDA(cudaMemcpyAsync(d_maps, maps.data(), maps_bytes, cudaMemcpyHostToDevice, ctx->stream));

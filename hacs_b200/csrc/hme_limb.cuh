@@ -53,13 +53,15 @@ struct SplitArgs {
     int a_blocks;        // blocks of the A part
     int b_blocks_k;      // B part: blocks along k (64 k each)
     bool a_vec;          // A rows 16-byte aligned: vector loads
+    uint64_t a_plane;    // bytes between A limb planes (0: M * Kp)
+    uint64_t b_plane;    // bytes between B limb planes (0: N * Kp)
 };
 
 template <int L>
 __device__ __forceinline__ void split_a_part(const SplitArgs& s, int block) {
     const int kch = s.Kp >> 4;
     const size_t total = static_cast<size_t>(s.M) * kch;
-    const size_t plane = static_cast<size_t>(s.M) * s.Kp;
+    const size_t plane = s.a_plane ? s.a_plane : static_cast<size_t>(s.M) * s.Kp;
     for (size_t idx = static_cast<size_t>(block) * blockDim.x + threadIdx.x; idx < total;
          idx += static_cast<size_t>(s.a_blocks) * blockDim.x) {
         const int row = static_cast<int>(idx / kch);
@@ -114,7 +116,7 @@ __device__ __forceinline__ void split_b_part(const SplitArgs& s, int block, uint
             for (int j = 0; j < L; ++j) out[i][j][e >> 2] |= ((v >> (8 * j)) & 0xffu) << (8 * (e & 3));
         }
     }
-    const size_t plane = static_cast<size_t>(s.N) * s.Kp;
+    const size_t plane = s.b_plane ? s.b_plane : static_cast<size_t>(s.N) * s.Kp;
 #pragma unroll
     for (int i = 0; i < L; ++i)
 #pragma unroll

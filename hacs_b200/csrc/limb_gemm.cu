@@ -229,15 +229,24 @@ __global__ void __launch_bounds__(kThreads, 1)
                 __syncwarp();
                 const int col = tn * BN + c0 + col_in;
                 if (col < g.N) {
-#pragma unroll 4
-                    for (int rr = half; rr < 32; rr += 2) {
-                        const int row = row0 + rr;
-                        if (row >= g.M) break;
-                        uint32_t* dst = g.C + static_cast<size_t>(row) * g.ldc + col;
+                    // all 16 rows' C values in flight at once, then combine and store
+                    const int rlim = min(32, g.M - row0);
+                    uint32_t old[16];
+                    if (g.op != HME_SET) {
+#pragma unroll
+                        for (int t = 0; t < 16; ++t) {
+                            const int rr = half + 2 * t;
+                            old[t] = rr < rlim ? g.C[static_cast<size_t>(row0 + rr) * g.ldc + col] : 0u;
+                        }
+                    }
+#pragma unroll
+                    for (int t = 0; t < 16; ++t) {
+                        const int rr = half + 2 * t;
+                        if (rr >= rlim) break;
                         uint32_t o = stage[rr][col_in];
-                        if (g.op == HME_ADD) o = mod_add(*dst, o, g.p);
-                        else if (g.op == HME_SUB) o = mod_sub(*dst, o, g.p);
-                        *dst = o;
+                        if (g.op == HME_ADD) o = mod_add(old[t], o, g.p);
+                        else if (g.op == HME_SUB) o = mod_sub(old[t], o, g.p);
+                        g.C[static_cast<size_t>(row0 + rr) * g.ldc + col] = o;
                     }
                 }
                 __syncwarp();
