@@ -77,6 +77,23 @@ PROTOTYPES.update({
     "hme_batch_rank_u32_dev": (C.c_int, [vp, u32, C.POINTER(HmeJob), u32p]),
     "hme_batch_gemm_rank_u32_dev": (C.c_int, [vp, u32, C.POINTER(HmeJob), u32p]),
     "hme_gen_jobs_u32_dev": (C.c_int, [vp, u32, C.POINTER(HmeGenSpec)]),
+    "hme_gemm_variant_count": (C.c_int, []),
+    "hme_gemm_u32_dev_variant": (C.c_int, [vp, C.c_int, u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int]),
+    "hme_ctx_set_gemm_variant": (C.c_int, [vp, C.c_int]),
+    "hme_ctx_set_sched_policy": (C.c_int, [vp, C.c_int]),
+    "hme_autotune_gemm": (C.c_int, [vp, u32, u32, u32, u32, C.c_int, C.POINTER(C.c_float)]),
+    "hme_mlp_param_count": (C.c_int, []),
+    "hme_mlp_create": (C.c_int, [vp, C.c_uint64, C.POINTER(vp)]),
+    "hme_mlp_destroy": (C.c_int, [vp]),
+    "hme_mlp_get_params": (C.c_int, [vp, C.POINTER(C.c_float)]),
+    "hme_mlp_set_params": (C.c_int, [vp, C.POINTER(C.c_float)]),
+    "hme_mlp_loss_grad": (C.c_int, [vp, u32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float)]),
+    "hme_mlp_train": (C.c_int, [vp, u32, C.POINTER(C.c_float), C.POINTER(C.c_float), u32, u32, C.c_float,
+                                C.c_uint64, C.POINTER(C.c_float)]),
+    "hme_mlp_predict_bf16": (C.c_int, [vp, u32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "hme_sched_plan": (C.c_int, [vp, vp, u32, u32p, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                 C.POINTER(C.c_int)]),
 })
 
 _lib = None

@@ -126,6 +126,7 @@ int hme_ctx_destroy(hme_ctx* ctx) {
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
         ctx->ws.release();
+        sched_release(ctx);
         ctx->timer.clear();
         for (cudaEvent_t e : ctx->timer.pool) cudaEventDestroy(e);
         if (ctx->d_err) cudaFree(ctx->d_err);

@@ -116,6 +116,9 @@ struct hme_ctx {
     hme::Workspace ws;
     hme::KernelTimer timer;
     hme::ElimOptions elim;
+    int fixed_variant = -1;          // >= 0: every GEMM of this context uses that variant
+    int sched_policy = 0;            // 0 shape heuristic, 1 learned planner table
+    void* sched_table = nullptr;     // planner decisions by shape class (sched.cu)
 };
 
 // Bracket one kernel launch with timing events when the context's timer is on.
@@ -160,9 +163,27 @@ inline int guard(F&& f) {
 // Deterministic primality for 32-bit moduli (Miller-Rabin, bases 2, 7, 61).
 bool is_prime_u32(uint32_t p);
 
-// ---- the limb GEMM (limb_gemm.cu) ------------------------------------------
-// C op= A*B mod p with device pointers, on ctx->stream.
+// ---- the GEMM variants (limb_gemm.cu, simt_gemm.cu) -----------------------
+// The schedules of one product; every variant computes the same residues.
+enum GemmVariant : int {
+    kVariantWide = 0,    // INT8-limb tcgen05 GEMM, wide tiles (L*BN ~ 256)
+    kVariantNarrow = 1,  // INT8-limb tcgen05 GEMM, half-width tiles (twice the tiles)
+    kVariantSimt32 = 2,  // CUDA-core GEMM, 32 x 32 tiles, one launch
+    kVariantSimt64 = 3,  // CUDA-core GEMM, 64 x 64 tiles, one launch
+    kGemmVariants = 4,
+};
+// C op= A*B mod p with device pointers, on ctx->stream; the variant comes from
+// the context's scheduler (sched.cu) unless a fixed variant is set.
 void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
                      size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op);
+void gemm_u32_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
+                      size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int variant);
+void simt_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
+                          size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int tile);
+// The shape heuristic (the method without a learned model).
+int gemm_default_variant(const hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n);
+// The scheduler's choice for one product (sched.cu), and its tear-down.
+int sched_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k);
+void sched_release(hme_ctx* ctx);
 
 }  // namespace hme

@@ -361,9 +361,27 @@ void encode_tma_u8(CUtensorMap* map, void* base, int rank, const cuuint64_t* dim
     encode_u8(map, base, rank, dims, strides, box);
 }
 
+int gemm_default_variant(const hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n) {
+    // Wide tiles (L*BN = 256 columns of TMEM per accumulator) unless that leaves
+    // SMs idle; then half-width tiles, which double the tile count.
+    const uint32_t L = mp.limbs;
+    const uint32_t tiles_m = (m + kBM - 1) / kBM;
+    const uint32_t bn = 256 / L > 64 ? 256 / L : 64;
+    const size_t tiles = static_cast<size_t>(tiles_m) * ((n + bn - 1) / bn);
+    return 4 * tiles < 3 * static_cast<size_t>(ctx->num_sms) ? kVariantNarrow : kVariantWide;
+}
+
 void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
                      size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op) {
+    int v = ctx->fixed_variant;
+    if (v < 0) v = sched_variant(ctx, mp, m, n, k);
+    gemm_u32_variant(ctx, mp, m, n, k, A, lda, B, ldb, C, ldc, op, v);
+}
+
+void gemm_u32_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
+                      size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int variant) {
     HME_REQUIRE(op == HME_SET || op == HME_ADD || op == HME_SUB, "gemm: op must be HME_SET, HME_ADD or HME_SUB");
+    HME_REQUIRE(variant >= 0 && variant < kGemmVariants, "gemm: unknown variant");
     HME_REQUIRE(mp.p >= 2, "gemm: modulus must be >= 2");
     HME_REQUIRE(m < (1u << 30) && n < (1u << 30) && k < (1u << 30), "gemm: dimension too large");
     if (m == 0 || n == 0) return;
@@ -379,6 +397,10 @@ void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, 
     }
     HME_REQUIRE(A && B && C, "gemm: null pointer");
     HME_REQUIRE(lda >= k && ldb >= n, "gemm: leading dimension too small");
+    if (variant == kVariantSimt32 || variant == kVariantSimt64) {
+        simt_gemm_u32_device(ctx, mp, m, n, k, A, lda, B, ldb, C, ldc, op, variant == kVariantSimt32 ? 32 : 64);
+        return;
+    }
     const int L = static_cast<int>(mp.limbs);
     // K padded to whole 128-byte k-blocks (the split kernel writes the pad as
     // zeros), so no TMA box ever reaches past the planes' K extent
@@ -405,11 +427,7 @@ void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, 
         }
         HME_CUDA(cudaGetLastError());
     }
-    // Wide tiles (L*BN = 256 columns of TMEM per accumulator) unless that leaves
-    // SMs idle; then half-width tiles, which double the tile count.
-    const uint32_t tiles_m = (m + kBM - 1) / kBM;
-    auto tiles_for = [&](uint32_t bn) { return static_cast<size_t>(tiles_m) * ((n + bn - 1) / bn); };
-    const bool narrow = 4 * tiles_for(256 / L > 64 ? 256 / L : 64) < 3 * static_cast<size_t>(ctx->num_sms);
+    const bool narrow = variant == kVariantNarrow;
     switch (L) {
         case 1: if (narrow) launch_gemm<1, 128>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op);
                 else launch_gemm<1, 256>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;

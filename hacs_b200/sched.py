@@ -1,0 +1,199 @@
+"""The learned scheduler's host side: features, the MLP handle, timing
+collection with the exhaustive autotuner, training, planning and regret.
+
+A schedule is a GEMM variant (hme_gemm_u32_dev_variant: 0 limb tcgen05 wide
+tiles, 1 limb tcgen05 half-width tiles, 2 CUDA-core 32 x 32, 3 CUDA-core
+64 x 64).  Every variant computes the same residues, so neither the MLP nor
+the autotuner can change a value -- only the time.  The MLP (5 -> 3 x 64 -> 4,
+hand-written CUDA kernels: FP32 training, BF16 inference) predicts each
+variant's normalised log-time from (log2 m, log2 n, log2 k, log2 p, density);
+the exhaustive autotuner (hme_autotune_gemm) times all variants, supplies the
+training data, and judges the MLP's regret.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+WEIGHTS = os.path.join(DATA, "sched_mlp.npz")
+TIMINGS = os.path.join(DATA, "sched_timings.npz")
+N_VARIANTS = 4
+VARIANT_NAMES = ("tensor-wide", "tensor-narrow", "simt-32", "simt-64")
+
+_fp = C.POINTER(C.c_float)
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def raw_features(p, m, n, k, density) -> np.ndarray:
+    p, m, n, k, d = (np.asarray(x, dtype=np.float64) for x in (p, m, n, k, density))
+    return np.stack([np.log2(m), np.log2(n), np.log2(k), np.log2(p), d], axis=-1)
+
+
+class MLP:
+    """One scheduler network on an Engine's device (libhme hme_mlp)."""
+
+    def __init__(self, engine, seed: int = 1):
+        self._lib = _lib.lib()
+        self.engine = engine
+        h = C.c_void_p()
+        check(self._lib.hme_mlp_create(engine._h, seed, C.byref(h)))
+        self._h = h
+        self.n_params = int(self._lib.hme_mlp_param_count())
+        self.x_mean = np.zeros(5, np.float32)
+        self.x_std = np.ones(5, np.float32)
+        self.y_mean = 0.0
+        self.y_std = 1.0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hme_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- parameters --------------------------------------------------------------
+    def get_params(self) -> np.ndarray:
+        w = np.zeros(self.n_params, np.float32)
+        check(self._lib.hme_mlp_get_params(self._h, w.ctypes.data_as(_fp)))
+        return w
+
+    def set_params(self, w) -> None:
+        w = _f32(w)
+        assert w.size == self.n_params
+        check(self._lib.hme_mlp_set_params(self._h, w.ctypes.data_as(_fp)))
+
+    def save(self, path: str = WEIGHTS) -> None:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        np.savez(path, params=self.get_params(), x_mean=self.x_mean, x_std=self.x_std,
+                 y_mean=np.float32(self.y_mean), y_std=np.float32(self.y_std))
+
+    def load(self, path: str = WEIGHTS) -> None:
+        d = np.load(path)
+        self.set_params(d["params"])
+        self.x_mean, self.x_std = d["x_mean"].astype(np.float32), d["x_std"].astype(np.float32)
+        self.y_mean, self.y_std = float(d["y_mean"]), float(d["y_std"])
+
+    # ---- raw kernels on normalised data ------------------------------------------------
+    def loss_grad(self, X, Y):
+        X, Y = _f32(X), _f32(Y)
+        loss = C.c_float()
+        g = np.zeros(self.n_params, np.float32)
+        check(self._lib.hme_mlp_loss_grad(self._h, X.shape[0], X.ctypes.data_as(_fp), Y.ctypes.data_as(_fp),
+                                          C.byref(loss), g.ctypes.data_as(_fp)))
+        return loss.value, g
+
+    def train_normalised(self, X, Y, epochs=200, batch=256, lr=2e-3, seed=7) -> float:
+        X, Y = _f32(X), _f32(Y)
+        loss = C.c_float()
+        check(self._lib.hme_mlp_train(self._h, X.shape[0], X.ctypes.data_as(_fp), Y.ctypes.data_as(_fp), epochs,
+                                      batch, lr, seed, C.byref(loss)))
+        return loss.value
+
+    def predict_normalised(self, X) -> np.ndarray:
+        X = _f32(X)
+        Y = np.zeros((X.shape[0], N_VARIANTS), np.float32)
+        check(self._lib.hme_mlp_predict_bf16(self._h, X.shape[0], X.ctypes.data_as(_fp), Y.ctypes.data_as(_fp)))
+        return Y
+
+    # ---- on raw features / measured times ------------------------------------------------
+    def fit(self, F, T, **kw) -> float:
+        """Train on raw features F (n x 5) and measured times T (n x 4, ms)."""
+        F = np.asarray(F, np.float64)
+        self.x_mean = F.mean(0).astype(np.float32)
+        self.x_std = np.maximum(F.std(0), 1e-3).astype(np.float32)
+        L = np.log(np.maximum(np.asarray(T, np.float64), 1e-6))
+        self.y_mean, self.y_std = float(L.mean()), float(max(L.std(), 1e-3))
+        return self.train_normalised((F - self.x_mean) / self.x_std, (L - self.y_mean) / self.y_std, **kw)
+
+    def choose(self, F) -> np.ndarray:
+        F = np.asarray(F, np.float64)
+        return np.argmin(self.predict_normalised((F - self.x_mean) / self.x_std), axis=1)
+
+    def norm(self) -> np.ndarray:
+        return np.concatenate([self.x_mean, self.x_std]).astype(np.float32)
+
+    def plan(self, shapes, density=None) -> np.ndarray:
+        """hme_sched_plan: BF16 inference + arg-min for rows (p, m, n, k); records the
+        decisions in the engine's learned plan (policy 1)."""
+        S = np.ascontiguousarray(shapes, dtype=np.uint32)
+        n = S.shape[0]
+        d = _f32(np.ones(n) if density is None else density)
+        v = np.zeros(max(1, n), np.int32)
+        nm = self.norm()
+        check(self._lib.hme_sched_plan(self.engine._h, self._h, n, S.ctypes.data_as(_lib.u32p),
+                                       d.ctypes.data_as(_fp), nm.ctypes.data_as(_fp),
+                                       v.ctypes.data_as(C.POINTER(C.c_int))))
+        return v[:n]
+
+
+def heuristic_choice(F, num_sms: int = 148) -> np.ndarray:
+    """The method without the MLP: always the tensor-core GEMM, wide tiles unless
+    fewer than 3/4 of the SMs would get one (the engine's shape heuristic)."""
+    F = np.asarray(F, np.float64)
+    m, n, p = 2.0 ** F[:, 0], 2.0 ** F[:, 1], 2.0 ** F[:, 3]
+    L = np.where(p <= 256, 1, np.where(p <= 65536, 2, np.where(p <= 2 ** 24, 3, 4)))
+    bn = np.maximum(256 // L, 64)
+    tiles = np.ceil(m / 128) * np.ceil(n / bn)
+    return np.where(4 * tiles < 3 * num_sms, 1, 0)
+
+
+def regret(T, choice) -> float:
+    """Mean relative excess time of the chosen variants over the best measured ones."""
+    T = np.asarray(T, np.float64)
+    best = T.min(1)
+    got = T[np.arange(T.shape[0]), np.asarray(choice)]
+    return float(np.mean((got - best) / best))
+
+
+def sample_shapes(n: int, seed: int = 11):
+    """Seeded GEMM shapes drawn from the configurations' mix: config-4 jobs
+    (squares 16..1024, both moduli, dense or banded), config-2/3 trailing
+    updates (m, n 64..2048, k in {32, 64, 128}, p = 2^31 - 19, 2^16, 3^10) and
+    config-1 products (128..2048 cubes at 65521).  Rows (p, m, n, k), density."""
+    rng = np.random.default_rng(seed)
+    kind = rng.integers(0, 3, n)
+    P = np.zeros(n, np.int64)
+    S = np.zeros((n, 3), np.int64)
+    dens = np.ones(n)
+    for i in range(n):
+        if kind[i] == 0:
+            s = int(np.rint(16 * 64 ** rng.random()))
+            P[i] = (65521, 2147483629)[rng.integers(0, 2)]
+            S[i] = (s, s, s)
+            dens[i] = (1.0, 0.05)[rng.integers(0, 2)]
+        elif kind[i] == 1:
+            P[i] = (2147483629, 65536, 59049)[rng.integers(0, 3)]
+            S[i] = (int(64 * 32 ** rng.random()), int(64 * 32 ** rng.random()), (32, 64, 128)[rng.integers(0, 3)])
+        else:
+            s = int(128 * 16 ** rng.random())
+            P[i] = 65521
+            S[i] = (s, s, s)
+    return np.column_stack([P, S]).astype(np.uint32), dens
+
+
+def autotune(engine, p, m, n, k, reps: int = 3) -> np.ndarray:
+    ms = np.zeros(N_VARIANTS, np.float32)
+    check(_lib.lib().hme_autotune_gemm(engine._h, int(p), int(m), int(n), int(k), reps, ms.ctypes.data_as(_fp)))
+    return ms
+
+
+def collect(engine, n: int, seed: int = 11, reps: int = 3):
+    """Time every variant on n seeded shapes: (shapes, density, times ms)."""
+    shapes, dens = sample_shapes(n, seed)
+    T = np.zeros((n, N_VARIANTS), np.float32)
+    for i, (p, m, nn, k) in enumerate(shapes):
+        T[i] = autotune(engine, p, m, nn, k, reps)
+    return shapes, dens, T

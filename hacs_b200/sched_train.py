@@ -1,0 +1,63 @@
+"""Collect autotuner timings on this GPU and train the scheduler MLP.
+
+    python -m hacs_b200.sched_train [--shapes 20000] [--reps 3] [--epochs 300]
+
+Times every GEMM variant on `--shapes` seeded shapes from the configurations'
+mix with the exhaustive autotuner (hme_autotune_gemm), trains the MLP on the
+GPU (hme_mlp_train: the library's FP32 forward / backward / Adam kernels) on
+80 % of them, reports the BF16-inference regret against the autotuner's best on
+the other 20 % next to the shape heuristic's, and writes
+hacs_b200/data/sched_timings.npz and hacs_b200/data/sched_mlp.npz.
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+import hacs_b200  # noqa: E402
+from hacs_b200 import sched  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--shapes", type=int, default=20000)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--reuse", action="store_true", help="train on the existing timing file")
+    args = ap.parse_args()
+    eng = hacs_b200.Engine(0)
+    if args.reuse and os.path.exists(sched.TIMINGS):
+        d = np.load(sched.TIMINGS)
+        shapes, dens, T = d["shapes"], d["density"], d["ms"]
+    else:
+        t0 = time.time()
+        shapes, dens, T = sched.collect(eng, args.shapes, args.seed, args.reps)
+        print(f"timed {len(shapes)} shapes x {sched.N_VARIANTS} variants in {time.time() - t0:.1f} s", flush=True)
+        os.makedirs(sched.DATA, exist_ok=True)
+        np.savez_compressed(sched.TIMINGS, shapes=shapes, density=dens, ms=T)
+    F = sched.raw_features(shapes[:, 0], shapes[:, 1], shapes[:, 2], shapes[:, 3], dens)
+    n = len(F)
+    cut = int(0.8 * n)
+    mlp = sched.MLP(eng, seed=5)
+    t0 = time.time()
+    loss = mlp.fit(F[:cut], T[:cut], epochs=args.epochs, batch=256, lr=2e-3)
+    tt = time.time() - t0
+    mlp.save(sched.WEIGHTS)
+    ch = mlp.choose(F[cut:])
+    rep = {"train_shapes": cut, "test_shapes": n - cut, "train_loss": loss, "train_s": tt,
+           "regret_mlp": sched.regret(T[cut:], ch),
+           "regret_heuristic": sched.regret(T[cut:], sched.heuristic_choice(F[cut:])),
+           "regret_always_wide": sched.regret(T[cut:], np.zeros(n - cut, int)),
+           "variant_share_best": np.bincount(T[cut:].argmin(1), minlength=4).tolist(),
+           "variant_share_mlp": np.bincount(ch, minlength=4).tolist()}
+    print(json.dumps(rep), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -207,6 +207,47 @@ HME_API int hme_batch_rank_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *
 HME_API int hme_batch_gemm_rank_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, uint32_t *ranks);
 HME_API int hme_gen_jobs_u32_dev(hme_ctx *ctx, uint32_t nmat, const hme_gen_spec *specs);
 
+/* ---- scheduler: GEMM variants, exhaustive autotuner, learned MLP planner -------
+ * Variants (every one computes the same residues; a schedule changes speed
+ * only): 0 limb tcgen05 GEMM with wide tiles, 1 with half-width tiles, 2 the
+ * CUDA-core GEMM with 32 x 32 tiles, 3 with 64 x 64 tiles.  The reference has
+ * no autotuner and no learned scheduler (its static rules:
+ * src/Engine/EngineCostModel.h:22-51, pick_tile src/Cuda/cuda_kernels.cu:354-359).
+ * hme_gemm_u32_dev_variant: the GEMM with an explicit variant.
+ * hme_ctx_set_gemm_variant: pin every GEMM of the context to one variant
+ *   (-1 = the scheduler decides).
+ * hme_ctx_set_sched_policy: 0 the shape heuristic, 1 the learned plan
+ *   (decisions recorded by hme_sched_plan, heuristic for unplanned shapes).
+ * hme_autotune_gemm: the exhaustive autotuner: the median device time (ms) of
+ *   each variant on an m x k x n product mod p into ms[hme_gemm_variant_count()].
+ * hme_mlp_*: the scheduler's MLP, 5 -> 64 -> 64 -> 64 -> 4, ReLU, trained on
+ *   the GPU (FP32 forward + backward of the mean squared error, Adam) and run
+ *   in BF16 for inference.  X rows are 5 normalised features, Y rows 4
+ *   normalised log-times.  hme_mlp_loss_grad returns the loss and its full
+ *   parameter gradient (for checks against a CPU reference).
+ * hme_sched_plan: BF16 inference for n products (shapes rows: p, m, n, k;
+ *   optional density), arg-min variant per product into variants[], recorded
+ *   in the context's plan; norm holds the 5 feature means then 5 std devs. */
+typedef struct hme_mlp hme_mlp;
+HME_API int hme_gemm_variant_count(void);
+HME_API int hme_gemm_u32_dev_variant(hme_ctx *ctx, int variant, uint32_t p, uint32_t m, uint32_t n, uint32_t k,
+                                     const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t *C,
+                                     size_t ldc, int op);
+HME_API int hme_ctx_set_gemm_variant(hme_ctx *ctx, int variant);
+HME_API int hme_ctx_set_sched_policy(hme_ctx *ctx, int policy);
+HME_API int hme_autotune_gemm(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, int reps, float *ms);
+HME_API int hme_mlp_param_count(void);
+HME_API int hme_mlp_create(hme_ctx *ctx, uint64_t seed, hme_mlp **out);
+HME_API int hme_mlp_destroy(hme_mlp *mlp);
+HME_API int hme_mlp_get_params(hme_mlp *mlp, float *params);
+HME_API int hme_mlp_set_params(hme_mlp *mlp, const float *params);
+HME_API int hme_mlp_loss_grad(hme_mlp *mlp, uint32_t n, const float *X, const float *Y, float *loss, float *grad);
+HME_API int hme_mlp_train(hme_mlp *mlp, uint32_t n, const float *X, const float *Y, uint32_t epochs, uint32_t batch,
+                          float lr, uint64_t seed, float *final_loss);
+HME_API int hme_mlp_predict_bf16(hme_mlp *mlp, uint32_t n, const float *X, float *Y);
+HME_API int hme_sched_plan(hme_ctx *ctx, hme_mlp *mlp, uint32_t n, const uint32_t *shapes, const float *density,
+                           const float *norm, int *variants);
+
 /* The GEMM above (same kernels, same result bits) for callers that cannot
  * allocate device memory when they call it -- a plugin inside another runtime
  * that owns the device-memory budget, or a latency-critical path where
