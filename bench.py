@@ -46,6 +46,15 @@ L2_FLUSH_BYTES = 256 << 20
 PEAK_FALLBACK_BF16_TFLOPS = 1590.0
 
 
+def _json(o):
+    """json default for numpy scalars and arrays."""
+    if hasattr(o, "item") and getattr(o, "ndim", 0) == 0:
+        return o.item()
+    if hasattr(o, "tolist"):
+        return o.tolist()
+    return str(o)
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -216,7 +225,7 @@ def run_reference(args):
                          "sample": f"{args.steps} x GEMM {n}^3 p={p} on {thr} host threads"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=_json), flush=True)
     return 0
 
 
@@ -410,6 +419,39 @@ def extra_jobstream(eng, plain, n_jobs=10000, sample=500):
     return out
 
 
+def extra_scheduler(eng, n_stream=50000, sample=2000):
+    """Config 5: the trained MLP (committed weights, trained on this engine's own
+    autotuner timings) plans a 50,000-job stream drawn from the configurations'
+    mix with one BF16 inference launch; on a sample, the chosen variants' device
+    times against the exhaustive autotuner's best (regret) and the heuristic."""
+    from hacs_b200 import sched
+
+    if not os.path.exists(sched.WEIGHTS):
+        return {"unavailable": "no trained weights in the package"}
+    mlp = sched.MLP(eng)
+    mlp.load()
+    shapes, dens = sched.sample_shapes(n_stream, seed=2027)
+    mlp.plan(shapes[:64], dens[:64])  # warm
+    t0 = time.perf_counter()
+    plan = mlp.plan(shapes, dens)
+    t_plan = time.perf_counter() - t0
+    T = np.stack([sched.autotune(eng, *shapes[i]) for i in range(sample)])
+    F = sched.raw_features(shapes[:sample, 0], shapes[:sample, 1], shapes[:sample, 2], shapes[:sample, 3],
+                           dens[:sample])
+    heur = sched.heuristic_choice(F)
+    rows = np.arange(sample)
+    out = {"workload": f"{n_stream}-job mixed stream (configs 1-4 shapes), MLP plan; regret on {sample} jobs "
+                       "against the exhaustive autotuner (config 5)",
+           "plan_ms": t_plan * 1e3, "plan_jobs_per_s": n_stream / t_plan,
+           "regret_mlp": sched.regret(T, plan[:sample]), "regret_heuristic": sched.regret(T, heur),
+           "sample_jobs_per_s_mlp": sample / (T[rows, plan[:sample]].sum() / 1e3),
+           "sample_jobs_per_s_heuristic": sample / (T[rows, heur].sum() / 1e3),
+           "sample_jobs_per_s_best": sample / (T.min(1).sum() / 1e3),
+           "variant_share": np.bincount(plan, minlength=sched.N_VARIANTS).tolist()}
+    mlp.close()
+    return out
+
+
 def run_case(args):
     """One kernel configuration for an ncu capture (prints a short JSON, not a bench line)."""
     import torch
@@ -430,7 +472,7 @@ def run_case(args):
         for _ in range(max(1, args.warmup + args.steps)):
             Rr, piv, d = eng.rref_det(p, A)
         dt = (time.perf_counter() - t0) / max(1, args.warmup + args.steps)
-        print(json.dumps({"case": args.case, "rank": int(len(piv)), "det": int(d), "s_per_rref": dt,
+        print(json.dumps(default=_json, obj={"case": args.case, "rank": int(len(piv)), "det": int(d), "s_per_rref": dt,
                           "rref_fnv": hex(gen.fnv_matrix(Rr))}), flush=True)
         eng.close()
         return 0
@@ -445,7 +487,7 @@ def run_case(args):
     Cm = torch.empty((n, n), dtype=torch.int32, device="cuda")
     ms = time_device(lambda: eng.gemm_dev(p, A, B, Cm), max(1, args.steps), args.warmup)
     eng.sync()
-    print(json.dumps({"case": args.case, "ms_per_gemm": ms / max(1, args.steps),
+    print(json.dumps(default=_json, obj={"case": args.case, "ms_per_gemm": ms / max(1, args.steps),
                       "tops": 2.0 * n ** 3 * max(1, args.steps) / ms / 1e9}), flush=True)
     eng.close()
     return 0
@@ -523,12 +565,13 @@ def main():
     for _ in range(3):
         eng.gemm(p, A_pin, B_pin, out=C_pin)
     barrier(ws)
-    t0 = time.perf_counter()
+    e2e_s = 0.0
     for _ in range(args.steps):
         flush()
         torch.cuda.synchronize()
-        eng.gemm(p, A_pin, B_pin, out=C_pin)
-    e2e_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        eng.gemm(p, A_pin, B_pin, out=C_pin)  # synchronous: H2D copies, split, GEMM, D2H copy
+        e2e_s += time.perf_counter() - t0
     barrier(ws)
     e2e_s = max_over_ranks(e2e_s, ws)
     e2e_ok = gen.fnv_matrix(C_pin) == 0x572E8347446366C6
@@ -570,9 +613,10 @@ def main():
         ext["rref_config2"] = extra_rref(eng)
         ext.update(extra_ring(eng))
         ext["jobstream_config4"] = extra_jobstream(eng, plain)
+        ext["scheduler_config5"] = extra_scheduler(eng)
         line["extras"] = ext
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=_json), flush=True)
     eng.close()
     if ws > 1:
         import torch.distributed as dist
