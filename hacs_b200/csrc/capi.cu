@@ -64,9 +64,10 @@ void KernelTimer::clear() {
 void bind(hme_ctx* ctx) { HME_CUDA(cudaSetDevice(ctx->device)); }
 
 void check_device_error(hme_ctx* ctx) {
+    // one stream-ordered read of the error word into pinned memory, one synchronisation
+    HME_CUDA(cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     HME_CUDA(cudaStreamSynchronize(ctx->stream));
-    int code = 0;
-    HME_CUDA(cudaMemcpy(&code, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    const int code = *static_cast<volatile int*>(ctx->h_err);
     if (code != 0) {
         const int zero = 0;
         HME_CUDA(cudaMemcpy(ctx->d_err, &zero, sizeof(int), cudaMemcpyHostToDevice));
@@ -110,9 +111,12 @@ int hme_ctx_create(int device, hme_ctx** out) {
             c->stream = c->own_stream;
             HME_CUDA(cudaMalloc(&c->d_err, sizeof(int)));
             HME_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+            HME_CUDA(cudaMallocHost(&c->h_err, sizeof(int)));
+            *c->h_err = 0;
         } catch (...) {
             if (c->own_stream) cudaStreamDestroy(c->own_stream);
             if (c->d_err) cudaFree(c->d_err);
+            if (c->h_err) cudaFreeHost(c->h_err);
             delete c;
             throw;
         }
@@ -129,7 +133,13 @@ int hme_ctx_destroy(hme_ctx* ctx) {
         sched_release(ctx);
         ctx->timer.clear();
         for (cudaEvent_t e : ctx->timer.pool) cudaEventDestroy(e);
+        if (ctx->copy_in) cudaStreamSynchronize(ctx->copy_in);
+        if (ctx->copy_out) cudaStreamSynchronize(ctx->copy_out);
+        for (cudaEvent_t e : ctx->pipe_ev) cudaEventDestroy(e);
+        if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+        if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
         if (ctx->d_err) cudaFree(ctx->d_err);
+        if (ctx->h_err) cudaFreeHost(ctx->h_err);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         delete ctx;
     });
@@ -209,21 +219,31 @@ int hme_gemm_u32(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, c
         HME_REQUIRE(C != nullptr && ldc >= n, "gemm: bad C");
         HME_REQUIRE(k == 0 || (A && B && lda >= k && ldb >= n), "gemm: bad A/B");
         bind(ctx);
+        const ModParams mp = make_mod(p);
+        if (k > 0) {
+            int v = ctx->fixed_variant;
+            if (v < 0) v = sched_variant(ctx, mp, m, n, k);
+            if (v == kVariantWide || v == kVariantNarrow) {
+                gemm_u32_host(ctx, mp, m, n, k, A, lda, B, ldb, C, ldc, op, v);
+                check_device_error(ctx);
+                return;
+            }
+        }
         // compact device copies (row-major, ld = cols) in the context's staging slots
         uint32_t* dA = static_cast<uint32_t*>(ctx->ws.get(kSlotStageA, sizeof(uint32_t) * static_cast<size_t>(m) * k));
         uint32_t* dB = static_cast<uint32_t*>(ctx->ws.get(kSlotStageB, sizeof(uint32_t) * static_cast<size_t>(k) * n));
         uint32_t* dC = static_cast<uint32_t*>(ctx->ws.get(kSlotStageC, sizeof(uint32_t) * static_cast<size_t>(m) * n));
         if (k) {
-            HME_CUDA(cudaMemcpy2DAsync(dA, sizeof(uint32_t) * k, A, sizeof(uint32_t) * lda, sizeof(uint32_t) * k, m,
+            HME_CUDA(copy_rows_async(dA, sizeof(uint32_t) * k, A, sizeof(uint32_t) * lda, sizeof(uint32_t) * k, m,
                                        cudaMemcpyHostToDevice, ctx->stream));
-            HME_CUDA(cudaMemcpy2DAsync(dB, sizeof(uint32_t) * n, B, sizeof(uint32_t) * ldb, sizeof(uint32_t) * n, k,
+            HME_CUDA(copy_rows_async(dB, sizeof(uint32_t) * n, B, sizeof(uint32_t) * ldb, sizeof(uint32_t) * n, k,
                                        cudaMemcpyHostToDevice, ctx->stream));
         }
         if (op != HME_SET)
-            HME_CUDA(cudaMemcpy2DAsync(dC, sizeof(uint32_t) * n, C, sizeof(uint32_t) * ldc, sizeof(uint32_t) * n, m,
+            HME_CUDA(copy_rows_async(dC, sizeof(uint32_t) * n, C, sizeof(uint32_t) * ldc, sizeof(uint32_t) * n, m,
                                        cudaMemcpyHostToDevice, ctx->stream));
-        gemm_u32_device(ctx, make_mod(p), m, n, k, dA, k, dB, n, dC, n, op);
-        HME_CUDA(cudaMemcpy2DAsync(C, sizeof(uint32_t) * ldc, dC, sizeof(uint32_t) * n, sizeof(uint32_t) * n, m,
+        gemm_u32_device(ctx, mp, m, n, k, dA, k, dB, n, dC, n, op);
+        HME_CUDA(copy_rows_async(C, sizeof(uint32_t) * ldc, dC, sizeof(uint32_t) * n, sizeof(uint32_t) * n, m,
                                    cudaMemcpyDeviceToHost, ctx->stream));
         check_device_error(ctx);
     });

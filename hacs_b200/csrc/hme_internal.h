@@ -112,6 +112,10 @@ struct hme_ctx {
     cudaStream_t stream = nullptr;      // active stream
     cudaStream_t own_stream = nullptr;  // created by the context
     int* d_err = nullptr;               // device error word written by bounded waits
+    int* h_err = nullptr;               // pinned host copy of d_err (read after each synchronising call)
+    cudaStream_t copy_in = nullptr;     // host-pointer GEMM: host -> device copies (created on first use)
+    cudaStream_t copy_out = nullptr;    // host-pointer GEMM: device -> host copies
+    std::vector<cudaEvent_t> pipe_ev;   // events of the host-pointer GEMM pipeline (reused)
     uint64_t launches = 0;
     hme::Workspace ws;
     hme::KernelTimer timer;
@@ -131,6 +135,15 @@ struct hme_ctx {
     } while (0)
 
 namespace hme {
+
+// Copy `rows` rows of `width` bytes between pitched buffers: one linear copy
+// when both sides are contiguous (the DMA engines stream a linear copy at full
+// PCIe rate), a pitched 2D copy otherwise.
+inline cudaError_t copy_rows_async(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+                                   size_t rows, cudaMemcpyKind kind, cudaStream_t st) {
+    if (dpitch == width && spitch == width) return cudaMemcpyAsync(dst, src, width * rows, kind, st);
+    return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, st);
+}
 
 // Fails with HME_ETIMEOUT (and clears the word) when a kernel on this context
 // recorded a device-side wait that ran out.  Synchronises the stream.
@@ -178,6 +191,11 @@ void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, 
                      size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op);
 void gemm_u32_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
                       size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int variant);
+// C op= A*B mod p with HOST pointers: copies in, product, copy out, with the
+// copies of row chunks pipelined against the GEMMs of the chunks before them
+// (limb_gemm.cu).  Synchronous; tensor-core variants only.
+void gemm_u32_host(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
+                   size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int variant);
 void simt_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
                           size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int tile);
 // The shape heuristic (the method without a learned model).

@@ -92,10 +92,19 @@ __device__ __forceinline__ void split_a_part(const SplitArgs& s, int block) {
 template <int L>
 __device__ __forceinline__ void split_b_part(const SplitArgs& s, int block, uint32_t (*tile)[33]) {
     const int k0 = (block % s.b_blocks_k) * 64, n0 = (block / s.b_blocks_k) * 32;
-    for (int t = threadIdx.x; t < 64 * 32; t += 256) {
-        const int kk = t >> 5, nn = t & 31;
-        const int k = k0 + kk, n = n0 + nn;
-        tile[kk][nn] = (k < s.K && n < s.N) ? __ldg(s.B + static_cast<size_t>(k) * s.ldb + n) : 0u;
+    // all eight loads of a thread in flight before the first shared-memory store
+    // (blockDim.x == 256: 8 x 256 = the 64 x 32 tile)
+    uint32_t v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int t = threadIdx.x + 256 * q;
+        const int k = k0 + (t >> 5), n = n0 + (t & 31);
+        v[q] = (k < s.K && n < s.N) ? __ldg(s.B + static_cast<size_t>(k) * s.ldb + n) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int t = threadIdx.x + 256 * q;
+        tile[t >> 5][t & 31] = v[q];
     }
     __syncthreads();
     const int nn = threadIdx.x >> 3, kc = threadIdx.x & 7;

@@ -109,6 +109,15 @@ __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
+// ---- programmatic dependent launch ------------------------------------------------
+// A kernel launched with programmatic stream serialisation may start while the
+// kernel before it in the stream is still running; grid_dep_wait() blocks until
+// that kernel has completed and its memory operations are visible (it returns
+// at once for a kernel launched without the attribute).  grid_dep_launch() lets
+// the next kernel's CTAs start being scheduled.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---- tcgen05: tensor memory ----------------------------------------------------
 // Allocation / deallocation are warp-collective (.sync.aligned): call from one full warp.
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {

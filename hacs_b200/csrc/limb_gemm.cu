@@ -121,6 +121,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
+    // the set-up above overlaps the tail of the limb split when this grid is a
+    // programmatic dependent of it; the planes are read only after this point
+    grid_dep_wait();
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
@@ -267,6 +270,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 template <int L>
 __global__ void __launch_bounds__(256) limb_split_kernel(const SplitArgs s) {
     __shared__ uint32_t tile[64][33];
+    grid_dep_launch();  // the GEMM that follows may start its set-up
     if (static_cast<int>(blockIdx.x) < s.a_blocks)
         split_a_part<L>(s, blockIdx.x);
     else
@@ -300,9 +304,15 @@ void encode_u8(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, c
     if (r != CUDA_SUCCESS) throw Error(HME_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")");
 }
 
+// a_plane: bytes between consecutive A limb planes (M * Kp for planes of
+// exactly these m rows; larger when the m rows are a slice of taller planes).
+// pdl: the launch directly follows the limb split on the same stream, so the
+// first K chunk may be a programmatic dependent of it (off while per-kernel
+// timing events sit between launches).
 template <int L, int BN>
 void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, int Kp,
-                 uint8_t* planesA, uint8_t* planesB, uint32_t* C, size_t ldc, int op) {
+                 uint8_t* planesA, uint64_t a_plane, uint8_t* planesB, uint32_t* C, size_t ldc, int op,
+                 bool pdl) {
     using CF = Cfg<L, BN>;
     static std::once_flag attr_once;
     std::call_once(attr_once, [] {
@@ -311,7 +321,7 @@ void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint
     CUtensorMap tmA, tmB;
     {
         const cuuint64_t dims[3] = {static_cast<cuuint64_t>(Kp), m, static_cast<cuuint64_t>(L)};
-        const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * m};
+        const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(a_plane)};
         const cuuint32_t box[3] = {kBK, kBM, 1};
         encode_u8(&tmA, planesA, 3, dims, strides, box);
     }
@@ -342,8 +352,17 @@ void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint
         g.k_begin = static_cast<int>(kb0);
         g.kblocks = static_cast<int>((kc + kBK - 1) / kBK);
         g.op = kb0 == 0 ? op : (op == HME_SET ? HME_ADD : op);
-        HME_TIMED(ctx, "limb_gemm", limb_gemm_kernel<L, BN><<<grid, kThreads, CF::SMEM, ctx->stream>>>(tmA, tmB, g));
-        HME_CUDA(cudaGetLastError());
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = CF::SMEM;
+        cfg.stream = ctx->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = (pdl && kb0 == 0 && !ctx->timer.on) ? 1 : 0;
+        HME_TIMED(ctx, "limb_gemm", HME_CUDA(cudaLaunchKernelEx(&cfg, limb_gemm_kernel<L, BN>, tmA, tmB, g)));
     }
 }
 
@@ -360,6 +379,51 @@ void encode_tma_u8(CUtensorMap* map, void* base, int rank, const cuuint64_t* dim
                    const cuuint32_t* box) {
     encode_u8(map, base, rank, dims, strides, box);
 }
+
+namespace {
+
+// Limb split of A (m rows, when do_a) and/or B (n columns, when do_b) in one launch.
+// a_plane: bytes between A limb planes (0: m * Kp).
+void launch_split(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, int Kp, const uint32_t* A,
+                  size_t lda, const uint32_t* B, size_t ldb, uint8_t* pa, uint64_t a_plane, uint8_t* pb, bool do_a,
+                  bool do_b) {
+    SplitArgs sa{};
+    sa.A = A; sa.lda = lda; sa.B = B; sa.ldb = ldb;
+    sa.M = static_cast<int>(m); sa.N = static_cast<int>(n); sa.K = static_cast<int>(k); sa.Kp = Kp;
+    sa.p = mp.p; sa.barrett = mp.barrett;
+    sa.planesA = pa; sa.planesB = pb;
+    sa.a_plane = a_plane;
+    const size_t work = static_cast<size_t>(m) * (Kp / 16);
+    sa.a_blocks = do_a ? static_cast<int>(std::min<size_t>((work + 255) / 256, static_cast<size_t>(ctx->num_sms) * 8))
+                       : 0;
+    sa.b_blocks_k = (Kp + 63) / 64;
+    sa.a_vec = do_a && ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && ((lda & 3) == 0);
+    const int grid = sa.a_blocks + (do_b ? sa.b_blocks_k * static_cast<int>((n + 31) / 32) : 0);
+    if (grid == 0) return;
+    switch (mp.limbs) {
+        case 1: HME_TIMED(ctx, "limb_split", limb_split_kernel<1><<<grid, 256, 0, ctx->stream>>>(sa)); break;
+        case 2: HME_TIMED(ctx, "limb_split", limb_split_kernel<2><<<grid, 256, 0, ctx->stream>>>(sa)); break;
+        case 3: HME_TIMED(ctx, "limb_split", limb_split_kernel<3><<<grid, 256, 0, ctx->stream>>>(sa)); break;
+        default: HME_TIMED(ctx, "limb_split", limb_split_kernel<4><<<grid, 256, 0, ctx->stream>>>(sa)); break;
+    }
+    HME_CUDA(cudaGetLastError());
+}
+
+void launch_gemm_variant(hme_ctx* ctx, const ModParams& mp, bool narrow, uint32_t m, uint32_t n, uint32_t k, int Kp,
+                         uint8_t* pa, uint64_t a_plane, uint8_t* pb, uint32_t* C, size_t ldc, int op, bool pdl) {
+    switch (mp.limbs) {
+        case 1: if (narrow) launch_gemm<1, 128>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
+                else launch_gemm<1, 256>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+        case 2: if (narrow) launch_gemm<2, 64>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
+                else launch_gemm<2, 128>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+        case 3: if (narrow) launch_gemm<3, 32>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
+                else launch_gemm<3, 80>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+        default: if (narrow) launch_gemm<4, 32>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
+                else launch_gemm<4, 64>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+    }
+}
+
+}  // namespace
 
 int gemm_default_variant(const hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n) {
     // Wide tiles (L*BN = 256 columns of TMEM per accumulator) unless that leaves
@@ -407,37 +471,89 @@ void gemm_u32_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n,
     const int Kp = static_cast<int>((k + kBK - 1) / kBK * kBK);
     uint8_t* pa = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesA, static_cast<size_t>(L) * m * Kp));
     uint8_t* pb = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesB, static_cast<size_t>(L) * L * n * Kp));
+    launch_split(ctx, mp, m, n, k, Kp, A, lda, B, ldb, pa, 0, pb, true, true);
+    launch_gemm_variant(ctx, mp, variant == kVariantNarrow, m, n, k, Kp, pa, static_cast<uint64_t>(Kp) * m, pb, C,
+                        ldc, op, true);
+}
 
-    {
-        SplitArgs sa{};
-        sa.A = A; sa.lda = lda; sa.B = B; sa.ldb = ldb;
-        sa.M = static_cast<int>(m); sa.N = static_cast<int>(n); sa.K = static_cast<int>(k); sa.Kp = Kp;
-        sa.p = mp.p; sa.barrett = mp.barrett;
-        sa.planesA = pa; sa.planesB = pb;
-        const size_t work = static_cast<size_t>(m) * (Kp / 16);
-        sa.a_blocks = static_cast<int>(std::min<size_t>((work + 255) / 256, static_cast<size_t>(ctx->num_sms) * 8));
-        sa.b_blocks_k = (Kp + 63) / 64;
-        sa.a_vec = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && ((lda & 3) == 0);
-        const int grid = sa.a_blocks + sa.b_blocks_k * static_cast<int>((n + 31) / 32);
-        switch (L) {
-            case 1: HME_TIMED(ctx, "limb_split", limb_split_kernel<1><<<grid, 256, 0, ctx->stream>>>(sa)); break;
-            case 2: HME_TIMED(ctx, "limb_split", limb_split_kernel<2><<<grid, 256, 0, ctx->stream>>>(sa)); break;
-            case 3: HME_TIMED(ctx, "limb_split", limb_split_kernel<3><<<grid, 256, 0, ctx->stream>>>(sa)); break;
-            default: HME_TIMED(ctx, "limb_split", limb_split_kernel<4><<<grid, 256, 0, ctx->stream>>>(sa)); break;
-        }
-        HME_CUDA(cudaGetLastError());
+void gemm_u32_host(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
+                   size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int variant) {
+    // Pipeline over row chunks of A and C (multiples of the 128-row tile, 1 to
+    // 8 chunks): B is copied and split first; then chunk i's rows of A
+    // (and of C for Add/Sub) are copied on copy_in while chunk i-1 is split
+    // and multiplied on the context stream and chunk i-2's rows of C go back on
+    // copy_out.  The host<->device copies run in both directions at once and
+    // hide the compute; what is left is the copy of B and one chunk's tail.
+    HME_REQUIRE(variant == kVariantWide || variant == kVariantNarrow, "gemm_u32_host: tensor-core variants only");
+    HME_REQUIRE(m > 0 && n > 0 && k > 0, "gemm_u32_host: empty product");
+    const int L = static_cast<int>(mp.limbs);
+    const int Kp = static_cast<int>((k + kBK - 1) / kBK * kBK);
+    const uint32_t tiles_m = (m + kBM - 1) / kBM;
+    // chunks of >= 2 MiB of C: every copy carries a fixed cost on the PCIe
+    // path, so small chunks lose more than their overlap gains (measured on
+    // B200: 1024^3 runs fastest with two chunks)
+    const size_t c_bytes = sizeof(uint32_t) * static_cast<size_t>(m) * n;
+    const uint32_t by_size = static_cast<uint32_t>(std::min<size_t>(8, std::max<size_t>(1, c_bytes >> 21)));
+    const uint32_t chunks_max = std::min<uint32_t>(by_size, tiles_m);
+    const uint32_t rows_per = (tiles_m + chunks_max - 1) / chunks_max * kBM;
+    const int nc = static_cast<int>((m + rows_per - 1) / rows_per);
+
+    uint32_t* dA = static_cast<uint32_t*>(ctx->ws.get(kSlotStageA, sizeof(uint32_t) * static_cast<size_t>(m) * k));
+    uint32_t* dB = static_cast<uint32_t*>(ctx->ws.get(kSlotStageB, sizeof(uint32_t) * static_cast<size_t>(k) * n));
+    uint32_t* dC = static_cast<uint32_t*>(ctx->ws.get(kSlotStageC, sizeof(uint32_t) * static_cast<size_t>(m) * n));
+    uint8_t* pa = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesA, static_cast<size_t>(L) * m * Kp));
+    uint8_t* pb = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesB, static_cast<size_t>(L) * L * n * Kp));
+
+    if (!ctx->copy_in) HME_CUDA(cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
+    if (!ctx->copy_out) HME_CUDA(cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
+    const size_t nev = 2 * static_cast<size_t>(nc) + 3;
+    while (ctx->pipe_ev.size() < nev) {
+        cudaEvent_t e;
+        HME_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->pipe_ev.push_back(e);
     }
-    const bool narrow = variant == kVariantNarrow;
-    switch (L) {
-        case 1: if (narrow) launch_gemm<1, 128>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op);
-                else launch_gemm<1, 256>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
-        case 2: if (narrow) launch_gemm<2, 64>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op);
-                else launch_gemm<2, 128>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
-        case 3: if (narrow) launch_gemm<3, 32>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op);
-                else launch_gemm<3, 80>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
-        default: if (narrow) launch_gemm<4, 32>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op);
-                else launch_gemm<4, 64>(ctx, mp, m, n, k, Kp, pa, pb, C, ldc, op); break;
+    cudaEvent_t ev_start = ctx->pipe_ev[0], ev_b = ctx->pipe_ev[1], ev_out = ctx->pipe_ev[2];
+    cudaEvent_t* ev_a = ctx->pipe_ev.data() + 3;
+    cudaEvent_t* ev_c = ev_a + nc;
+    const cudaStream_t s0 = ctx->stream;
+
+    // the copies start after earlier work on the context stream (it may still use the staging buffers)
+    HME_CUDA(cudaEventRecord(ev_start, s0));
+    HME_CUDA(cudaStreamWaitEvent(ctx->copy_in, ev_start, 0));
+    HME_CUDA(cudaStreamWaitEvent(ctx->copy_out, ev_start, 0));
+    const size_t w = sizeof(uint32_t);
+    HME_CUDA(copy_rows_async(dB, w * n, B, w * ldb, w * n, k, cudaMemcpyHostToDevice, ctx->copy_in));
+    HME_CUDA(cudaEventRecord(ev_b, ctx->copy_in));
+    for (int i = 0; i < nc; ++i) {
+        const uint32_t r0 = static_cast<uint32_t>(i) * rows_per, mc = std::min(rows_per, m - r0);
+        HME_CUDA(copy_rows_async(dA + static_cast<size_t>(r0) * k, w * k, A + static_cast<size_t>(r0) * lda,
+                                   w * lda, w * k, mc, cudaMemcpyHostToDevice, ctx->copy_in));
+        if (op != HME_SET)
+            HME_CUDA(copy_rows_async(dC + static_cast<size_t>(r0) * n, w * n, C + static_cast<size_t>(r0) * ldc,
+                                       w * ldc, w * n, mc, cudaMemcpyHostToDevice, ctx->copy_in));
+        HME_CUDA(cudaEventRecord(ev_a[i], ctx->copy_in));
     }
+    HME_CUDA(cudaStreamWaitEvent(s0, ev_b, 0));
+    launch_split(ctx, mp, 0, n, k, Kp, nullptr, 0, dB, n, nullptr, 0, pb, false, true);
+    const uint64_t a_plane = static_cast<uint64_t>(Kp) * m;
+    for (int i = 0; i < nc; ++i) {
+        const uint32_t r0 = static_cast<uint32_t>(i) * rows_per, mc = std::min(rows_per, m - r0);
+        HME_CUDA(cudaStreamWaitEvent(s0, ev_a[i], 0));
+        uint8_t* pa_i = pa + static_cast<size_t>(r0) * Kp;
+        launch_split(ctx, mp, mc, 0, k, Kp, dA + static_cast<size_t>(r0) * k, k, nullptr, 0, pa_i, a_plane, nullptr,
+                     true, false);
+        const bool narrow = ctx->fixed_variant >= 0 ? variant == kVariantNarrow
+                                                    : gemm_default_variant(ctx, mp, mc, n) == kVariantNarrow;
+        launch_gemm_variant(ctx, mp, narrow, mc, n, k, Kp, pa_i, a_plane, pb, dC + static_cast<size_t>(r0) * n, n,
+                            op, true);
+        HME_CUDA(cudaEventRecord(ev_c[i], s0));
+        // enqueued right behind the chunk's GEMM, so the copy back starts as soon as the chunk is done
+        HME_CUDA(cudaStreamWaitEvent(ctx->copy_out, ev_c[i], 0));
+        HME_CUDA(copy_rows_async(C + static_cast<size_t>(r0) * ldc, w * ldc, dC + static_cast<size_t>(r0) * n, w * n,
+                                   w * n, mc, cudaMemcpyDeviceToHost, ctx->copy_out));
+    }
+    HME_CUDA(cudaEventRecord(ev_out, ctx->copy_out));
+    HME_CUDA(cudaStreamWaitEvent(s0, ev_out, 0));
 }
 
 }  // namespace hme

@@ -91,3 +91,33 @@ def test_gemm_device_pointers_strided(engine):
     got = dC[:, :n].cpu().numpy().view(np.uint32)
     assert np.array_equal(got, O.gemm(p, A, B, C0, ADD))
     assert np.all(dC[:, n:].cpu().numpy() == 0)  # padding untouched
+
+
+@pytest.mark.parametrize("p,m,n,k,op", [
+    (65521, 2000, 1100, 300, SET),      # 4 row chunks (>= 2 MiB of C each), the last one ragged
+    (2147483629, 1500, 1500, 200, SUB), # 4 limbs, Sub: C's rows are copied in chunk by chunk
+    (65521, 1000, 300, 700, SET),       # one chunk
+    (251, 640, 1024, 129, ADD),         # 1 limb
+    (16777213, 129, 64, 12000, SET),    # 3 limbs, K beyond one exact-accumulation chunk, 2 row chunks
+])
+def test_gemm_host_pointers_strided_pipeline(engine, p, m, n, k, op):
+    """hme_gemm_u32 (host pointers) with leading dimensions larger than the
+    rows: the chunked copy/compute pipeline must read and write only the
+    m x n (m x k, k x n) windows."""
+    import ctypes as C
+
+    from hacs_b200 import check
+
+    rng = np.random.default_rng(m + n + k)
+    lda, ldb, ldc = k + 5, n + 3, n + 9
+    Ah = _rand(rng, (m, lda), p)
+    Bh = _rand(rng, (k, ldb), p)
+    Ch = _rand(rng, (m, ldc), p)
+    want = O.gemm(p, Ah[:, :k], Bh[:, :n], Ch[:, :n].copy(), op)
+    pad = Ch[:, n:].copy()
+    u = C.POINTER(C.c_uint32)
+    rc = engine._lib.hme_gemm_u32(engine._h, p, m, n, k, Ah.ctypes.data_as(u), lda, Bh.ctypes.data_as(u), ldb,
+                                  Ch.ctypes.data_as(u), ldc, op)
+    check(rc)
+    assert np.array_equal(Ch[:, :n], want)
+    assert np.array_equal(Ch[:, n:], pad)
