@@ -160,6 +160,10 @@ class Engine:
     def set_elim_options(self, panel: int = 0, rows_per_cta: int = 0, panel_ctas: int = 0, back_block: int = 0):
         check(self._lib.hme_ctx_set_elim_options(self._h, panel, rows_per_cta, panel_ctas, back_block))
 
+    def set_panel_kernel(self, mode: int) -> None:
+        """LU panel kernel: 0 automatic, 1 cooperative grid kernel, 2 thread-block cluster kernel."""
+        check(self._lib.hme_ctx_set_panel_kernel(self._h, mode))
+
     def rref(self, p: int, A):
         """(RREF(A), pivot columns): the reference's elim::rref result."""
         R = _u32(A).copy()

@@ -88,10 +88,37 @@ struct Ring {
     uint32_t ell, k;
     uint32_t unit_exp;   // phi(q) - 1: u^unit_exp is the inverse of a unit u
     uint32_t max_v;      // pivots of valuation <= max_v only (0: unit pivots)
+    uint32_t mont_qinv;  // q odd: -q^-1 mod 2^32 (Montgomery reduction)
+    uint32_t mont_r2;    // q odd: 2^64 mod q
     uint32_t pw[32];     // ell^0 .. ell^k
 };
 
+// Montgomery product x * y * 2^-32 mod q for odd q < 2^32 and x, y < q: the
+// sum T + m q may carry out of 64 bits when q > 2^31, so the carry is kept.
+__device__ __forceinline__ uint32_t mont_mul(uint32_t x, uint32_t y, uint32_t q, uint32_t qinv) {
+    const uint64_t t = static_cast<uint64_t>(x) * y;
+    const uint32_t mq = static_cast<uint32_t>(t) * qinv;
+    const uint64_t u = t + static_cast<uint64_t>(mq) * q;
+    const uint64_t r = (u >> 32) + (u < t ? (1ull << 32) : 0ull);  // < 2q
+    return static_cast<uint32_t>(r >= q ? r - q : r);
+}
+
+// u^(q-2) mod q (Fermat) for an odd prime q, left-to-right square and
+// multiply in the Montgomery domain: about 2 log2 q dependent products.
+__device__ __forceinline__ uint32_t inv_fermat(uint32_t u, const Ring& R) {
+    const uint32_t q = R.q, qi = R.mont_qinv;
+    const uint32_t um = mont_mul(u, R.mont_r2, q, qi);  // u * 2^32 mod q
+    const uint32_t e = q - 2;
+    uint32_t r = um;
+    for (int b = 30 - __clz(e); b >= 0; --b) {
+        r = mont_mul(r, r, q, qi);
+        if ((e >> b) & 1u) r = mont_mul(r, um, q, qi);
+    }
+    return mont_mul(r, 1u, q, qi);  // out of the Montgomery domain
+}
+
 __device__ __forceinline__ uint32_t unit_inverse(uint32_t u, const Ring& R) {
+    if (R.k == 1 && R.ell != 2) return inv_fermat(u % R.q, R);
     if (R.ell == 2) {
         uint32_t x = u;  // correct to 3 bits for odd u
         for (int i = 0; i < 5; ++i) x *= 2u - u * x;
@@ -339,6 +366,274 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
     if (ok && blockIdx.x == 0 && threadIdx.x == 0) *a.k_out = k;
 }
 
+// ---- the panel on one thread-block cluster ---------------------------------------
+// The same factorisation as panel_factor_kernel, for panels whose active rows
+// fit the shared memory of one cluster (up to kClusterMax CTAs).  Each CTA
+// keeps its slice of rows in shared memory, column-major, for the whole panel;
+// the per-column exchange goes through distributed shared memory.
+//
+// Fraction-free row updates.  A column step needs no modular inverse: with the
+// pivot x_p = ell^v * w (w a unit) every other active row becomes
+//     row <- (w * row - (x_i / ell^v) * pivot_row) * rho          (mod q)
+// with rho = 2^-32 in the Montgomery arithmetic of odd q (one reduction per
+// element) and rho = 1 for q = 2^k (wraparound).  Every active row, pivot-free
+// or not, is multiplied by the same unit w * rho, so after step t the active
+// rows hold S_t times the values of the classical elimination, S_t = prod of
+// (w_s rho) over s < t, and (x_i / ell^v) is stored as the raw multiplier.  The
+// classical multiplier is (x_i / ell^v) * w_t^-1 and the classical pivot row
+// t is its frozen raw row times S_t^-1; valuations (and zero / non-zero) do
+// not change under unit scaling, so the pivot sequence is the classical one.
+// After the last column every CTA computes the w_t^-1 in parallel and the
+// prefix products S_t^-1, and rescales its rows once: the panel leaves the
+// kernel as panel_factor_kernel leaves it (entry for entry over a field and for
+// unit pivots; for pivots of valuation v > 0 the multiplier x / ell^v is only
+// defined mod ell^(k-v), and the kernel's lift, consistent with the row
+// updates it made, may differ from that kernel's by a multiple of ell^(k-v)).
+// Like that kernel it updates only the columns right of each pivot.
+//
+// Per column:
+//   1. every CTA pushes its best pivot key and that row's values (columns
+//      [c, cend)) into a receive slot of every CTA of the cluster;
+//   2. one hardware cluster barrier (release / acquire), reached once per
+//      column by every thread of every CTA whatever the data;
+//   3. every warp takes the smallest key of the slots (a warp min), and the
+//      CTA updates its rows with the pivot row from its own receive slot.
+// Receive slots are double-buffered by column parity: a CTA writes slot parity
+// (it & 1) of column it only after passing barrier it - 1, when every CTA has
+// finished column it - 2.  A cluster barrier before the first push makes sure
+// every CTA of the cluster runs before any shared memory of it is written;
+// after the last barrier no CTA touches another's shared memory.
+constexpr int kClusterThreads = 1024;
+constexpr int kClusterMax = 16;
+constexpr int kClusterSmemMax = 200 * 1024;
+constexpr int kClusterRowsMax = kClusterThreads;  // rows per CTA: one row per thread slot
+constexpr int kKeyRowBits = 27;                   // 32-bit pivot key: valuation << 27 | row
+constexpr uint32_t kKeyRowMask = (1u << kKeyRowBits) - 1u;
+constexpr uint32_t kNoKey32 = 0xffffffffu;
+
+enum : int { kArithPow2 = 0, kArithMont31 = 1, kArithMont32 = 2 };
+
+// column stride of the column-major slice: odd, so a warp storing one row's
+// consecutive columns hits 32 different banks
+__host__ __device__ constexpr int cluster_stride(int rows) { return rows | 1; }
+
+__host__ __device__ constexpr size_t cluster_smem_bytes(int rows, int bw) {
+    return sizeof(uint32_t) * static_cast<size_t>(cluster_stride(rows)) * bw + static_cast<size_t>(rows) + 16;
+}
+
+__device__ __forceinline__ void cluster_barrier_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pivot_key32(uint32_t x, int row, const Ring& R) {
+    if (x == 0) return kNoKey32;
+    const uint32_t v = R.k == 1 ? 0u : R.max_v == 0 ? (x % R.ell == 0 ? 1u : 0u) : valuation(x, R, R.max_v);
+    if (v > R.max_v) return kNoKey32;
+    return (v << kKeyRowBits) | static_cast<uint32_t>(row);
+}
+
+// x / ell^v for x divisible by ell^v
+__device__ __forceinline__ uint32_t div_pw(uint32_t x, uint32_t v, const Ring& R) {
+    return v == 0 ? x : R.ell == 2 ? x >> v : x / R.pw[v];
+}
+
+// The negated multiplier as the row update wants it.
+template <int ARITH>
+__device__ __forceinline__ uint32_t ff_negate(uint32_t xp, const Ring& R) {
+    if constexpr (ARITH == kArithPow2) return 0u - xp;
+    else return xp == 0 ? 0u : R.q - xp;
+}
+
+// (w * y + xn * pr) * rho mod q, xn the negated multiplier (ff_negate)
+template <int ARITH>
+__device__ __forceinline__ uint32_t ff_update(uint32_t w, uint32_t y, uint32_t xn, uint32_t pr, const Ring& R) {
+    if constexpr (ARITH == kArithPow2) {
+        return (w * y + xn * pr) & (R.q - 1u);
+    } else if constexpr (ARITH == kArithMont31) {
+        // q < 2^31: both products < 2^62, t < 2^63, t + m q < 2^64
+        const uint64_t t = static_cast<uint64_t>(w) * y + static_cast<uint64_t>(xn) * pr;
+        const uint32_t mq = static_cast<uint32_t>(t) * R.mont_qinv;
+        const uint32_t r = static_cast<uint32_t>((t + static_cast<uint64_t>(mq) * R.q) >> 32);
+        return r >= R.q ? r - R.q : r;
+    } else {
+        return mod_add(mont_mul(w, y, R.q, R.mont_qinv), mont_mul(xn, pr, R.q, R.mont_qinv), R.q);
+    }
+}
+
+template <int ARITH>
+__global__ void __launch_bounds__(kClusterThreads, 1) panel_cluster_kernel(const PanelArgs a) {
+    extern __shared__ __align__(16) uint32_t s_dyn[];
+    __shared__ uint32_t r_key[2][kClusterMax];               // pushed keys, by parity and sender
+    __shared__ uint32_t r_row[2][kClusterMax][kMaxPanel];     // pushed candidate rows (from column c)
+    __shared__ uint32_t s_cand[2];                            // this CTA's best key, by parity
+    __shared__ uint32_t s_w[kMaxPanel];                       // unit part of each step's raw pivot
+    __shared__ uint32_t s_inv[kMaxPanel];                     // its inverse
+    __shared__ uint32_t s_sinv[kMaxPanel + 1];                // S_t^-1
+    __shared__ int s_colstep[kMaxPanel];                      // step t of pivot column c0 + j; else -1 - pivots left of it
+
+    const uint32_t crank = cluster_ctarank(), csize = cluster_nctarank();
+    const int rows = a.m - a.r0;
+    const int rpc = (rows + static_cast<int>(csize) - 1) / static_cast<int>(csize);
+    const int row_begin = a.r0 + static_cast<int>(crank) * rpc;
+    const int nloc = max(0, min(a.m, row_begin + rpc) - row_begin);
+    const int bw = a.bw, rs = cluster_stride(rpc);
+    uint32_t* S = s_dyn;                                                           // [bw][rs]
+    unsigned char* s_step = reinterpret_cast<unsigned char*>(S + static_cast<size_t>(bw) * rs);  // [rpc]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int nwarps = kClusterThreads / 32;
+    // thread -> (row li, phase sub): consecutive threads take consecutive rows,
+    // so a warp reads one column of consecutive rows; g threads share a row
+    int lg = 0;
+    while ((1 << lg) < nloc) ++lg;
+    const int nslots = 1 << lg, g = kClusterThreads >> lg;
+    const int li = tid & (nslots - 1), sub = tid >> lg;
+    const bool has_row = li < nloc;
+
+    for (int r = warp; r < nloc; r += nwarps) {
+        const uint32_t* src = a.A + static_cast<size_t>(row_begin + r) * a.ld + a.c0;
+        for (int j = lane; j < bw; j += 32) S[j * rs + r] = src[j];
+    }
+    for (int i = tid; i < rpc; i += kClusterThreads) s_step[i] = 0;
+    for (int j = tid; j < bw; j += kClusterThreads) s_colstep[j] = -1;
+    if (tid == 0) s_cand[0] = s_cand[1] = kNoKey32;
+    __syncthreads();
+    {
+        uint32_t key = kNoKey32;
+        if (has_row && sub == 0) key = pivot_key32(S[li], row_begin + li, a.R);
+        key = __reduce_min_sync(0xffffffffu, key);
+        if (lane == 0 && key != kNoKey32) atomicMin(&s_cand[0], key);
+    }
+    // every CTA of the cluster runs (its shared memory may be written) and s_cand[0] is complete
+    cluster_barrier_all();
+
+    const uint32_t rkey_addr = smem_u32(&r_key[0][0]);
+    const uint32_t rrow_addr = smem_u32(&r_row[0][0][0]);
+    int k = 0;
+    int pend_col = -1;  // ring mode: multiplier x / ell^v stored after the column's CTA barrier
+    uint32_t pend_xp = 0;
+    for (int it = 0; it < bw; ++it) {
+        const int par = it & 1;
+        if (pend_col >= 0) {
+            S[pend_col * rs + li] = pend_xp;
+            pend_col = -1;
+        }
+        // (1) push this CTA's candidate for column c0 + it to every CTA (itself included)
+        {
+            const uint32_t mine = s_cand[par];
+            if (warp < static_cast<int>(csize)) {
+                const uint32_t d = static_cast<uint32_t>(warp);
+                const uint32_t slot = par * kClusterMax + crank;
+                if (lane == 0) st_dsmem_u32(dsmem_addr(rkey_addr + 4u * slot, d), mine);
+                if (mine != kNoKey32) {
+                    const int lm = static_cast<int>(mine & kKeyRowMask) - row_begin;
+                    const uint32_t dst = dsmem_addr(rrow_addr + 4u * slot * kMaxPanel, d);
+                    for (int j = lane; j < bw - it; j += 32) st_dsmem_u32(dst + 4u * j, S[(it + j) * rs + lm]);
+                }
+            }
+            if (tid == 0) s_cand[par ^ 1] = kNoKey32;  // collects column it + 1's candidate below
+        }
+        // (2) every push of this column lands before any CTA reads its slots
+        cluster_barrier_all();
+        // (3) the pivot: the smallest (valuation, row) key of the cluster
+        const uint32_t kd = lane < static_cast<int>(csize) ? r_key[par][lane] : kNoKey32;
+        const uint32_t pkey = __reduce_min_sync(0xffffffffu, kd);
+        uint32_t key = kNoKey32;
+        if (pkey == kNoKey32) {
+            // no pivot in this column: every active row is unchanged; scan column it + 1
+            if (tid == 0) s_colstep[it] = -1 - k;
+            if (it + 1 < bw && has_row && sub == 0 && s_step[li] == 0)
+                key = pivot_key32(S[(it + 1) * rs + li], row_begin + li, a.R);
+        } else {
+            const int owner = __ffs(__ballot_sync(0xffffffffu, kd == pkey)) - 1;
+            const int prow = static_cast<int>(pkey & kKeyRowMask);
+            const uint32_t v = pkey >> kKeyRowBits;
+            const uint32_t* prv = r_row[par][owner];  // pivot row, column c0 + it at index 0
+            const uint32_t w = div_pw(prv[0], v, a.R);
+            const int oli = owner == static_cast<int>(crank) ? prow - row_begin : -1;
+            if (tid == 0) {
+                s_w[k] = w;
+                s_colstep[it] = k;
+                if (oli >= 0) s_step[oli] = static_cast<unsigned char>(k + 1);
+                if (crank == 0) {
+                    a.pivot_rows[k] = prow;
+                    a.pivot_cols[k] = a.c0 + it;
+                }
+            }
+            if (has_row && li != oli && s_step[li] == 0) {
+                const uint32_t xp = div_pw(S[it * rs + li], v, a.R);
+                const uint32_t xn = ff_negate<ARITH>(xp, a.R);
+                for (int j = it + 1 + sub; j < bw; j += g) {
+                    const uint32_t y = ff_update<ARITH>(w, S[j * rs + li], xn, prv[j - it], a.R);
+                    S[j * rs + li] = y;
+                    if (j == it + 1) key = pivot_key32(y, row_begin + li, a.R);
+                }
+                if (v != 0 && sub == 0) {
+                    pend_col = it;
+                    pend_xp = xp;
+                }
+            }
+            ++k;
+        }
+        key = __reduce_min_sync(0xffffffffu, key);
+        if (lane == 0 && key != kNoKey32) atomicMin(&s_cand[par ^ 1], key);
+        __syncthreads();
+    }
+    if (pend_col >= 0) S[pend_col * rs + li] = pend_xp;
+
+    // ---- back to the classical values: w_t^-1 and S_t^-1 = prod_{s<t} w_s^-1 rho^-1
+    for (int t = tid; t < k; t += kClusterThreads) s_inv[t] = unit_inverse(s_w[t], a.R);
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t q = a.R.q;
+        const uint64_t bm = a.R.barrett;
+        const uint32_t one = 1u % q;
+        // rho^-1 = 2^32 mod q (Montgomery) or 1
+        const uint32_t rinv = ARITH == kArithPow2 ? one : mont_mul(a.R.mont_r2, 1u, q, a.R.mont_qinv);
+        uint32_t f[kMaxPanel / 32];
+        uint32_t run = one;
+#pragma unroll
+        for (int e = 0; e < kMaxPanel / 32; ++e) {
+            const int t = lane * (kMaxPanel / 32) + e;
+            f[e] = t < k ? mod_mul(s_inv[t], rinv, q, bm) : one;
+            run = mod_mul(run, f[e], q, bm);
+        }
+        // inclusive scan of the lane products, then exclusive per element
+        uint32_t incl = run;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl = mod_mul(incl, y, q, bm);
+        }
+        uint32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) ex = one;
+#pragma unroll
+        for (int e = 0; e < kMaxPanel / 32; ++e) {
+            s_sinv[lane * (kMaxPanel / 32) + e] = ex;
+            ex = mod_mul(ex, f[e], q, bm);
+        }
+        if (lane == 31) s_sinv[kMaxPanel] = ex;
+    }
+    __syncthreads();
+    if (has_row) {
+        const int st = s_step[li];
+        const int tau = st ? st - 1 : k;  // the step that froze this row's scale
+        const uint32_t sc = s_sinv[tau];
+        for (int j = sub; j < bw; j += g) {
+            // a multiplier of step t < tau: times w_t^-1; any other entry was last
+            // scaled by the step before min(tau, pivots left of column j)
+            const int t = s_colstep[j];
+            const uint32_t f = t >= 0 ? (t < tau ? s_inv[t] : sc) : s_sinv[min(tau, -1 - t)];
+            S[j * rs + li] = mod_mul(S[j * rs + li], f, a.R.q, a.R.barrett);
+        }
+    }
+    __syncthreads();
+    for (int r = warp; r < nloc; r += nwarps) {
+        uint32_t* dst = a.A + static_cast<size_t>(row_begin + r) * a.ld + a.c0;
+        for (int j = lane; j < bw; j += 32) dst[j] = S[j * rs + r];
+    }
+    if (crank == 0 && tid == 0) *a.k_out = k;
+}
+
 // ---- row permutation of columns [c0, n) for rows [r0, m) -------------------------
 // tmp[i'][j'] = A[perm[i']][c0 + j']
 __global__ void gather_rows_kernel(const uint32_t* __restrict__ A, uint64_t ld, const int* __restrict__ perm,
@@ -376,55 +671,58 @@ __global__ void gather_cols_kernel(const uint32_t* __restrict__ A, uint64_t ld, 
 // pcols[b*bb ..]: T(t, s) = A[row0 + b*bb + t][pcols[b*bb + s]].
 //   UPPER: T upper triangular with non-zero diagonal (the U1 blocks of the RREF)
 //   !UPPER: T unit lower triangular, strictly-lower part read (the L11 of a panel)
-// out + b*bb*bb receives T^-1 (nb x nb, row-major, ld nb).  Thread j solves
-// T x = e_j for column j of the inverse by substitution in shared memory.
+// out + b*bb*bb receives T^-1 (nb x nb, row-major, ld nb).
+// UPPER is reduced to the unit case: T = D T' with D its diagonal, and
+// T^-1 = T'^-1 D^-1 (columns of T'^-1 scaled on the way out).  The unit
+// triangular inverse X = T'^-1 is built right-looking from X = I: at step t
+// row t of X is final, and every later row r (earlier, for UPPER) takes
+// X[r] -= T'[r][t] * X[t] over the non-zero columns of X[t] -- one rank-1
+// update and one CTA barrier per step, lanes over columns, warps over rows.
 template <bool UPPER>
-__global__ void tri_inv_kernel(const uint32_t* __restrict__ A, uint64_t ld, int row0, const int* __restrict__ pcols,
-                               int total, int bb, uint32_t p, uint64_t barrett, uint32_t kmax,
-                               uint32_t* __restrict__ out) {
+__global__ void __launch_bounds__(1024) tri_inv_kernel(const uint32_t* __restrict__ A, uint64_t ld, int row0,
+                                                       const int* __restrict__ pcols, int total, int bb, uint32_t p,
+                                                       uint64_t barrett, uint32_t kmax, uint32_t* __restrict__ out) {
     extern __shared__ uint32_t smem_ti[];
+    (void)kmax;
     const int i0 = blockIdx.x * bb;
     const int nb = min(bb, total - i0);
-    uint32_t* T = smem_ti;             // nb x nb
-    uint32_t* X = smem_ti + nb * nb;   // nb x nb, column j owned by thread j
+    uint32_t* T = smem_ti;             // nb x nb: T' (unit diagonal implied)
+    uint32_t* X = smem_ti + nb * nb;   // nb x nb
     uint32_t* dinv = X + nb * nb;      // nb
-    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-        const int t = idx / nb, s = idx % nb;
-        const bool keep = UPPER ? (s > t) : (s < t);
-        T[idx] = keep ? A[static_cast<size_t>(row0 + i0 + t) * ld + pcols[i0 + s]] : 0u;
-        X[idx] = 0;
-    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int t = threadIdx.x; t < nb; t += blockDim.x)
         dinv[t] = UPPER ? inv_binary_xgcd(A[static_cast<size_t>(row0 + i0 + t) * ld + pcols[i0 + t]], p) : 1u % p;
     __syncthreads();
-    // one warp per column of the inverse; the dot product of each
-    // substitution step is split over the lanes and summed by shuffles
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    (void)kmax;
-    for (int j = warp; j < nb; j += nw) {
-        if (lane == 0) X[j * nb + j] = dinv[j];
-        __syncwarp();
-        const int tb = UPPER ? j - 1 : j + 1;
-        const int te = UPPER ? -1 : nb;
-        const int dt = UPPER ? -1 : 1;
-        for (int t = tb; t != te; t += dt) {
-            // UPPER: sum_{s=t+1..j} T[t][s] x_s ; LOWER: sum_{s=j..t-1} T[t][s] x_s
-            const int s0 = UPPER ? t + 1 : j, s1 = UPPER ? j : t - 1;
-            uint32_t part = 0;
-            for (int s2 = s0 + lane; s2 <= s1; s2 += 32)
-                part = mod_add(part, mod_mul(T[t * nb + s2], X[s2 * nb + j], p, barrett), p);
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) part = mod_add(part, __shfl_xor_sync(0xffffffffu, part, off), p);
-            if (lane == 0) {
-                const uint32_t neg = part == 0 ? 0u : p - part;
-                X[t * nb + j] = UPPER ? mod_mul(neg, dinv[t], p, barrett) : neg;
-            }
-            __syncwarp();
-        }
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+        const int t = idx / nb, s2 = idx - t * nb;
+        const bool keep = UPPER ? (s2 > t) : (s2 < t);
+        uint32_t v = keep ? A[static_cast<size_t>(row0 + i0 + t) * ld + pcols[i0 + s2]] : 0u;
+        if (UPPER && keep) v = mod_mul(v, dinv[t], p, barrett);
+        T[idx] = v;
+        X[idx] = s2 == t ? 1u % p : 0u;
     }
     __syncthreads();
+    for (int st = 0; st + 1 < nb; ++st) {
+        const int t = UPPER ? nb - 1 - st : st;
+        // LOWER: rows r > t, columns j <= t;  UPPER: rows r < t, columns j >= t
+        const int rbeg = UPPER ? 0 : t + 1, rend = UPPER ? t : nb;
+        const int jbeg = UPPER ? t : 0, jend = UPPER ? nb : t + 1;
+        const uint32_t* xt = X + t * nb;
+        for (int r = rbeg + warp; r < rend; r += nw) {
+            const uint32_t l = T[r * nb + t];
+            if (l == 0) continue;
+            const uint32_t nl = p - l;
+            uint32_t* xr = X + r * nb;
+            for (int j = jbeg + lane; j < jend; j += 32)
+                xr[j] = reduce_u64(static_cast<uint64_t>(nl) * xt[j] + xr[j], p, barrett);
+        }
+        __syncthreads();
+    }
     uint32_t* o = out + static_cast<size_t>(blockIdx.x) * bb * bb;
-    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) o[idx] = X[idx];
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+        const uint32_t v = X[idx];
+        o[idx] = UPPER ? mod_mul(v, dinv[idx % nb], p, barrett) : v;
+    }
 }
 
 // R (m x n, ld ldr): rows < rank: identity at the pivot columns, X at the free
@@ -494,11 +792,47 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         // phi(ell^k) - 1 = ell^(k-1) (ell - 1) - 1
         rg.unit_exp = static_cast<uint32_t>(static_cast<uint64_t>(rg.pw[rg.k - 1]) * (rg.ell - 1) - 1);
     }
+    if (p & 1u) {
+        uint32_t x = p;  // p^-1 mod 2^32 by Newton's iteration (x = p is right to 3 bits)
+        for (int i = 0; i < 5; ++i) x *= 2u - p * x;
+        rg.mont_qinv = 0u - x;
+        rg.mont_r2 = static_cast<uint32_t>(((static_cast<unsigned __int128>(1) << 64)) % p);
+    }
     const int lu_cols = ring && ring->lu_cols > 0 ? std::min(ring->lu_cols, n) : n;
 
     static std::once_flag attr_once;
+    static int cluster_cap = 0;  // largest cluster the panel kernel can be launched with (0: none)
     std::call_once(attr_once, [] {
         cudaFuncSetAttribute(panel_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax);
+        bool attrs_ok = true;
+        for (const void* fn : {reinterpret_cast<const void*>(panel_cluster_kernel<kArithPow2>),
+                               reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont31>),
+                               reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont32>)}) {
+            attrs_ok = attrs_ok &&
+                       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kClusterSmemMax) ==
+                           cudaSuccess &&
+                       cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
+        }
+        if (attrs_ok) {
+            for (int cs = kClusterMax; cs >= 1 && cluster_cap == 0; cs /= 2) {
+                cudaLaunchConfig_t cfg{};
+                cfg.gridDim = dim3(cs);
+                cfg.blockDim = dim3(kClusterThreads);
+                cfg.dynamicSmemBytes = kClusterSmemMax;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = cs;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                int n = 0;
+                if (cudaOccupancyMaxActiveClusters(&n, panel_cluster_kernel<kArithMont31>, &cfg) == cudaSuccess &&
+                    n >= 1)
+                    cluster_cap = cs;
+            }
+        }
+        cudaGetLastError();  // a refused query leaves no error behind
         const int smem2 = sizeof(uint32_t) * (2 * kMaxPanel * kMaxPanel + kMaxPanel);
         cudaFuncSetAttribute(tri_inv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
         cudaFuncSetAttribute(tri_inv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
@@ -545,17 +879,57 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         pa.bar = d_s->bar;
         pa.err = ctx->d_err;
         const int rows = m - r0;
-        const int rpc_want = std::max(1, opt.rows_per_cta > 0 ? opt.rows_per_cta : 32);
-        const int want_grid = std::max(1, std::min(grid_cap, (rows + rpc_want - 1) / rpc_want));
-        const int rpc = (rows + want_grid - 1) / want_grid;
-        const size_t slice_bytes = sizeof(uint32_t) * static_cast<size_t>(rpc) * w;
-        const size_t extra = 5 * static_cast<size_t>(rpc) + 16;  // multipliers + pivot flags
-        int smem_rows = slice_bytes + extra <= kPanelSmemMax ? 1 : 0;
-        const size_t dyn = (smem_rows ? slice_bytes : 0) + extra;
-        void* args[] = {&pa, &smem_rows};
-        HME_TIMED(ctx, "panel_factor",
-                  HME_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(panel_factor_kernel), want_grid,
-                                                       kPanelThreads, args, dyn, ctx->stream)));
+        // the cluster kernel when the active rows fit the shared memory of one cluster:
+        // the cluster doubles (up to the largest the device runs) until each CTA
+        // holds at most rows_per_cta rows, and further while a slice does not fit
+        int cs = 0;
+        if (opt.panel_kernel != 1 && cluster_cap > 0) {
+            const size_t want = static_cast<size_t>(std::max(1, opt.rows_per_cta > 0 ? opt.rows_per_cta : 32));
+            auto rpc_of = [&](int c) { return (static_cast<size_t>(rows) + c - 1) / c; };
+            auto fits = [&](int c) {
+                const size_t rpc = rpc_of(c);
+                return rpc <= static_cast<size_t>(kClusterRowsMax) &&
+                       cluster_smem_bytes(static_cast<int>(rpc), w) <= static_cast<size_t>(kClusterSmemMax);
+            };
+            int c = 1;
+            while (c < cluster_cap && (rpc_of(c) > want || !fits(c))) c *= 2;
+            if (fits(c)) cs = c;
+        }
+        HME_REQUIRE(opt.panel_kernel != 2 || cs > 0, "elim: the panel does not fit one cluster");
+        if (cs > 0) {
+            const int rpc = static_cast<int>((static_cast<size_t>(rows) + cs - 1) / cs);
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(cs);
+            cfg.blockDim = dim3(kClusterThreads);
+            cfg.dynamicSmemBytes = cluster_smem_bytes(rpc, w);
+            cfg.stream = ctx->stream;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = cs;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            // q = 2^k: wraparound; odd q < 2^31: one Montgomery reduction per element; else two
+            if (rg.ell == 2)
+                HME_TIMED(ctx, "panel_factor", HME_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel<kArithPow2>, pa)));
+            else if (p < (1u << 31))
+                HME_TIMED(ctx, "panel_factor", HME_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel<kArithMont31>, pa)));
+            else
+                HME_TIMED(ctx, "panel_factor", HME_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel<kArithMont32>, pa)));
+        } else {
+            const int rpc_want = std::max(1, opt.rows_per_cta > 0 ? opt.rows_per_cta : 32);
+            const int want_grid = std::max(1, std::min(grid_cap, (rows + rpc_want - 1) / rpc_want));
+            const int rpc = (rows + want_grid - 1) / want_grid;
+            const size_t slice_bytes = sizeof(uint32_t) * static_cast<size_t>(rpc) * w;
+            const size_t extra = 5 * static_cast<size_t>(rpc) + 16;  // multipliers + pivot flags
+            int smem_rows = slice_bytes + extra <= kPanelSmemMax ? 1 : 0;
+            const size_t dyn = (smem_rows ? slice_bytes : 0) + extra;
+            void* args[] = {&pa, &smem_rows};
+            HME_TIMED(ctx, "panel_factor",
+                      HME_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(panel_factor_kernel), want_grid,
+                                                           kPanelThreads, args, dyn, ctx->stream)));
+        }
         HME_CUDA(cudaMemcpyAsync(&h_s, d_s, sizeof(Scratch), cudaMemcpyDeviceToHost, ctx->stream));
         check_device_error(ctx);  // synchronises
         const int k = h_s.k;

@@ -129,6 +129,14 @@ int hme_ctx_set_elim_options(hme_ctx* ctx, int panel, int rows_per_cta, int pane
     });
 }
 
+int hme_ctx_set_panel_kernel(hme_ctx* ctx, int mode) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        HME_REQUIRE(mode >= 0 && mode <= 2, "panel kernel mode must be 0 (automatic), 1 (grid) or 2 (cluster)");
+        opts(ctx).panel_kernel = mode;
+    });
+}
+
 int hme_rref_u32_dev(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t* A, size_t lda, uint32_t* pivots,
                      uint32_t* rank) {
     return guard([&] {

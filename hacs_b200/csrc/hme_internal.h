@@ -86,6 +86,7 @@ struct ElimOptions {
     int panel_ctas = 0;     // cap on the panel kernel's grid (0 = one CTA per SM)
     int back_block = 128;   // block of the RREF backward substitution
     bool want_diag = false; // return the U diagonal (determinant)
+    int panel_kernel = 0;   // 0 automatic, 1 cooperative grid kernel, 2 cluster kernel where the panel fits
 };
 
 // Optional per-kernel CUDA-event timing (bench / profiling use): when enabled,

@@ -129,7 +129,12 @@ HME_API int hme_gemm_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, u
  *   HME_ENOTINSPAN when a column of Y is outside the span of B's columns.
  * hme_ctx_set_elim_options: panel width (<= 128), rows per CTA of the panel
  *   kernel, cap on its grid, block of the backward substitution (0 = default).
- *   Tuning only: no option changes a value. */
+ *   Tuning only: no option changes a value.
+ * hme_ctx_set_panel_kernel: which kernel factors the LU panels: 0 automatic
+ *   (the thread-block-cluster kernel whenever the panel's active rows fit the
+ *   shared memory of one cluster, else the cooperative grid kernel), 1 always
+ *   the grid kernel, 2 the cluster kernel (HME_EINVAL from a factorisation
+ *   whose panel does not fit).  Tuning only: both give the same values. */
 HME_API int hme_rref_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t *A, size_t lda,
                          uint32_t *pivots, uint32_t *rank);
 HME_API int hme_rref_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t *A, size_t lda,
@@ -146,6 +151,7 @@ HME_API int hme_inverse_u32(hme_ctx *ctx, uint32_t p, uint32_t n, const uint32_t
 HME_API int hme_solve_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t nb, uint32_t ny, const uint32_t *B,
                           size_t ldb, const uint32_t *Y, size_t ldy, uint32_t *X, size_t ldx);
 HME_API int hme_ctx_set_elim_options(hme_ctx *ctx, int panel, int rows_per_cta, int panel_ctas, int back_block);
+HME_API int hme_ctx_set_panel_kernel(hme_ctx *ctx, int mode);
 
 /* ---- Howell and Smith forms over Z/ell^k (ell prime, ell^k < 2^32) ----------
  * Input canonical in [0, ell^k) (else HME_EINVAL, the reference's entry check).

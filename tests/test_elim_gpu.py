@@ -155,3 +155,53 @@ def test_rref_config2_full_size_golden(engine):
     assert gen.fnv_matrix(piv.reshape(1, -1)) == int(c["pivots_fnv"], 16)
     assert gen.fnv_matrix(Rr) == int(c["rref_fnv"], 16)
     assert d == c["det"] == 0
+
+
+@pytest.mark.parametrize("p", [3, 65521, 2147483629, 4294967291])
+def test_panel_kernels_agree(engine, p):
+    """The thread-block-cluster panel kernel (DSMEM exchange, one cluster) and
+    the cooperative grid kernel give the oracle's RREF and pivots, on shapes
+    that take 1, 2, 4, 8 and 16 CTAs per cluster and on one whose panel does
+    not fit a cluster (the automatic choice falls back to the grid kernel)."""
+    rng = np.random.default_rng(p % 977)
+    cases = [(100, 80, 50), (400, 100, 90), (600, 300, 200), (1500, 700, 690), (3000, 200, 150), (5000, 130, 128)]
+    try:
+        for (m, n, r) in cases:
+            A = _ranked(rng, m, n, r, p)
+            R2, p2 = O.rref(p, A)
+            for mode in (2, 1, 0):
+                engine.set_panel_kernel(mode)
+                R1, p1 = engine.rref(p, A)
+                assert np.array_equal(p1, p2), (p, m, n, mode)
+                assert np.array_equal(R1, R2), (p, m, n, mode)
+        # 20000 active rows x 64 columns: more than one cluster's shared memory
+        A = _ranked(rng, 20000, 64, 40, p)
+        engine.set_panel_kernel(2)
+        with pytest.raises(HmeError):
+            engine.rref(p, A)
+        engine.set_panel_kernel(0)
+        R1, p1 = engine.rref(p, A)
+        R2, p2 = O.rref(p, A)
+        assert np.array_equal(p1, p2) and np.array_equal(R1, R2)
+    finally:
+        engine.set_panel_kernel(0)
+
+
+@pytest.mark.parametrize("ell,k", [(2, 16), (3, 10), (2, 31), (5, 3)])
+def test_panel_kernels_agree_ring(engine, ell, k):
+    """Both panel kernels in the ring mode (minimal-valuation pivots) give the
+    reference's Howell form and Smith valuations."""
+    rng = np.random.default_rng(ell * 100 + k)
+    q = ell ** k
+    A = rng.integers(0, q, (300, 260), dtype=np.uint64).astype(np.uint32)
+    A[:, 5] = ((A[:, 5].astype(np.uint64) * ell) % q).astype(np.uint32)
+    want_h = O.howell(ell, k, A)
+    want_s = O.smith(ell, k, A)
+    try:
+        for mode in (2, 1):
+            engine.set_panel_kernel(mode)
+            H, piv, pv = engine.howell(ell, k, A)
+            assert np.array_equal(H, want_h[0]) and np.array_equal(piv, want_h[1]), (ell, k, mode)
+            assert np.array_equal(engine.smith(ell, k, A), want_s), (ell, k, mode)
+    finally:
+        engine.set_panel_kernel(0)
