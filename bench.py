@@ -476,11 +476,80 @@ def run_case(args):
                           "rref_fnv": hex(gen.fnv_matrix(Rr))}), flush=True)
         eng.close()
         return 0
+    if kind in ("howell", "smith"):
+        # howell:<n>:<ell>:<k> / smith:<n>:<ell>:<k>: planted U*D*V (the config-3 family), host pointers
+        from hacs_b200 import gen
+
+        n, ell, k = int(parts[1]), int(parts[2]), int(parts[3])
+        eng = hacs_b200.Engine(0)
+        M, _ = gen.planted_udv(n, ell, k, 0x33)
+        fn = (lambda: eng.howell(ell, k, M)) if kind == "howell" else (lambda: eng.smith(ell, k, M))
+        t0 = time.perf_counter()
+        for _ in range(max(1, args.warmup + args.steps)):
+            out = fn()
+        dt = (time.perf_counter() - t0) / max(1, args.warmup + args.steps)
+        size = int(out[0].shape[0]) if kind == "howell" else int(len(out))
+        print(json.dumps(default=_json, obj={"case": args.case, "s_per_call": dt, "rows_or_invariants": size}),
+              flush=True)
+        eng.close()
+        return 0
+    if kind == "jobs":
+        # jobs:<count>: the first <count> jobs of the config-4 stream, batched GEMM + rank
+        import ctypes as C_
+
+        from hacs_b200 import gen
+
+        nj = int(parts[1])
+        eng = hacs_b200.Engine(0)
+        s, fam, pj, sa, sb = gen.job_stream(10000)
+        s, fam, pj, sa, sb = s[:nj], fam[:nj], pj[:nj], sa[:nj], sb[:nj]
+        tot = int((s * s).sum())
+        bufs = [torch.empty(tot, dtype=torch.int32, device="cuda") for _ in range(3)]
+        jobs, specs, off = [], [], 0
+        for j in range(nj):
+            n = int(s[j])
+            A, B, Cm = (b[off:off + n * n].view(n, n) for b in bufs)
+            off += n * n
+            jobs.append({"p": int(pj[j]), "A": A, "B": B, "C": Cm})
+            specs += [(A, int(pj[j]), int(fam[j]), int(sa[j])), (B, int(pj[j]), int(fam[j]), int(sb[j]))]
+        arr = eng._jobs(jobs)
+        ranks = np.zeros(nj, np.uint32)
+        t0 = time.perf_counter()
+        for _ in range(max(1, args.warmup + args.steps)):
+            eng.gen_jobs_dev(specs)
+            hacs_b200.check(eng._lib.hme_batch_gemm_rank_u32_dev(eng._h, nj, arr,
+                                                                 ranks.ctypes.data_as(C_.POINTER(C_.c_uint32))))
+        dt = (time.perf_counter() - t0) / max(1, args.warmup + args.steps)
+        print(json.dumps(default=_json, obj={"case": args.case, "s_per_stream": dt, "rank_sum": int(ranks.sum())}),
+              flush=True)
+        eng.close()
+        return 0
+    if kind == "mlp":
+        # mlp:<rows>: scheduler MLP training epochs (FP32 forward + backward, Adam) and a BF16 plan
+        from hacs_b200 import sched
+
+        rows = int(parts[1])
+        eng = hacs_b200.Engine(0)
+        rng = np.random.default_rng(5)
+        X = rng.standard_normal((rows, 5)).astype(np.float32)
+        Y = rng.standard_normal((rows, sched.N_VARIANTS)).astype(np.float32)
+        mlp = sched.MLP(eng)
+        loss = mlp.train_normalised(X, Y, epochs=max(1, args.steps), batch=256)
+        shapes, dens = sched.sample_shapes(rows, seed=3)
+        plan = mlp.plan(shapes, dens)
+        print(json.dumps(default=_json, obj={"case": args.case, "loss": float(loss),
+                          "plan_share": np.bincount(plan, minlength=sched.N_VARIANTS).tolist()}), flush=True)
+        mlp.close()
+        eng.close()
+        return 0
+    # gemm:<n>:<p> (scheduler's variant) or gemm:<n>:<p>:<variant> (0 wide, 1 narrow, 2 simt32, 3 simt64)
     n, p = int(parts[1]), int(parts[2])
     assert kind == "gemm"
     torch.cuda.set_stream(torch.cuda.Stream())
     eng = hacs_b200.Engine(0)
     eng.use_torch_stream()
+    if len(parts) > 3:
+        hacs_b200.check(eng._lib.hme_ctx_set_gemm_variant(eng._h, int(parts[3])))
     g = torch.Generator(device="cuda").manual_seed(1)
     A = torch.randint(0, p, (n, n), dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
     B = torch.randint(0, p, (n, n), dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
@@ -502,8 +571,11 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the 8192^3 and plain-method lines")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--case", default=None,
-                    help="profiling case instead of the bench line: gemm:<n>:<p> runs W + K GEMMs of n^3 "
-                         "mod p; rref:<n>:<rank>:<p> runs W + K device RREFs of a rank-deficient n x n matrix")
+                    help="profiling case instead of the bench line: gemm:<n>:<p>[:<variant>] runs W + K GEMMs "
+                         "of n^3 mod p; rref:<n>:<rank>:<p> runs W + K device RREFs of a rank-deficient n x n "
+                         "matrix; howell:<n>:<ell>:<k> / smith:<n>:<ell>:<k> runs W + K forms of a planted "
+                         "U*D*V; jobs:<count> runs W + K batched GEMM + rank streams of the first <count> jobs; "
+                         "mlp:<rows> trains the scheduler MLP for K epochs and plans <rows> shapes")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -161,7 +161,8 @@ class Engine:
         check(self._lib.hme_ctx_set_elim_options(self._h, panel, rows_per_cta, panel_ctas, back_block))
 
     def set_panel_kernel(self, mode: int) -> None:
-        """LU panel kernel: 0 automatic, 1 cooperative grid kernel, 2 thread-block cluster kernel."""
+        """LU panel kernel: 0 automatic, 1 cooperative grid kernel, 2 thread-block cluster kernel,
+        3 cluster kernel with 1024 threads per CTA."""
         check(self._lib.hme_ctx_set_panel_kernel(self._h, mode))
 
     def rref(self, p: int, A):

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "hme_internal.h"
+#include "hme_ptx.cuh"
 
 namespace hme {
 
@@ -71,6 +72,8 @@ void check_device_error(hme_ctx* ctx) {
     if (code != 0) {
         const int zero = 0;
         HME_CUDA(cudaMemcpy(ctx->d_err, &zero, sizeof(int), cudaMemcpyHostToDevice));
+        if (code == DERR_LAUNCH_SHAPE)
+            throw Error(HME_ECUDA, "a kernel was launched with a shape it does not support and did nothing");
         throw Error(HME_ETIMEOUT, "a bounded device-side wait ran out (device code " + std::to_string(code) +
                                       "); the kernel returned early and its output is incomplete");
     }

@@ -403,10 +403,10 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
 // finished column it - 2.  A cluster barrier before the first push makes sure
 // every CTA of the cluster runs before any shared memory of it is written;
 // after the last barrier no CTA touches another's shared memory.
-constexpr int kClusterThreads = 1024;
+constexpr int kClusterThreads = 1024;  // threads per CTA: 512 or 1024 (template NT)
 constexpr int kClusterMax = 16;
 constexpr int kClusterSmemMax = 200 * 1024;
-constexpr int kClusterRowsMax = kClusterThreads;  // rows per CTA: one row per thread slot
+constexpr int kClusterRowsMax = kClusterThreads;  // rows per CTA: at most one row per thread
 constexpr int kKeyRowBits = 27;                   // 32-bit pivot key: valuation << 27 | row
 constexpr uint32_t kKeyRowMask = (1u << kKeyRowBits) - 1u;
 constexpr uint32_t kNoKey32 = 0xffffffffu;
@@ -460,8 +460,8 @@ __device__ __forceinline__ uint32_t ff_update(uint32_t w, uint32_t y, uint32_t x
     }
 }
 
-template <int ARITH>
-__global__ void __launch_bounds__(kClusterThreads, 1) panel_cluster_kernel(const PanelArgs a) {
+template <int ARITH, int NT>
+__global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(const PanelArgs a) {
     extern __shared__ __align__(16) uint32_t s_dyn[];
     __shared__ uint32_t r_key[2][kClusterMax];               // pushed keys, by parity and sender
     __shared__ uint32_t r_row[2][kClusterMax][kMaxPanel];     // pushed candidate rows (from column c)
@@ -476,16 +476,20 @@ __global__ void __launch_bounds__(kClusterThreads, 1) panel_cluster_kernel(const
     const int rpc = (rows + static_cast<int>(csize) - 1) / static_cast<int>(csize);
     const int row_begin = a.r0 + static_cast<int>(crank) * rpc;
     const int nloc = max(0, min(a.m, row_begin + rpc) - row_begin);
+    if (rpc > NT) {  // the host never launches this; the test is the same in every CTA, before any barrier
+        if (crank == 0 && threadIdx.x == 0) atomicCAS(a.err, 0, DERR_LAUNCH_SHAPE);
+        return;
+    }
     const int bw = a.bw, rs = cluster_stride(rpc);
     uint32_t* S = s_dyn;                                                           // [bw][rs]
     unsigned char* s_step = reinterpret_cast<unsigned char*>(S + static_cast<size_t>(bw) * rs);  // [rpc]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int nwarps = kClusterThreads / 32;
+    constexpr int nwarps = NT / 32;
     // thread -> (row li, phase sub): consecutive threads take consecutive rows,
     // so a warp reads one column of consecutive rows; g threads share a row
     int lg = 0;
     while ((1 << lg) < nloc) ++lg;
-    const int nslots = 1 << lg, g = kClusterThreads >> lg;
+    const int nslots = 1 << lg, g = NT >> lg;
     const int li = tid & (nslots - 1), sub = tid >> lg;
     const bool has_row = li < nloc;
 
@@ -493,8 +497,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) panel_cluster_kernel(const
         const uint32_t* src = a.A + static_cast<size_t>(row_begin + r) * a.ld + a.c0;
         for (int j = lane; j < bw; j += 32) S[j * rs + r] = src[j];
     }
-    for (int i = tid; i < rpc; i += kClusterThreads) s_step[i] = 0;
-    for (int j = tid; j < bw; j += kClusterThreads) s_colstep[j] = -1;
+    for (int i = tid; i < rpc; i += NT) s_step[i] = 0;
+    for (int j = tid; j < bw; j += NT) s_colstep[j] = -1;
     if (tid == 0) s_cand[0] = s_cand[1] = kNoKey32;
     __syncthreads();
     {
@@ -562,11 +566,25 @@ __global__ void __launch_bounds__(kClusterThreads, 1) panel_cluster_kernel(const
             if (has_row && li != oli && s_step[li] == 0) {
                 const uint32_t xp = div_pw(S[it * rs + li], v, a.R);
                 const uint32_t xn = ff_negate<ARITH>(xp, a.R);
-                for (int j = it + 1 + sub; j < bw; j += g) {
-                    const uint32_t y = ff_update<ARITH>(w, S[j * rs + li], xn, prv[j - it], a.R);
-                    S[j * rs + li] = y;
-                    if (j == it + 1) key = pivot_key32(y, row_begin + li, a.R);
+                int j = it + 1 + sub;
+                uint32_t* sp = S + j * rs + li;
+                const uint32_t* pp = prv + (j - it);
+                const int sstep = g * rs;
+                if (sub == 0 && j < bw) {  // column it + 1: the next column's candidate
+                    const uint32_t y = ff_update<ARITH>(w, *sp, xn, *pp, a.R);
+                    *sp = y;
+                    key = pivot_key32(y, row_begin + li, a.R);
+                    j += g;
+                    sp += sstep;
+                    pp += g;
                 }
+                for (; j + g < bw; j += 2 * g, sp += 2 * sstep, pp += 2 * g) {
+                    const uint32_t y0 = ff_update<ARITH>(w, sp[0], xn, pp[0], a.R);
+                    const uint32_t y1 = ff_update<ARITH>(w, sp[sstep], xn, pp[g], a.R);
+                    sp[0] = y0;
+                    sp[sstep] = y1;
+                }
+                if (j < bw) *sp = ff_update<ARITH>(w, *sp, xn, *pp, a.R);
                 if (v != 0 && sub == 0) {
                     pend_col = it;
                     pend_xp = xp;
@@ -581,7 +599,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) panel_cluster_kernel(const
     if (pend_col >= 0) S[pend_col * rs + li] = pend_xp;
 
     // ---- back to the classical values: w_t^-1 and S_t^-1 = prod_{s<t} w_s^-1 rho^-1
-    for (int t = tid; t < k; t += kClusterThreads) s_inv[t] = unit_inverse(s_w[t], a.R);
+    for (int t = tid; t < k; t += NT) s_inv[t] = unit_inverse(s_w[t], a.R);
     __syncthreads();
     if (warp == 0) {
         const uint32_t q = a.R.q;
@@ -725,6 +743,80 @@ __global__ void __launch_bounds__(1024) tri_inv_kernel(const uint32_t* __restric
     }
 }
 
+// U12 = L11^-1 A12 in place.  L11: the unit-lower k x k block of the panel's
+// pivot rows (rows row0 .. row0+k-1 of A) at the pivot columns pcols[0..k),
+// strictly-lower part read; A12: the same rows at columns [c1, c1 + trail).
+// Each CTA takes kTrsmCols columns into shared memory; forward substitution
+// runs per column in one warp, lane l holding rows l, l+32, l+64, l+96 in
+// registers: at step t the value of row t is final, a shuffle broadcasts it,
+// and every later row r takes x_r -= L[r][t] x_t.  The columns are
+// independent, so after the loads no block barrier is needed until the
+// write-back.  L11 sits in shared memory with an odd row stride, so the 32
+// lanes reading L[r][t] for 32 rows hit 32 banks.
+constexpr int kTrsmCols = 32;
+
+__global__ void __launch_bounds__(32 * kTrsmCols) trsm_unit_lower_kernel(uint32_t* __restrict__ A, uint64_t ld,
+                                                                         int row0, const int* __restrict__ pcols,
+                                                                         int k, int c1, int trail, uint32_t p,
+                                                                         uint64_t barrett) {
+    extern __shared__ uint32_t smem_tr[];
+    const int ls = k | 1;
+    constexpr int xs = kTrsmCols + 1;
+    uint32_t* Ls = smem_tr;               // [k][ls]
+    uint32_t* X = smem_tr + k * ls;       // [k][xs]
+    const int cbase = c1 + static_cast<int>(blockIdx.x) * kTrsmCols;
+    const int ncols = min(kTrsmCols, c1 + trail - cbase);
+    for (int idx = threadIdx.x; idx < k * k; idx += blockDim.x) {
+        const int r = idx / k, t = idx - r * k;
+        Ls[r * ls + t] = t < r ? A[static_cast<size_t>(row0 + r) * ld + pcols[t]] : 0u;
+    }
+    for (int idx = threadIdx.x; idx < k * kTrsmCols; idx += blockDim.x) {
+        const int r = idx / kTrsmCols, c = idx - r * kTrsmCols;
+        X[r * xs + c] = c < ncols ? A[static_cast<size_t>(row0 + r) * ld + cbase + c] : 0u;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < ncols) {
+        uint32_t x[kMaxPanel / 32];
+#pragma unroll
+        for (int q = 0; q < kMaxPanel / 32; ++q) {
+            const int r = lane + 32 * q;
+            x[q] = r < k ? X[r * xs + warp] : 0u;
+        }
+#pragma unroll
+        for (int qt = 0; qt < kMaxPanel / 32; ++qt) {
+            if (32 * qt >= k - 1) break;
+            for (int tt = 0; tt < 32; ++tt) {
+                const int t = 32 * qt + tt;
+                if (t >= k - 1) break;
+                const uint32_t xt = __shfl_sync(0xffffffffu, x[qt], tt);
+#pragma unroll
+                for (int q = qt; q < kMaxPanel / 32; ++q) {
+                    const int r = lane + 32 * q;
+                    if (r > t && r < k) {
+                        const uint32_t l = Ls[r * ls + t];
+                        if (l) x[q] = reduce_u64(static_cast<uint64_t>(p - l) * xt + x[q], p, barrett);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kMaxPanel / 32; ++q) {
+            const int r = lane + 32 * q;
+            if (r < k) X[r * xs + warp] = x[q];
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < k * kTrsmCols; idx += blockDim.x) {
+        const int r = idx / kTrsmCols, c = idx - r * kTrsmCols;
+        if (c < ncols) A[static_cast<size_t>(row0 + r) * ld + cbase + c] = X[r * xs + c];
+    }
+}
+
+size_t trsm_smem_bytes(int k) {
+    return sizeof(uint32_t) * (static_cast<size_t>(k) * (k | 1) + static_cast<size_t>(k) * (kTrsmCols + 1));
+}
+
 // R (m x n, ld ldr): rows < rank: identity at the pivot columns, X at the free
 // columns; rows >= rank: zero.
 __global__ void assemble_rref_kernel(uint32_t* __restrict__ R, uint64_t ldr, int m, int n, int rank,
@@ -805,9 +897,12 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     std::call_once(attr_once, [] {
         cudaFuncSetAttribute(panel_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax);
         bool attrs_ok = true;
-        for (const void* fn : {reinterpret_cast<const void*>(panel_cluster_kernel<kArithPow2>),
-                               reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont31>),
-                               reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont32>)}) {
+        for (const void* fn : {reinterpret_cast<const void*>(panel_cluster_kernel<kArithPow2, 512>),
+                               reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont31, 512>),
+                               reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont32, 512>),
+                               reinterpret_cast<const void*>(panel_cluster_kernel<kArithPow2, 1024>),
+                               reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont31, 1024>),
+                               reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont32, 1024>)}) {
             attrs_ok = attrs_ok &&
                        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kClusterSmemMax) ==
                            cudaSuccess &&
@@ -827,7 +922,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
                 cfg.attrs = at;
                 cfg.numAttrs = 1;
                 int n = 0;
-                if (cudaOccupancyMaxActiveClusters(&n, panel_cluster_kernel<kArithMont31>, &cfg) == cudaSuccess &&
+                if (cudaOccupancyMaxActiveClusters(&n, panel_cluster_kernel<kArithMont31, 1024>, &cfg) == cudaSuccess &&
                     n >= 1)
                     cluster_cap = cs;
             }
@@ -836,6 +931,8 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         const int smem2 = sizeof(uint32_t) * (2 * kMaxPanel * kMaxPanel + kMaxPanel);
         cudaFuncSetAttribute(tri_inv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
         cudaFuncSetAttribute(tri_inv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
+        cudaFuncSetAttribute(trsm_unit_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(trsm_smem_bytes(kMaxPanel)));
     });
 
     // device scratch
@@ -895,7 +992,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             while (c < cluster_cap && (rpc_of(c) > want || !fits(c))) c *= 2;
             if (fits(c)) cs = c;
         }
-        HME_REQUIRE(opt.panel_kernel != 2 || cs > 0, "elim: the panel does not fit one cluster");
+        HME_REQUIRE(opt.panel_kernel < 2 || cs > 0, "elim: the panel does not fit one cluster");
         if (cs > 0) {
             const int rpc = static_cast<int>((static_cast<size_t>(rows) + cs - 1) / cs);
             cudaLaunchConfig_t cfg{};
@@ -910,13 +1007,24 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             at[0].val.clusterDim.z = 1;
             cfg.attrs = at;
             cfg.numAttrs = 1;
-            // q = 2^k: wraparound; odd q < 2^31: one Montgomery reduction per element; else two
-            if (rg.ell == 2)
-                HME_TIMED(ctx, "panel_factor", HME_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel<kArithPow2>, pa)));
-            else if (p < (1u << 31))
-                HME_TIMED(ctx, "panel_factor", HME_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel<kArithMont31>, pa)));
-            else
-                HME_TIMED(ctx, "panel_factor", HME_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel<kArithMont32>, pa)));
+            // q = 2^k: wraparound; odd q < 2^31: one Montgomery reduction per element; else two.
+            // 512 threads per CTA while a CTA holds at most 512 rows (half the per-column
+            // control work of 1024 threads), unless the panel-kernel setting asks for 1024
+            const bool t512 = rpc <= 512 && opt.panel_kernel != 3;
+            cfg.blockDim = dim3(t512 ? 512 : 1024);
+            auto launch = [&](auto kern) {
+                HME_TIMED(ctx, "panel_factor", HME_CUDA(cudaLaunchKernelEx(&cfg, kern, pa)));
+            };
+            if (rg.ell == 2) {
+                if (t512) launch(panel_cluster_kernel<kArithPow2, 512>);
+                else launch(panel_cluster_kernel<kArithPow2, 1024>);
+            } else if (p < (1u << 31)) {
+                if (t512) launch(panel_cluster_kernel<kArithMont31, 512>);
+                else launch(panel_cluster_kernel<kArithMont31, 1024>);
+            } else {
+                if (t512) launch(panel_cluster_kernel<kArithMont32, 512>);
+                else launch(panel_cluster_kernel<kArithMont32, 1024>);
+            }
         } else {
             const int rpc_want = std::max(1, opt.rows_per_cta > 0 ? opt.rows_per_cta : 32);
             const int want_grid = std::max(1, std::min(grid_cap, (rows + rpc_want - 1) / rpc_want));
@@ -973,20 +1081,12 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         const int trail = n - c1;
         const int below = m - r0 - k;
         if (trail > 0) {
-            // (3) U12 = L11^-1 A12: invert the unit-lower k x k L11 in shared memory,
-            //     then one limb GEMM into a scratch buffer, copied back over A12
+            // (3) U12 = L11^-1 A12 in place: forward substitution, one warp per column
             if (k > 1) {
-                uint32_t* Linv = static_cast<uint32_t*>(ctx->ws.get(kSlotElim5, sizeof(uint32_t) * kMaxPanel * kMaxPanel));
-                const size_t sm = sizeof(uint32_t) * (2 * static_cast<size_t>(k) * k + k);
-                HME_TIMED(ctx, "tri_inv", tri_inv_kernel<false><<<1, 1024, sm, ctx->stream>>>(
-                                              A, ld, r0, d_s->pivot_cols, k, k, p, mp.barrett, kmax_for(p), Linv));
+                const int g = (trail + kTrsmCols - 1) / kTrsmCols;
+                HME_TIMED(ctx, "trsm", trsm_unit_lower_kernel<<<g, 32 * kTrsmCols, trsm_smem_bytes(k), ctx->stream>>>(
+                                           A, ld, r0, d_s->pivot_cols, k, c1, trail, p, mp.barrett));
                 HME_CUDA(cudaGetLastError());
-                uint32_t* T = static_cast<uint32_t*>(ctx->ws.get(kSlotElim6, sizeof(uint32_t) * static_cast<size_t>(k) * trail));
-                gemm_u32_device(ctx, mp, k, trail, k, Linv, k, A + static_cast<size_t>(r0) * ld + c1, ld, T, trail,
-                                HME_SET);
-                HME_CUDA(cudaMemcpy2DAsync(A + static_cast<size_t>(r0) * ld + c1, sizeof(uint32_t) * ld, T,
-                                           sizeof(uint32_t) * trail, sizeof(uint32_t) * trail, k,
-                                           cudaMemcpyDeviceToDevice, ctx->stream));
             }
             // (4) A22 -= L21 * U12
             if (below > 0) {

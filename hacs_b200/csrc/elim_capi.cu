@@ -132,7 +132,8 @@ int hme_ctx_set_elim_options(hme_ctx* ctx, int panel, int rows_per_cta, int pane
 int hme_ctx_set_panel_kernel(hme_ctx* ctx, int mode) {
     return guard([&] {
         HME_REQUIRE(ctx != nullptr, "null context");
-        HME_REQUIRE(mode >= 0 && mode <= 2, "panel kernel mode must be 0 (automatic), 1 (grid) or 2 (cluster)");
+        HME_REQUIRE(mode >= 0 && mode <= 3,
+                    "panel kernel mode must be 0 (automatic), 1 (grid), 2 (cluster) or 3 (cluster, 1024 threads)");
         opts(ctx).panel_kernel = mode;
     });
 }

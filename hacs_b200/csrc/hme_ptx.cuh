@@ -26,6 +26,7 @@ enum DeviceErr : int {
     DERR_WAIT_DRAIN = 5,      // tear-down wait for in-flight copies / MMAs ran out
     DERR_TMEM_ADDR = 6,       // tensor-memory allocation returned an unusable address
     DERR_GRID_BARRIER = 7,    // a cooperative kernel's grid barrier waited too long
+    DERR_LAUNCH_SHAPE = 8,    // a kernel found its launch shape outside what it supports and did nothing
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

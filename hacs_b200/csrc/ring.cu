@@ -35,6 +35,7 @@ namespace {
 
 constexpr int kHowellThreads = 1024;
 constexpr int kReduceBlock = 64;
+constexpr size_t kHowellLeadSmemMax = 192 * 1024;  // leading-column table of the Howell pass (48k rows)
 
 struct RingK {
     uint32_t q, ell, k;
@@ -66,6 +67,12 @@ __device__ __forceinline__ uint32_t pow_mod_d(uint32_t b, uint32_t e, uint32_t q
         e >>= 1;
     }
     return r;
+}
+
+// floor(2^64 / d) for 2 <= d < 2^32 (the Barrett constant of a small modulus)
+__device__ __forceinline__ uint64_t make_barrett_d(uint32_t d) {
+    const uint64_t q = ~0ull / d;  // floor((2^64 - 1) / d)
+    return (q + 1) * d == 0 ? q + 1 : q;  // d divides 2^64 only for powers of two
 }
 
 __device__ __forceinline__ uint32_t val_k(uint32_t x, const RingK& R) {
@@ -153,7 +160,7 @@ struct PassArgs {
     int* err;
 };
 
-__global__ void __launch_bounds__(kHowellThreads) howell_pass_kernel(const PassArgs a) {
+__global__ void __launch_bounds__(kHowellThreads) howell_pass_scan_kernel(const PassArgs a) {
     __shared__ unsigned long long s_best;
     __shared__ int s_nel;
     __shared__ int s_el[kHowellThreads];
@@ -234,6 +241,152 @@ __global__ void __launch_bounds__(kHowellThreads) howell_pass_kernel(const PassA
             __syncthreads();
             if (threadIdx.x == 0 && s_closure_nz) {
                 a.alive[nid] = 1;
+                s_nrows = nid + 1;
+            }
+        }
+        if (threadIdx.x == 0) {
+            a.piv_id[s_h] = pid;
+            a.piv_col[s_h] = c;
+            a.piv_v[s_h] = static_cast<int>(v);
+            ++s_h;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *a.h_out = s_h;
+        *a.nrows_out = s_nrows;
+    }
+}
+
+// The inverse of a unit u of Z/ell^k by Newton's iteration x <- x (2 - u x),
+// which doubles the ell-adic precision per step: in 32-bit wraparound from
+// x = u (right to 3 bits) for ell = 2; from the inverse mod ell,
+// u^(ell - 2) mod ell, for odd ell (1 -> 2 -> 4 -> ... >= k digits).
+__device__ __forceinline__ uint32_t ring_unit_inverse(uint32_t u, const RingK& R) {
+    if (R.ell == 2) {
+        uint32_t x = u;
+        for (int i = 0; i < 5; ++i) x *= 2u - u * x;
+        return R.k >= 32 ? x : (x & (R.q - 1u));
+    }
+    const uint32_t u0 = u % R.ell;
+    uint32_t x = pow_mod_d(u0, R.ell - 2, R.ell, make_barrett_d(R.ell));
+    for (uint32_t prec = 1; prec < R.k; prec *= 2) {
+        const uint32_t ux = mod_mul(u % R.q, x, R.q, R.barrett);
+        x = mod_mul(x, mod_sub(2u % R.q, ux, R.q), R.q, R.barrett);
+    }
+    return x;
+}
+
+// The pass with a leading-column table in shared memory.  Every live row's
+// first non-zero column is at least the current column c (eliminating column
+// c' zeroes it in every row that had a non-zero there), so the rows with a
+// non-zero in column c are exactly those whose leading column IS c: the scan
+// per column reads the table, not the store.  A row reduced by the pivot gets
+// its new leading column from the same warp pass that updates it; consumed
+// pivot rows, zero rows and unused slots hold n (never a candidate).  On
+// entry piv_col[0 .. r) holds the echelon rows' pivot columns (their leading
+// columns: the entries left of them are zero).
+__global__ void __launch_bounds__(kHowellThreads) howell_pass_kernel(const PassArgs a) {
+    extern __shared__ int s_lead[];  // [cap]
+    __shared__ unsigned long long s_best;
+    __shared__ int s_nel, s_over;
+    __shared__ int s_el[kHowellThreads];
+    __shared__ uint32_t s_ui;
+    __shared__ int s_nrows, s_h, s_zlead;
+    const RingK& R = a.R;
+    const int none = a.n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < a.cap; i += blockDim.x) s_lead[i] = i < a.r ? a.piv_col[i] : none;
+    if (threadIdx.x == 0) {
+        s_nrows = a.r;
+        s_h = 0;
+    }
+    __syncthreads();
+    for (int c = 0; c < a.n; ++c) {
+        if (threadIdx.x == 0) {
+            s_best = ~0ull;
+            s_nel = 0;
+            s_over = 0;
+        }
+        __syncthreads();
+        const int nrows = s_nrows;
+        // the candidates: smallest (valuation, id) and the list of all of them
+        for (int id = threadIdx.x; id < nrows; id += blockDim.x) {
+            if (s_lead[id] != c) continue;
+            const uint32_t x = a.W[static_cast<size_t>(id) * a.ld + c];
+            atomicMin(&s_best, (static_cast<unsigned long long>(val_k(x, R)) << 32) | static_cast<unsigned>(id));
+            const int slot = atomicAdd(&s_nel, 1);
+            if (slot < kHowellThreads) s_el[slot] = id;
+            else s_over = 1;
+        }
+        __syncthreads();
+        const unsigned long long best = s_best;
+        if (best == ~0ull) continue;
+        const int pid = static_cast<int>(best & 0xffffffffu);
+        const uint32_t v = static_cast<uint32_t>(best >> 32);
+        uint32_t* P = a.W + static_cast<size_t>(pid) * a.ld;
+        if (threadIdx.x == 0) {
+            s_lead[pid] = none;  // consumed
+            s_ui = ring_unit_inverse(P[c] / R.pw[v], R);
+            s_zlead = none;
+        }
+        __syncthreads();
+        // scale the pivot row so that it leads with ell^v exactly
+        const uint32_t ui = s_ui;
+        for (int j = c + threadIdx.x; j < a.n; j += blockDim.x) P[j] = mod_mul(P[j], ui, R.q, R.barrett);
+        __syncthreads();
+        // R -= (R[c] / ell^v) * P over columns [c, n) for every other candidate,
+        // one warp per row; more than one CTA-size of candidates: rescan
+        for (;;) {
+            const int nel = min(s_nel, kHowellThreads);
+            for (int t = warp; t < nel; t += nw) {
+                const int id = s_el[t];
+                if (id == pid) continue;
+                uint32_t* Rw = a.W + static_cast<size_t>(id) * a.ld;
+                const uint32_t f = Rw[c] / R.pw[v];
+                __syncwarp();
+                int first = none;
+                for (int j = c + lane; j < a.n; j += 32) {
+                    const uint32_t y = mod_sub(Rw[j], mod_mul(f, P[j], R.q, R.barrett), R.q);
+                    Rw[j] = y;
+                    if (y != 0 && first == none) first = j;
+                }
+                first = __reduce_min_sync(0xffffffffu, first);
+                if (lane == 0) s_lead[id] = first;
+            }
+            __syncthreads();
+            if (!s_over) break;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_nel = 0;
+                s_over = 0;
+            }
+            __syncthreads();
+            for (int id = threadIdx.x; id < nrows; id += blockDim.x) {
+                if (s_lead[id] != c) continue;
+                const int slot = atomicAdd(&s_nel, 1);
+                if (slot < kHowellThreads) s_el[slot] = id;
+                else s_over = 1;
+            }
+            __syncthreads();
+        }
+        // Howell closure: ell^(k - v) * P, zero in columns <= c, appended at the bottom
+        if (v > 0) {
+            const int nid = s_nrows;
+            if (nid >= a.cap) {
+                if (threadIdx.x == 0) atomicCAS(a.err, 0, 64);  // store exhausted: cannot happen (<= n closures)
+                return;
+            }
+            uint32_t* Z = a.W + static_cast<size_t>(nid) * a.ld;
+            const uint32_t f = R.pw[R.k - v];
+            for (int j = threadIdx.x; j < a.n; j += blockDim.x) {
+                const uint32_t z = j > c ? mod_mul(P[j], f, R.q, R.barrett) : 0u;
+                Z[j] = z;
+                if (z) atomicMin(&s_zlead, j);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0 && s_zlead != none) {
+                s_lead[nid] = s_zlead;
                 s_nrows = nid + 1;
             }
         }
@@ -468,7 +621,15 @@ HowellOut howell_device(hme_ctx* ctx, uint32_t ell, uint32_t k, const uint32_t* 
     pa.h_out = d_cnt;
     pa.nrows_out = d_cnt + 1;
     pa.err = ctx->d_err;
-    HME_TIMED(ctx, "howell_pass", howell_pass_kernel<<<1, kHowellThreads, 0, ctx->stream>>>(pa));
+    // the leading-column table in shared memory when it fits, else the store-scanning pass
+    const size_t lead_bytes = sizeof(int) * static_cast<size_t>(cap);
+    if (lead_bytes <= kHowellLeadSmemMax) {
+        HME_CUDA(cudaFuncSetAttribute(howell_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(kHowellLeadSmemMax)));
+        HME_TIMED(ctx, "howell_pass", howell_pass_kernel<<<1, kHowellThreads, lead_bytes, ctx->stream>>>(pa));
+    } else {
+        HME_TIMED(ctx, "howell_pass", howell_pass_scan_kernel<<<1, kHowellThreads, 0, ctx->stream>>>(pa));
+    }
     HME_CUDA(cudaGetLastError());
     int hc[2] = {0, 0};
     HME_CUDA(cudaMemcpyAsync(hc, d_cnt, sizeof(int) * 2, cudaMemcpyDeviceToHost, ctx->stream));

@@ -134,7 +134,9 @@ HME_API int hme_gemm_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, u
  *   (the thread-block-cluster kernel whenever the panel's active rows fit the
  *   shared memory of one cluster, else the cooperative grid kernel), 1 always
  *   the grid kernel, 2 the cluster kernel (HME_EINVAL from a factorisation
- *   whose panel does not fit).  Tuning only: both give the same values. */
+ *   whose panel does not fit), 3 the cluster kernel with 1024 threads per CTA
+ *   (2 uses 512 while a CTA holds at most 512 rows).  Tuning only: every mode
+ *   gives the same outputs. */
 HME_API int hme_rref_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t *A, size_t lda,
                          uint32_t *pivots, uint32_t *rank);
 HME_API int hme_rref_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t *A, size_t lda,
