@@ -4,8 +4,9 @@
 //
 // The per-problem table lives in device memory: the TMA descriptors of each
 // problem's planes (CUtensorMap objects in global memory), C, ldc, the shape
-// and the op.  A CTA walks global tile indices; a binary search over the tile
-// prefix finds the problem of each tile.  Warp roles, pipeline, tensor-memory
+// and the op.  A CTA walks global tile indices; a per-tile table gives each
+// tile's problem in one load (a search over thousands of problems would be a
+// chain of dependent loads per tile, longer than a one-k-block tile's work).  Warp roles, pipeline, tensor-memory
 // double buffer and epilogue are those of limb_gemm_kernel.  This is the
 // batched path the reference lacks: its GemmBatch (src/Cuda/CudaKernels.h:
 // 141-185, cuda_kernels.cu:831-946) runs one launch per SAME-shape batch, so
@@ -44,26 +45,16 @@ struct GroupedProblem {
     int a_row0, b_col0;
 };
 
-__device__ __forceinline__ int find_problem(const GroupedProblem* __restrict__ probs, int nprob, int tile) {
-    int lo = 0, hi = nprob - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (probs[mid].tile_begin <= tile) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 __device__ __forceinline__ void grouped_drain(uint64_t* bar, uint32_t parity, int* err) {
     int never = 0;
     mbar_wait(bar, parity, &never, err, DERR_WAIT_DRAIN);
 }
 
-template <int L, int BN>
+template <int L, int BN, int KB>
 __global__ void __launch_bounds__(kThreads, 1)
-    grouped_limb_gemm_kernel(const GroupedProblem* __restrict__ probs, int nprob, int total_tiles, uint32_t p,
-                             uint64_t barrett, int* err) {
-    using CF = Cfg<L, BN>;
+    grouped_limb_gemm_kernel(const GroupedProblem* __restrict__ probs, const int* __restrict__ tile_prob,
+                             int total_tiles, uint32_t p, uint64_t barrett, int* err) {
+    using CF = Cfg<L, BN, KB>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
@@ -87,7 +78,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&acc_full[a], 1);
-            mbar_init(&acc_empty[a], 128);
+            mbar_init(&acc_empty[a], 32 * kEpiWarps);
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -108,7 +99,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             int it = 0;
             bool ok = true;
             for (int tile = blockIdx.x; ok && tile < total_tiles; tile += gridDim.x) {
-                const int pi = find_problem(probs, nprob, tile);
+                const int pi = tile_prob[tile];
                 const GroupedProblem& P = probs[pi];
                 const int local = tile - P.tile_begin;
                 const int tm = local / P.tiles_n, tn = local - tm * P.tiles_n;
@@ -121,8 +112,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                             break;
                         }
                         mbar_arrive_expect_tx(&full[s], CF::STAGE_BYTES);
-                        tma_load_3d(sA + s * CF::A_BYTES, P.tmA, &full[s], kb * kBK, P.a_row0 + tm * kBM, i);
-                        tma_load_4d(sB + s * CF::B_BYTES, P.tmB, &full[s], kb * kBK, P.b_col0 + tn * BN, 0, i);
+                        tma_load_3d(sA + s * CF::A_BYTES, P.tmA, &full[s], kb * KB, P.a_row0 + tm * kBM, i);
+                        tma_load_4d(sB + s * CF::B_BYTES, P.tmB, &full[s], kb * KB, P.b_col0 + tn * BN, 0, i);
                     }
                 }
             }
@@ -135,7 +126,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             int it = 0, lt = 0;
             bool ok = true, issued_any = false;
             for (int tile = blockIdx.x; ok && tile < total_tiles; tile += gridDim.x, ++lt) {
-                const int kblocks = probs[find_problem(probs, nprob, tile)].kblocks;
+                const int kblocks = probs[tile_prob[tile]].kblocks;
                 const int a = lt & 1;
                 const uint32_t aph = (lt >> 1) & 1;
                 if (!mbar_wait(&acc_empty[a], aph ^ 1, abort_flag, err, DERR_WAIT_ACCUM_FREE)) {
@@ -153,10 +144,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                             break;
                         }
                         tc_fence_after();
-                        const uint64_t adesc = smem_desc_k128(smem_u32(sA + s * CF::A_BYTES));
-                        const uint64_t bdesc = smem_desc_k128(smem_u32(sB + s * CF::B_BYTES));
+                        const uint64_t adesc = smem_desc_kmajor<KB>(smem_u32(sA + s * CF::A_BYTES));
+                        const uint64_t bdesc = smem_desc_kmajor<KB>(smem_u32(sB + s * CF::B_BYTES));
 #pragma unroll
-                        for (int kk = 0; kk < kBK / 32; ++kk)
+                        for (int kk = 0; kk < KB / 32; ++kk)
                             mma_u8(d, adesc + 2 * kk, bdesc + 2 * kk, CF::IDESC, (i | kb | kk) != 0);
                         issued_any = true;
                         mma_commit(&empty[s]);
@@ -173,19 +164,34 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int q = warp & 3;
         const uint32_t lane_base = static_cast<uint32_t>(q * 32) << 16;
         uint32_t (*stage)[17] = reinterpret_cast<uint32_t (*)[17]>(epi_stage + (warp - 2) * 32 * 17);
+        const int chalf = (warp - 2) >> 2;  // the two warps of a lane quarter take alternate 16-column chunks
         const int half = lane >> 4, col_in = lane & 15;
+        // Add / Sub read C: each lane prefetches its row of this warp's quarter of
+        // a tile into L2 one tile ahead, so the old values come from L2 and the
+        // HBM reads of the next tile overlap this tile's drain
+        auto prefetch_tile = [&](int t) {
+            if (t >= total_tiles) return;
+            const GroupedProblem& Q = probs[tile_prob[t]];
+            if (Q.op == HME_SET) return;
+            const int lq = t - Q.tile_begin;
+            const int qm = lq / Q.tiles_n, qn = lq - qm * Q.tiles_n;
+            const int row = qm * kBM + q * 32 + lane;
+            if (chalf == 0 && row < Q.M) prefetch_l2_span(Q.C + static_cast<size_t>(row) * Q.ldc + qn * BN, min(BN, Q.N - qn * BN));
+        };
+        prefetch_tile(blockIdx.x);
         int lt = 0;
         for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++lt) {
+            prefetch_tile(tile + gridDim.x);
             const int a = lt & 1;
             const uint32_t aph = (lt >> 1) & 1;
             if (!mbar_wait(&acc_full[a], aph, abort_flag, err, DERR_WAIT_ACCUM)) break;
             tc_fence_after();
-            const GroupedProblem& P = probs[find_problem(probs, nprob, tile)];
+            const GroupedProblem& P = probs[tile_prob[tile]];
             const int local = tile - P.tile_begin;
             const int tm = local / P.tiles_n, tn = local - tm * P.tiles_n;
             const int row0 = tm * kBM + q * 32;
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 16) {
+            for (int c0 = 16 * chalf; c0 < BN; c0 += 32) {
                 uint32_t v[L][16];
 #pragma unroll
                 for (int j = 0; j < L; ++j)
@@ -245,16 +251,11 @@ struct GroupedSplitJob {
 };
 
 template <int L>
-__global__ void __launch_bounds__(256) grouped_split_kernel(const GroupedSplitJob* __restrict__ jobs, int njobs) {
+__global__ void __launch_bounds__(256) grouped_split_kernel(const GroupedSplitJob* __restrict__ jobs,
+                                                            const int* __restrict__ block_job) {
     __shared__ uint32_t tile[64][33];
-    int lo = 0, hi = njobs - 1;
     const int b = blockIdx.x;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (jobs[mid].block_begin <= b) lo = mid;
-        else hi = mid - 1;
-    }
-    const GroupedSplitJob& J = jobs[lo];
+    const GroupedSplitJob& J = jobs[block_job[b]];
     const int local = b - J.block_begin;
     if (local < J.s.a_blocks)
         split_a_part<L>(J.s, local);
@@ -264,16 +265,18 @@ __global__ void __launch_bounds__(256) grouped_split_kernel(const GroupedSplitJo
 
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
-template <int L, int BN>
-void launch_grouped(hme_ctx* ctx, const ModParams& mp, const GroupedProblem* d_probs, int nprob, int total_tiles) {
-    using CF = Cfg<L, BN>;
+template <int L, int BN, int KB>
+void launch_grouped(hme_ctx* ctx, const ModParams& mp, const GroupedProblem* d_probs, const int* d_tile_prob,
+                    int total_tiles) {
+    using CF = Cfg<L, BN, KB>;
     static std::once_flag once;
     std::call_once(once, [] {
-        cudaFuncSetAttribute(grouped_limb_gemm_kernel<L, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM);
+        cudaFuncSetAttribute(grouped_limb_gemm_kernel<L, BN, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             CF::SMEM);
     });
     const int grid = std::min(total_tiles, ctx->num_sms);
-    HME_TIMED(ctx, "grouped_gemm", grouped_limb_gemm_kernel<L, BN><<<grid, kThreads, CF::SMEM, ctx->stream>>>(
-                                       d_probs, nprob, total_tiles, mp.p, mp.barrett, ctx->d_err));
+    HME_TIMED(ctx, "grouped_gemm", grouped_limb_gemm_kernel<L, BN, KB><<<grid, kThreads, CF::SMEM, ctx->stream>>>(
+                                       d_probs, d_tile_prob, total_tiles, mp.p, mp.barrett, ctx->d_err));
     HME_CUDA(cudaGetLastError());
 }
 
@@ -295,13 +298,19 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
     for (const GemmJob& j : jobs) tiles_wide += static_cast<size_t>((j.M + kBM - 1) / kBM) * ((j.N + BNw - 1) / BNw);
     const bool narrow = tiles_wide < static_cast<size_t>(ctx->num_sms);
     const int BN = narrow ? BNn : BNw;
+    // k-block: the narrowest swizzle row (32, 64 or 128 bytes) that holds every
+    // K of the launch (the rank rounds' updates have K = the round's pivots), so
+    // no zero padding is streamed or multiplied
+    uint32_t kmax = 0;
+    for (const GemmJob& j : jobs) kmax = std::max(kmax, j.K);
+    const int KBsel = kmax <= 32 ? 32 : kmax <= 64 ? 64 : kBK;
 
     // plane layout: problems bucketed by padded K; per bucket one stacked tensor
     // for the A planes (rows of all problems) and one for the B planes
     std::vector<int> kp_of(nj), bucket_of(nj);
     std::vector<int> bucket_kp;
     for (int t = 0; t < nj; ++t) {
-        kp_of[t] = static_cast<int>((jobs[t].K + kBK - 1) / kBK * kBK);
+        kp_of[t] = static_cast<int>((jobs[t].K + KBsel - 1) / KBsel * KBsel);
         auto it = std::find(bucket_kp.begin(), bucket_kp.end(), kp_of[t]);
         if (it == bucket_kp.end()) {
             bucket_of[t] = static_cast<int>(bucket_kp.size());
@@ -363,25 +372,34 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
     const size_t maps_bytes = sizeof(CUtensorMap) * 2 * static_cast<size_t>(nb);
     const size_t probs_bytes = sizeof(GroupedProblem) * static_cast<size_t>(nj);
     const size_t split_bytes = sizeof(GroupedSplitJob) * static_cast<size_t>(nj);
+    // per-tile problem and per-split-block job (tile counts known only after the layout)
+    size_t total_tiles = 0;
+    for (const GemmJob& j : jobs) total_tiles += static_cast<size_t>((j.M + kBM - 1) / kBM) * ((j.N + BN - 1) / BN);
+    HME_REQUIRE(total_tiles < (1u << 31) && static_cast<size_t>(blocks) < (1u << 31), "grouped gemm: too many tiles");
+    const size_t index_bytes = sizeof(int) * (total_tiles + static_cast<size_t>(blocks));
     uint8_t* tables = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs1, align256(maps_bytes) + align256(probs_bytes) +
-                                                                         align256(split_bytes)));
+                                                                         align256(split_bytes) + align256(index_bytes)));
     CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(tables);
     GroupedProblem* d_probs = reinterpret_cast<GroupedProblem*>(tables + align256(maps_bytes));
     GroupedSplitJob* d_split = reinterpret_cast<GroupedSplitJob*>(tables + align256(maps_bytes) + align256(probs_bytes));
+    int* d_tile_prob = reinterpret_cast<int*>(tables + align256(maps_bytes) + align256(probs_bytes) +
+                                              align256(split_bytes));
+    int* d_block_job = d_tile_prob + total_tiles;
     std::vector<CUtensorMap> maps(2 * static_cast<size_t>(nb));
     for (int b = 0; b < nb; ++b) {
         const cuuint64_t Kp = static_cast<cuuint64_t>(bucket_kp[b]);
         {
             const cuuint64_t dims[3] = {Kp, b_rows[b], static_cast<cuuint64_t>(L)};
             const cuuint64_t strides[2] = {Kp, Kp * b_rows[b]};
-            const cuuint32_t box[3] = {kBK, kBM, 1};
-            encode_tma_u8(&maps[2 * b], planes + offA[b], 3, dims, strides, box);
+            const cuuint32_t box[3] = {static_cast<cuuint32_t>(KBsel), kBM, 1};
+            encode_tma_u8_kb(&maps[2 * b], planes + offA[b], 3, dims, strides, box, KBsel);
         }
         {
             const cuuint64_t dims[4] = {Kp, b_cols[b], static_cast<cuuint64_t>(L), static_cast<cuuint64_t>(L)};
             const cuuint64_t strides[3] = {Kp, Kp * b_cols[b], Kp * b_cols[b] * L};
-            const cuuint32_t box[4] = {kBK, static_cast<cuuint32_t>(BN), static_cast<cuuint32_t>(L), 1};
-            encode_tma_u8(&maps[2 * b + 1], planes + offB[b], 4, dims, strides, box);
+            const cuuint32_t box[4] = {static_cast<cuuint32_t>(KBsel), static_cast<cuuint32_t>(BN),
+                                       static_cast<cuuint32_t>(L), 1};
+            encode_tma_u8_kb(&maps[2 * b + 1], planes + offB[b], 4, dims, strides, box, KBsel);
         }
     }
     std::vector<GroupedProblem> probs(nj);
@@ -395,7 +413,7 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
         P.ldc = j.ldc;
         P.M = static_cast<int>(j.M);
         P.N = static_cast<int>(j.N);
-        P.kblocks = kp_of[t] / kBK;
+        P.kblocks = kp_of[t] / KBsel;
         P.op = j.op;
         P.tiles_n = static_cast<int>((j.N + BN - 1) / BN);
         P.tile_begin = tiles;
@@ -406,10 +424,28 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
     HME_CUDA(cudaMemcpyAsync(d_maps, maps.data(), maps_bytes, cudaMemcpyHostToDevice, ctx->stream));
     HME_CUDA(cudaMemcpyAsync(d_probs, probs.data(), probs_bytes, cudaMemcpyHostToDevice, ctx->stream));
     HME_CUDA(cudaMemcpyAsync(d_split, split.data(), split_bytes, cudaMemcpyHostToDevice, ctx->stream));
-    HME_TIMED(ctx, "grouped_split", grouped_split_kernel<L><<<blocks, 256, 0, ctx->stream>>>(d_split, nj));
+    std::vector<int> index(total_tiles + static_cast<size_t>(blocks));
+    for (int t = 0; t < nj; ++t) {
+        const int nt = static_cast<int>((jobs[t].M + kBM - 1) / kBM) * probs[t].tiles_n;
+        std::fill(index.begin() + probs[t].tile_begin, index.begin() + probs[t].tile_begin + nt, t);
+        const int nbk = split[t].s.a_blocks + split[t].b_blocks;
+        std::fill(index.begin() + total_tiles + split[t].block_begin,
+                  index.begin() + total_tiles + split[t].block_begin + nbk, t);
+    }
+    HME_REQUIRE(static_cast<size_t>(tiles) == total_tiles, "grouped gemm: tile count mismatch");
+    HME_CUDA(cudaMemcpyAsync(d_tile_prob, index.data(), index_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    HME_TIMED(ctx, "grouped_split", grouped_split_kernel<L><<<blocks, 256, 0, ctx->stream>>>(d_split, d_block_job));
     HME_CUDA(cudaGetLastError());
-    if (narrow) launch_grouped<L, BNn>(ctx, mp, d_probs, nj, tiles);
-    else launch_grouped<L, BNw>(ctx, mp, d_probs, nj, tiles);
+    if (KBsel == 32) {
+        if (narrow) launch_grouped<L, BNn, 32>(ctx, mp, d_probs, d_tile_prob, tiles);
+        else launch_grouped<L, BNw, 32>(ctx, mp, d_probs, d_tile_prob, tiles);
+    } else if (KBsel == 64) {
+        if (narrow) launch_grouped<L, BNn, 64>(ctx, mp, d_probs, d_tile_prob, tiles);
+        else launch_grouped<L, BNw, 64>(ctx, mp, d_probs, d_tile_prob, tiles);
+    } else {
+        if (narrow) launch_grouped<L, BNn, kBK>(ctx, mp, d_probs, d_tile_prob, tiles);
+        else launch_grouped<L, BNw, kBK>(ctx, mp, d_probs, d_tile_prob, tiles);
+    }
     // the host tables must outlive the asynchronous uploads
     HME_CUDA(cudaStreamSynchronize(ctx->stream));
 }

@@ -14,21 +14,25 @@ namespace limb {
 
 constexpr int kBM = 128;     // UMMA M (rows of C per tile, one TMEM lane each)
 constexpr int kBK = 128;     // bytes of K per pipeline stage: one 128-byte swizzle row
-constexpr int kThreads = 192;
+constexpr int kEpiWarps = 8;                 // epilogue warps: two per TMEM lane quarter
+constexpr int kThreads = 64 + 32 * kEpiWarps;  // + the TMA warp and the MMA warp
 
-template <int L, int BN>
+// KB: bytes of K per pipeline stage = the width of one swizzle row (128, 64 or
+// 32; products whose K fits a narrower row stream no zero padding).
+template <int L, int BN, int KB = kBK>
 struct Cfg {
+    static_assert(KB == 128 || KB == 64 || KB == 32, "k-block of 128, 64 or 32 bytes");
     static constexpr int UN = L * BN;  // UMMA N: L accumulators of BN columns
     static_assert(UN % 16 == 0 && UN >= 16 && UN <= 256, "UMMA N must be a multiple of 16 in [16, 256]");
     static_assert(BN % 16 == 0, "the epilogue drains 16 columns at a time");
-    static constexpr int A_BYTES = kBM * kBK;
-    static constexpr int B_BYTES = UN * kBK;
+    static constexpr int A_BYTES = kBM * KB;
+    static constexpr int B_BYTES = UN * KB;
     static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-    static constexpr int STAGES = UN > 128 ? 4 : UN > 64 ? 6 : 8;
+    static constexpr int STAGES = (196608 / STAGE_BYTES) < 12 ? (196608 / STAGE_BYTES) : 12;
     static constexpr int ACC_STRIDE = UN <= 32 ? 32 : UN <= 64 ? 64 : UN <= 128 ? 128 : 256;
     static constexpr int TMEM_COLS = 2 * ACC_STRIDE;
     static constexpr int BAR_BYTES = 256;
-    static constexpr int EPI_BYTES = 4 * 32 * 17 * 4;  // per-warp 32 x 16 staging chunk (+1 column of padding)
+    static constexpr int EPI_BYTES = kEpiWarps * 32 * 17 * 4;  // per-warp 32 x 16 staging chunk (+1 column of padding)
     static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + BAR_BYTES + EPI_BYTES;
     static constexpr uint32_t IDESC = idesc_u8(kBM, UN);
     static_assert((2 * STAGES + 5) * 8 + 8 <= BAR_BYTES, "barrier area too small");
@@ -139,5 +143,8 @@ __device__ __forceinline__ void split_b_part(const SplitArgs& s, int block, uint
 // Host: encode a tiled uint8 TMA descriptor with 128-byte swizzle (limb planes).
 void encode_tma_u8(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
                    const cuuint32_t* box);
+// The same with the swizzle matching a k-block of kb bytes (128, 64 or 32).
+void encode_tma_u8_kb(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
+                      const cuuint32_t* box, int kb);
 
 }  // namespace hme

@@ -89,6 +89,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
     }
 }
 
+// ---- L2 prefetch ----------------------------------------------------------------
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+// Prefetch into L2 the 128-byte lines of w u32 values at p (one row segment).
+__device__ __forceinline__ void prefetch_l2_span(const uint32_t* p, int w) {
+    if (w <= 0) return;
+    const uintptr_t b = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(127);
+    const uintptr_t e = reinterpret_cast<uintptr_t>(p + w);
+    for (uintptr_t q = b; q < e; q += 128) prefetch_l2(reinterpret_cast<const void*>(q));
+}
+
 // ---- thread-block clusters: ranks and distributed shared memory ----
 __device__ __forceinline__ uint32_t cluster_ctarank() {
     uint32_t r;
@@ -218,6 +230,22 @@ __device__ __forceinline__ uint64_t smem_desc_k128(uint32_t smem_addr) {
     d |= static_cast<uint64_t>(1024 >> 4) << 32;
     d |= static_cast<uint64_t>(1) << 46;
     d |= static_cast<uint64_t>(2) << 61;
+    return d;
+}
+// The same for a K-major operand written by TMA with KB-byte swizzle (KB = 128,
+// 64 or 32): rows of KB bytes, 8-row atoms 8*KB bytes apart, layout type 2
+// (SWIZZLE_128B), 4 (SWIZZLE_64B) or 6 (SWIZZLE_32B).  Tile base aligned to the
+// atom (8*KB bytes).
+template <int KB>
+__device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t smem_addr) {
+    static_assert(KB == 128 || KB == 64 || KB == 32, "swizzle width");
+    constexpr uint64_t layout = KB == 128 ? 2 : KB == 64 ? 4 : 6;
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((smem_addr & 0x3FFFFu) >> 4);
+    d |= static_cast<uint64_t>(1) << 16;
+    d |= static_cast<uint64_t>((8 * KB) >> 4) << 32;
+    d |= static_cast<uint64_t>(1) << 46;
+    d |= layout << 61;
     return d;
 }
 // Instruction descriptor, kind::i8: s32 accumulator, unsigned 8-bit A and B,

@@ -21,6 +21,7 @@
 #include <mutex>
 #include <vector>
 
+#include "hme_elim.h"
 #include "hme_grouped.h"
 #include "hme_internal.h"
 #include "hme_ptx.cuh"
@@ -28,8 +29,8 @@
 namespace hme {
 namespace {
 
-constexpr int kRankThreads = 1024;
-constexpr int kMaxBw = 32;
+constexpr int kMaxBw = 128;   // panel columns per round (at most: a job's last panel)
+constexpr int kRoundBw = 32;  // panel columns of the rounds before a job's last panel
 constexpr int kRankSmem = 200 * 1024;
 
 __device__ __forceinline__ uint64_t splitmix_at(uint64_t seed, uint64_t i) {
@@ -39,31 +40,6 @@ __device__ __forceinline__ uint64_t splitmix_at(uint64_t seed, uint64_t i) {
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     return z ^ (z >> 31);
 }
-
-__device__ __forceinline__ uint32_t inv_xgcd(uint32_t u, uint32_t q) {
-    if (u == 0) return 0;
-    uint32_t a = u, b = q, x1 = 1, x2 = 0;
-    for (int it = 0; a != 1 && b != 1; ++it) {
-        if (a == 0 || b == 0 || it > 128) return 0;
-        while ((a & 1) == 0) {
-            a >>= 1;
-            x1 = (x1 & 1) ? static_cast<uint32_t>((static_cast<uint64_t>(x1) + q) >> 1) : x1 >> 1;
-        }
-        while ((b & 1) == 0) {
-            b >>= 1;
-            x2 = (x2 & 1) ? static_cast<uint32_t>((static_cast<uint64_t>(x2) + q) >> 1) : x2 >> 1;
-        }
-        if (a >= b) {
-            a -= b;
-            x1 = x1 >= x2 ? x1 - x2 : static_cast<uint32_t>(static_cast<uint64_t>(x1) + q - x2);
-        } else {
-            b -= a;
-            x2 = x2 >= x1 ? x2 - x1 : static_cast<uint32_t>(static_cast<uint64_t>(x2) + q - x1);
-        }
-    }
-    return a == 1 ? x1 : x2;
-}
-
 
 // ---- generator ----------------------------------------------------------------------
 struct GenJob {
@@ -103,8 +79,11 @@ struct RankJob {
     int m, n;
     uint32_t p;
     uint64_t barrett;
+    uint32_t qinv;  // p odd: -p^-1 mod 2^32 (Montgomery)
+    uint32_t r2;    // p odd: 2^64 mod p
     int r0, c0, w;  // active rows [r0, m), panel columns [c0, c0 + w)
-    int slot;       // index of the job's output slot
+    int slot;       // the job's index
+    int out;        // its output slot in this round (its position in the round's table)
 };
 
 struct RankOut {
@@ -113,80 +92,177 @@ struct RankOut {
     int pivot_cols[kMaxBw];
 };
 
-// One CTA per job: factor the panel A[r0:m, c0:c0+w) in shared memory (field
-// elimination, pivot = the topmost active row with a non-zero; pivot rows stay
-// in place and leave the active set; multipliers are stored in the pivot
-// columns), then write the panel back.
-__global__ void __launch_bounds__(kRankThreads) batch_panel_kernel(const RankJob* __restrict__ jobs,
-                                                                   RankOut* __restrict__ outs) {
-    extern __shared__ uint32_t sp[];  // rows x w panel, then flags
-    __shared__ int s_piv;
-    __shared__ uint32_t s_prow[kMaxBw];
-    __shared__ uint32_t s_inv;
-    __shared__ int s_k;
-    const RankJob J = jobs[blockIdx.x];
-    const int rows = J.m - J.r0, w = J.w;
-    unsigned char* isp = reinterpret_cast<unsigned char*>(sp + static_cast<size_t>(rows) * w);
-    for (int idx = threadIdx.x; idx < rows * w; idx += blockDim.x) {
-        const int i = idx / w, j = idx % w;
-        sp[idx] = J.A[static_cast<size_t>(J.r0 + i) * J.ld + J.c0 + j];
+// One CTA per job: factor the panel A[r0:m, c0:c0+w) in shared memory over
+// F_p (pivot = the topmost active row with a non-zero; pivot rows stay in place
+// and leave the active set; multipliers are stored in the pivot columns), then
+// write the panel back.  The panel is column-major in shared memory, rows over
+// consecutive threads (g threads per row).  Row updates are fraction-free:
+// row <- (w row - x pivot_row) * rho, w the pivot (rho = 2^-32 with one
+// Montgomery reduction per element for odd p < 2^31, else rho = 1), so no
+// column needs a modular inverse; every active row takes the same unit
+// factor w rho per pivot, and the panel is brought back to the classical
+// values once at the end (multipliers times w_t^-1, every other entry times
+// the inverse of the scale in force when the row left the active set or the
+// column was passed).  One CTA barrier per column: the candidate of column
+// c + 1 collects in a triple-buffered slot.
+__device__ __forceinline__ uint32_t batch_ff_update(bool mont, uint32_t w, uint32_t y, uint32_t xn, uint32_t pr,
+                                                    const RankJob& J) {
+    if (mont) {
+        const uint64_t t = static_cast<uint64_t>(w) * y + static_cast<uint64_t>(xn) * pr;  // < 2^63
+        const uint32_t mq = static_cast<uint32_t>(t) * J.qinv;
+        const uint32_t r = static_cast<uint32_t>((t + static_cast<uint64_t>(mq) * J.p) >> 32);
+        return r >= J.p ? r - J.p : r;
     }
-    for (int i = threadIdx.x; i < rows; i += blockDim.x) isp[i] = 0;
-    if (threadIdx.x == 0) s_k = 0;
-    __syncthreads();
-    for (int jc = 0; jc < w; ++jc) {
-        if (threadIdx.x == 0) s_piv = INT_MAX;
-        __syncthreads();
-        for (int i = threadIdx.x; i < rows; i += blockDim.x)
-            if (!isp[i] && sp[i * w + jc] != 0) atomicMin(&s_piv, i);
-        __syncthreads();
-        const int pr = s_piv;
-        if (pr == INT_MAX) continue;
-        for (int j = threadIdx.x; j < w; j += blockDim.x) s_prow[j] = sp[pr * w + j];
-        if (threadIdx.x == 0) {
-            isp[pr] = 1;
-            s_inv = inv_xgcd(sp[pr * w + jc], J.p);
-            RankOut& o = outs[J.slot];
-            o.pivot_rows[s_k] = J.r0 + pr;
-            o.pivot_cols[s_k] = J.c0 + jc;
-            ++s_k;
-        }
-        __syncthreads();
-        const uint32_t inv = s_inv;
-        const int width = w - jc - 1;
-        // multipliers, then the (row, column) updates
-        for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-            if (isp[i]) continue;
-            const uint32_t x = sp[i * w + jc];
-            if (x != 0) sp[i * w + jc] = mod_mul(x, inv, J.p, J.barrett);
-        }
-        __syncthreads();
-        if (width > 0) {
-            for (int e = threadIdx.x; e < rows * width; e += blockDim.x) {
-                const int i = e / width, j = jc + 1 + e % width;
-                if (isp[i]) continue;
-                const uint32_t l = sp[i * w + jc];
-                if (l == 0) continue;
-                sp[i * w + j] = mod_sub(sp[i * w + j], mod_mul(l, s_prow[j], J.p, J.barrett), J.p);
-            }
-        }
-        __syncthreads();
-    }
-    for (int idx = threadIdx.x; idx < rows * w; idx += blockDim.x) {
-        const int i = idx / w, j = idx % w;
-        J.A[static_cast<size_t>(J.r0 + i) * J.ld + J.c0 + j] = sp[idx];
-    }
-    if (threadIdx.x == 0) outs[J.slot].k = s_k;
+    return mod_add(mod_mul(w, y, J.p, J.barrett), mod_mul(xn, pr, J.p, J.barrett), J.p);
 }
 
-// Row permutation of columns [c0, n) for rows [r0, m): pivot rows first (in
-// pivot order), then the other rows in order.  Per job a permutation segment
-// in `perm` (absolute row indices) and a scratch segment in `tmp`.
+template <int NT>
+__global__ void __launch_bounds__(NT) batch_panel_kernel(const RankJob* __restrict__ jobs, RankOut* __restrict__ outs,
+                                                         int* err) {
+    extern __shared__ uint32_t sp[];  // [w][rs] column-major panel, then a step byte per row
+    __shared__ int s_cand[3];
+    __shared__ uint32_t s_w[kMaxBw], s_inv[kMaxBw], s_sinv[kMaxBw + 1];
+    __shared__ int s_colstep[kMaxBw], s_prow[kMaxBw], s_pcol[kMaxBw];
+    const RankJob J = jobs[blockIdx.x];
+    const int rows = J.m - J.r0, w = J.w, rs = rows | 1;
+    uint32_t* S = sp;
+    unsigned char* s_step = reinterpret_cast<unsigned char*>(S + static_cast<size_t>(w) * rs);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NT / 32;
+    constexpr int NONE = INT_MAX;
+    int lg = 0;
+    while ((1 << lg) < rows) ++lg;
+    if ((1 << lg) > NT) {  // the host never launches this; uniform for the CTA
+        if (tid == 0) atomicCAS(err, 0, DERR_LAUNCH_SHAPE);
+        return;
+    }
+    const int nslots = 1 << lg, g = NT >> lg;
+    const int li = tid & (nslots - 1), sub = tid >> lg;
+    const bool has_row = li < rows;
+    const bool mont = (J.p & 1u) && J.p < (1u << 31);
+
+    for (int r = warp; r < rows; r += NW) {
+        const uint32_t* src = J.A + static_cast<size_t>(J.r0 + r) * J.ld + J.c0;
+        for (int j = lane; j < w; j += 32) S[j * rs + r] = src[j];
+    }
+    for (int i = tid; i < rows; i += NT) s_step[i] = 0;
+    if (tid < 3) s_cand[tid] = NONE;
+    __syncthreads();
+    {
+        int key = (has_row && sub == 0 && S[li] != 0) ? li : NONE;
+        key = __reduce_min_sync(0xffffffffu, key);
+        if (lane == 0 && key != NONE) atomicMin(&s_cand[0], key);
+    }
+    __syncthreads();
+    int k = 0;
+    for (int it = 0; it < w; ++it) {
+        const int cur = it % 3, nxt = (it + 1) % 3;
+        const int piv = s_cand[cur];
+        if (tid == 0) s_cand[(it + 2) % 3] = NONE;  // last read in step it - 1, next written in step it + 1
+        int key = NONE;
+        if (piv == NONE) {
+            if (tid == 0) s_colstep[it] = -1 - k;
+            if (it + 1 < w && has_row && sub == 0 && s_step[li] == 0 && S[(it + 1) * rs + li] != 0) key = li;
+        } else {
+            const uint32_t wt = S[it * rs + piv];
+            if (tid == 0) {
+                s_w[k] = wt;
+                s_colstep[it] = k;
+                s_prow[k] = piv;
+                s_pcol[k] = it;
+                s_step[piv] = static_cast<unsigned char>(k + 1);
+            }
+            if (has_row && li != piv && s_step[li] == 0) {
+                const uint32_t xp = S[it * rs + li];
+                const uint32_t xn = xp == 0 ? 0u : J.p - xp;
+                for (int j = it + 1 + sub; j < w; j += g) {
+                    const uint32_t y = batch_ff_update(mont, wt, S[j * rs + li], xn, S[j * rs + piv], J);
+                    S[j * rs + li] = y;
+                    if (j == it + 1 && y != 0) key = li;
+                }
+            }
+            ++k;
+        }
+        key = __reduce_min_sync(0xffffffffu, key);
+        if (lane == 0 && key != NONE) atomicMin(&s_cand[nxt], key);
+        __syncthreads();
+    }
+    // ---- classical values back: w_t^-1 and the prefix products of (w_s rho)^-1
+    for (int t = tid; t < k; t += NT) {
+        // Fermat: w^(p-2) mod p (p prime)
+        uint32_t b = s_w[t], e = J.p - 2, r = 1u % J.p;
+        while (e) {
+            if (e & 1u) r = mod_mul(r, b, J.p, J.barrett);
+            b = mod_mul(b, b, J.p, J.barrett);
+            e >>= 1;
+        }
+        s_inv[t] = r;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // exclusive prefix products of f_t = w_t^-1 rho^-1, four consecutive t per lane
+        const uint32_t one = 1u % J.p;
+        const uint32_t rinv = mont ? static_cast<uint32_t>((1ull << 32) % J.p) : one;  // rho^-1
+        constexpr int per = kMaxBw / 32;
+        uint32_t f[per];
+        uint32_t run = one;
+#pragma unroll
+        for (int e = 0; e < per; ++e) {
+            const int t = lane * per + e;
+            f[e] = t < k ? mod_mul(s_inv[t], rinv, J.p, J.barrett) : one;
+            run = mod_mul(run, f[e], J.p, J.barrett);
+        }
+        uint32_t incl = run;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl = mod_mul(incl, y, J.p, J.barrett);
+        }
+        uint32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) ex = one;
+#pragma unroll
+        for (int e = 0; e < per; ++e) {
+            s_sinv[lane * per + e] = ex;
+            ex = mod_mul(ex, f[e], J.p, J.barrett);
+        }
+        if (lane == 31) s_sinv[kMaxBw] = ex;
+    }
+    __syncthreads();
+    if (has_row) {
+        const int st = s_step[li];
+        const int tau = st ? st - 1 : k;
+        const uint32_t sc = s_sinv[tau];
+        for (int j = sub; j < w; j += g) {
+            const int t = s_colstep[j];
+            const uint32_t f = t >= 0 ? (t < tau ? s_inv[t] : sc) : s_sinv[min(tau, -1 - t)];
+            S[j * rs + li] = mod_mul(S[j * rs + li], f, J.p, J.barrett);
+        }
+    }
+    __syncthreads();
+    for (int r = warp; r < rows; r += NW) {
+        uint32_t* dst = J.A + static_cast<size_t>(J.r0 + r) * J.ld + J.c0;
+        for (int j = lane; j < w; j += 32) dst[j] = S[j * rs + r];
+    }
+    if (tid == 0) {
+        RankOut& o = outs[J.out];
+        for (int t = 0; t < k; ++t) {
+            o.pivot_rows[t] = J.r0 + s_prow[t];
+            o.pivot_cols[t] = J.c0 + s_pcol[t];
+        }
+        o.k = k;
+    }
+}
+
+// Row moves of columns [c0, n): the pivot rows go to rows r0 .. r0+k-1 by
+// swaps (a rank needs no particular order of the other rows), so at most 2k
+// rows move: row dst[i] receives the old row src[i].  Per job a segment of the
+// src / dst lists and a scratch segment in `tmp`.
 struct PermJob {
     uint32_t* A;
     uint64_t ld;
-    int r0, rows, c0, cols;
-    const int* perm;
+    int rows, c0, cols;  // rows = rows that move
+    const int* src;
+    const int* dst;
     uint32_t* tmp;
 };
 __global__ void batch_gather_rows_kernel(const PermJob* __restrict__ jobs) {
@@ -195,7 +271,7 @@ __global__ void batch_gather_rows_kernel(const PermJob* __restrict__ jobs) {
     for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
          idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
         const int i = static_cast<int>(idx / J.cols), j = static_cast<int>(idx % J.cols);
-        J.tmp[idx] = J.A[static_cast<size_t>(J.perm[i]) * J.ld + J.c0 + j];
+        J.tmp[idx] = J.A[static_cast<size_t>(J.src[i]) * J.ld + J.c0 + j];
     }
 }
 __global__ void batch_scatter_rows_kernel(const PermJob* __restrict__ jobs) {
@@ -204,7 +280,7 @@ __global__ void batch_scatter_rows_kernel(const PermJob* __restrict__ jobs) {
     for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
          idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
         const int i = static_cast<int>(idx / J.cols), j = static_cast<int>(idx % J.cols);
-        J.A[static_cast<size_t>(J.r0 + i) * J.ld + J.c0 + j] = J.tmp[idx];
+        J.A[static_cast<size_t>(J.dst[i]) * J.ld + J.c0 + j] = J.tmp[idx];
     }
 }
 
@@ -217,28 +293,74 @@ struct SolveJob {
     int r0, k, m, c1, ntrail;
     uint32_t p;
     uint64_t barrett;
-    int pcols[kMaxBw];
-    uint32_t* L21;  // (m - r0 - k) x k
+    const int* pcols;  // the panel's pivot columns (in the device copy of the panel's output)
+    uint32_t* L21;     // (m - r0 - k) x k
 };
-__global__ void batch_trsm_kernel(const SolveJob* __restrict__ jobs) {
-    __shared__ uint32_t sL[kMaxBw * kMaxBw];
+// One warp per trailing column: lane l holds rows l, l+32, l+64, l+96 (k <= 128);
+// at step t the value of row t is final and a shuffle broadcasts it.  The
+// columns of a 32-column tile go through shared memory so the global accesses
+// run along rows; L11 (k x k, odd row stride) in dynamic shared memory.
+constexpr int kBatchTrsmCols = 32;
+size_t batch_trsm_smem(int k) {
+    return sizeof(uint32_t) * (static_cast<size_t>(k) * (k | 1) + static_cast<size_t>(k) * (kBatchTrsmCols + 1));
+}
+__global__ void __launch_bounds__(256) batch_trsm_kernel(const SolveJob* __restrict__ jobs) {
+    extern __shared__ uint32_t smem_bt[];
     const SolveJob& J = jobs[blockIdx.y];
     const int k = J.k;
+    if (k < 2) return;  // the test is the same for the whole CTA
+    const int ls = k | 1;
+    constexpr int xs = kBatchTrsmCols + 1;
+    uint32_t* sL = smem_bt;
+    uint32_t* sX = smem_bt + k * ls;
     for (int idx = threadIdx.x; idx < k * k; idx += blockDim.x) {
         const int t = idx / k, s = idx % k;
-        sL[idx] = s < t ? J.A[static_cast<size_t>(J.r0 + t) * J.ld + J.pcols[s]] : 0u;
+        sL[t * ls + s] = s < t ? J.A[static_cast<size_t>(J.r0 + t) * J.ld + J.pcols[s]] : 0u;
     }
-    __syncthreads();
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < J.ntrail; j += gridDim.x * blockDim.x) {
-        uint32_t* col = J.A + static_cast<size_t>(J.r0) * J.ld + J.c1 + j;
-        for (int t = 1; t < k; ++t) {
-            uint32_t sub = 0;
-            for (int s = 0; s < t; ++s) {
-                const uint32_t l = sL[t * k + s];
-                if (l) sub = mod_add(sub, mod_mul(l, col[static_cast<size_t>(s) * J.ld], J.p, J.barrett), J.p);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    constexpr int per = kMaxBw / 32;
+    for (int c0 = blockIdx.x * kBatchTrsmCols; c0 < J.ntrail; c0 += gridDim.x * kBatchTrsmCols) {
+        const int nc = min(kBatchTrsmCols, J.ntrail - c0);
+        __syncthreads();  // sL ready / the previous tile written back
+        for (int idx = threadIdx.x; idx < k * kBatchTrsmCols; idx += blockDim.x) {
+            const int r = idx / kBatchTrsmCols, c = idx % kBatchTrsmCols;
+            if (c < nc) sX[r * xs + c] = J.A[static_cast<size_t>(J.r0 + r) * J.ld + J.c1 + c0 + c];
+        }
+        __syncthreads();
+        for (int c = warp; c < nc; c += nw) {
+            uint32_t x[per];
+#pragma unroll
+            for (int q = 0; q < per; ++q) {
+                const int r = lane + 32 * q;
+                x[q] = r < k ? sX[r * xs + c] : 0u;
             }
-            uint32_t* x = col + static_cast<size_t>(t) * J.ld;
-            *x = mod_sub(*x, sub, J.p);
+#pragma unroll
+            for (int qt = 0; qt < per; ++qt) {
+                if (32 * qt >= k - 1) break;
+                for (int tt = 0; tt < 32; ++tt) {
+                    const int t = 32 * qt + tt;
+                    if (t >= k - 1) break;
+                    const uint32_t xt = __shfl_sync(0xffffffffu, x[qt], tt);
+#pragma unroll
+                    for (int q = qt; q < per; ++q) {
+                        const int r = lane + 32 * q;
+                        if (r > t && r < k) {
+                            const uint32_t l = sL[r * ls + t];
+                            if (l) x[q] = reduce_u64(static_cast<uint64_t>(J.p - l) * xt + x[q], J.p, J.barrett);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < per; ++q) {
+                const int r = lane + 32 * q;
+                if (r < k) sX[r * xs + c] = x[q];
+            }
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < k * kBatchTrsmCols; idx += blockDim.x) {
+            const int r = idx / kBatchTrsmCols, c = idx % kBatchTrsmCols;
+            if (c < nc) J.A[static_cast<size_t>(J.r0 + r) * J.ld + J.c1 + c0 + c] = sX[r * xs + c];
         }
     }
 }
@@ -261,7 +383,12 @@ size_t a256(size_t x) { return (x + 255) / 256 * 256; }
 void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::vector<int>& ranks) {
     static std::once_flag once;
     std::call_once(once, [] {
-        cudaFuncSetAttribute(batch_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
+        cudaFuncSetAttribute(batch_panel_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
+        cudaFuncSetAttribute(batch_panel_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
+        cudaFuncSetAttribute(batch_panel_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
+        cudaFuncSetAttribute(batch_panel_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
+        cudaFuncSetAttribute(batch_trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(batch_trsm_smem(kMaxBw)));
     });
     const int nj = static_cast<int>(mats.size());
     ranks.assign(nj, 0);
@@ -276,69 +403,145 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
         J.n = static_cast<int>(M.n);
         J.p = M.p;
         J.barrett = make_mod(M.p).barrett;
+        if (M.p & 1u) {
+            uint32_t x = M.p;  // p^-1 mod 2^32 by Newton's iteration
+            for (int i = 0; i < 5; ++i) x *= 2u - M.p * x;
+            J.qinv = 0u - x;
+            J.r2 = static_cast<uint32_t>((static_cast<unsigned __int128>(1) << 64) % M.p);
+        }
         J.r0 = 0;
         J.c0 = 0;
         // the panel (m - r0) x w must fit shared memory
-        const int wmax = static_cast<int>(std::min<size_t>(kMaxBw, (kRankSmem - 4096) / (5 * std::max<size_t>(1, M.m))));
-        HME_REQUIRE(wmax >= 1, "batch rank: matrix too tall for the shared-memory panel");
-        J.w = wmax;
+        J.w = 0;  // set per round from the active rows
         J.slot = j;
     }
     RankOut* d_out = static_cast<RankOut*>(ctx->ws.get(kSlotJobs2, sizeof(RankOut) * static_cast<size_t>(nj) + 256));
-    std::vector<RankOut> h_out(nj);
+    // the per-round panel outputs come back into pinned host memory (up to ~1 KB per job)
+    struct PinnedOut {
+        RankOut* p = nullptr;
+        ~PinnedOut() {
+            if (p) cudaFreeHost(p);
+        }
+    } pinned;
+    HME_CUDA(cudaMallocHost(reinterpret_cast<void**>(&pinned.p), sizeof(RankOut) * std::max(1, nj)));
+    RankOut* h_out = pinned.p;
+    std::vector<int> scratch_content, scratch_where;
     std::vector<int> active;
     for (int j = 0; j < nj; ++j)
-        if (st[j].m > 0 && st[j].n > 0) active.push_back(j);
+        if (st[j].m > 1024 && st[j].n > 0) {
+            // taller than one panel CTA holds: the single-matrix elimination (cluster / grid panels)
+            ElimOptions o = ctx->elim;
+            const ElimResult r = elim_device(ctx, make_mod(st[j].p), st[j].A, st[j].ld, st[j].m, st[j].n, false,
+                                             nullptr, 0, o);
+            st[j].r0 = r.rank;
+        } else if (st[j].m > 0 && st[j].n > 0) {
+            active.push_back(j);
+        }
     while (!active.empty()) {
-        // (1) panels of every active job
+        // (1) panels of every active job, in buckets of active rows: each bucket
+        // launches with the threads and shared memory its largest panel needs
+        constexpr int kBuckets = 4;
+        constexpr int bucket_threads[kBuckets] = {128, 256, 512, 1024};
+        auto bucket_of = [&](int rows) { return rows <= 64 ? 0 : rows <= 128 ? 1 : rows <= 256 ? 2 : 3; };
         std::vector<RankJob> round;
         round.reserve(active.size());
-        size_t max_smem = 0;
+        int bcount[kBuckets] = {0, 0, 0, 0};
+        size_t bsmem[kBuckets] = {0, 0, 0, 0};
         for (int j : active) {
             RankJob J = st[j];
-            J.w = std::min(J.w, J.n - J.c0);
+            const int rows = J.m - J.r0;
+            // the job's remaining columns in one last panel when they fit the shared memory
+            // (up to kMaxBw: no trailing update at all), else a kRoundBw-column panel (a
+            // wider one would grow the CUDA-core panel and pivot-block solve work, which
+            // scale with the width, faster than it saves trailing-update traffic)
+            const size_t wfit = (kRankSmem - static_cast<size_t>(rows) - 16) / (sizeof(uint32_t) * (rows | 1));
+            const size_t left = static_cast<size_t>(J.n - J.c0);
+            J.w = static_cast<int>(left <= std::min<size_t>(kMaxBw, wfit) ? left
+                                                                          : std::min<size_t>(kRoundBw, wfit));
+            HME_REQUIRE(J.w >= 1 && rows <= 1024, "batch rank: matrix too tall for the shared-memory panel");
+            const int b = bucket_of(rows);
+            ++bcount[b];
+            bsmem[b] = std::max(bsmem[b], sizeof(uint32_t) * static_cast<size_t>(J.w) * (rows | 1) + rows + 16);
             round.push_back(J);
-            max_smem = std::max(max_smem, static_cast<size_t>(J.m - J.r0) * J.w * 4 + (J.m - J.r0) + 16);
         }
+        std::stable_sort(round.begin(), round.end(), [&](const RankJob& x, const RankJob& y) {
+            return bucket_of(x.m - x.r0) < bucket_of(y.m - y.r0);
+        });
+        for (size_t t = 0; t < round.size(); ++t) round[t].out = static_cast<int>(t);
         RankJob* d_jobs = static_cast<RankJob*>(ctx->ws.get(kSlotJobs3, sizeof(RankJob) * round.size() + 256));
         HME_CUDA(cudaMemcpyAsync(d_jobs, round.data(), sizeof(RankJob) * round.size(), cudaMemcpyHostToDevice,
                                  ctx->stream));
-        HME_TIMED(ctx, "batch_panel", batch_panel_kernel<<<static_cast<int>(round.size()), kRankThreads, max_smem,
-                                                           ctx->stream>>>(d_jobs, d_out));
-        HME_CUDA(cudaGetLastError());
-        HME_CUDA(cudaMemcpyAsync(h_out.data(), d_out, sizeof(RankOut) * nj, cudaMemcpyDeviceToHost, ctx->stream));
+        for (int b = 0, off = 0; b < kBuckets; off += bcount[b], ++b) {
+            if (!bcount[b]) continue;
+            const RankJob* dj = d_jobs + off;
+            switch (bucket_threads[b]) {
+                case 128: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<128><<<bcount[b], 128, bsmem[b], ctx->stream>>>(dj, d_out, ctx->d_err)); break;
+                case 256: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<256><<<bcount[b], 256, bsmem[b], ctx->stream>>>(dj, d_out, ctx->d_err)); break;
+                case 512: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<512><<<bcount[b], 512, bsmem[b], ctx->stream>>>(dj, d_out, ctx->d_err)); break;
+                default: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<1024><<<bcount[b], 1024, bsmem[b], ctx->stream>>>(dj, d_out, ctx->d_err)); break;
+            }
+            HME_CUDA(cudaGetLastError());
+        }
+        HME_CUDA(cudaMemcpyAsync(h_out, d_out, sizeof(RankOut) * round.size(), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
         HME_CUDA(cudaStreamSynchronize(ctx->stream));
         // (2) row permutations, (3) solves, (4) trailing updates, per job with pivots
         std::vector<PermJob> perms;
-        std::vector<int> perm_rows;
+        std::vector<int> perm_rows, perm_dst;
         std::vector<SolveJob> solves;
         size_t tmp_elems = 0, l21_elems = 0;
         std::vector<size_t> tmp_off, perm_off, l21_off;
         for (const RankJob& J : round) {
-            const RankOut& o = h_out[J.slot];
-            if (o.k == 0) continue;
+            const RankOut& o = h_out[J.out];
+            // no pivots, or the job's last panel (no columns right of it): nothing to move or update
+            if (o.k == 0 || J.c0 + J.w >= J.n) continue;
             const int rows = J.m - J.r0, cols = J.n - J.c0;
-            // pivot rows first, in pivot order; skipped when they already are
-            bool identity = true;
-            for (int t = 0; t < o.k; ++t) identity = identity && o.pivot_rows[t] == J.r0 + t;
+            // the pivot rows to r0 .. r0+k-1 by swaps; only rows whose content changes move
             PermJob pj{};
             pj.A = J.A;
             pj.ld = J.ld;
-            pj.r0 = J.r0;
-            pj.rows = identity ? 0 : rows;
             pj.c0 = J.c0;
             pj.cols = cols;
             perm_off.push_back(perm_rows.size());
             tmp_off.push_back(tmp_elems);
-            if (!identity) {
-                std::vector<char> isp(rows, 0);
+            {
+                // content[pos] = original row now at pos; where[orig] = its position (touched rows only)
+                std::vector<int>& content = scratch_content;
+                std::vector<int>& where = scratch_where;
+                content.resize(rows);
+                where.resize(rows);
                 for (int t = 0; t < o.k; ++t) {
-                    perm_rows.push_back(o.pivot_rows[t]);
-                    isp[o.pivot_rows[t] - J.r0] = 1;
+                    const int a = t, b0 = o.pivot_rows[t] - J.r0;
+                    content[a] = a;
+                    where[a] = a;
+                    content[b0] = b0;
+                    where[b0] = b0;
                 }
-                for (int i = 0; i < rows; ++i)
-                    if (!isp[i]) perm_rows.push_back(J.r0 + i);
-                tmp_elems += a256(static_cast<size_t>(rows) * cols);
+                for (int t = 0; t < o.k; ++t) {
+                    const int a = t, b = where[o.pivot_rows[t] - J.r0];
+                    if (a == b) continue;
+                    const int ca = content[a], cb = content[b];
+                    content[a] = cb;
+                    content[b] = ca;
+                    where[cb] = a;
+                    where[ca] = b;
+                }
+                int moved = 0;
+                std::vector<int> touched;
+                for (int t = 0; t < o.k; ++t) {
+                    touched.push_back(t);
+                    touched.push_back(o.pivot_rows[t] - J.r0);
+                }
+                std::sort(touched.begin(), touched.end());
+                touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+                for (int pos : touched)
+                    if (content[pos] != pos) {
+                        perm_rows.push_back(J.r0 + content[pos]);  // src
+                        perm_dst.push_back(J.r0 + pos);             // dst
+                        ++moved;
+                    }
+                pj.rows = moved;
+                if (moved) tmp_elems += a256(static_cast<size_t>(moved) * cols);
             }
             perms.push_back(pj);
             SolveJob sj{};
@@ -351,36 +554,43 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
             sj.ntrail = J.n - sj.c1;
             sj.p = J.p;
             sj.barrett = J.barrett;
-            for (int t = 0; t < o.k; ++t) sj.pcols[t] = o.pivot_cols[t];
+            sj.pcols = d_out[J.out].pivot_cols;
             solves.push_back(sj);
             l21_off.push_back(l21_elems);
             l21_elems += a256(static_cast<size_t>(J.m - J.r0 - o.k) * o.k);
         }
         if (!perms.empty()) {
             const int np = static_cast<int>(perms.size());
-            int* d_perm = static_cast<int*>(ctx->ws.get(kSlotJobs4, sizeof(int) * perm_rows.size() + 256));
+            int* d_perm = static_cast<int*>(ctx->ws.get(kSlotJobs4, 2 * sizeof(int) * perm_rows.size() + 256));
+            int* d_dst = d_perm + perm_rows.size();
             uint32_t* d_tmp = static_cast<uint32_t*>(ctx->ws.get(kSlotJobs5, sizeof(uint32_t) * tmp_elems + 256));
             uint32_t* d_l21 = static_cast<uint32_t*>(ctx->ws.get(kSlotJobs6, sizeof(uint32_t) * l21_elems + 256));
             for (int t = 0; t < np; ++t) {
-                perms[t].perm = d_perm + perm_off[t];
+                perms[t].src = d_perm + perm_off[t];
+                perms[t].dst = d_dst + perm_off[t];
                 perms[t].tmp = d_tmp + tmp_off[t];
                 solves[t].L21 = d_l21 + l21_off[t];
             }
             uint8_t* tab = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs7, a256(sizeof(PermJob) * np) + a256(sizeof(SolveJob) * np)));
             PermJob* d_pj = reinterpret_cast<PermJob*>(tab);
             SolveJob* d_sj = reinterpret_cast<SolveJob*>(tab + a256(sizeof(PermJob) * np));
-            if (!perm_rows.empty())
+            if (!perm_rows.empty()) {
+                perm_rows.insert(perm_rows.end(), perm_dst.begin(), perm_dst.end());
                 HME_CUDA(cudaMemcpyAsync(d_perm, perm_rows.data(), sizeof(int) * perm_rows.size(),
                                          cudaMemcpyHostToDevice, ctx->stream));
+            }
             HME_CUDA(cudaMemcpyAsync(d_pj, perms.data(), sizeof(PermJob) * np, cudaMemcpyHostToDevice, ctx->stream));
             HME_CUDA(cudaMemcpyAsync(d_sj, solves.data(), sizeof(SolveJob) * np, cudaMemcpyHostToDevice, ctx->stream));
+            int kmax = 1;
+            for (const SolveJob& sj : solves) kmax = std::max(kmax, sj.k);
+            const size_t trsm_smem = batch_trsm_smem(kmax);
             // grid.y = job (<= 65535 per launch: chunked)
             for (int b0 = 0; b0 < np; b0 += 65535) {
                 const int nb = std::min(65535, np - b0);
                 const dim3 g(32, nb);
                 HME_TIMED(ctx, "batch_permute", batch_gather_rows_kernel<<<g, 256, 0, ctx->stream>>>(d_pj + b0));
                 HME_TIMED(ctx, "batch_permute", batch_scatter_rows_kernel<<<g, 256, 0, ctx->stream>>>(d_pj + b0));
-                HME_TIMED(ctx, "batch_trsm", batch_trsm_kernel<<<dim3(8, nb), 128, 0, ctx->stream>>>(d_sj + b0));
+                HME_TIMED(ctx, "batch_trsm", batch_trsm_kernel<<<dim3(32, nb), 256, trsm_smem, ctx->stream>>>(d_sj + b0));
                 HME_TIMED(ctx, "batch_gather", batch_gather_l21_kernel<<<dim3(16, nb), 256, 0, ctx->stream>>>(d_sj + b0));
             }
             HME_CUDA(cudaGetLastError());
@@ -415,7 +625,7 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
         std::vector<int> next;
         for (const RankJob& J : round) {
             RankJob& S = st[J.slot];
-            const int k = h_out[J.slot].k;
+            const int k = h_out[J.out].k;
             S.r0 += k;
             S.c0 += J.w;
             if (S.r0 < S.m && S.c0 < S.n) next.push_back(J.slot);

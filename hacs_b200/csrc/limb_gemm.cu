@@ -22,9 +22,10 @@
 // B planes [i][j][n][k] (L x L x N x Kp bytes), K contiguous (K-major for both
 // tensor-core operands), Kp = K rounded up to 16 bytes for TMA strides.
 //
-// Kernel: persistent, one CTA per SM, 6 warps: warp 0 issues TMA loads
+// Kernel: persistent, one CTA per SM, 10 warps: warp 0 issues TMA loads
 // (128-byte swizzle, no multicast), warp 1 owns tensor memory and issues the
-// MMAs, warps 2-5 drain the double-buffered accumulator (2 x L*BN columns of
+// MMAs, warps 2-9 (two per TMEM lane quarter, alternate 16-column chunks)
+// drain the double-buffered accumulator (2 x L*BN columns of
 // TMEM) into C while the next tile's MMAs run.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -73,11 +74,11 @@ __device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity, int* 
     mbar_wait(bar, parity, &never, err, DERR_WAIT_DRAIN);
 }
 
-template <int L, int BN>
+template <int L, int BN, int KB = kBK>
 __global__ void __launch_bounds__(kThreads, 1)
     limb_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const GemmArgs g) {
-    using CF = Cfg<L, BN>;
+    using CF = Cfg<L, BN, KB>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
@@ -102,7 +103,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&acc_full[a], 1);
-            mbar_init(&acc_empty[a], 128);
+            mbar_init(&acc_empty[a], 32 * kEpiWarps);
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                             break;
                         }
                         mbar_arrive_expect_tx(&full[s], CF::STAGE_BYTES);
-                        const int kx = g.k_begin + kb * kBK;
+                        const int kx = g.k_begin + kb * KB;
                         tma_load_3d(sA + s * CF::A_BYTES, &tmA, &full[s], kx, tm * kBM, i);
                         tma_load_4d(sB + s * CF::B_BYTES, &tmB, &full[s], kx, tn * BN, 0, i);
                     }
@@ -177,10 +178,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                             break;
                         }
                         tc_fence_after();
-                        const uint64_t adesc = smem_desc_k128(smem_u32(sA + s * CF::A_BYTES));
-                        const uint64_t bdesc = smem_desc_k128(smem_u32(sB + s * CF::B_BYTES));
+                        const uint64_t adesc = smem_desc_kmajor<KB>(smem_u32(sA + s * CF::A_BYTES));
+                        const uint64_t bdesc = smem_desc_kmajor<KB>(smem_u32(sB + s * CF::B_BYTES));
 #pragma unroll
-                        for (int kk = 0; kk < kBK / 32; ++kk) {
+                        for (int kk = 0; kk < KB / 32; ++kk) {
                             // +32 bytes along K inside the swizzle atom = +2 in the 16-byte address field
                             mma_u8(d, adesc + 2 * kk, bdesc + 2 * kk, CF::IDESC, (i | kb | kk) != 0);
                         }
@@ -204,9 +205,22 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int q = warp & 3;  // the TMEM lane quarter this warp may read
         const uint32_t lane_base = static_cast<uint32_t>(q * 32) << 16;
         uint32_t (*stage)[17] = reinterpret_cast<uint32_t (*)[17]>(epi_stage + (warp - 2) * 32 * 17);
+        const int chalf = (warp - 2) >> 2;  // the two warps of a lane quarter take alternate 16-column chunks
         const int half = lane >> 4, col_in = lane & 15;
+        // Add / Sub read C: each lane prefetches its row of this warp's quarter of
+        // a tile into L2 one tile ahead (the first tile before its accumulator is
+        // ready), so the old values come from L2 when the drain reads them
+        auto prefetch_tile = [&](int t) {
+            if (g.op == HME_SET || t >= total_tiles) return;
+            int qm, qn;
+            tile_coords(t, g, qm, qn);
+            const int row = qm * kBM + q * 32 + lane;
+            if (chalf == 0 && row < g.M) prefetch_l2_span(g.C + static_cast<size_t>(row) * g.ldc + qn * BN, min(BN, g.N - qn * BN));
+        };
+        prefetch_tile(blockIdx.x);
         int lt = 0;
         for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++lt) {
+            prefetch_tile(tile + gridDim.x);
             const int a = lt & 1;
             const uint32_t aph = (lt >> 1) & 1;
             if (!mbar_wait(&acc_full[a], aph, abort_flag, g.err, DERR_WAIT_ACCUM)) break;
@@ -215,7 +229,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             tile_coords(tile, g, tm, tn);
             const int row0 = tm * kBM + q * 32;
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 16) {
+            for (int c0 = 16 * chalf; c0 < BN; c0 += 32) {
                 uint32_t v[L][16];
 #pragma unroll
                 for (int j = 0; j < L; ++j)
@@ -296,11 +310,15 @@ EncodeTiledFn encode_fn() {
 }
 
 void encode_u8(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
-               const cuuint32_t* box) {
+               const cuuint32_t* box, int kb = 128) {
     cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUtensorMapSwizzle sw = kb == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                  : kb == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                             : CU_TENSOR_MAP_SWIZZLE_32B;
+    if (kb != 128 && kb != 64 && kb != 32) throw Error(HME_EINVAL, "tensor map: k-block must be 128, 64 or 32 bytes");
     const CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, rank, base, dims, strides, box, estr,
-                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw Error(HME_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")");
 }
 
@@ -309,29 +327,29 @@ void encode_u8(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, c
 // pdl: the launch directly follows the limb split on the same stream, so the
 // first K chunk may be a programmatic dependent of it (off while per-kernel
 // timing events sit between launches).
-template <int L, int BN>
+template <int L, int BN, int KB = kBK>
 void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, int Kp,
                  uint8_t* planesA, uint64_t a_plane, uint8_t* planesB, uint32_t* C, size_t ldc, int op,
                  bool pdl) {
-    using CF = Cfg<L, BN>;
+    using CF = Cfg<L, BN, KB>;
     static std::once_flag attr_once;
     std::call_once(attr_once, [] {
-        cudaFuncSetAttribute(limb_gemm_kernel<L, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM);
+        cudaFuncSetAttribute(limb_gemm_kernel<L, BN, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM);
     });
     CUtensorMap tmA, tmB;
     {
         const cuuint64_t dims[3] = {static_cast<cuuint64_t>(Kp), m, static_cast<cuuint64_t>(L)};
         const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(a_plane)};
-        const cuuint32_t box[3] = {kBK, kBM, 1};
-        encode_u8(&tmA, planesA, 3, dims, strides, box);
+        const cuuint32_t box[3] = {KB, kBM, 1};
+        encode_u8(&tmA, planesA, 3, dims, strides, box, KB);
     }
     {
         const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), n, static_cast<cuuint64_t>(L),
                                     static_cast<cuuint64_t>(L)};
         const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * n,
                                        static_cast<cuuint64_t>(Kp) * n * L};
-        const cuuint32_t box[4] = {kBK, BN, static_cast<cuuint32_t>(L), 1};
-        encode_u8(&tmB, planesB, 4, dims, strides, box);
+        const cuuint32_t box[4] = {KB, BN, static_cast<cuuint32_t>(L), 1};
+        encode_u8(&tmB, planesB, 4, dims, strides, box, KB);
     }
     GemmArgs g{};
     g.C = C;
@@ -350,7 +368,7 @@ void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint
     for (uint32_t kb0 = 0; kb0 < k; kb0 += chunk) {
         const uint32_t kc = std::min(chunk, k - kb0);
         g.k_begin = static_cast<int>(kb0);
-        g.kblocks = static_cast<int>((kc + kBK - 1) / kBK);
+        g.kblocks = static_cast<int>((kc + KB - 1) / KB);
         g.op = kb0 == 0 ? op : (op == HME_SET ? HME_ADD : op);
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(grid);
@@ -362,7 +380,7 @@ void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = (pdl && kb0 == 0 && !ctx->timer.on) ? 1 : 0;
-        HME_TIMED(ctx, "limb_gemm", HME_CUDA(cudaLaunchKernelEx(&cfg, limb_gemm_kernel<L, BN>, tmA, tmB, g)));
+        HME_TIMED(ctx, "limb_gemm", HME_CUDA(cudaLaunchKernelEx(&cfg, limb_gemm_kernel<L, BN, KB>, tmA, tmB, g)));
     }
 }
 
@@ -378,6 +396,10 @@ __global__ void fill_zero_kernel(uint32_t* C, uint64_t ldc, int m, int n) {
 void encode_tma_u8(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
                    const cuuint32_t* box) {
     encode_u8(map, base, rank, dims, strides, box);
+}
+void encode_tma_u8_kb(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
+                      const cuuint32_t* box, int kb) {
+    encode_u8(map, base, rank, dims, strides, box, kb);
 }
 
 namespace {
@@ -409,17 +431,34 @@ void launch_split(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uin
     HME_CUDA(cudaGetLastError());
 }
 
+// kb: the k-block (swizzle row) width the planes were padded to: 32, 64 or 128
+template <int KB>
+void launch_gemm_variant_kb(hme_ctx* ctx, const ModParams& mp, bool narrow, uint32_t m, uint32_t n, uint32_t k,
+                            int Kp, uint8_t* pa, uint64_t a_plane, uint8_t* pb, uint32_t* C, size_t ldc, int op,
+                            bool pdl) {
+    switch (mp.limbs) {
+        case 1: if (narrow) launch_gemm<1, 128, KB>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
+                else launch_gemm<1, 256, KB>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+        case 2: if (narrow) launch_gemm<2, 64, KB>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
+                else launch_gemm<2, 128, KB>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+        case 3: if (narrow) launch_gemm<3, 32, KB>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
+                else launch_gemm<3, 80, KB>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+        default: if (narrow) launch_gemm<4, 32, KB>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
+                else launch_gemm<4, 64, KB>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+    }
+}
+
+// The narrowest k-block that holds K (products with a short K, like the
+// elimination's trailing updates with K = the panel's pivots, stream and
+// multiply no zero padding); longer K use the 128-byte row.
+int kblock_for(uint32_t k) { return k <= 32 ? 32 : k <= 64 ? 64 : kBK; }
+
 void launch_gemm_variant(hme_ctx* ctx, const ModParams& mp, bool narrow, uint32_t m, uint32_t n, uint32_t k, int Kp,
                          uint8_t* pa, uint64_t a_plane, uint8_t* pb, uint32_t* C, size_t ldc, int op, bool pdl) {
-    switch (mp.limbs) {
-        case 1: if (narrow) launch_gemm<1, 128>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
-                else launch_gemm<1, 256>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
-        case 2: if (narrow) launch_gemm<2, 64>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
-                else launch_gemm<2, 128>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
-        case 3: if (narrow) launch_gemm<3, 32>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
-                else launch_gemm<3, 80>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
-        default: if (narrow) launch_gemm<4, 32>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl);
-                else launch_gemm<4, 64>(ctx, mp, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+    switch (kblock_for(k)) {
+        case 32: launch_gemm_variant_kb<32>(ctx, mp, narrow, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+        case 64: launch_gemm_variant_kb<64>(ctx, mp, narrow, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
+        default: launch_gemm_variant_kb<kBK>(ctx, mp, narrow, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, pdl); break;
     }
 }
 
@@ -466,9 +505,9 @@ void gemm_u32_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n,
         return;
     }
     const int L = static_cast<int>(mp.limbs);
-    // K padded to whole 128-byte k-blocks (the split kernel writes the pad as
-    // zeros), so no TMA box ever reaches past the planes' K extent
-    const int Kp = static_cast<int>((k + kBK - 1) / kBK * kBK);
+    // K padded to whole k-blocks of the width kblock_for picks (the split kernel
+    // writes the pad as zeros), so no TMA box ever reaches past the planes' K extent
+    const int Kp = static_cast<int>((k + kblock_for(k) - 1) / kblock_for(k) * kblock_for(k));
     uint8_t* pa = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesA, static_cast<size_t>(L) * m * Kp));
     uint8_t* pb = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesB, static_cast<size_t>(L) * L * n * Kp));
     launch_split(ctx, mp, m, n, k, Kp, A, lda, B, ldb, pa, 0, pb, true, true);
@@ -487,7 +526,7 @@ void gemm_u32_host(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, ui
     HME_REQUIRE(variant == kVariantWide || variant == kVariantNarrow, "gemm_u32_host: tensor-core variants only");
     HME_REQUIRE(m > 0 && n > 0 && k > 0, "gemm_u32_host: empty product");
     const int L = static_cast<int>(mp.limbs);
-    const int Kp = static_cast<int>((k + kBK - 1) / kBK * kBK);
+    const int Kp = static_cast<int>((k + kblock_for(k) - 1) / kblock_for(k) * kblock_for(k));
     const uint32_t tiles_m = (m + kBM - 1) / kBM;
     // chunks of >= 2 MiB of C: every copy carries a fixed cost on the PCIe
     // path, so small chunks lose more than their overlap gains (measured on

@@ -74,3 +74,47 @@ def test_batch_gemm_rank_config4_sample(engine):
                         [(jb["B"], jb["p"], int(fam[j]), int(sb[j])) for j, jb in enumerate(jobs)])
     ranks = engine.batch_gemm_rank_dev(jobs)
     assert list(ranks) == want
+
+
+@pytest.mark.parametrize("p", [251, 65521, 16777213, 2147483629, 4294967291])
+def test_batch_gemm_short_k_matches_oracle(engine, p):
+    """A batch whose every K is at most 32 runs with 32-byte k-blocks (no zero
+    padding to the 128-byte row): ragged M and N, K from 1 to 32, tiles that
+    share the stacked plane tensors, all limb counts."""
+    import torch
+
+    rng = np.random.default_rng(p % 991)
+    shapes = [(1, 1, 1), (5, 32, 7), (130, 17, 65), (128, 32, 128), (257, 31, 300), (64, 9, 500), (300, 24, 33)]
+    jobs, want = [], []
+    for (m, k, n) in shapes:
+        A = rng.integers(0, p, (m, k), dtype=np.uint64).astype(np.uint32)
+        B = rng.integers(0, p, (k, n), dtype=np.uint64).astype(np.uint32)
+        want.append(O.gemm(p, A, B))
+        jobs.append({"p": p, "A": _dev(A), "B": _dev(B), "C": torch.zeros((m, n), dtype=torch.int32, device="cuda")})
+    torch.cuda.synchronize()
+    engine.batch_gemm_dev(jobs)
+    engine.sync()
+    for j, C in zip(jobs, want):
+        assert np.array_equal(j["C"].cpu().numpy().view(np.uint32), C), (p, j["C"].shape)
+
+
+def test_batch_rank_wide_panels_and_tall_jobs(engine):
+    """Rank rounds with panels up to 128 columns (a job of side <= 128 finishes
+    in one panel, larger ones take several rounds with widths set by their
+    active rows), rank-deficient jobs, and jobs taller than one panel CTA
+    holds (more than 1024 rows: the single-matrix elimination)."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    jobs, want = [], []
+    for t, (m, n, r) in enumerate([(100, 120, 90), (128, 128, 128), (129, 200, 60), (390, 390, 390),
+                                   (700, 500, 300), (1024, 1024, 1000), (1100, 300, 250), (2000, 64, 64)]):
+        p = (65521, 2147483629)[t % 2]
+        L = rng.integers(0, p, (m, r), dtype=np.uint64).astype(np.uint32)
+        R = rng.integers(0, p, (r, n), dtype=np.uint64).astype(np.uint32)
+        A = O.gemm(p, L, R)
+        want.append(len(O.rref(p, A)[1]))
+        jobs.append({"p": p, "A": None, "B": None, "C": _dev(A)})
+    torch.cuda.synchronize()
+    ranks = engine.batch_rank_dev(jobs)
+    assert list(ranks) == want
