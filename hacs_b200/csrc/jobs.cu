@@ -308,7 +308,8 @@ __global__ void __launch_bounds__(256) batch_trsm_kernel(const SolveJob* __restr
     extern __shared__ uint32_t smem_bt[];
     const SolveJob& J = jobs[blockIdx.y];
     const int k = J.k;
-    if (k < 2) return;  // the test is the same for the whole CTA
+    // nothing to solve, or no columns for this CTA: the test is the same for the whole CTA
+    if (k < 2 || static_cast<int>(blockIdx.x) * kBatchTrsmCols >= J.ntrail) return;
     const int ls = k | 1;
     constexpr int xs = kBatchTrsmCols + 1;
     uint32_t* sL = smem_bt;
@@ -327,12 +328,15 @@ __global__ void __launch_bounds__(256) batch_trsm_kernel(const SolveJob* __restr
             if (c < nc) sX[r * xs + c] = J.A[static_cast<size_t>(J.r0 + r) * J.ld + J.c1 + c0 + c];
         }
         __syncthreads();
-        for (int c = warp; c < nc; c += nw) {
-            uint32_t x[per];
+        // two columns per warp pass: independent update chains share each L11 load
+        for (int c = 2 * warp; c < nc; c += 2 * nw) {
+            const bool two = c + 1 < nc;
+            uint32_t x[per], y[per];
 #pragma unroll
             for (int q = 0; q < per; ++q) {
                 const int r = lane + 32 * q;
                 x[q] = r < k ? sX[r * xs + c] : 0u;
+                y[q] = (r < k && two) ? sX[r * xs + c + 1] : 0u;
             }
 #pragma unroll
             for (int qt = 0; qt < per; ++qt) {
@@ -341,12 +345,14 @@ __global__ void __launch_bounds__(256) batch_trsm_kernel(const SolveJob* __restr
                     const int t = 32 * qt + tt;
                     if (t >= k - 1) break;
                     const uint32_t xt = __shfl_sync(0xffffffffu, x[qt], tt);
+                    const uint32_t yt = __shfl_sync(0xffffffffu, y[qt], tt);
 #pragma unroll
                     for (int q = qt; q < per; ++q) {
                         const int r = lane + 32 * q;
                         if (r > t && r < k) {
-                            const uint32_t l = sL[r * ls + t];
-                            if (l) x[q] = reduce_u64(static_cast<uint64_t>(J.p - l) * xt + x[q], J.p, J.barrett);
+                            const uint32_t nl = J.p - sL[r * ls + t];
+                            x[q] = reduce_u64(static_cast<uint64_t>(nl) * xt + x[q], J.p, J.barrett);
+                            y[q] = reduce_u64(static_cast<uint64_t>(nl) * yt + y[q], J.p, J.barrett);
                         }
                     }
                 }
@@ -354,7 +360,10 @@ __global__ void __launch_bounds__(256) batch_trsm_kernel(const SolveJob* __restr
 #pragma unroll
             for (int q = 0; q < per; ++q) {
                 const int r = lane + 32 * q;
-                if (r < k) sX[r * xs + c] = x[q];
+                if (r < k) {
+                    sX[r * xs + c] = x[q];
+                    if (two) sX[r * xs + c + 1] = y[q];
+                }
             }
         }
         __syncthreads();
