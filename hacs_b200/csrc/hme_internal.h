@@ -66,6 +66,7 @@ enum WorkspaceSlot : int {
     kSlotJobs7 = 25,
     kSlotSched0 = 26,  // scheduler / autotuner
     kSlotSched1 = 27,
+    kSlotJobs8 = 28,   // batched job stream: the pivot blocks' inverses
 };
 
 struct Workspace {

@@ -295,81 +295,105 @@ struct SolveJob {
     uint64_t barrett;
     const int* pcols;  // the panel's pivot columns (in the device copy of the panel's output)
     uint32_t* L21;     // (m - r0 - k) x k
+    uint32_t* Linv;    // k x k: L11^-1
+    uint32_t kmax;     // products a 64-bit sum starting below p holds before a reduction
 };
-// One warp per trailing column: lane l holds rows l, l+32, l+64, l+96 (k <= 128);
-// at step t the value of row t is final and a shuffle broadcasts it.  The
-// columns of a 32-column tile go through shared memory so the global accesses
-// run along rows; L11 (k x k, odd row stride) in dynamic shared memory.
+// U12 = L11^-1 A12 for every job with a pivot block, in two launches:
+// batch_linv_kernel, one CTA per job: L11^-1 column by column (forward
+// substitution on e_j, one warp per column, lane l holding rows l, l+32, ...;
+// at step t row t is final and a shuffle broadcasts it), into the job's slot;
+// batch_apply_kernel, one CTA per (job, 32 trailing columns): the product
+// L11^-1 A12 with lane = column and warps over rows, each output a dot
+// product accumulated in 64 bits and reduced once per kmax products -- no
+// sequential dependency, so no idle lanes.
 constexpr int kBatchTrsmCols = 32;
-size_t batch_trsm_smem(int k) {
+size_t batch_linv_smem(int k) { return sizeof(uint32_t) * static_cast<size_t>(k) * (k | 1); }
+size_t batch_apply_smem(int k) {
     return sizeof(uint32_t) * (static_cast<size_t>(k) * (k | 1) + static_cast<size_t>(k) * (kBatchTrsmCols + 1));
 }
-__global__ void __launch_bounds__(256) batch_trsm_kernel(const SolveJob* __restrict__ jobs) {
-    extern __shared__ uint32_t smem_bt[];
+
+__global__ void __launch_bounds__(256) batch_linv_kernel(const SolveJob* __restrict__ jobs) {
+    extern __shared__ uint32_t smem_bl[];
+    const SolveJob& J = jobs[blockIdx.x];
+    const int k = J.k;
+    if (k < 2 || J.ntrail <= 0) return;  // the test is the same for the whole CTA
+    const int ls = k | 1;
+    uint32_t* sL = smem_bl;
+    for (int idx = threadIdx.x; idx < k * k; idx += blockDim.x) {
+        const int t = idx / k, s = idx % k;
+        sL[t * ls + s] = s < t ? J.A[static_cast<size_t>(J.r0 + t) * J.ld + J.pcols[s]] : 0u;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    constexpr int per = kMaxBw / 32;
+    for (int j = warp; j < k; j += nw) {
+        uint32_t x[per];
+#pragma unroll
+        for (int q = 0; q < per; ++q) x[q] = (lane + 32 * q == j) ? 1u % J.p : 0u;
+#pragma unroll
+        for (int qt = 0; qt < per; ++qt) {
+            if (32 * qt >= k - 1) break;
+            if (32 * qt + 31 < j) continue;  // rows above j stay zero
+            for (int tt = 0; tt < 32; ++tt) {
+                const int t = 32 * qt + tt;
+                if (t >= k - 1) break;
+                if (t < j) continue;
+                const uint32_t xt = __shfl_sync(0xffffffffu, x[qt], tt);
+#pragma unroll
+                for (int q = qt; q < per; ++q) {
+                    const int r = lane + 32 * q;
+                    if (r > t && r < k) {
+                        const uint32_t l = sL[r * ls + t];
+                        if (l) x[q] = reduce_u64(static_cast<uint64_t>(J.p - l) * xt + x[q], J.p, J.barrett);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < per; ++q) {
+            const int r = lane + 32 * q;
+            if (r < k) J.Linv[static_cast<size_t>(r) * k + j] = x[q];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) batch_apply_kernel(const SolveJob* __restrict__ jobs) {
+    extern __shared__ uint32_t smem_ba[];
     const SolveJob& J = jobs[blockIdx.y];
     const int k = J.k;
     // nothing to solve, or no columns for this CTA: the test is the same for the whole CTA
     if (k < 2 || static_cast<int>(blockIdx.x) * kBatchTrsmCols >= J.ntrail) return;
     const int ls = k | 1;
     constexpr int xs = kBatchTrsmCols + 1;
-    uint32_t* sL = smem_bt;
-    uint32_t* sX = smem_bt + k * ls;
+    uint32_t* Li = smem_ba;
+    uint32_t* X = smem_ba + k * ls;
     for (int idx = threadIdx.x; idx < k * k; idx += blockDim.x) {
-        const int t = idx / k, s = idx % k;
-        sL[t * ls + s] = s < t ? J.A[static_cast<size_t>(J.r0 + t) * J.ld + J.pcols[s]] : 0u;
+        const int r = idx / k, s = idx - r * k;
+        Li[r * ls + s] = J.Linv[idx];
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    constexpr int per = kMaxBw / 32;
     for (int c0 = blockIdx.x * kBatchTrsmCols; c0 < J.ntrail; c0 += gridDim.x * kBatchTrsmCols) {
         const int nc = min(kBatchTrsmCols, J.ntrail - c0);
-        __syncthreads();  // sL ready / the previous tile written back
+        __syncthreads();  // Li ready / the previous tile consumed
         for (int idx = threadIdx.x; idx < k * kBatchTrsmCols; idx += blockDim.x) {
             const int r = idx / kBatchTrsmCols, c = idx % kBatchTrsmCols;
-            if (c < nc) sX[r * xs + c] = J.A[static_cast<size_t>(J.r0 + r) * J.ld + J.c1 + c0 + c];
+            if (c < nc) X[r * xs + c] = J.A[static_cast<size_t>(J.r0 + r) * J.ld + J.c1 + c0 + c];
         }
         __syncthreads();
-        // two columns per warp pass: independent update chains share each L11 load
-        for (int c = 2 * warp; c < nc; c += 2 * nw) {
-            const bool two = c + 1 < nc;
-            uint32_t x[per], y[per];
-#pragma unroll
-            for (int q = 0; q < per; ++q) {
-                const int r = lane + 32 * q;
-                x[q] = r < k ? sX[r * xs + c] : 0u;
-                y[q] = (r < k && two) ? sX[r * xs + c + 1] : 0u;
-            }
-#pragma unroll
-            for (int qt = 0; qt < per; ++qt) {
-                if (32 * qt >= k - 1) break;
-                for (int tt = 0; tt < 32; ++tt) {
-                    const int t = 32 * qt + tt;
-                    if (t >= k - 1) break;
-                    const uint32_t xt = __shfl_sync(0xffffffffu, x[qt], tt);
-                    const uint32_t yt = __shfl_sync(0xffffffffu, y[qt], tt);
-#pragma unroll
-                    for (int q = qt; q < per; ++q) {
-                        const int r = lane + 32 * q;
-                        if (r > t && r < k) {
-                            const uint32_t nl = J.p - sL[r * ls + t];
-                            x[q] = reduce_u64(static_cast<uint64_t>(nl) * xt + x[q], J.p, J.barrett);
-                            y[q] = reduce_u64(static_cast<uint64_t>(nl) * yt + y[q], J.p, J.barrett);
-                        }
+        if (lane < nc) {
+            for (int r = warp; r < k; r += nw) {
+                uint64_t acc = X[r * xs + lane];  // the unit diagonal
+                uint32_t cnt = 0;
+                const uint32_t* lr = Li + r * ls;
+                for (int s = 0; s < r; ++s) {
+                    acc += static_cast<uint64_t>(lr[s]) * X[s * xs + lane];
+                    if (++cnt == J.kmax) {
+                        acc = reduce_u64(acc, J.p, J.barrett);
+                        cnt = 0;
                     }
                 }
+                J.A[static_cast<size_t>(J.r0 + r) * J.ld + J.c1 + c0 + lane] = reduce_u64(acc, J.p, J.barrett);
             }
-#pragma unroll
-            for (int q = 0; q < per; ++q) {
-                const int r = lane + 32 * q;
-                if (r < k) {
-                    sX[r * xs + c] = x[q];
-                    if (two) sX[r * xs + c + 1] = y[q];
-                }
-            }
-        }
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < k * kBatchTrsmCols; idx += blockDim.x) {
-            const int r = idx / kBatchTrsmCols, c = idx % kBatchTrsmCols;
-            if (c < nc) J.A[static_cast<size_t>(J.r0 + r) * J.ld + J.c1 + c0 + c] = sX[r * xs + c];
         }
     }
 }
@@ -396,8 +420,10 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
         cudaFuncSetAttribute(batch_panel_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
         cudaFuncSetAttribute(batch_panel_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
         cudaFuncSetAttribute(batch_panel_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
-        cudaFuncSetAttribute(batch_trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(batch_trsm_smem(kMaxBw)));
+        cudaFuncSetAttribute(batch_linv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(batch_linv_smem(kMaxBw)));
+        cudaFuncSetAttribute(batch_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(batch_apply_smem(kMaxBw)));
     });
     const int nj = static_cast<int>(mats.size());
     ranks.assign(nj, 0);
@@ -499,7 +525,8 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
         std::vector<int> perm_rows, perm_dst;
         std::vector<SolveJob> solves;
         size_t tmp_elems = 0, l21_elems = 0;
-        std::vector<size_t> tmp_off, perm_off, l21_off;
+        std::vector<size_t> tmp_off, perm_off, l21_off, linv_off;
+        size_t linv_elems = 0;
         for (const RankJob& J : round) {
             const RankOut& o = h_out[J.out];
             // no pivots, or the job's last panel (no columns right of it): nothing to move or update
@@ -564,9 +591,16 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
             sj.p = J.p;
             sj.barrett = J.barrett;
             sj.pcols = d_out[J.out].pivot_cols;
+            {
+                const uint64_t d = static_cast<uint64_t>(J.p - 1) * (J.p - 1);
+                const uint64_t km = d == 0 ? (1u << 20) : (~0ull - (J.p - 1)) / d;
+                sj.kmax = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(km, 1u << 20)));
+            }
             solves.push_back(sj);
             l21_off.push_back(l21_elems);
             l21_elems += a256(static_cast<size_t>(J.m - J.r0 - o.k) * o.k);
+            linv_off.push_back(linv_elems);
+            linv_elems += a256(static_cast<size_t>(o.k) * o.k);
         }
         if (!perms.empty()) {
             const int np = static_cast<int>(perms.size());
@@ -574,11 +608,13 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
             int* d_dst = d_perm + perm_rows.size();
             uint32_t* d_tmp = static_cast<uint32_t*>(ctx->ws.get(kSlotJobs5, sizeof(uint32_t) * tmp_elems + 256));
             uint32_t* d_l21 = static_cast<uint32_t*>(ctx->ws.get(kSlotJobs6, sizeof(uint32_t) * l21_elems + 256));
+            uint32_t* d_linv = static_cast<uint32_t*>(ctx->ws.get(kSlotJobs8, sizeof(uint32_t) * linv_elems + 256));
             for (int t = 0; t < np; ++t) {
                 perms[t].src = d_perm + perm_off[t];
                 perms[t].dst = d_dst + perm_off[t];
                 perms[t].tmp = d_tmp + tmp_off[t];
                 solves[t].L21 = d_l21 + l21_off[t];
+                solves[t].Linv = d_linv + linv_off[t];
             }
             uint8_t* tab = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs7, a256(sizeof(PermJob) * np) + a256(sizeof(SolveJob) * np)));
             PermJob* d_pj = reinterpret_cast<PermJob*>(tab);
@@ -592,14 +628,15 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
             HME_CUDA(cudaMemcpyAsync(d_sj, solves.data(), sizeof(SolveJob) * np, cudaMemcpyHostToDevice, ctx->stream));
             int kmax = 1;
             for (const SolveJob& sj : solves) kmax = std::max(kmax, sj.k);
-            const size_t trsm_smem = batch_trsm_smem(kmax);
+            const size_t linv_smem = batch_linv_smem(kmax), apply_smem = batch_apply_smem(kmax);
             // grid.y = job (<= 65535 per launch: chunked)
             for (int b0 = 0; b0 < np; b0 += 65535) {
                 const int nb = std::min(65535, np - b0);
                 const dim3 g(32, nb);
                 HME_TIMED(ctx, "batch_permute", batch_gather_rows_kernel<<<g, 256, 0, ctx->stream>>>(d_pj + b0));
                 HME_TIMED(ctx, "batch_permute", batch_scatter_rows_kernel<<<g, 256, 0, ctx->stream>>>(d_pj + b0));
-                HME_TIMED(ctx, "batch_trsm", batch_trsm_kernel<<<dim3(32, nb), 256, trsm_smem, ctx->stream>>>(d_sj + b0));
+                HME_TIMED(ctx, "batch_trsm", batch_linv_kernel<<<nb, 256, linv_smem, ctx->stream>>>(d_sj + b0));
+                HME_TIMED(ctx, "batch_trsm", batch_apply_kernel<<<dim3(32, nb), 256, apply_smem, ctx->stream>>>(d_sj + b0));
                 HME_TIMED(ctx, "batch_gather", batch_gather_l21_kernel<<<dim3(16, nb), 256, 0, ctx->stream>>>(d_sj + b0));
             }
             HME_CUDA(cudaGetLastError());
