@@ -28,23 +28,6 @@ namespace {
 
 using namespace limb;
 
-// Problems with the same padded K share one stacked plane tensor per operand
-// (their rows / columns at offsets a_row0 / b_col0); tiles that run past a
-// problem's rows or columns read a neighbour's planes, which only reach
-// accumulator rows and columns the epilogue does not store.
-struct GroupedProblem {
-    const CUtensorMap* tmA;  // stacked limb planes of the A operands: dims {Kp, rows, L}
-    const CUtensorMap* tmB;  // stacked limb planes of 256^i B: dims {Kp, cols, L, L}
-    uint32_t* C;
-    uint64_t ldc;
-    int M, N;
-    int kblocks;
-    int op;
-    int tiles_n;
-    int tile_begin;
-    int a_row0, b_col0;
-};
-
 __device__ __forceinline__ void grouped_drain(uint64_t* bar, uint32_t parity, int* err) {
     int never = 0;
     mbar_wait(bar, parity, &never, err, DERR_WAIT_DRAIN);
@@ -53,7 +36,10 @@ __device__ __forceinline__ void grouped_drain(uint64_t* bar, uint32_t parity, in
 template <int L, int BN, int KB>
 __global__ void __launch_bounds__(kThreads, 1)
     grouped_limb_gemm_kernel(const GroupedProblem* __restrict__ probs, const int* __restrict__ tile_prob,
-                             int total_tiles, uint32_t p, uint64_t barrett, int* err) {
+                             int total_tiles_arg, const int* __restrict__ d_total, uint32_t p, uint64_t barrett,
+                             int* err) {
+    // the tile count: a launch argument, or read from device memory (tables built on the device)
+    const int total_tiles = d_total ? *d_total : total_tiles_arg;
     using CF = Cfg<L, BN, KB>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -243,40 +229,42 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-// One launch splits every problem's operands into limb planes.
-struct GroupedSplitJob {
-    SplitArgs s;
-    int b_blocks;     // blocks of the B part
-    int block_begin;  // prefix over all jobs (A part then B part)
-};
-
 template <int L>
 __global__ void __launch_bounds__(256) grouped_split_kernel(const GroupedSplitJob* __restrict__ jobs,
-                                                            const int* __restrict__ block_job) {
+                                                            const int* __restrict__ block_job, int nblocks_arg,
+                                                            const int* __restrict__ d_nblocks) {
     __shared__ uint32_t tile[64][33];
-    const int b = blockIdx.x;
-    const GroupedSplitJob& J = jobs[block_job[b]];
-    const int local = b - J.block_begin;
-    if (local < J.s.a_blocks)
-        split_a_part<L>(J.s, local);
-    else
-        split_b_part<L>(J.s, local - J.s.a_blocks, tile);
+    const int nblocks = d_nblocks ? *d_nblocks : nblocks_arg;
+    for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+        __syncthreads();  // the previous block's use of the tile is over
+        const GroupedSplitJob& J = jobs[block_job[b]];
+        const int local = b - J.block_begin;
+        if (local < J.s.a_blocks)
+            split_a_part<L>(J.s, local);
+        else
+            split_b_part<L>(J.s, local - J.s.a_blocks, tile);
+    }
 }
 
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 template <int L, int BN, int KB>
-void launch_grouped(hme_ctx* ctx, const ModParams& mp, const GroupedProblem* d_probs, const int* d_tile_prob,
-                    int total_tiles) {
-    using CF = Cfg<L, BN, KB>;
+void ensure_grouped_attr() {
     static std::once_flag once;
     std::call_once(once, [] {
         cudaFuncSetAttribute(grouped_limb_gemm_kernel<L, BN, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             CF::SMEM);
+                             Cfg<L, BN, KB>::SMEM);
     });
-    const int grid = std::min(total_tiles, ctx->num_sms);
+}
+
+template <int L, int BN, int KB>
+void launch_grouped(hme_ctx* ctx, const ModParams& mp, const GroupedProblem* d_probs, const int* d_tile_prob,
+                    int total_tiles, const int* d_total = nullptr) {
+    using CF = Cfg<L, BN, KB>;
+    ensure_grouped_attr<L, BN, KB>();
+    const int grid = d_total ? ctx->num_sms : std::min(total_tiles, ctx->num_sms);
     HME_TIMED(ctx, "grouped_gemm", grouped_limb_gemm_kernel<L, BN, KB><<<grid, kThreads, CF::SMEM, ctx->stream>>>(
-                                       d_probs, d_tile_prob, total_tiles, mp.p, mp.barrett, ctx->d_err));
+                                       d_probs, d_tile_prob, total_tiles, d_total, mp.p, mp.barrett, ctx->d_err));
     HME_CUDA(cudaGetLastError());
 }
 
@@ -292,7 +280,7 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
     if (jobs.empty()) return;
     const int nj = static_cast<int>(jobs.size());
     // tile width: wide (L*BN close to 256) unless the whole group leaves SMs idle
-    constexpr int BNw = L == 1 ? 256 : L == 2 ? 128 : L == 3 ? 80 : 64;
+    constexpr int BNw = grouped_bn_wide(L);
     constexpr int BNn = L == 1 ? 128 : L == 2 ? 64 : 32;
     size_t tiles_wide = 0;
     for (const GemmJob& j : jobs) tiles_wide += static_cast<size_t>((j.M + kBM - 1) / kBM) * ((j.N + BNw - 1) / BNw);
@@ -434,7 +422,8 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
     }
     HME_REQUIRE(static_cast<size_t>(tiles) == total_tiles, "grouped gemm: tile count mismatch");
     HME_CUDA(cudaMemcpyAsync(d_tile_prob, index.data(), index_bytes, cudaMemcpyHostToDevice, ctx->stream));
-    HME_TIMED(ctx, "grouped_split", grouped_split_kernel<L><<<blocks, 256, 0, ctx->stream>>>(d_split, d_block_job));
+    HME_TIMED(ctx, "grouped_split",
+              grouped_split_kernel<L><<<blocks, 256, 0, ctx->stream>>>(d_split, d_block_job, blocks, nullptr));
     HME_CUDA(cudaGetLastError());
     if (KBsel == 32) {
         if (narrow) launch_grouped<L, BNn, 32>(ctx, mp, d_probs, d_tile_prob, tiles);
@@ -450,7 +439,38 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
     HME_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
+template <int L>
+void launch_device_tables(hme_ctx* ctx, const ModParams& mp, const GroupedSplitJob* d_split, const int* d_block_job,
+                          const int* d_nblocks, const GroupedProblem* d_probs, const int* d_tile_prob,
+                          const int* d_ntiles) {
+    const int split_grid = ctx->num_sms * 8;
+    HME_TIMED(ctx, "grouped_split", grouped_split_kernel<L><<<split_grid, 256, 0, ctx->stream>>>(d_split, d_block_job,
+                                                                                              0, d_nblocks));
+    HME_CUDA(cudaGetLastError());
+    launch_grouped<L, grouped_bn_wide(L), 32>(ctx, mp, d_probs, d_tile_prob, 0, d_ntiles);
+}
+
 }  // namespace
+
+void grouped_prepare_device_tables(uint32_t limbs) {
+    switch (limbs) {
+        case 1: ensure_grouped_attr<1, grouped_bn_wide(1), 32>(); break;
+        case 2: ensure_grouped_attr<2, grouped_bn_wide(2), 32>(); break;
+        case 3: ensure_grouped_attr<3, grouped_bn_wide(3), 32>(); break;
+        default: ensure_grouped_attr<4, grouped_bn_wide(4), 32>(); break;
+    }
+}
+
+void grouped_launch_device_tables(hme_ctx* ctx, const ModParams& mp, const GroupedSplitJob* d_split,
+                                  const int* d_block_job, const int* d_nblocks, const GroupedProblem* d_probs,
+                                  const int* d_tile_prob, const int* d_ntiles) {
+    switch (mp.limbs) {
+        case 1: launch_device_tables<1>(ctx, mp, d_split, d_block_job, d_nblocks, d_probs, d_tile_prob, d_ntiles); break;
+        case 2: launch_device_tables<2>(ctx, mp, d_split, d_block_job, d_nblocks, d_probs, d_tile_prob, d_ntiles); break;
+        case 3: launch_device_tables<3>(ctx, mp, d_split, d_block_job, d_nblocks, d_probs, d_tile_prob, d_ntiles); break;
+        default: launch_device_tables<4>(ctx, mp, d_split, d_block_job, d_nblocks, d_probs, d_tile_prob, d_ntiles); break;
+    }
+}
 
 void grouped_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs) {
     switch (mp.limbs) {

@@ -3,9 +3,50 @@
 #include <cstdint>
 #include <vector>
 
+#include <cuda.h>
+
 #include "hme_internal.h"
+#include "hme_limb.cuh"
 
 namespace hme {
+
+// One problem of a grouped launch.  Problems with the same padded K share one
+// stacked plane tensor per operand (their rows / columns at offsets a_row0 /
+// b_col0); tiles that run past a problem's rows or columns read a neighbour's
+// planes, which only reach accumulator rows and columns the epilogue does not
+// store.
+struct GroupedProblem {
+    const CUtensorMap* tmA;  // stacked limb planes of the A operands: dims {Kp, rows, L}
+    const CUtensorMap* tmB;  // stacked limb planes of 256^i B: dims {Kp, cols, L, L}
+    uint32_t* C;
+    uint64_t ldc;
+    int M, N;
+    int kblocks;
+    int op;
+    int tiles_n;
+    int tile_begin;
+    int a_row0, b_col0;
+};
+
+// One problem's limb split in the grouped split launch.
+struct GroupedSplitJob {
+    limb::SplitArgs s;
+    int b_blocks;     // blocks of the B part
+    int block_begin;  // prefix over all jobs (A part then B part)
+};
+
+// The wide tile width of the grouped GEMM for L limbs (L * BN close to 256).
+constexpr int grouped_bn_wide(int L) { return L == 1 ? 256 : L == 2 ? 128 : L == 3 ? 80 : 64; }
+
+// The grouped split + GEMM on tables built on the device (32-byte k-blocks, wide
+// tiles): block and tile counts, the per-block job and per-tile problem indexes
+// are read from device memory when the kernels run, so the launches have fixed
+// shapes (persistent grids) and can be captured in a CUDA graph.
+// Kernel attributes of those launches, set outside any stream capture.
+void grouped_prepare_device_tables(uint32_t limbs);
+void grouped_launch_device_tables(hme_ctx* ctx, const ModParams& mp, const GroupedSplitJob* d_split,
+                                  const int* d_block_job, const int* d_nblocks, const GroupedProblem* d_probs,
+                                  const int* d_tile_prob, const int* d_ntiles);
 
 struct GemmJob {
     uint32_t M = 0, N = 0, K = 0;

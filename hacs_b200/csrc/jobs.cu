@@ -10,8 +10,12 @@
 //   rank: a round-based blocked LU over all jobs at once -- per round, one
 //     CTA per job factors that job's next panel of columns in shared memory,
 //     then batched kernels move the pivot rows up and solve the pivot rows'
-//     trailing block, and ONE grouped limb GEMM applies every job's trailing
-//     update.  A job leaves the rounds when its columns or rows run out.
+//     trailing block, and ONE grouped limb GEMM per modulus applies every
+//     job's trailing update.  A job leaves the rounds when its columns or rows
+//     run out.  The rounds are planned on the device (bucket lists, row moves,
+//     solve entries, GEMM tile tables), so a round is a fixed launch sequence:
+//     it is captured once in a CUDA graph and replayed, with no host round trip
+//     between rounds.
 // Also here: the seeded device generator of the config-4 stream's matrices.
 #include <cuda_runtime.h>
 
@@ -86,6 +90,20 @@ struct RankJob {
     int out;        // its output slot in this round (its position in the round's table)
 };
 
+// Per-job state of the device-driven rounds: the job's RankJob (r0, c0 and the
+// round's w advance on the device) and its fixed buffers.
+struct RankDev {
+    RankJob J;
+    int active;
+    int group;            // modulus group
+    int a_row0, b_col0;   // the job's rows / columns in its group's stacked plane tensors
+    uint32_t* L21;        // m x 32: L21 of the round (ld = k)
+    uint32_t* Linv;       // 32 x 32: L11^-1 of the round
+    uint32_t* tmp;        // 64 x n: rows in flight during the row moves
+    int* mv;              // 64 sources, then 64 destinations
+    uint32_t kmax;        // delayed-reduction bound of p
+};
+
 struct RankOut {
     int k;
     int pivot_rows[kMaxBw];
@@ -117,13 +135,17 @@ __device__ __forceinline__ uint32_t batch_ff_update(bool mont, uint32_t w, uint3
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) batch_panel_kernel(const RankJob* __restrict__ jobs, RankOut* __restrict__ outs,
-                                                         int* err) {
+__global__ void __launch_bounds__(NT) batch_panel_kernel(const RankDev* __restrict__ devs,
+                                                         const int* __restrict__ list, const int* __restrict__ count,
+                                                         RankOut* __restrict__ outs, int* err) {
     extern __shared__ uint32_t sp[];  // [w][rs] column-major panel, then a step byte per row
     __shared__ int s_cand[3];
     __shared__ uint32_t s_w[kMaxBw], s_inv[kMaxBw], s_sinv[kMaxBw + 1];
     __shared__ int s_colstep[kMaxBw], s_prow[kMaxBw], s_pcol[kMaxBw];
-    const RankJob J = jobs[blockIdx.x];
+    const int njobs = *count;
+    for (int ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+    __syncthreads();  // the previous job's shared state is no longer read
+    const RankJob J = devs[list[ji]].J;
     const int rows = J.m - J.r0, w = J.w, rs = rows | 1;
     uint32_t* S = sp;
     unsigned char* s_step = reinterpret_cast<unsigned char*>(S + static_cast<size_t>(w) * rs);
@@ -132,9 +154,9 @@ __global__ void __launch_bounds__(NT) batch_panel_kernel(const RankJob* __restri
     constexpr int NONE = INT_MAX;
     int lg = 0;
     while ((1 << lg) < rows) ++lg;
-    if ((1 << lg) > NT) {  // the host never launches this; uniform for the CTA
+    if ((1 << lg) > NT) {  // the planner never lists this; uniform for the CTA
         if (tid == 0) atomicCAS(err, 0, DERR_LAUNCH_SHAPE);
-        return;
+        continue;
     }
     const int nslots = 1 << lg, g = NT >> lg;
     const int li = tid & (nslots - 1), sub = tid >> lg;
@@ -251,6 +273,7 @@ __global__ void __launch_bounds__(NT) batch_panel_kernel(const RankJob* __restri
         }
         o.k = k;
     }
+    }  // jobs of this CTA
 }
 
 // Row moves of columns [c0, n): the pivot rows go to rows r0 .. r0+k-1 by
@@ -410,10 +433,421 @@ __global__ void batch_gather_l21_kernel(const SolveJob* __restrict__ jobs) {
 
 size_t a256(size_t x) { return (x + 255) / 256 * 256; }
 
+// ---- device-driven rounds ----------------------------------------------------------------
+// A modulus group: its jobs are the contiguous range [begin, end) of the job
+// arrays; one grouped split + GEMM launch per round reads its tables.
+struct RankGroup {
+    const CUtensorMap* tmA;  // stacked A planes of the group: {32, sum_m, L}
+    const CUtensorMap* tmB;  // stacked B planes: {32, sum_n, L, L}
+    uint8_t* planesA;
+    uint8_t* planesB;
+    uint64_t sum_m, sum_n;
+    int bn;                  // grouped GEMM tile width
+    int begin, end;
+    int* tile_prob;          // per tile: the job (index within the group)
+    int* block_job;          // per split block: the job (index within the group)
+    int* totals;             // [0] tiles, [1] split blocks of the round
+};
+
+constexpr int kRowClasses = 4;
+constexpr int kBuckets2 = 2 * kRowClasses;  // row class x {a 32-column round, a job's last panel}
+__host__ __device__ inline int row_class(int rows) { return rows <= 64 ? 0 : rows <= 128 ? 1 : rows <= 256 ? 2 : 3; }
+__host__ __device__ inline int row_class_max(int c) { return c == 0 ? 64 : c == 1 ? 128 : c == 2 ? 256 : 1024; }
+__host__ __device__ inline int row_class_threads(int c) { return c == 0 ? 128 : c == 1 ? 256 : c == 2 ? 512 : 1024; }
+
+// Each active job: the round's panel width (its remaining columns in one last
+// panel when they fit the shared memory, else kRoundBw) and its bucket.
+__global__ void rank_plan_kernel(RankDev* __restrict__ devs, int nj, int* __restrict__ lists,
+                                 int* __restrict__ counters) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nj; j += gridDim.x * blockDim.x) {
+        RankDev& D = devs[j];
+        if (!D.active) continue;
+        const int rows = D.J.m - D.J.r0, left = D.J.n - D.J.c0;
+        const int wfit = (kRankSmem - rows - 16) / (4 * (rows | 1));
+        const bool last = left <= min(kMaxBw, wfit);
+        D.J.w = last ? left : min(kRoundBw, wfit);
+        const int b = row_class(rows) + (last ? kRowClasses : 0);
+        const int idx = atomicAdd(&counters[b], 1);
+        lists[static_cast<size_t>(b) * nj + idx] = j;
+    }
+}
+
+// After the panels: each job's row moves, solve, L21 gather, split and GEMM
+// entries of this round (empty when it has nothing to do), its tile and split
+// block counts, and its advance to the next round.
+__global__ void rank_post_kernel(RankDev* __restrict__ devs, int nj, const RankOut* __restrict__ outs,
+                                 PermJob* __restrict__ perms, SolveJob* __restrict__ solves,
+                                 GroupedProblem* __restrict__ gprob, GroupedSplitJob* __restrict__ gsplit,
+                                 int* __restrict__ tiles, int* __restrict__ blocks,
+                                 const RankGroup* __restrict__ groups) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nj; j += gridDim.x * blockDim.x) {
+        RankDev& D = devs[j];
+        RankJob& J = D.J;
+        PermJob& pj = perms[j];
+        SolveJob& sj = solves[j];
+        pj.rows = 0;
+        sj.k = 0;
+        sj.m = 0;
+        sj.r0 = 0;
+        sj.ntrail = 0;
+        tiles[j] = 0;
+        blocks[j] = 0;
+        if (!D.active) continue;
+        const RankOut& o = outs[j];
+        const int k = o.k;
+        const int c1 = J.c0 + J.w;
+        const int below = J.m - J.r0 - k, ntrail = J.n - c1;
+        if (k > 0 && ntrail > 0 && below > 0) {
+            // the pivot rows to r0 .. r0+k-1 by swaps: positions relative to r0,
+            // touched[] holds (position, original row now there) pairs
+            int pos[2 * kRoundBw], cont[2 * kRoundBw];
+            int nt = 0;
+            auto find = [&](int x) {
+                for (int i = 0; i < nt; ++i)
+                    if (pos[i] == x) return i;
+                pos[nt] = x;
+                cont[nt] = x;
+                return nt++;
+            };
+            for (int t = 0; t < k; ++t) {
+                const int a = find(t);
+                const int orig = o.pivot_rows[t] - J.r0;
+                int b = -1;  // the position now holding original row `orig`
+                for (int i = 0; i < nt; ++i)
+                    if (cont[i] == orig) b = i;
+                if (b < 0) b = find(orig);  // untouched so far: still at its own position
+                if (a != b) {
+                    const int ca = cont[a];
+                    cont[a] = cont[b];
+                    cont[b] = ca;
+                }
+            }
+            int moved = 0;
+            for (int i = 0; i < nt; ++i)
+                if (cont[i] != pos[i]) {
+                    D.mv[moved] = J.r0 + cont[i];
+                    D.mv[2 * kRoundBw + moved] = J.r0 + pos[i];
+                    ++moved;
+                }
+            pj.A = J.A;
+            pj.ld = J.ld;
+            pj.rows = moved;
+            pj.c0 = J.c0;
+            pj.cols = J.n - J.c0;
+            pj.src = D.mv;
+            pj.dst = D.mv + 2 * kRoundBw;
+            pj.tmp = D.tmp;
+            // U12 = L11^-1 A12, L21, and A22 -= L21 U12
+            sj.A = J.A;
+            sj.ld = J.ld;
+            sj.r0 = J.r0;
+            sj.k = k;
+            sj.m = J.m;
+            sj.c1 = c1;
+            sj.ntrail = ntrail;
+            sj.p = J.p;
+            sj.barrett = J.barrett;
+            sj.pcols = o.pivot_cols;
+            sj.L21 = D.L21;
+            sj.Linv = D.Linv;
+            sj.kmax = D.kmax;
+            const RankGroup& G = groups[D.group];
+            const int jl = j - G.begin;
+            GroupedProblem& gp = gprob[j];
+            gp.tmA = G.tmA;
+            gp.tmB = G.tmB;
+            gp.C = J.A + static_cast<size_t>(J.r0 + k) * J.ld + c1;
+            gp.ldc = J.ld;
+            gp.M = below;
+            gp.N = ntrail;
+            gp.kblocks = 1;
+            gp.op = HME_SUB;
+            gp.tiles_n = (ntrail + G.bn - 1) / G.bn;
+            gp.a_row0 = D.a_row0;
+            gp.b_col0 = D.b_col0;
+            tiles[j] = ((below + limb::kBM - 1) / limb::kBM) * gp.tiles_n;
+            GroupedSplitJob& gs = gsplit[j];
+            limb::SplitArgs& sa = gs.s;
+            sa.A = D.L21;
+            sa.lda = static_cast<uint64_t>(k);
+            sa.B = J.A + static_cast<size_t>(J.r0) * J.ld + c1;
+            sa.ldb = J.ld;
+            sa.M = below;
+            sa.N = ntrail;
+            sa.K = k;
+            sa.Kp = 32;
+            sa.p = J.p;
+            sa.barrett = J.barrett;
+            sa.planesA = G.planesA + static_cast<size_t>(D.a_row0) * 32;
+            sa.planesB = G.planesB + static_cast<size_t>(D.b_col0) * 32;
+            sa.a_plane = G.sum_m * 32;
+            sa.b_plane = G.sum_n * 32;
+            sa.a_blocks = min(64, max(1, (below * 2 + 255) / 256));
+            sa.b_blocks_k = 1;
+            sa.a_vec = (k & 3) == 0;
+            gs.b_blocks = (ntrail + 31) / 32;
+            blocks[j] = sa.a_blocks + gs.b_blocks;
+            (void)jl;
+        }
+        J.r0 += k;
+        J.c0 = c1;
+        D.active = J.r0 < J.m && J.c0 < J.n;
+    }
+}
+
+// Per group (one CTA each): exclusive prefix sums of the jobs' tile and block
+// counts into the GEMM and split tables, and the totals.
+__global__ void __launch_bounds__(1024) rank_scan_kernel(const RankGroup* __restrict__ groups,
+                                                         const int* __restrict__ tiles,
+                                                         const int* __restrict__ blocks,
+                                                         GroupedProblem* __restrict__ gprob,
+                                                         GroupedSplitJob* __restrict__ gsplit) {
+    __shared__ int w_t[32], w_b[32];
+    const RankGroup& G = groups[blockIdx.x];
+    const int n = G.end - G.begin;
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int i0 = G.begin + static_cast<int>(threadIdx.x) * per;
+    const int i1 = min(G.end, i0 + per);
+    int st = 0, sb = 0;
+    for (int i = i0; i < i1; ++i) {
+        st += tiles[i];
+        sb += blocks[i];
+    }
+    // exclusive scan of (st, sb) over the threads
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int it = st, ib = sb;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int yt = __shfl_up_sync(0xffffffffu, it, off), yb = __shfl_up_sync(0xffffffffu, ib, off);
+        if (lane >= off) {
+            it += yt;
+            ib += yb;
+        }
+    }
+    if (lane == 31) {
+        w_t[warp] = it;
+        w_b[warp] = ib;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int vt = lane < static_cast<int>(blockDim.x >> 5) ? w_t[lane] : 0;
+        int vb = lane < static_cast<int>(blockDim.x >> 5) ? w_b[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int yt = __shfl_up_sync(0xffffffffu, vt, off), yb = __shfl_up_sync(0xffffffffu, vb, off);
+            if (lane >= off) {
+                vt += yt;
+                vb += yb;
+            }
+        }
+        w_t[lane] = vt;  // inclusive prefix over warps
+        w_b[lane] = vb;
+    }
+    __syncthreads();
+    int bt = it - st + (warp > 0 ? w_t[warp - 1] : 0);
+    int bb = ib - sb + (warp > 0 ? w_b[warp - 1] : 0);
+    for (int i = i0; i < i1; ++i) {
+        gprob[i].tile_begin = bt;
+        gsplit[i].block_begin = bb;
+        bt += tiles[i];
+        bb += blocks[i];
+    }
+    if (threadIdx.x == blockDim.x - 1) {
+        G.totals[0] = bt;
+        G.totals[1] = bb;
+    }
+}
+
+// The per-tile problem and per-block job indexes of every group.
+__global__ void rank_fill_kernel(const RankGroup* __restrict__ groups, const RankDev* __restrict__ devs, int nj,
+                                 const int* __restrict__ tiles, const int* __restrict__ blocks,
+                                 const GroupedProblem* __restrict__ gprob, const GroupedSplitJob* __restrict__ gsplit) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nj; j += gridDim.x * blockDim.x) {
+        const RankGroup& G = groups[devs[j].group];
+        const int jl = j - G.begin;
+        for (int t = 0; t < tiles[j]; ++t) G.tile_prob[gprob[j].tile_begin + t] = jl;
+        for (int b = 0; b < blocks[j]; ++b) G.block_job[gsplit[j].block_begin + b] = jl;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------------------
+// Batched rank with the rounds planned on the device: per-job state and every
+// buffer live at offsets fixed before the first round, and small kernels build
+// each round's bucket lists, row moves, solve entries and grouped-GEMM tables,
+// so a round is a fixed sequence of launches with no host round trip.  The
+// sequence is captured once in a CUDA graph and replayed until every job can
+// have finished (the widest job's column count / 32 + 2 rounds; jobs that are
+// done drop out of every kernel at once).  With per-kernel timing on, the
+// rounds are launched directly instead, so each launch gets its events.
 void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::vector<int>& ranks) {
+    const int nj_all = static_cast<int>(mats.size());
+    ranks.assign(nj_all, 0);
+    // jobs taller than one panel CTA holds: the single-matrix elimination
+    std::vector<int> order;
+    order.reserve(nj_all);
+    for (int j = 0; j < nj_all; ++j) {
+        const BatchMatrix& M = mats[j];
+        HME_REQUIRE(is_prime_u32(M.p), "batch rank: every modulus must be prime");
+        if (M.m == 0 || M.n == 0) continue;
+        if (M.m > 1024) {
+            ElimOptions o = ctx->elim;
+            const ElimResult r = elim_device(ctx, make_mod(M.p), M.A, M.ld, static_cast<int>(M.m),
+                                             static_cast<int>(M.n), false, nullptr, 0, o);
+            ranks[j] = r.rank;
+        } else {
+            order.push_back(j);
+        }
+    }
+    if (order.empty()) return;
+    // modulus groups: jobs sorted by modulus (stable)
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return mats[x].p < mats[y].p; });
+    const int nj = static_cast<int>(order.size());
+    std::vector<uint32_t> gmod;
+    std::vector<int> gbegin;
+    for (int i = 0; i < nj; ++i)
+        if (i == 0 || mats[order[i]].p != mats[order[i - 1]].p) {
+            gmod.push_back(mats[order[i]].p);
+            gbegin.push_back(i);
+        }
+    const int ng = static_cast<int>(gmod.size());
+    gbegin.push_back(nj);
+
+    // ---- fixed layout: per-job state and buffers, per-group planes and tables
+    std::vector<RankDev> devs(nj);
+    std::vector<RankGroup> groups(ng);
+    size_t buf_bytes = 0, plane_bytes = 0;
+    std::vector<size_t> off_l21(nj), off_linv(nj), off_tmp(nj), off_mv(nj), g_planes(ng);
+    std::vector<size_t> g_tiles(ng, 0), g_blocks(ng, 0);
+    uint32_t max_n = 0;
+    for (int g = 0; g < ng; ++g) {
+        const ModParams mp = make_mod(gmod[g]);
+        const int L = static_cast<int>(mp.limbs);
+        uint64_t sm = 0, sn = 0;
+        for (int i = gbegin[g]; i < gbegin[g + 1]; ++i) {
+            const BatchMatrix& M = mats[order[i]];
+            RankDev& D = devs[i];
+            D = RankDev{};
+            RankJob& J = D.J;
+            J.A = M.A;
+            J.ld = M.ld;
+            J.m = static_cast<int>(M.m);
+            J.n = static_cast<int>(M.n);
+            J.p = M.p;
+            J.barrett = mp.barrett;
+            if (M.p & 1u) {
+                uint32_t x = M.p;  // p^-1 mod 2^32 by Newton's iteration
+                for (int t = 0; t < 5; ++t) x *= 2u - M.p * x;
+                J.qinv = 0u - x;
+                J.r2 = static_cast<uint32_t>((static_cast<unsigned __int128>(1) << 64) % M.p);
+            }
+            J.slot = i;
+            J.out = i;
+            D.active = 1;
+            D.group = g;
+            D.a_row0 = static_cast<int>(sm);
+            D.b_col0 = static_cast<int>(sn);
+            sm += M.m;
+            sn += M.n;
+            {
+                const uint64_t d = static_cast<uint64_t>(M.p - 1) * (M.p - 1);
+                const uint64_t km = d == 0 ? (1u << 20) : (~0ull - (M.p - 1)) / d;
+                D.kmax = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(km, 1u << 20)));
+            }
+            off_l21[i] = buf_bytes;
+            buf_bytes += a256(sizeof(uint32_t) * M.m * kRoundBw);
+            off_linv[i] = buf_bytes;
+            buf_bytes += a256(sizeof(uint32_t) * kRoundBw * kRoundBw);
+            off_tmp[i] = buf_bytes;
+            buf_bytes += a256(sizeof(uint32_t) * 2 * kRoundBw * M.n);
+            off_mv[i] = buf_bytes;
+            buf_bytes += a256(sizeof(int) * 4 * kRoundBw);
+            const int bn = grouped_bn_wide(L);
+            g_tiles[g] += static_cast<size_t>((M.m + limb::kBM - 1) / limb::kBM) * ((M.n + bn - 1) / bn);
+            g_blocks[g] += 64 + (M.n + 31) / 32;
+            max_n = std::max(max_n, M.n);
+        }
+        RankGroup& G = groups[g];
+        G.sum_m = sm;
+        G.sum_n = sn;
+        G.bn = grouped_bn_wide(L);
+        G.begin = gbegin[g];
+        G.end = gbegin[g + 1];
+        g_planes[g] = plane_bytes;
+        plane_bytes += a256(static_cast<size_t>(L) * sm * 32) + a256(static_cast<size_t>(L) * L * sn * 32);
+    }
+    // tables: states, outputs, entries, counts, lists, groups, tensor maps, indexes
+    size_t tb = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = tb;
+        tb += a256(bytes);
+        return o;
+    };
+    const size_t o_devs = take(sizeof(RankDev) * nj), o_outs = take(sizeof(RankOut) * nj);
+    const size_t o_perm = take(sizeof(PermJob) * nj), o_solve = take(sizeof(SolveJob) * nj);
+    const size_t o_gprob = take(sizeof(GroupedProblem) * nj), o_gsplit = take(sizeof(GroupedSplitJob) * nj);
+    const size_t o_tiles = take(sizeof(int) * nj), o_blocks = take(sizeof(int) * nj);
+    const size_t o_lists = take(sizeof(int) * kBuckets2 * static_cast<size_t>(nj));
+    const size_t o_counters = take(sizeof(int) * kBuckets2);
+    const size_t o_groups = take(sizeof(RankGroup) * ng), o_maps = take(sizeof(CUtensorMap) * 2 * ng);
+    const size_t o_totals = take(sizeof(int) * 2 * ng);
+    std::vector<size_t> o_tp(ng), o_bj(ng);
+    for (int g = 0; g < ng; ++g) {
+        o_tp[g] = take(sizeof(int) * std::max<size_t>(1, g_tiles[g]));
+        o_bj[g] = take(sizeof(int) * std::max<size_t>(1, g_blocks[g]));
+    }
+    uint8_t* tables = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs1, tb));
+    uint8_t* bufs = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs4, std::max<size_t>(256, buf_bytes)));
+    uint8_t* planes = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs0, std::max<size_t>(256, plane_bytes)));
+    RankDev* d_devs = reinterpret_cast<RankDev*>(tables + o_devs);
+    RankOut* d_outs = reinterpret_cast<RankOut*>(tables + o_outs);
+    PermJob* d_perm = reinterpret_cast<PermJob*>(tables + o_perm);
+    SolveJob* d_solve = reinterpret_cast<SolveJob*>(tables + o_solve);
+    GroupedProblem* d_gprob = reinterpret_cast<GroupedProblem*>(tables + o_gprob);
+    GroupedSplitJob* d_gsplit = reinterpret_cast<GroupedSplitJob*>(tables + o_gsplit);
+    int* d_tiles = reinterpret_cast<int*>(tables + o_tiles);
+    int* d_blocks = reinterpret_cast<int*>(tables + o_blocks);
+    int* d_lists = reinterpret_cast<int*>(tables + o_lists);
+    int* d_counters = reinterpret_cast<int*>(tables + o_counters);
+    RankGroup* d_groups = reinterpret_cast<RankGroup*>(tables + o_groups);
+    CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(tables + o_maps);
+    int* d_totals = reinterpret_cast<int*>(tables + o_totals);
+    for (int i = 0; i < nj; ++i) {
+        devs[i].L21 = reinterpret_cast<uint32_t*>(bufs + off_l21[i]);
+        devs[i].Linv = reinterpret_cast<uint32_t*>(bufs + off_linv[i]);
+        devs[i].tmp = reinterpret_cast<uint32_t*>(bufs + off_tmp[i]);
+        devs[i].mv = reinterpret_cast<int*>(bufs + off_mv[i]);
+    }
+    std::vector<CUtensorMap> maps(2 * static_cast<size_t>(ng));
+    for (int g = 0; g < ng; ++g) {
+        RankGroup& G = groups[g];
+        const int L = static_cast<int>(make_mod(gmod[g]).limbs);
+        G.planesA = planes + g_planes[g];
+        G.planesB = G.planesA + a256(static_cast<size_t>(L) * G.sum_m * 32);
+        {
+            const cuuint64_t dims[3] = {32, G.sum_m, static_cast<cuuint64_t>(L)};
+            const cuuint64_t strides[2] = {32, 32 * G.sum_m};
+            const cuuint32_t box[3] = {32, limb::kBM, 1};
+            encode_tma_u8_kb(&maps[2 * g], G.planesA, 3, dims, strides, box, 32);
+        }
+        {
+            const cuuint64_t dims[4] = {32, G.sum_n, static_cast<cuuint64_t>(L), static_cast<cuuint64_t>(L)};
+            const cuuint64_t strides[3] = {32, 32 * G.sum_n, 32 * G.sum_n * L};
+            const cuuint32_t box[4] = {32, static_cast<cuuint32_t>(G.bn), static_cast<cuuint32_t>(L), 1};
+            encode_tma_u8_kb(&maps[2 * g + 1], G.planesB, 4, dims, strides, box, 32);
+        }
+        G.tmA = d_maps + 2 * g;
+        G.tmB = d_maps + 2 * g + 1;
+        G.tile_prob = reinterpret_cast<int*>(tables + o_tp[g]);
+        G.block_job = reinterpret_cast<int*>(tables + o_bj[g]);
+        G.totals = d_totals + 2 * g;
+    }
+    HME_CUDA(cudaMemcpyAsync(d_devs, devs.data(), sizeof(RankDev) * nj, cudaMemcpyHostToDevice, ctx->stream));
+    HME_CUDA(cudaMemcpyAsync(d_groups, groups.data(), sizeof(RankGroup) * ng, cudaMemcpyHostToDevice, ctx->stream));
+    HME_CUDA(cudaMemcpyAsync(d_maps, maps.data(), sizeof(CUtensorMap) * 2 * ng, cudaMemcpyHostToDevice, ctx->stream));
+
+    // ---- launch shapes of a round (fixed)
     static std::once_flag once;
     std::call_once(once, [] {
         cudaFuncSetAttribute(batch_panel_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
@@ -425,261 +859,91 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
         cudaFuncSetAttribute(batch_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(batch_apply_smem(kMaxBw)));
     });
-    const int nj = static_cast<int>(mats.size());
-    ranks.assign(nj, 0);
-    std::vector<RankJob> st(nj);
-    for (int j = 0; j < nj; ++j) {
-        const BatchMatrix& M = mats[j];
-        HME_REQUIRE(is_prime_u32(M.p), "batch rank: every modulus must be prime");
-        RankJob& J = st[j];
-        J.A = M.A;
-        J.ld = M.ld;
-        J.m = static_cast<int>(M.m);
-        J.n = static_cast<int>(M.n);
-        J.p = M.p;
-        J.barrett = make_mod(M.p).barrett;
-        if (M.p & 1u) {
-            uint32_t x = M.p;  // p^-1 mod 2^32 by Newton's iteration
-            for (int i = 0; i < 5; ++i) x *= 2u - M.p * x;
-            J.qinv = 0u - x;
-            J.r2 = static_cast<uint32_t>((static_cast<unsigned __int128>(1) << 64) % M.p);
+    size_t bucket_smem[kBuckets2];
+    int bucket_grid[kBuckets2];
+    for (int b = 0; b < kBuckets2; ++b) {
+        const int c = b % kRowClasses, R = row_class_max(c);
+        const size_t w = b < kRowClasses ? kRoundBw : kMaxBw;
+        bucket_smem[b] = std::min<size_t>(kRankSmem, sizeof(uint32_t) * (R | 1) * w + R + 16);
+        int occ = 1;
+        const int nt = row_class_threads(c);
+        switch (nt) {
+            case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_panel_kernel<128>, nt, bucket_smem[b]); break;
+            case 256: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_panel_kernel<256>, nt, bucket_smem[b]); break;
+            case 512: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_panel_kernel<512>, nt, bucket_smem[b]); break;
+            default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_panel_kernel<1024>, nt, bucket_smem[b]); break;
         }
-        J.r0 = 0;
-        J.c0 = 0;
-        // the panel (m - r0) x w must fit shared memory
-        J.w = 0;  // set per round from the active rows
-        J.slot = j;
+        bucket_grid[b] = std::max(1, std::min(nj, ctx->num_sms * std::max(1, occ)));
     }
-    RankOut* d_out = static_cast<RankOut*>(ctx->ws.get(kSlotJobs2, sizeof(RankOut) * static_cast<size_t>(nj) + 256));
-    // the per-round panel outputs come back into pinned host memory (up to ~1 KB per job)
-    struct PinnedOut {
-        RankOut* p = nullptr;
-        ~PinnedOut() {
-            if (p) cudaFreeHost(p);
-        }
-    } pinned;
-    HME_CUDA(cudaMallocHost(reinterpret_cast<void**>(&pinned.p), sizeof(RankOut) * std::max(1, nj)));
-    RankOut* h_out = pinned.p;
-    std::vector<int> scratch_content, scratch_where;
-    std::vector<int> active;
-    for (int j = 0; j < nj; ++j)
-        if (st[j].m > 1024 && st[j].n > 0) {
-            // taller than one panel CTA holds: the single-matrix elimination (cluster / grid panels)
-            ElimOptions o = ctx->elim;
-            const ElimResult r = elim_device(ctx, make_mod(st[j].p), st[j].A, st[j].ld, st[j].m, st[j].n, false,
-                                             nullptr, 0, o);
-            st[j].r0 = r.rank;
-        } else if (st[j].m > 0 && st[j].n > 0) {
-            active.push_back(j);
-        }
-    while (!active.empty()) {
-        // (1) panels of every active job, in buckets of active rows: each bucket
-        // launches with the threads and shared memory its largest panel needs
-        constexpr int kBuckets = 4;
-        constexpr int bucket_threads[kBuckets] = {128, 256, 512, 1024};
-        auto bucket_of = [&](int rows) { return rows <= 64 ? 0 : rows <= 128 ? 1 : rows <= 256 ? 2 : 3; };
-        std::vector<RankJob> round;
-        round.reserve(active.size());
-        int bcount[kBuckets] = {0, 0, 0, 0};
-        size_t bsmem[kBuckets] = {0, 0, 0, 0};
-        for (int j : active) {
-            RankJob J = st[j];
-            const int rows = J.m - J.r0;
-            // the job's remaining columns in one last panel when they fit the shared memory
-            // (up to kMaxBw: no trailing update at all), else a kRoundBw-column panel (a
-            // wider one would grow the CUDA-core panel and pivot-block solve work, which
-            // scale with the width, faster than it saves trailing-update traffic)
-            const size_t wfit = (kRankSmem - static_cast<size_t>(rows) - 16) / (sizeof(uint32_t) * (rows | 1));
-            const size_t left = static_cast<size_t>(J.n - J.c0);
-            J.w = static_cast<int>(left <= std::min<size_t>(kMaxBw, wfit) ? left
-                                                                          : std::min<size_t>(kRoundBw, wfit));
-            HME_REQUIRE(J.w >= 1 && rows <= 1024, "batch rank: matrix too tall for the shared-memory panel");
-            const int b = bucket_of(rows);
-            ++bcount[b];
-            bsmem[b] = std::max(bsmem[b], sizeof(uint32_t) * static_cast<size_t>(J.w) * (rows | 1) + rows + 16);
-            round.push_back(J);
-        }
-        std::stable_sort(round.begin(), round.end(), [&](const RankJob& x, const RankJob& y) {
-            return bucket_of(x.m - x.r0) < bucket_of(y.m - y.r0);
-        });
-        for (size_t t = 0; t < round.size(); ++t) round[t].out = static_cast<int>(t);
-        RankJob* d_jobs = static_cast<RankJob*>(ctx->ws.get(kSlotJobs3, sizeof(RankJob) * round.size() + 256));
-        HME_CUDA(cudaMemcpyAsync(d_jobs, round.data(), sizeof(RankJob) * round.size(), cudaMemcpyHostToDevice,
-                                 ctx->stream));
-        for (int b = 0, off = 0; b < kBuckets; off += bcount[b], ++b) {
-            if (!bcount[b]) continue;
-            const RankJob* dj = d_jobs + off;
-            switch (bucket_threads[b]) {
-                case 128: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<128><<<bcount[b], 128, bsmem[b], ctx->stream>>>(dj, d_out, ctx->d_err)); break;
-                case 256: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<256><<<bcount[b], 256, bsmem[b], ctx->stream>>>(dj, d_out, ctx->d_err)); break;
-                case 512: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<512><<<bcount[b], 512, bsmem[b], ctx->stream>>>(dj, d_out, ctx->d_err)); break;
-                default: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<1024><<<bcount[b], 1024, bsmem[b], ctx->stream>>>(dj, d_out, ctx->d_err)); break;
+    HME_CUDA(cudaGetLastError());
+    const size_t linv_smem = batch_linv_smem(kRoundBw), apply_smem = batch_apply_smem(kRoundBw);
+    const int small_grid = std::max(1, std::min((nj + 255) / 256, ctx->num_sms * 8));
+    auto round = [&]() {
+        HME_CUDA(cudaMemsetAsync(d_counters, 0, sizeof(int) * kBuckets2, ctx->stream));
+        HME_TIMED(ctx, "rank_plan", rank_plan_kernel<<<small_grid, 256, 0, ctx->stream>>>(d_devs, nj, d_lists, d_counters));
+        for (int b = 0; b < kBuckets2; ++b) {
+            const int* list = d_lists + static_cast<size_t>(b) * nj;
+            const int* cnt = d_counters + b;
+            const int nt = row_class_threads(b % kRowClasses);
+            switch (nt) {
+                case 128: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<128><<<bucket_grid[b], 128, bucket_smem[b], ctx->stream>>>(d_devs, list, cnt, d_outs, ctx->d_err)); break;
+                case 256: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<256><<<bucket_grid[b], 256, bucket_smem[b], ctx->stream>>>(d_devs, list, cnt, d_outs, ctx->d_err)); break;
+                case 512: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<512><<<bucket_grid[b], 512, bucket_smem[b], ctx->stream>>>(d_devs, list, cnt, d_outs, ctx->d_err)); break;
+                default: HME_TIMED(ctx, "batch_panel", batch_panel_kernel<1024><<<bucket_grid[b], 1024, bucket_smem[b], ctx->stream>>>(d_devs, list, cnt, d_outs, ctx->d_err)); break;
             }
-            HME_CUDA(cudaGetLastError());
         }
-        HME_CUDA(cudaMemcpyAsync(h_out, d_out, sizeof(RankOut) * round.size(), cudaMemcpyDeviceToHost,
-                                 ctx->stream));
+        HME_TIMED(ctx, "rank_post", rank_post_kernel<<<small_grid, 256, 0, ctx->stream>>>(
+                                         d_devs, nj, d_outs, d_perm, d_solve, d_gprob, d_gsplit, d_tiles, d_blocks, d_groups));
+        HME_TIMED(ctx, "rank_post", rank_scan_kernel<<<ng, 1024, 0, ctx->stream>>>(d_groups, d_tiles, d_blocks, d_gprob,
+                                                                                  d_gsplit));
+        HME_TIMED(ctx, "rank_post", rank_fill_kernel<<<small_grid, 256, 0, ctx->stream>>>(d_groups, d_devs, nj, d_tiles,
+                                                                                         d_blocks, d_gprob, d_gsplit));
+        for (int b0 = 0; b0 < nj; b0 += 65535) {
+            const int nb = std::min(65535, nj - b0);
+            HME_TIMED(ctx, "batch_permute", batch_gather_rows_kernel<<<dim3(8, nb), 256, 0, ctx->stream>>>(d_perm + b0));
+            HME_TIMED(ctx, "batch_permute", batch_scatter_rows_kernel<<<dim3(8, nb), 256, 0, ctx->stream>>>(d_perm + b0));
+            HME_TIMED(ctx, "batch_trsm", batch_linv_kernel<<<nb, 256, linv_smem, ctx->stream>>>(d_solve + b0));
+            HME_TIMED(ctx, "batch_trsm", batch_apply_kernel<<<dim3(32, nb), 256, apply_smem, ctx->stream>>>(d_solve + b0));
+            HME_TIMED(ctx, "batch_gather", batch_gather_l21_kernel<<<dim3(8, nb), 256, 0, ctx->stream>>>(d_solve + b0));
+        }
+        for (int g = 0; g < ng; ++g) {
+            const RankGroup& G = groups[g];
+            grouped_launch_device_tables(ctx, make_mod(gmod[g]), d_gsplit + G.begin, G.block_job, G.totals + 1,
+                                         d_gprob + G.begin, G.tile_prob, G.totals);
+        }
+        HME_CUDA(cudaGetLastError());
+    };
+    for (int g = 0; g < ng; ++g) grouped_prepare_device_tables(make_mod(gmod[g]).limbs);
+    const int rounds = static_cast<int>((max_n + kRoundBw - 1) / kRoundBw) + 2;
+    if (ctx->timer.on) {
+        for (int r = 0; r < rounds; ++r) round();
+    } else {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        HME_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            round();
+        } catch (...) {
+            cudaStreamEndCapture(ctx->stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        HME_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+        struct GraphGuard {
+            cudaGraph_t g;
+            cudaGraphExec_t* e;
+            ~GraphGuard() {
+                if (*e) cudaGraphExecDestroy(*e);
+                if (g) cudaGraphDestroy(g);
+            }
+        } guard{graph, &exec};
+        HME_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        for (int r = 0; r < rounds; ++r) HME_CUDA(cudaGraphLaunch(exec, ctx->stream));
         HME_CUDA(cudaStreamSynchronize(ctx->stream));
-        // (2) row permutations, (3) solves, (4) trailing updates, per job with pivots
-        std::vector<PermJob> perms;
-        std::vector<int> perm_rows, perm_dst;
-        std::vector<SolveJob> solves;
-        size_t tmp_elems = 0, l21_elems = 0;
-        std::vector<size_t> tmp_off, perm_off, l21_off, linv_off;
-        size_t linv_elems = 0;
-        for (const RankJob& J : round) {
-            const RankOut& o = h_out[J.out];
-            // no pivots, or the job's last panel (no columns right of it): nothing to move or update
-            if (o.k == 0 || J.c0 + J.w >= J.n) continue;
-            const int rows = J.m - J.r0, cols = J.n - J.c0;
-            // the pivot rows to r0 .. r0+k-1 by swaps; only rows whose content changes move
-            PermJob pj{};
-            pj.A = J.A;
-            pj.ld = J.ld;
-            pj.c0 = J.c0;
-            pj.cols = cols;
-            perm_off.push_back(perm_rows.size());
-            tmp_off.push_back(tmp_elems);
-            {
-                // content[pos] = original row now at pos; where[orig] = its position (touched rows only)
-                std::vector<int>& content = scratch_content;
-                std::vector<int>& where = scratch_where;
-                content.resize(rows);
-                where.resize(rows);
-                for (int t = 0; t < o.k; ++t) {
-                    const int a = t, b0 = o.pivot_rows[t] - J.r0;
-                    content[a] = a;
-                    where[a] = a;
-                    content[b0] = b0;
-                    where[b0] = b0;
-                }
-                for (int t = 0; t < o.k; ++t) {
-                    const int a = t, b = where[o.pivot_rows[t] - J.r0];
-                    if (a == b) continue;
-                    const int ca = content[a], cb = content[b];
-                    content[a] = cb;
-                    content[b] = ca;
-                    where[cb] = a;
-                    where[ca] = b;
-                }
-                int moved = 0;
-                std::vector<int> touched;
-                for (int t = 0; t < o.k; ++t) {
-                    touched.push_back(t);
-                    touched.push_back(o.pivot_rows[t] - J.r0);
-                }
-                std::sort(touched.begin(), touched.end());
-                touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
-                for (int pos : touched)
-                    if (content[pos] != pos) {
-                        perm_rows.push_back(J.r0 + content[pos]);  // src
-                        perm_dst.push_back(J.r0 + pos);             // dst
-                        ++moved;
-                    }
-                pj.rows = moved;
-                if (moved) tmp_elems += a256(static_cast<size_t>(moved) * cols);
-            }
-            perms.push_back(pj);
-            SolveJob sj{};
-            sj.A = J.A;
-            sj.ld = J.ld;
-            sj.r0 = J.r0;
-            sj.k = o.k;
-            sj.m = J.m;
-            sj.c1 = J.c0 + J.w;
-            sj.ntrail = J.n - sj.c1;
-            sj.p = J.p;
-            sj.barrett = J.barrett;
-            sj.pcols = d_out[J.out].pivot_cols;
-            {
-                const uint64_t d = static_cast<uint64_t>(J.p - 1) * (J.p - 1);
-                const uint64_t km = d == 0 ? (1u << 20) : (~0ull - (J.p - 1)) / d;
-                sj.kmax = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(km, 1u << 20)));
-            }
-            solves.push_back(sj);
-            l21_off.push_back(l21_elems);
-            l21_elems += a256(static_cast<size_t>(J.m - J.r0 - o.k) * o.k);
-            linv_off.push_back(linv_elems);
-            linv_elems += a256(static_cast<size_t>(o.k) * o.k);
-        }
-        if (!perms.empty()) {
-            const int np = static_cast<int>(perms.size());
-            int* d_perm = static_cast<int*>(ctx->ws.get(kSlotJobs4, 2 * sizeof(int) * perm_rows.size() + 256));
-            int* d_dst = d_perm + perm_rows.size();
-            uint32_t* d_tmp = static_cast<uint32_t*>(ctx->ws.get(kSlotJobs5, sizeof(uint32_t) * tmp_elems + 256));
-            uint32_t* d_l21 = static_cast<uint32_t*>(ctx->ws.get(kSlotJobs6, sizeof(uint32_t) * l21_elems + 256));
-            uint32_t* d_linv = static_cast<uint32_t*>(ctx->ws.get(kSlotJobs8, sizeof(uint32_t) * linv_elems + 256));
-            for (int t = 0; t < np; ++t) {
-                perms[t].src = d_perm + perm_off[t];
-                perms[t].dst = d_dst + perm_off[t];
-                perms[t].tmp = d_tmp + tmp_off[t];
-                solves[t].L21 = d_l21 + l21_off[t];
-                solves[t].Linv = d_linv + linv_off[t];
-            }
-            uint8_t* tab = static_cast<uint8_t*>(ctx->ws.get(kSlotJobs7, a256(sizeof(PermJob) * np) + a256(sizeof(SolveJob) * np)));
-            PermJob* d_pj = reinterpret_cast<PermJob*>(tab);
-            SolveJob* d_sj = reinterpret_cast<SolveJob*>(tab + a256(sizeof(PermJob) * np));
-            if (!perm_rows.empty()) {
-                perm_rows.insert(perm_rows.end(), perm_dst.begin(), perm_dst.end());
-                HME_CUDA(cudaMemcpyAsync(d_perm, perm_rows.data(), sizeof(int) * perm_rows.size(),
-                                         cudaMemcpyHostToDevice, ctx->stream));
-            }
-            HME_CUDA(cudaMemcpyAsync(d_pj, perms.data(), sizeof(PermJob) * np, cudaMemcpyHostToDevice, ctx->stream));
-            HME_CUDA(cudaMemcpyAsync(d_sj, solves.data(), sizeof(SolveJob) * np, cudaMemcpyHostToDevice, ctx->stream));
-            int kmax = 1;
-            for (const SolveJob& sj : solves) kmax = std::max(kmax, sj.k);
-            const size_t linv_smem = batch_linv_smem(kmax), apply_smem = batch_apply_smem(kmax);
-            // grid.y = job (<= 65535 per launch: chunked)
-            for (int b0 = 0; b0 < np; b0 += 65535) {
-                const int nb = std::min(65535, np - b0);
-                const dim3 g(32, nb);
-                HME_TIMED(ctx, "batch_permute", batch_gather_rows_kernel<<<g, 256, 0, ctx->stream>>>(d_pj + b0));
-                HME_TIMED(ctx, "batch_permute", batch_scatter_rows_kernel<<<g, 256, 0, ctx->stream>>>(d_pj + b0));
-                HME_TIMED(ctx, "batch_trsm", batch_linv_kernel<<<nb, 256, linv_smem, ctx->stream>>>(d_sj + b0));
-                HME_TIMED(ctx, "batch_trsm", batch_apply_kernel<<<dim3(32, nb), 256, apply_smem, ctx->stream>>>(d_sj + b0));
-                HME_TIMED(ctx, "batch_gather", batch_gather_l21_kernel<<<dim3(16, nb), 256, 0, ctx->stream>>>(d_sj + b0));
-            }
-            HME_CUDA(cudaGetLastError());
-            // one grouped GEMM per modulus: A22 -= L21 * U12
-            std::vector<uint32_t> mods;
-            for (const SolveJob& sj : solves)
-                if (std::find(mods.begin(), mods.end(), sj.p) == mods.end()) mods.push_back(sj.p);
-            for (uint32_t p : mods) {
-                std::vector<GemmJob> gj;
-                for (int t = 0; t < np; ++t) {
-                    const SolveJob& sj = solves[t];
-                    if (sj.p != p) continue;
-                    const int below = sj.m - sj.r0 - sj.k;
-                    if (below <= 0 || sj.ntrail <= 0) continue;
-                    GemmJob g;
-                    g.M = below;
-                    g.N = sj.ntrail;
-                    g.K = sj.k;
-                    g.A = sj.L21;
-                    g.lda = sj.k;
-                    g.B = sj.A + static_cast<size_t>(sj.r0) * sj.ld + sj.c1;
-                    g.ldb = sj.ld;
-                    g.C = sj.A + static_cast<size_t>(sj.r0 + sj.k) * sj.ld + sj.c1;
-                    g.ldc = sj.ld;
-                    g.op = HME_SUB;
-                    gj.push_back(g);
-                }
-                if (!gj.empty()) grouped_gemm_u32_device(ctx, make_mod(p), gj);
-            }
-        }
-        // (5) advance
-        std::vector<int> next;
-        for (const RankJob& J : round) {
-            RankJob& S = st[J.slot];
-            const int k = h_out[J.out].k;
-            S.r0 += k;
-            S.c0 += J.w;
-            if (S.r0 < S.m && S.c0 < S.n) next.push_back(J.slot);
-        }
-        active.swap(next);
     }
     check_device_error(ctx);
-    for (int j = 0; j < nj; ++j) ranks[j] = st[j].r0;
+    HME_CUDA(cudaMemcpy(devs.data(), d_devs, sizeof(RankDev) * nj, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nj; ++i) ranks[order[i]] = devs[i].J.r0;
 }
 
 void gen_jobs_device(hme_ctx* ctx, const std::vector<GenSpec>& specs) {
