@@ -542,6 +542,45 @@ def run_case(args):
         mlp.close()
         eng.close()
         return 0
+    if kind == "level12":
+        # level12:<m>:<n>:<p>: the device level-1 / level-2 operations on m x n operands (larger than L2 at
+        # 8192 x 8192), each timed alone with CUDA events; GB/s of algorithmic bytes
+        m, n, p = int(parts[1]), int(parts[2]), int(parts[3])
+        torch.cuda.set_stream(torch.cuda.Stream())
+        eng = hacs_b200.Engine(0)
+        eng.use_torch_stream()
+        g = torch.Generator(device="cuda").manual_seed(2)
+
+        def rnd(*shape):
+            return torch.randint(0, p, shape, dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
+
+        X, Y, Z = rnd(m, n), rnd(m, n), torch.empty((n, m), dtype=torch.int32, device="cuda")
+        x, y = rnd(n), rnd(m)
+        rows = torch.randperm(m, device="cuda", generator=g)[: m // 2].to(torch.int32)
+        W = torch.empty((m // 2, n), dtype=torch.int32, device="cuda")
+        acc = torch.randint(0, 2**62, (m, n), dtype=torch.int64, device="cuda", generator=g)
+        nrhs = 256
+        T, Bt = rnd(m, m), rnd(m, nrhs)
+        steps, warm = max(1, args.steps), args.warmup
+        ops = {  # name -> (call, algorithmic bytes per call)
+            "gemv": (lambda: eng.gemv_dev(p, X, x, y), 4 * (m * n + n + 2 * m)),
+            "axpy": (lambda: eng.axpy_dev(p, 7 % p, X, Y), 12 * m * n),
+            "scal": (lambda: eng.scal_dev(p, 3 % p, Y), 8 * m * n),
+            "copy": (lambda: eng.copy_dev(X, Y), 8 * m * n),
+            "transpose": (lambda: eng.transpose_dev(X, Z), 8 * m * n),
+            "fill": (lambda: eng.fill_dev(Y, 1), 4 * m * n),
+            "gather_rows": (lambda: eng.gather_dev(p, 1, 5 % p, X, 0, None, W, False, rows), 8 * (m // 2) * n),
+            "canonicalise_acc64": (lambda: eng.canonicalise_acc64_dev(p, acc, Y), 12 * m * n),
+            "trsm_unit_lower": (lambda: eng.trsm_unit_dev(p, T, Bt, True), 4 * (m * m // 2 + 2 * m * nrhs)),
+        }
+        out = {"case": args.case}
+        for name, (fn, nbytes) in ops.items():
+            ms = time_device(fn, steps, warm) / steps
+            out[name] = {"ms": round(ms, 4), "gbs": round(nbytes / ms / 1e6, 1)}
+        eng.sync()
+        print(json.dumps(default=_json, obj=out), flush=True)
+        eng.close()
+        return 0
     # gemm:<n>:<p> (scheduler's variant) or gemm:<n>:<p>:<variant> (0 wide, 1 narrow, 2 simt32, 3 simt64)
     n, p = int(parts[1]), int(parts[2])
     assert kind == "gemm"
@@ -575,7 +614,8 @@ def main():
                          "of n^3 mod p; rref:<n>:<rank>:<p> runs W + K device RREFs of a rank-deficient n x n "
                          "matrix; howell:<n>:<ell>:<k> / smith:<n>:<ell>:<k> runs W + K forms of a planted "
                          "U*D*V; jobs:<count> runs W + K batched GEMM + rank streams of the first <count> jobs; "
-                         "mlp:<rows> trains the scheduler MLP for K epochs and plans <rows> shapes")
+                         "mlp:<rows> trains the scheduler MLP for K epochs and plans <rows> shapes; level12:<m>:<n>:<p> "
+                         "times the device level-1 / level-2 operations on m x n operands")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -66,6 +66,31 @@ def _dev_ptr(t) -> int:
     return t.data_ptr()
 
 
+def _view(t, elem: int = 4):
+    """(pointer, rows, cols, row stride, column stride) of a 1-D (a column) or
+    2-D CUDA tensor view with any strides, strides in elements."""
+    import torch
+
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("device entry points take CUDA torch tensors")
+    if t.element_size() != elem:
+        raise TypeError(f"device view must hold {8 * elem}-bit words")
+    if t.dim() == 1:
+        return t.data_ptr(), t.shape[0], 1, t.stride(0), 1
+    if t.dim() != 2:
+        raise ValueError("device views are 1-D or 2-D")
+    return t.data_ptr(), t.shape[0], t.shape[1], t.stride(0), t.stride(1)
+
+
+def _index_ptr(idx, count: int):
+    """Device pointer of a contiguous 32-bit index list of `count` entries, or None."""
+    if idx is None:
+        return None
+    if idx.numel() != count or not idx.is_contiguous() or idx.element_size() != 4 or not idx.is_cuda:
+        raise ValueError("index lists are contiguous 32-bit CUDA tensors, one entry per output row / column")
+    return idx.data_ptr()
+
+
 class Engine:
     """One libhme context: a device, a stream and the device workspace."""
 
@@ -155,6 +180,99 @@ class Engine:
             raise ValueError("gemm_dev: shape mismatch")
         check(self._lib.hme_gemm_u32_dev(self._h, p, m, n, k, _dev_ptr(A), A.stride(0), _dev_ptr(B), B.stride(0),
                                          _dev_ptr(C), C.stride(0), op))
+
+    # ---- device level-1 / level-2 operations (engine::cuda::*, src/Cuda/CudaKernels.h:120-247) ----
+    def gemm_nt_dev(self, p: int, A, B, C, op: int = SET) -> None:
+        """C op= A*B^T mod p with B given n x k (row-major)."""
+        m, k = A.shape
+        n = B.shape[0]
+        if B.shape[1] != k or tuple(C.shape) != (m, n):
+            raise ValueError("gemm_nt_dev: shape mismatch")
+        check(self._lib.hme_gemm_nt_u32_dev(self._h, p, m, n, k, _dev_ptr(A), A.stride(0), _dev_ptr(B), B.stride(0),
+                                            _dev_ptr(C), C.stride(0), op))
+
+    def schur_update_dev(self, p: int, L, U, C) -> None:
+        """C -= L*U mod p."""
+        m, k = L.shape
+        n = U.shape[1]
+        if U.shape[0] != k or tuple(C.shape) != (m, n):
+            raise ValueError("schur_update_dev: shape mismatch")
+        check(self._lib.hme_schur_update_u32_dev(self._h, p, m, n, k, _dev_ptr(L), L.stride(0), _dev_ptr(U),
+                                                 U.stride(0), _dev_ptr(C), C.stride(0)))
+
+    def gemv_dev(self, p: int, A, x, y, op: int = SET) -> None:
+        """y op= A*x mod p; A any strides, x (k,) / (k, 1) and y (m,) / (m, 1) views."""
+        a, xv, yv = _view(A), _view(x), _view(y)
+        m, k = a[1], a[2]
+        if xv[1] != k or yv[1] != m or xv[2] != 1 or yv[2] != 1:
+            raise ValueError("gemv_dev: shape mismatch")
+        check(self._lib.hme_gemv_u32_dev(self._h, p, m, k, a[0], a[3], a[4], xv[0], xv[3], yv[0], yv[3], op))
+
+    def axpy_dev(self, p: int, alpha: int, x, y, subtract: bool = False) -> None:
+        """y = y +/- alpha*x mod p (equal-shape views, any strides)."""
+        xv, yv = _view(x), _view(y)
+        if xv[1:3] != yv[1:3]:
+            raise ValueError("axpy_dev: shape mismatch")
+        check(self._lib.hme_axpy_u32_dev(self._h, p, alpha, xv[1], xv[2], xv[0], xv[3], xv[4], yv[0], yv[3], yv[4],
+                                         1 if subtract else 0))
+
+    def scal_dev(self, p: int, alpha: int, x) -> None:
+        """x = alpha*x mod p."""
+        v = _view(x)
+        check(self._lib.hme_scal_u32_dev(self._h, p, alpha, v[1], v[2], v[0], v[3], v[4]))
+
+    def copy_dev(self, src, dst) -> None:
+        s, d = _view(src), _view(dst)
+        if s[1:3] != d[1:3]:
+            raise ValueError("copy_dev: shape mismatch")
+        check(self._lib.hme_copy_u32_dev(self._h, s[1], s[2], s[0], s[3], s[4], d[0], d[3], d[4]))
+
+    def transpose_dev(self, src, dst) -> None:
+        """dst(i, j) = src(j, i)."""
+        s, d = _view(src), _view(dst)
+        if (s[1], s[2]) != (d[2], d[1]):
+            raise ValueError("transpose_dev: shape mismatch")
+        check(self._lib.hme_transpose_u32_dev(self._h, d[1], d[2], s[0], s[3], s[4], d[0], d[3], d[4]))
+
+    def fill_dev(self, x, value: int) -> None:
+        v = _view(x)
+        check(self._lib.hme_fill_u32_dev(self._h, v[1], v[2], v[0], v[3], v[4], value))
+
+    def axpy_identity_dev(self, p: int, alpha: int, y, subtract: bool = False) -> None:
+        """y(i, i) +/-= alpha for every diagonal cell of the window."""
+        v = _view(y)
+        check(self._lib.hme_axpy_identity_u32_dev(self._h, p, alpha, v[1], v[2], v[0], v[3], v[4],
+                                                  1 if subtract else 0))
+
+    def gather_dev(self, p: int, alpha: int, beta: int, a, row_off: int, cols, c, accumulate: bool = False,
+                   rows=None) -> None:
+        """c(i, t) [+]= alpha [row_off + r(i) == col(t)] + beta a(r(i), col(t)); r(i) = rows[i] or i,
+        col(t) = cols[t] or t; `a` may be None (identity source)."""
+        cv = _view(c)
+        av = _view(a) if a is not None else (0, 0, 0, 0, 0)
+        check(self._lib.hme_gather_u32_dev(self._h, p, alpha, beta, av[0] or None, av[1], av[2], av[3], av[4],
+                                           row_off, _index_ptr(cols, cv[2]), _index_ptr(rows, cv[1]), cv[1], cv[2],
+                                           cv[0], cv[3], cv[4], 1 if accumulate else 0))
+
+    def canonicalise_dev(self, p: int, v) -> None:
+        """v = v >= p ? v - p : v in place (entries below 2p)."""
+        x = _view(v)
+        check(self._lib.hme_canonicalise_u32_dev(self._h, p, x[1], x[2], x[0], x[3], x[4]))
+
+    def canonicalise_acc64_dev(self, p: int, acc, dst) -> None:
+        """dst = acc mod p for an int64 / uint64 accumulator view."""
+        a, d = _view(acc, 8), _view(dst)
+        if a[1:3] != d[1:3]:
+            raise ValueError("canonicalise_acc64_dev: shape mismatch")
+        check(self._lib.hme_canonicalise_acc64_u32_dev(self._h, p, a[1], a[2], a[0], a[3], a[4], d[0], d[3], d[4]))
+
+    def trsm_unit_dev(self, p: int, T, B, lower: bool) -> None:
+        """B <- T^-1 B mod p in place; T m x m unit lower / upper triangular (strict triangle read)."""
+        m = T.shape[0]
+        if T.shape[1] != m or B.shape[0] != m:
+            raise ValueError("trsm_unit_dev: shape mismatch")
+        check(self._lib.hme_trsm_unit_u32_dev(self._h, p, 1 if lower else 0, m, B.shape[1], _dev_ptr(T),
+                                              T.stride(0), _dev_ptr(B), B.stride(0)))
 
     # ---- elimination over F_p ------------------------------------------------------
     def set_elim_options(self, panel: int = 0, rows_per_cta: int = 0, panel_ctas: int = 0, back_block: int = 0):

@@ -57,6 +57,20 @@ PROTOTYPES = {
     "hme_gemm_u32": (C.c_int, [vp, u32, u32, u32, u32, u32p, sz, u32p, sz, u32p, sz, C.c_int]),
     "hme_gemm_u32_dev": (C.c_int, [vp, u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int]),
     "hme_gemm_u32_dev_noalloc": (C.c_int, [u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int, vp]),
+    "hme_gemm_nt_u32_dev": (C.c_int, [vp, u32, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int]),
+    "hme_schur_update_u32_dev": (C.c_int, [vp, u32, u32, u32, u32, vp, sz, vp, sz, vp, sz]),
+    "hme_gemv_u32_dev": (C.c_int, [vp, u32, u32, u32, vp, sz, sz, vp, sz, vp, sz, C.c_int]),
+    "hme_axpy_u32_dev": (C.c_int, [vp, u32, u32, u32, u32, vp, sz, sz, vp, sz, sz, C.c_int]),
+    "hme_scal_u32_dev": (C.c_int, [vp, u32, u32, u32, u32, vp, sz, sz]),
+    "hme_copy_u32_dev": (C.c_int, [vp, u32, u32, vp, sz, sz, vp, sz, sz]),
+    "hme_transpose_u32_dev": (C.c_int, [vp, u32, u32, vp, sz, sz, vp, sz, sz]),
+    "hme_fill_u32_dev": (C.c_int, [vp, u32, u32, vp, sz, sz, u32]),
+    "hme_axpy_identity_u32_dev": (C.c_int, [vp, u32, u32, u32, u32, vp, sz, sz, C.c_int]),
+    "hme_gather_u32_dev": (C.c_int, [vp, u32, u32, u32, vp, u32, u32, sz, sz, u32, vp, vp, u32, u32, vp, sz, sz,
+                                     C.c_int]),
+    "hme_canonicalise_u32_dev": (C.c_int, [vp, u32, u32, u32, vp, sz, sz]),
+    "hme_canonicalise_acc64_u32_dev": (C.c_int, [vp, u32, u32, u32, vp, sz, sz, vp, sz, sz]),
+    "hme_trsm_unit_u32_dev": (C.c_int, [vp, u32, C.c_int, u32, u32, vp, sz, vp, sz]),
 }
 
 

@@ -95,6 +95,66 @@ HME_API int hme_gemm_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint3
 HME_API int hme_gemm_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A,
                      size_t lda, const uint32_t *B, size_t ldb, uint32_t *C, size_t ldc, int op);
 
+/* ---- device level-1 / level-2 operations ----------------------------------
+ * The rest of the device layer the tape's DeviceBackend drives, on device
+ * pointers, asynchronous on the context's stream.  A view is (pointer, rows,
+ * cols, row stride, column stride), strides in elements, as the reference's
+ * DeviceView; residues are canonical (< p) unless stated; every result is the
+ * exact residue.  Semantics of engine::cuda::* (src/Cuda/CudaKernels.h):
+ *
+ * hme_gemm_nt_u32_dev       C op= A B^T, B given n x k row-major   (:126-129)
+ * hme_schur_update_u32_dev  C -= L U                                (:131-134)
+ * hme_gemv_u32_dev          y op= A x, x k x 1, y m x 1            (:189-192)
+ * hme_axpy_u32_dev          y = y +/- alpha x, alpha canonical     (:194-197)
+ * hme_scal_u32_dev          x = alpha x                             (:199-200)
+ * hme_copy_u32_dev          dst = src, windows must not overlap     (:203-204)
+ * hme_transpose_u32_dev     dst(i, j) = src(j, i); dst rows x cols  (:207-208)
+ * hme_fill_u32_dev          x(i, j) = value                         (:212-213)
+ * hme_axpy_identity_u32_dev y(i, i) +/-= alpha, i < min(rows, cols) (:218-219)
+ * hme_gather_u32_dev        c(i, t) [+]= alpha [row_off + r(i) == col(t)]
+ *                             + beta a(r(i), col(t)), r(i) = rows[i] or i,
+ *                             col(t) = cols[t] or t; a (a_rows x a_cols)
+ *                             may be NULL (beta ignored) and must not
+ *                             overlap c; indices are not range-checked;
+ *                             accumulate 0 = Set                (:228-231)
+ * hme_canonicalise_u32_dev  v = v >= p ? v - p : v (Lazy2p form, 2p <= 2^32)
+ *                                                                   (:233-234)
+ * hme_canonicalise_acc64_u32_dev  dst = acc mod p, u64 accumulators (:237-238)
+ * hme_trsm_unit_u32_dev     B <- T^-1 B in place, T m x m unit lower (lower
+ *                             != 0) or unit upper, only the strict triangle
+ *                             read; T and B row-major; T must not overlap B
+ *                                                                   (:245-247)
+ * Bodies of the reference: src/Cuda/cuda_kernels.cu:952-1130. */
+HME_API int hme_gemm_nt_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A,
+                                size_t lda, const uint32_t *B, size_t ldb, uint32_t *C, size_t ldc, int op);
+HME_API int hme_schur_update_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *L,
+                                     size_t ldl, const uint32_t *U, size_t ldu, uint32_t *C, size_t ldc);
+HME_API int hme_gemv_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t k, const uint32_t *A, size_t a_rs,
+                             size_t a_cs, const uint32_t *x, size_t x_rs, uint32_t *y, size_t y_rs, int op);
+HME_API int hme_axpy_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t alpha, uint32_t rows, uint32_t cols, const uint32_t *x,
+                             size_t x_rs, size_t x_cs, uint32_t *y, size_t y_rs, size_t y_cs, int subtract);
+HME_API int hme_scal_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t alpha, uint32_t rows, uint32_t cols, uint32_t *x,
+                             size_t rs, size_t cs);
+HME_API int hme_copy_u32_dev(hme_ctx *ctx, uint32_t rows, uint32_t cols, const uint32_t *src, size_t s_rs, size_t s_cs,
+                             uint32_t *dst, size_t d_rs, size_t d_cs);
+HME_API int hme_transpose_u32_dev(hme_ctx *ctx, uint32_t rows_dst, uint32_t cols_dst, const uint32_t *src,
+                                  size_t s_rs, size_t s_cs, uint32_t *dst, size_t d_rs, size_t d_cs);
+HME_API int hme_fill_u32_dev(hme_ctx *ctx, uint32_t rows, uint32_t cols, uint32_t *x, size_t rs, size_t cs,
+                             uint32_t value);
+HME_API int hme_axpy_identity_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t alpha, uint32_t rows, uint32_t cols,
+                                      uint32_t *y, size_t rs, size_t cs, int subtract);
+HME_API int hme_gather_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t alpha, uint32_t beta, const uint32_t *a,
+                               uint32_t a_rows, uint32_t a_cols, size_t a_rs, size_t a_cs, uint32_t row_off,
+                               const uint32_t *cols, const uint32_t *rows, uint32_t c_rows, uint32_t c_cols,
+                               uint32_t *c, size_t c_rs, size_t c_cs, int accumulate);
+HME_API int hme_canonicalise_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t rows, uint32_t cols, uint32_t *v, size_t rs,
+                                     size_t cs);
+HME_API int hme_canonicalise_acc64_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t rows, uint32_t cols,
+                                           const uint64_t *acc, size_t a_rs, size_t a_cs, uint32_t *dst,
+                                           size_t d_rs, size_t d_cs);
+HME_API int hme_trsm_unit_u32_dev(hme_ctx *ctx, uint32_t p, int lower, uint32_t m, uint32_t n, const uint32_t *T,
+                                  size_t ldt, uint32_t *B, size_t ldb);
+
 /* ---- elimination over F_p (p prime, p < 2^32) --------------------------------
  * Device-resident blocked LU: a cooperative panel kernel (pivot = leftmost
  * column with a non-zero in the Schur complement, topmost such row), row
