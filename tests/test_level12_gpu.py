@@ -220,3 +220,78 @@ def test_contract_checks(engine):
     engine.fill_dev(y, 3)  # empty views are no-ops
     engine.copy_dev(x, x)  # a self-copy is a no-op
     engine.sync()
+
+
+@pytest.mark.parametrize("p", [251, 65521, 2147483629, 4294967291])
+def test_vector_paths_on_aligned_views(engine, p):
+    """16-byte vector paths: contiguous operands and windows whose rows start
+    16-byte aligned (column offset 4, row stride a multiple of 4), next to a
+    window one column off alignment (scalar path) in the same buffer."""
+    import torch
+
+    rng = np.random.default_rng(p % 7919)
+    for rows, cols in [(1, 4), (3, 1024), (257, 4100), (4096, 64)]:
+        for c0 in (4, 5):
+            xb = _dev(_rand(rng, p, (rows, cols + 12)))
+            yb0 = _rand(rng, p, (rows, cols + 12))
+            yb = _dev(yb0)
+            x, y = xb[:, c0 : c0 + cols], yb[:, c0 : c0 + cols]
+            alpha = int(rng.integers(0, p))
+            xh, yh = _host(x.contiguous()), _host(y.contiguous())
+            engine.axpy_dev(p, alpha, x, y, True)
+            engine.sync()
+            assert np.array_equal(_host(y.contiguous()), L12.axpy(p, alpha, xh, yh, True)), (rows, cols, c0)
+            engine.scal_dev(p, alpha, y)
+            engine.sync()
+            yh = L12.axpy(p, alpha, xh, yh, True)
+            assert np.array_equal(_host(y.contiguous()), L12.scal(p, alpha, yh))
+            engine.copy_dev(x, y)
+            engine.fill_dev(x, 7 % p)
+            engine.sync()
+            assert np.array_equal(_host(y.contiguous()), xh)
+            assert (_host(x.contiguous()) == 7 % p).all()
+            # the buffer's columns outside the window are untouched
+            out = _host(yb)
+            assert np.array_equal(out[:, :c0], yb0[:, :c0]) and np.array_equal(out[:, c0 + cols :], yb0[:, c0 + cols :])
+    if p <= 2**31:
+        lazy = rng.integers(0, 2 * p, (300, 516), dtype=np.uint64).astype(np.uint32)
+        v = _dev(lazy)
+        engine.canonicalise_dev(p, v[:, 4:516])
+        engine.sync()
+        want = lazy.copy()
+        want[:, 4:516] = L12.canonicalise(p, lazy[:, 4:516])
+        assert np.array_equal(_host(v), want)
+    acc = rng.integers(0, 2**64 - 1, (100, 1028), dtype=np.uint64, endpoint=True)
+    a = torch.from_numpy(acc.view(np.int64)).cuda()
+    d = torch.zeros((100, 1028), dtype=torch.int32, device="cuda")
+    engine.canonicalise_acc64_dev(p, a, d)
+    engine.sync()
+    assert np.array_equal(_host(d), L12.canonicalise_acc64(p, acc))
+    for m, k in [(1, 4), (65, 8192), (1000, 516)]:
+        A_h, x_h, y0 = _rand(rng, p, (m, k)), _rand(rng, p, k), _rand(rng, p, m)
+        y = _dev(y0.reshape(1, m))[0]
+        engine.gemv_dev(p, _dev(A_h), _dev(x_h.reshape(1, k))[0], y, hacs_b200.ADD)
+        engine.sync()
+        assert np.array_equal(_host(y), L12.gemv(p, A_h, x_h, y0, hacs_b200.ADD)), (m, k)
+
+
+@pytest.mark.parametrize("p", [251, 4294967291])
+def test_gather_identity_vector_path(engine, p):
+    """The 4-column gather with no source (identity term only) and with a
+    source and row list, windows aligned for 16-byte accesses."""
+    import torch
+
+    rng = np.random.default_rng(p % 101)
+    for acc in (False, True):
+        c0 = _rand(rng, p, (64, 128))
+        c = _dev(c0)
+        engine.gather_dev(p, 5 % p, 0, None, 3, None, c, acc)
+        engine.sync()
+        assert np.array_equal(_host(c), L12.gather(p, 5 % p, 0, None, 3, None, c0, acc))
+    a_h = _rand(rng, p, (90, 256))
+    rows_h = rng.permutation(90)[:40].astype(np.uint32)
+    c0 = _rand(rng, p, (40, 256))
+    c = _dev(c0)
+    engine.gather_dev(p, 9 % p, 7 % p, _dev(a_h), 1, None, c, True, torch.from_numpy(rows_h.view(np.int32)).cuda())
+    engine.sync()
+    assert np.array_equal(_host(c), L12.gather(p, 9 % p, 7 % p, a_h, 1, None, c0, True, rows_h))
