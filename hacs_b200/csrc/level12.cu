@@ -138,6 +138,14 @@ __device__ __forceinline__ void mac96(uint64_t& lo, uint32_t& hi, uint32_t a, ui
     lo += prod;
     hi += lo < prod ? 1u : 0u;
 }
+// acc += a b, a 2^64 wraparound folded back as r64 = 2^64 mod p: acc stays
+// congruent to the exact sum.  After a wrap acc < a b <= (2^32 - 1)^2, so
+// adding r64 < 2^32 cannot wrap again.
+__device__ __forceinline__ void mac_fold(uint64_t& acc, uint32_t a, uint32_t b, uint32_t r64) {
+    const uint64_t prod = static_cast<uint64_t>(a) * b;
+    acc += prod;
+    acc += acc < prod ? r64 : 0u;
+}
 
 template <int V>
 __global__ void __launch_bounds__(kEwThreads) axpy_kernel(uint32_t alpha, const uint32_t* __restrict__ x, Strides xs,
@@ -449,8 +457,9 @@ __global__ void gemv_thread_kernel(const uint32_t* __restrict__ A, uint64_t a_rs
 // strict triangle and 0 elsewhere, for all 128 x 128 positions (pitch 129:
 // the 32 lanes' rows fall in 32 different banks), and the nb x 8 tile of B.
 // Lane l of a warp keeps rows l, l + 32, l + 64, l + 96 of its column as
-// exact 96-bit sums b_r + sum_t nT(r, t) x_t (no reduction per update, no
-// branch: entries outside the triangle are 0).  At step t the row-t sum is
+// 64-bit words congruent to b_r + sum_t nT(r, t) x_t (no reduction per
+// update, wraparounds folded back as 2^64 mod p; no branch: entries outside
+// the triangle are 0).  At step t the row-t sum is
 // reduced, broadcast by a shuffle, and added into every row; LOWER walks t up,
 // upper walks it down; at the end every row is reduced once.
 template <bool LOWER>
@@ -494,13 +503,9 @@ __global__ void __launch_bounds__(256) trsm_diag_kernel(const uint32_t* __restri
             for (int i = 0; i < 4; ++i) sB[(rr + 32 * i) * 9 + cc] = v[i];
         }
         __syncthreads();
-        uint64_t lo[4];
-        uint32_t hi[4];
+        uint64_t acc[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            lo[i] = sB[(lane + 32 * i) * 9 + warp];
-            hi[i] = 0;
-        }
+        for (int i = 0; i < 4; ++i) acc[i] = sB[(lane + 32 * i) * 9 + warp];
 #pragma unroll
         for (int qq = 0; qq < 4; ++qq) {
             const int q = LOWER ? qq : 3 - qq;  // the 32-row group holding the rows t of this pass
@@ -508,17 +513,17 @@ __global__ void __launch_bounds__(256) trsm_diag_kernel(const uint32_t* __restri
                 const uint32_t tn = min(32u, nb - 32 * q);
                 for (uint32_t st = 0; st < tn; ++st) {
                     const uint32_t tt = LOWER ? st : tn - 1 - st, t = 32 * q + tt;
-                    const uint32_t xt = __shfl_sync(0xffffffffu, fold96(lo[q], hi[q], p, barrett, r64), tt);
+                    const uint32_t xt = __shfl_sync(0xffffffffu, reduce_u64(acc[q], p, barrett), tt);
 #pragma unroll
                     for (int i = 0; i < 4; ++i) {
                         if (LOWER ? i < q : i > q) continue;  // rows already final
-                        mac96(lo[i], hi[i], sT[(lane + 32 * i) * tp + t], xt);
+                        mac_fold(acc[i], sT[(lane + 32 * i) * tp + t], xt, r64);
                     }
                 }
             }
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) sB[(lane + 32 * i) * 9 + warp] = fold96(lo[i], hi[i], p, barrett, r64);
+        for (int i = 0; i < 4; ++i) sB[(lane + 32 * i) * 9 + warp] = reduce_u64(acc[i], p, barrett);
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
