@@ -97,6 +97,15 @@ def ref():
         L.ref_smith_2k_u32.argtypes = [C.c_uint32] * 3 + [u32p, u32p, u32p, C.c_int]
         L.ref_smith_3k_u32.argtypes = [C.c_uint32] * 3 + [u32p, u32p, u32p, C.c_int]
         L.ref_howell_3k_u32.argtypes = [C.c_uint32] * 3 + [u32p] * 5 + [C.c_int]
+        u32 = C.c_uint32
+        u64p = C.POINTER(C.c_uint64)
+        L.ref_gemm_nt_u32.argtypes = [u32] * 4 + [u32p, u32, u32p, u32, u32p, u32, C.c_int]
+        L.ref_gemv_u32.argtypes = [u32] * 3 + [u32p, u32, u32p, u32p, C.c_int]
+        L.ref_axpy_scal_u32.argtypes = [u32] * 4 + [u32p, u32, u32p, u32, C.c_int]
+        L.ref_trmm_unit_u32.argtypes = [u32, C.c_int, u32, u32, u32p, u32, u32p, u32, u32p, u32]
+        L.ref_transpose_u32.argtypes = [u32, u32, u32p, u32, u32p, u32]
+        L.ref_canonicalise_u32.argtypes = [u32] * 3 + [u32p, u32]
+        L.ref_canonicalise_acc64_u32.argtypes = [u32] * 3 + [u64p, u32, u32p, u32]
         _REF = L
     return _REF
 
@@ -300,3 +309,67 @@ def ref_smith_3k(k: int, A, threads: int = 1) -> np.ndarray:
     c = C.c_uint32(0)
     _chk(ref().ref_smith_3k_u32(k, m, n, _p(A), _p(s), C.byref(c), threads), "ref")
     return s[: c.value].copy()
+
+
+# ---- the reference's level-1 / level-2 CPU kernels (Kernels.h:188-259) -------------
+def ref_gemm_nt(p: int, A, B, C, op: int) -> np.ndarray:
+    A, B = _u32(A), _u32(B)
+    m, k = A.shape
+    n = B.shape[0]
+    Cm = _u32(C).copy()
+    _chk(ref().ref_gemm_nt_u32(p, m, n, k, _p(A), max(k, 1), _p(B), max(k, 1), _p(Cm), n, op), "ref")
+    return Cm
+
+
+def ref_gemv(p: int, A, x, y, op: int) -> np.ndarray:
+    A, x = _u32(A), _u32(np.reshape(x, -1))
+    m, k = A.shape
+    yv = _u32(np.reshape(y, -1)).copy()
+    _chk(ref().ref_gemv_u32(p, m, k, _p(A), k, _p(x), _p(yv), op), "ref")
+    return yv
+
+
+def ref_axpy(p: int, alpha: int, x, y, subtract: bool) -> np.ndarray:
+    x = _u32(x).copy()
+    yv = _u32(y).copy()
+    r, c = x.shape
+    _chk(ref().ref_axpy_scal_u32(p, alpha, r, c, _p(x), c, _p(yv), c, 1 if subtract else 0), "ref")
+    return yv
+
+
+def ref_scal(p: int, alpha: int, x) -> np.ndarray:
+    xv = _u32(x).copy()
+    r, c = xv.shape
+    _chk(ref().ref_axpy_scal_u32(p, alpha, r, c, _p(xv), c, None, c, 0), "ref")
+    return xv
+
+
+def ref_trmm_unit(p: int, T, B, lower: bool) -> np.ndarray:
+    T, B = _u32(T), _u32(B)
+    m, n = B.shape
+    Cm = np.zeros((m, n), np.uint32)
+    _chk(ref().ref_trmm_unit_u32(p, 1 if lower else 0, m, n, _p(T), m, _p(B), n, _p(Cm), n), "ref")
+    return Cm
+
+
+def ref_transpose(A) -> np.ndarray:
+    A = _u32(A)
+    r, c = A.shape
+    T = np.zeros((c, r), np.uint32)
+    _chk(ref().ref_transpose_u32(r, c, _p(A), c, _p(T), r), "ref")
+    return T
+
+
+def ref_canonicalise(p: int, v) -> np.ndarray:
+    v = _u32(v).copy()
+    r, c = v.shape
+    _chk(ref().ref_canonicalise_u32(p, r, c, _p(v), c), "ref")
+    return v
+
+
+def ref_canonicalise_acc64(p: int, acc) -> np.ndarray:
+    acc = np.ascontiguousarray(acc, dtype=np.uint64)
+    r, c = acc.shape
+    d = np.zeros((r, c), np.uint32)
+    _chk(ref().ref_canonicalise_acc64_u32(p, r, c, acc.ctypes.data_as(C.POINTER(C.c_uint64)), c, _p(d), c), "ref")
+    return d

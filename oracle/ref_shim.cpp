@@ -10,6 +10,8 @@
 //
 // Reference entry points bound here:
 //   kernels::gemm<uint32_t>             src/ModArithmetic/Kernels.h:178-185 (Kernels.cpp:1418)
+//   kernels::gemm_nt / gemv / axpy / scal / trmm / transpose / canonicalise (both forms)
+//                                       src/ModArithmetic/Kernels.h:188-259
 //   elim::rref / column_rank_profile    src/ModArithmetic/DenseElim.h:158-169 (DenseElim.cpp:921)
 //   elim::kernel_basis                  src/ModArithmetic/DenseElim.h:176-179
 //   elim::inverse                       src/ModArithmetic/DenseElim.h:188-189
@@ -100,6 +102,92 @@ int ref_gemm_u32(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t*
         for (auto& th : pool) th.join();
         for (auto& e : errs)
             if (!e.empty()) throw std::runtime_error(e);
+    });
+}
+
+// Level-1 / level-2 CPU kernels of the reference, row-major with leading dims.
+// C op= A * B^T with B given n x k.
+int ref_gemm_nt_u32(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A, uint32_t lda,
+                    const uint32_t* B, uint32_t ldb, uint32_t* C, uint32_t ldc, int op) {
+    return guarded([&] {
+        const ModCtx<uint32_t> ctx(p);
+        const auto gop = op == 0 ? kernels::GemmOp::Set : op == 1 ? kernels::GemmOp::Add : kernels::GemmOp::Sub;
+        DenseBuf<uint32_t> bA = wrap(const_cast<uint32_t*>(A), m, k, lda);
+        DenseBuf<uint32_t> bB = wrap(const_cast<uint32_t*>(B), n, k, ldb);
+        DenseBuf<uint32_t> bC = wrap(C, m, n, ldc);
+        kernels::gemm_nt<uint32_t>(ctx, cview(bA), cview(bB), DenseView<uint32_t>(bC), gop);
+    });
+}
+
+// y op= A x; x and y contiguous vectors.
+int ref_gemv_u32(uint32_t p, uint32_t m, uint32_t k, const uint32_t* A, uint32_t lda, const uint32_t* x,
+                 uint32_t* y, int op) {
+    return guarded([&] {
+        const ModCtx<uint32_t> ctx(p);
+        const auto gop = op == 0 ? kernels::GemmOp::Set : op == 1 ? kernels::GemmOp::Add : kernels::GemmOp::Sub;
+        DenseBuf<uint32_t> bA = wrap(const_cast<uint32_t*>(A), m, k, lda);
+        DenseBuf<uint32_t> bx = wrap(const_cast<uint32_t*>(x), k, 1, 1);
+        DenseBuf<uint32_t> by = wrap(y, m, 1, 1);
+        kernels::gemv<uint32_t>(ctx, cview(bA), cview(bx), DenseView<uint32_t>(by), gop);
+    });
+}
+
+// y = y +/- alpha x (subtract != 0), or x = alpha x when y is null (scal).
+int ref_axpy_scal_u32(uint32_t p, uint32_t alpha, uint32_t rows, uint32_t cols, uint32_t* x, uint32_t ldx,
+                      uint32_t* y, uint32_t ldy, int subtract) {
+    return guarded([&] {
+        const ModCtx<uint32_t> ctx(p);
+        DenseBuf<uint32_t> bx = wrap(x, rows, cols, ldx);
+        if (y == nullptr) {
+            kernels::scal<uint32_t>(ctx, alpha, DenseView<uint32_t>(bx));
+            return;
+        }
+        DenseBuf<uint32_t> by = wrap(y, rows, cols, ldy);
+        kernels::axpy<uint32_t>(ctx, alpha, cview(bx), DenseView<uint32_t>(by), subtract != 0);
+    });
+}
+
+// C = T B with T m x m unit lower (lower != 0) or unit upper triangular.
+int ref_trmm_unit_u32(uint32_t p, int lower, uint32_t m, uint32_t n, const uint32_t* T, uint32_t ldt,
+                      const uint32_t* B, uint32_t ldb, uint32_t* C, uint32_t ldc) {
+    return guarded([&] {
+        const ModCtx<uint32_t> ctx(p);
+        DenseBuf<uint32_t> bT = wrap(const_cast<uint32_t*>(T), m, m, ldt);
+        bT.structure = lower ? Structure::LowerUnitri : Structure::UpperUnitri;
+        DenseBuf<uint32_t> bB = wrap(const_cast<uint32_t*>(B), m, n, ldb);
+        DenseBuf<uint32_t> bC = wrap(C, m, n, ldc);
+        kernels::trmm<uint32_t>(ctx, cview(bT), cview(bB), DenseView<uint32_t>(bC));
+    });
+}
+
+// dst (cols x rows) = src (rows x cols) transposed.
+int ref_transpose_u32(uint32_t rows, uint32_t cols, const uint32_t* src, uint32_t lds, uint32_t* dst, uint32_t ldd) {
+    return guarded([&] {
+        DenseBuf<uint32_t> bs = wrap(const_cast<uint32_t*>(src), rows, cols, lds);
+        DenseBuf<uint32_t> bd = wrap(dst, cols, rows, ldd);
+        kernels::transpose<uint32_t>(cview(bs), DenseView<uint32_t>(bd));
+    });
+}
+
+// v (entries below 2p) -> canonical in place.
+int ref_canonicalise_u32(uint32_t p, uint32_t rows, uint32_t cols, uint32_t* v, uint32_t ld) {
+    return guarded([&] {
+        const ModCtx<uint32_t> ctx(p);
+        DenseBuf<uint32_t> bv = wrap(v, rows, cols, ld);
+        bv.invariant = Invariant::Lazy2p;
+        kernels::canonicalise<uint32_t>(ctx, DenseView<uint32_t>(bv));
+    });
+}
+
+// dst = acc mod p for 64-bit accumulators.
+int ref_canonicalise_acc64_u32(uint32_t p, uint32_t rows, uint32_t cols, const uint64_t* acc, uint32_t lda,
+                               uint32_t* dst, uint32_t ldd) {
+    return guarded([&] {
+        const ModCtx<uint32_t> ctx(p);
+        DenseBuf<uint64_t> ba(const_cast<uint64_t*>(acc), static_cast<size_t>(rows) * lda, rows, cols,
+                              Layout::RowMajor, lda, Invariant::Accum64);
+        DenseBuf<uint32_t> bd = wrap(dst, rows, cols, ldd);
+        kernels::canonicalise(ctx, cview(ba), DenseView<uint32_t>(bd));
     });
 }
 
