@@ -42,4 +42,23 @@ int plain_gemm_u32_dev(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uin
     }
 }
 
+// The same for u64 residues (ModCtx<uint64_t>: Montgomery for odd p < 2^63, wide otherwise).
+int plain_gemm_u64_dev(uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t* A, size_t lda,
+                       const uint64_t* B, size_t ldb, uint64_t* C, size_t ldc, int op, void* stream) {
+    try {
+        const ModCtx<uint64_t> ctx(p);
+        cuda::DeviceView<const uint64_t> a(A, lda, 1, m, k);
+        cuda::DeviceView<const uint64_t> b(B, ldb, 1, k, n);
+        cuda::DeviceView<uint64_t> c(C, ldc, 1, m, n);
+        cuda::GemmOpts o;
+        o.imma = 0;
+        const auto gop = op == 0 ? kernels::GemmOp::Set : op == 1 ? kernels::GemmOp::Add : kernels::GemmOp::Sub;
+        cuda::gemm<uint64_t>(ctx, a, b, c, gop, cuda::Stream{stream}, o);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
 }  // extern "C"

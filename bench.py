@@ -237,6 +237,11 @@ def load_plain():
     L.plain_gemm_u32_dev.restype = C.c_int
     L.plain_gemm_u32_dev.argtypes = [C.c_uint32] * 4 + [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
                                                         C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]
+    if hasattr(L, "plain_gemm_u64_dev"):
+        L.plain_gemm_u64_dev.restype = C.c_int
+        L.plain_gemm_u64_dev.argtypes = [C.c_uint64] + [C.c_uint32] * 3 + [C.c_void_p, C.c_size_t, C.c_void_p,
+                                                                          C.c_size_t, C.c_void_p, C.c_size_t,
+                                                                          C.c_int, C.c_void_p]
     L.plain_last_error.restype = C.c_char_p
     return L
 
@@ -452,6 +457,39 @@ def extra_scheduler(eng, n_stream=50000, sample=2000):
     return out
 
 
+def gemm64_rate(n, p, steps=3, warmup=2):
+    """n^3 GEMM over u64 residues: hme (residue system over the limb GEMM) vs the plain method."""
+    import torch
+
+    import hacs_b200
+
+    torch.cuda.set_stream(torch.cuda.Stream())
+    eng = hacs_b200.Engine(0)
+    eng.use_torch_stream()
+    rng = np.random.default_rng(11)
+    A = torch.from_numpy(rng.integers(0, p, (n, n), dtype=np.uint64).view(np.int64)).cuda()
+    B = torch.from_numpy(rng.integers(0, p, (n, n), dtype=np.uint64).view(np.int64)).cuda()
+    Cm = torch.empty((n, n), dtype=torch.int64, device="cuda")
+    ms = time_device(lambda: eng.gemm_u64_dev(p, A, B, Cm), steps, warmup) / steps
+    eng.sync()
+    out = {"p": p, "n": n, "ms": ms, "tops": 2.0 * n ** 3 / ms / 1e9}
+    plain = load_plain()
+    if plain is not None and hasattr(plain, "plain_gemm_u64_dev"):
+        Cp = torch.empty_like(Cm)
+        st = torch.cuda.current_stream().cuda_stream
+
+        def run_plain():
+            rc = plain.plain_gemm_u64_dev(p, n, n, n, A.data_ptr(), n, B.data_ptr(), n, Cp.data_ptr(), n, 0, st)
+            if rc != 0:
+                raise RuntimeError(plain.plain_last_error().decode())
+
+        pms = time_device(run_plain, 1, 1)
+        out.update({"plain_gpu_ms": pms, "plain_gpu_tops": 2.0 * n ** 3 / pms / 1e9, "speedup_vs_plain": pms / ms,
+                    "bit_exact_vs_plain": bool(torch.equal(Cm, Cp))})
+    eng.close()
+    return out
+
+
 def run_case(args):
     """One kernel configuration for an ncu capture (prints a short JSON, not a bench line)."""
     import torch
@@ -542,6 +580,13 @@ def run_case(args):
         mlp.close()
         eng.close()
         return 0
+    if kind == "gemm64":
+        # gemm64:<n>:<p>: n^3 GEMM over u64 residues mod p (any p < 2^64) through hme_gemm_u64_dev, next to the
+        # reference's own u64 CUDA-core GEMM (the plain method) on the same device buffers
+        n, p = int(parts[1]), int(parts[2])
+        out = gemm64_rate(n, p, max(1, args.steps), args.warmup)
+        print(json.dumps(default=_json, obj={"case": args.case, **out}), flush=True)
+        return 0
     if kind == "level12":
         # level12:<m>:<n>:<p>: the device level-1 / level-2 operations on m x n operands (larger than L2 at
         # 8192 x 8192), each timed alone with CUDA events; GB/s of algorithmic bytes
@@ -615,7 +660,8 @@ def main():
                          "matrix; howell:<n>:<ell>:<k> / smith:<n>:<ell>:<k> runs W + K forms of a planted "
                          "U*D*V; jobs:<count> runs W + K batched GEMM + rank streams of the first <count> jobs; "
                          "mlp:<rows> trains the scheduler MLP for K epochs and plans <rows> shapes; level12:<m>:<n>:<p> "
-                         "times the device level-1 / level-2 operations on m x n operands")
+                         "times the device level-1 / level-2 operations on m x n operands; gemm64:<n>:<p> runs the "
+                         "u64-residue GEMM beside the plain method")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

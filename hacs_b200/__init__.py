@@ -181,6 +181,32 @@ class Engine:
         check(self._lib.hme_gemm_u32_dev(self._h, p, m, n, k, _dev_ptr(A), A.stride(0), _dev_ptr(B), B.stride(0),
                                          _dev_ptr(C), C.stride(0), op))
 
+    # ---- GEMM over u64 residues (engine::kernels::gemm<uint64_t>, Kernels.h:178-185) ----
+    def gemm_u64(self, p: int, A, B, C=None, op: int = SET) -> np.ndarray:
+        """C op= A*B mod p on host uint64 arrays, any modulus 2 <= p < 2^64 (canonical inputs)."""
+        A = np.ascontiguousarray(A, dtype=np.uint64)
+        B = np.ascontiguousarray(B, dtype=np.uint64)
+        m, k = A.shape
+        k2, n = B.shape
+        if k != k2:
+            raise ValueError("gemm_u64: inner dimensions differ")
+        out = np.zeros((m, n), np.uint64) if C is None else np.array(C, dtype=np.uint64, copy=True)
+        check(self._lib.hme_gemm_u64(self._h, p, m, n, k, A.ctypes.data, max(k, 1), B.ctypes.data, max(n, 1),
+                                     out.ctypes.data, max(n, 1), op))
+        return out
+
+    def gemm_u64_dev(self, p: int, A, B, C, op: int = SET) -> None:
+        """C op= A*B mod p on CUDA int64 / uint64 tensors (row-major), asynchronous on the engine's stream."""
+        for t in (A, B, C):
+            if t.element_size() != 8 or t.dim() != 2 or t.stride(1) != 1 or not t.is_cuda:
+                raise ValueError("gemm_u64_dev: 2-D CUDA 64-bit tensors with unit column stride")
+        m, k = A.shape
+        n = B.shape[1]
+        if B.shape[0] != k or tuple(C.shape) != (m, n):
+            raise ValueError("gemm_u64_dev: shape mismatch")
+        check(self._lib.hme_gemm_u64_dev(self._h, p, m, n, k, A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0),
+                                         C.data_ptr(), C.stride(0), op))
+
     # ---- device level-1 / level-2 operations (engine::cuda::*, src/Cuda/CudaKernels.h:120-247) ----
     def gemm_nt_dev(self, p: int, A, B, C, op: int = SET) -> None:
         """C op= A*B^T mod p with B given n x k (row-major)."""

@@ -71,6 +71,8 @@ PROTOTYPES = {
     "hme_canonicalise_u32_dev": (C.c_int, [vp, u32, u32, u32, vp, sz, sz]),
     "hme_canonicalise_acc64_u32_dev": (C.c_int, [vp, u32, u32, u32, vp, sz, sz, vp, sz, sz]),
     "hme_trsm_unit_u32_dev": (C.c_int, [vp, u32, C.c_int, u32, u32, vp, sz, vp, sz]),
+    "hme_gemm_u64": (C.c_int, [vp, C.c_uint64, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int]),
+    "hme_gemm_u64_dev": (C.c_int, [vp, C.c_uint64, u32, u32, u32, vp, sz, vp, sz, vp, sz, C.c_int]),
 }
 
 

@@ -1,0 +1,288 @@
+// The mod-p GEMM for u64 residues (any modulus 2 <= p < 2^64): C op= A*B mod p.
+//
+// Reference semantics: engine::kernels::gemm<uint64_t> / engine::cuda::gemm
+// <uint64_t> (src/ModArithmetic/Kernels.h:178-185; src/Cuda/cuda_kernels.cu
+// :151-163 and the u64 tiles :365-381): the exact sum of k products, reduced
+// to the canonical residue, combined by Set / Add / Sub.  The reference's u64
+// regime multiplies in Montgomery form (odd p < 2^63) or with a wide mulmod
+// (otherwise), one reduction per product, on CUDA cores.
+//
+// Method (residue number system).  With canonical inputs the exact integer
+// X = sum_k a_ik b_kj lies in [0, k (p-1)^2].  Pick t primes q_0 > q_1 > ...
+// just below 2^16 whose product M exceeds 4 k (p-1)^2.  Then:
+//   1. A_t = A mod q_t, B_t = B mod q_t (one pass over each operand);
+//   2. C_t = A_t B_t mod q_t: t products on the INT8-limb tensor-core GEMM
+//      (two limbs each, 4 limb products: 4t in all, against the 64 an
+//      8-limb u64 split would need);
+//   3. the CRT, element by element: y_t = C_t (M/q_t)^-1 mod q_t gives
+//      X = sum_t y_t M/q_t - w M with w = sum_t y_t / q_t - X/M, and since
+//      X/M < 1/4, w = rint(sum_t y_t / q_t) computed in double precision
+//      (error below 2^-45) is exact.  So X mod p = (sum_t y_t (M/q_t mod p)
+//      + w (p - M mod p)) mod p: a sum below 2^20 p, accumulated in 128 bits
+//      and reduced once (Montgomery REDC with the constants in Montgomery
+//      form for odd p < 2^63, a 128-bit remainder otherwise).
+// Moduli below 2^32 skip the RNS: the operands narrow to u32 and the u32 GEMM
+// computes the product mod p directly.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "hme_internal.h"
+
+namespace hme {
+namespace {
+
+constexpr int kMaxRns = 12;
+
+// The primes, the CRT constants and p's constants, passed by value.
+struct RnsPlan {
+    int t;
+    uint32_t q[kMaxRns];
+    uint64_t qbar[kMaxRns];  // floor(2^64 / q_t): reduce_u64 constant
+    uint32_t minv[kMaxRns];  // (M / q_t)^-1 mod q_t
+    double qinv[kMaxRns];    // 1 / q_t
+    uint64_t wm[kMaxRns];    // (M / q_t) mod p   (times 2^64 mod p when mont)
+    uint64_t mneg;           // (p - M mod p) mod p (times 2^64 mod p when mont)
+    uint64_t p;
+    uint64_t ninv;           // -p^-1 mod 2^64 (mont)
+    int mont;
+};
+
+using u128 = unsigned __int128;
+
+__device__ __forceinline__ void mac128(uint64_t& lo, uint64_t& hi, uint64_t a, uint64_t b) {
+    const uint64_t pl = a * b, ph = __umul64hi(a, b);
+    lo += pl;
+    hi += ph + (lo < pl ? 1u : 0u);
+}
+
+// (hi 2^64 + lo) 2^-64 mod p for hi 2^64 + lo < p 2^64, p odd and < 2^63
+__device__ __forceinline__ uint64_t redc(uint64_t lo, uint64_t hi, uint64_t p, uint64_t ninv) {
+    const uint64_t m = lo * ninv;
+    const uint64_t ml = m * p, mh = __umul64hi(m, p);
+    const uint64_t c = (lo + ml) < lo ? 1u : 0u;  // lo + m p == 0 mod 2^64
+    const uint64_t r = hi + mh + c;
+    return r >= p ? r - p : r;
+}
+
+__device__ __forceinline__ uint64_t add_mod64(uint64_t a, uint64_t b, uint64_t p) {
+    const uint64_t s = a + b;
+    return (s < a || s >= p) ? s - p : s;
+}
+__device__ __forceinline__ uint64_t sub_mod64(uint64_t a, uint64_t b, uint64_t p) {
+    return a >= b ? a - b : a + (p - b);
+}
+__device__ __forceinline__ uint64_t combine64(uint64_t old, uint64_t v, int op, uint64_t p) {
+    return op == HME_SET ? v : op == HME_ADD ? add_mod64(old, v, p) : sub_mod64(old, v, p);
+}
+
+// out[t][r][c] = X[r][c] mod q_t  (out planes rows x cols, contiguous)
+__global__ void __launch_bounds__(256) rns_residue_kernel(const uint64_t* __restrict__ X, uint64_t ldx, uint32_t rows,
+                                                          uint32_t cols, uint32_t* __restrict__ out,
+                                                          const __grid_constant__ RnsPlan P) {
+    const size_t plane = static_cast<size_t>(rows) * cols;
+    for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
+        for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
+            const uint64_t x = X[r * ldx + c];
+            const size_t o = static_cast<size_t>(r) * cols + c;
+            for (int t = 0; t < P.t; ++t) out[t * plane + o] = reduce_u64(x, P.q[t], P.qbar[t]);
+        }
+}
+
+// C[r][c] op= CRT(R[.][r][c]) mod p
+template <bool MONT>
+__global__ void __launch_bounds__(256) rns_crt_kernel(const uint32_t* __restrict__ R, uint32_t rows, uint32_t cols,
+                                                      uint64_t* __restrict__ C, uint64_t ldc, int op,
+                                                      const __grid_constant__ RnsPlan P) {
+    const size_t plane = static_cast<size_t>(rows) * cols;
+    for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
+        for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
+            const size_t o = static_cast<size_t>(r) * cols + c;
+            uint64_t lo = 0, hi = 0;
+            double wf = 0.0;
+            for (int t = 0; t < P.t; ++t) {
+                const uint32_t y = reduce_u64(static_cast<uint64_t>(R[t * plane + o]) * P.minv[t], P.q[t], P.qbar[t]);
+                wf = fma(static_cast<double>(y), P.qinv[t], wf);
+                mac128(lo, hi, y, P.wm[t]);
+            }
+            mac128(lo, hi, static_cast<uint64_t>(rint(wf)), P.mneg);
+            uint64_t v;
+            if constexpr (MONT)
+                v = redc(lo, hi, P.p, P.ninv);
+            else
+                v = static_cast<uint64_t>(((static_cast<u128>(hi) << 64) | lo) % P.p);
+            uint64_t* cp = C + r * ldc + c;
+            *cp = combine64(op == HME_SET ? 0u : *cp, v, op, P.p);
+        }
+}
+
+// u64 -> u32 (entries below p < 2^32)
+__global__ void __launch_bounds__(256) narrow_kernel(const uint64_t* __restrict__ X, uint64_t ldx, uint32_t rows,
+                                                     uint32_t cols, uint32_t* __restrict__ out) {
+    for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
+        for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x)
+            out[static_cast<size_t>(r) * cols + c] = static_cast<uint32_t>(X[r * ldx + c]);
+}
+// C[r][c] op= R[r][c]  mod p
+__global__ void __launch_bounds__(256) widen_kernel(const uint32_t* __restrict__ R, uint32_t rows, uint32_t cols,
+                                                    uint64_t* __restrict__ C, uint64_t ldc, int op, uint64_t p) {
+    for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
+        for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
+            uint64_t* cp = C + r * ldc + c;
+            *cp = combine64(op == HME_SET ? 0u : *cp, R[static_cast<size_t>(r) * cols + c], op, p);
+        }
+}
+__global__ void zero64_kernel(uint64_t* C, uint64_t ldc, uint32_t rows, uint32_t cols) {
+    for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
+        for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x)
+            C[r * ldc + c] = 0;
+}
+
+dim3 grid2d(uint32_t rows, uint32_t cols, int sms) {
+    const uint32_t gx = std::min<uint32_t>((cols + 255) / 256, 64);
+    const uint32_t gy = std::max<uint32_t>(1, std::min<uint32_t>(rows, static_cast<uint32_t>(sms) * 16 / gx + 1));
+    return dim3(gx, std::min<uint32_t>(gy, 65535));
+}
+
+uint64_t mulmod_host(uint64_t a, uint64_t b, uint64_t p) { return static_cast<uint64_t>(static_cast<u128>(a) * b % p); }
+uint32_t powmod32(uint32_t a, uint32_t e, uint32_t q) {
+    uint64_t r = 1, b = a % q;
+    for (; e; e >>= 1, b = b * b % q)
+        if (e & 1) r = r * b % q;
+    return static_cast<uint32_t>(r);
+}
+
+// The plan for modulus p >= 2^32 and inner dimension k.
+RnsPlan make_plan(uint64_t p, uint32_t k) {
+    RnsPlan P{};
+    // bits needed: M > 4 k (p-1)^2, with one bit of margin on the double-precision logs
+    const double need = std::log2(static_cast<double>(std::max<uint32_t>(k, 1))) +
+                        2.0 * std::log2(static_cast<double>(p - 1)) + 3.0;
+    double have = 0;
+    for (uint32_t q = 65521; q > 40000 && have <= need; q -= 2) {
+        if (!is_prime_u32(q)) continue;
+        HME_REQUIRE(P.t < kMaxRns, "gemm_u64: inner dimension too large for the residue system");
+        P.q[P.t++] = q;
+        have += std::log2(static_cast<double>(q));
+    }
+    HME_REQUIRE(have > need, "gemm_u64: inner dimension too large for the residue system");
+    P.p = p;
+    P.mont = (p & 1) && p < (uint64_t(1) << 63);
+    const uint64_t r64 = P.mont ? static_cast<uint64_t>((static_cast<u128>(1) << 64) % p) : 1;  // 2^64 mod p
+    uint64_t m_mod_p = 1;
+    for (int t = 0; t < P.t; ++t) m_mod_p = mulmod_host(m_mod_p, P.q[t], p);
+    for (int t = 0; t < P.t; ++t) {
+        const uint32_t q = P.q[t];
+        uint64_t mt_p = 1;   // (M / q_t) mod p
+        uint32_t mt_q = 1;   // (M / q_t) mod q_t
+        for (int s = 0; s < P.t; ++s)
+            if (s != t) {
+                mt_p = mulmod_host(mt_p, P.q[s], p);
+                mt_q = static_cast<uint32_t>(static_cast<uint64_t>(mt_q) * (P.q[s] % q) % q);
+            }
+        P.minv[t] = powmod32(mt_q, q - 2, q);
+        P.qbar[t] = make_mod(q).barrett;
+        P.qinv[t] = 1.0 / static_cast<double>(q);
+        P.wm[t] = P.mont ? mulmod_host(mt_p, r64, p) : mt_p;
+    }
+    const uint64_t neg = m_mod_p ? p - m_mod_p : 0;
+    P.mneg = P.mont ? mulmod_host(neg, r64, p) : neg;
+    if (P.mont) {
+        uint64_t inv = p;  // Newton: p inv == 1 mod 2^64
+        for (int i = 0; i < 6; ++i) inv *= 2 - p * inv;
+        P.ninv = 0 - inv;
+    }
+    return P;
+}
+
+// C op= A*B mod p, device pointers, on ctx->stream.
+void gemm_u64_device(hme_ctx* ctx, uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t* A, size_t lda,
+                     const uint64_t* B, size_t ldb, uint64_t* C, size_t ldc, int op) {
+    HME_REQUIRE(p >= 2, "gemm_u64: modulus must be >= 2");
+    HME_REQUIRE(op == HME_SET || op == HME_ADD || op == HME_SUB, "gemm_u64: op must be HME_SET, HME_ADD or HME_SUB");
+    if (m == 0 || n == 0) return;
+    HME_REQUIRE(C && ldc >= n, "gemm_u64: bad C");
+    if (k == 0) {
+        if (op == HME_SET) {
+            HME_TIMED(ctx, "zero64", zero64_kernel<<<grid2d(m, n, ctx->num_sms), 256, 0, ctx->stream>>>(C, ldc, m, n));
+            HME_CUDA(cudaGetLastError());
+        }
+        return;
+    }
+    HME_REQUIRE(A && B && lda >= k && ldb >= n, "gemm_u64: bad A / B");
+    const int sms = ctx->num_sms;
+    if (p < (uint64_t(1) << 32)) {
+        uint32_t* a32 = static_cast<uint32_t*>(ctx->ws.get(kSlotRns0, 4ull * m * k));
+        uint32_t* b32 = static_cast<uint32_t*>(ctx->ws.get(kSlotRns1, 4ull * k * n));
+        uint32_t* c32 = static_cast<uint32_t*>(ctx->ws.get(kSlotRns2, 4ull * m * n));
+        HME_TIMED(ctx, "narrow", narrow_kernel<<<grid2d(m, k, sms), 256, 0, ctx->stream>>>(A, lda, m, k, a32));
+        HME_TIMED(ctx, "narrow", narrow_kernel<<<grid2d(k, n, sms), 256, 0, ctx->stream>>>(B, ldb, k, n, b32));
+        HME_CUDA(cudaGetLastError());
+        gemm_u32_device(ctx, make_mod(static_cast<uint32_t>(p)), m, n, k, a32, k, b32, n, c32, n, HME_SET);
+        HME_TIMED(ctx, "widen", widen_kernel<<<grid2d(m, n, sms), 256, 0, ctx->stream>>>(c32, m, n, C, ldc, op, p));
+        HME_CUDA(cudaGetLastError());
+        return;
+    }
+    const RnsPlan P = make_plan(p, k);
+    const size_t pa = static_cast<size_t>(m) * k, pb = static_cast<size_t>(k) * n, pc = static_cast<size_t>(m) * n;
+    uint32_t* ra = static_cast<uint32_t*>(ctx->ws.get(kSlotRns0, 4 * pa * P.t));
+    uint32_t* rb = static_cast<uint32_t*>(ctx->ws.get(kSlotRns1, 4 * pb * P.t));
+    uint32_t* rc = static_cast<uint32_t*>(ctx->ws.get(kSlotRns2, 4 * pc * P.t));
+    HME_TIMED(ctx, "rns_residue", rns_residue_kernel<<<grid2d(m, k, sms), 256, 0, ctx->stream>>>(A, lda, m, k, ra, P));
+    HME_TIMED(ctx, "rns_residue", rns_residue_kernel<<<grid2d(k, n, sms), 256, 0, ctx->stream>>>(B, ldb, k, n, rb, P));
+    HME_CUDA(cudaGetLastError());
+    for (int t = 0; t < P.t; ++t)
+        gemm_u32_device(ctx, make_mod(P.q[t]), m, n, k, ra + t * pa, k, rb + t * pb, n, rc + t * pc, n, HME_SET);
+    if (P.mont)
+        HME_TIMED(ctx, "rns_crt", rns_crt_kernel<true><<<grid2d(m, n, sms), 256, 0, ctx->stream>>>(rc, m, n, C, ldc,
+                                                                                                  op, P));
+    else
+        HME_TIMED(ctx, "rns_crt", rns_crt_kernel<false><<<grid2d(m, n, sms), 256, 0, ctx->stream>>>(rc, m, n, C, ldc,
+                                                                                                   op, P));
+    HME_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+}  // namespace hme
+
+using namespace hme;
+
+extern "C" {
+
+int hme_gemm_u64_dev(hme_ctx* ctx, uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t* A, size_t lda,
+                     const uint64_t* B, size_t ldb, uint64_t* C, size_t ldc, int op) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        bind(ctx);
+        gemm_u64_device(ctx, p, m, n, k, A, lda, B, ldb, C, ldc, op);
+    });
+}
+
+int hme_gemm_u64(hme_ctx* ctx, uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t* A, size_t lda,
+                 const uint64_t* B, size_t ldb, uint64_t* C, size_t ldc, int op) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        HME_REQUIRE(op == HME_SET || op == HME_ADD || op == HME_SUB, "gemm_u64: op must be HME_SET, HME_ADD or HME_SUB");
+        if (m == 0 || n == 0) return;
+        HME_REQUIRE(C && ldc >= n && (k == 0 || (A && B && lda >= k && ldb >= n)), "gemm_u64: bad buffers");
+        bind(ctx);
+        uint64_t* dA = k ? static_cast<uint64_t*>(ctx->ws.get(kSlotStageA, 8ull * m * k)) : nullptr;
+        uint64_t* dB = k ? static_cast<uint64_t*>(ctx->ws.get(kSlotStageB, 8ull * k * n)) : nullptr;
+        uint64_t* dC = static_cast<uint64_t*>(ctx->ws.get(kSlotStageC, 8ull * m * n));
+        if (k) {
+            HME_CUDA(copy_rows_async(dA, 8ull * k, A, 8 * lda, 8ull * k, m, cudaMemcpyHostToDevice, ctx->stream));
+            HME_CUDA(copy_rows_async(dB, 8ull * n, B, 8 * ldb, 8ull * n, k, cudaMemcpyHostToDevice, ctx->stream));
+        }
+        if (op != HME_SET)
+            HME_CUDA(copy_rows_async(dC, 8ull * n, C, 8 * ldc, 8ull * n, m, cudaMemcpyHostToDevice, ctx->stream));
+        gemm_u64_device(ctx, p, m, n, k, dA, k, dB, n, dC, n, op);
+        if (op == HME_SET || k)
+            HME_CUDA(copy_rows_async(C, 8 * ldc, dC, 8ull * n, 8ull * n, m, cudaMemcpyDeviceToHost, ctx->stream));
+        HME_CUDA(cudaStreamSynchronize(ctx->stream));
+        check_device_error(ctx);
+    });
+}
+
+}  // extern "C"

@@ -67,6 +67,9 @@ enum WorkspaceSlot : int {
     kSlotSched0 = 26,  // scheduler / autotuner
     kSlotSched1 = 27,
     kSlotJobs8 = 28,   // batched job stream: the pivot blocks' inverses
+    kSlotRns0 = 29,    // u64 GEMM: residues of A, B and the products mod the RNS primes
+    kSlotRns1 = 30,
+    kSlotRns2 = 31,
 };
 
 struct Workspace {

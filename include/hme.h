@@ -95,6 +95,23 @@ HME_API int hme_gemm_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint3
 HME_API int hme_gemm_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A,
                      size_t lda, const uint32_t *B, size_t ldb, uint32_t *C, size_t ldc, int op);
 
+/* ---- dense mod-p GEMM over u64 residues -----------------------------------
+ * C op= A*B mod p for u64 residues, any modulus 2 <= p < 2^64; entries of A
+ * and B must be canonical (< p).  Bit-exact with engine::kernels::gemm
+ * <uint64_t> (src/ModArithmetic/Kernels.h:178-185) and the device u64 regime
+ * engine::cuda::gemm<uint64_t> (src/Cuda/cuda_kernels.cu:151-163, 365-381).
+ * Method: p < 2^32 runs the u32 limb GEMM directly; larger p runs t limb GEMMs
+ * modulo primes below 2^16 (t chosen so that their product exceeds
+ * 4 k (p-1)^2) and reconstructs each entry by the Chinese remainder theorem,
+ * reduced mod p once (Montgomery for odd p < 2^63).  Device workspace: 12 t
+ * (mk + kn + mn) bytes (t <= 12).
+ * hme_gemm_u64: host pointers (synchronous); hme_gemm_u64_dev: device
+ * pointers, asynchronous on the context's stream. */
+HME_API int hme_gemm_u64(hme_ctx *ctx, uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t *A, size_t lda,
+                         const uint64_t *B, size_t ldb, uint64_t *C, size_t ldc, int op);
+HME_API int hme_gemm_u64_dev(hme_ctx *ctx, uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t *A,
+                             size_t lda, const uint64_t *B, size_t ldb, uint64_t *C, size_t ldc, int op);
+
 /* ---- device level-1 / level-2 operations ----------------------------------
  * The rest of the device layer the tape's DeviceBackend drives, on device
  * pointers, asynchronous on the context's stream.  A view is (pointer, rows,

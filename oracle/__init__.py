@@ -54,6 +54,9 @@ def lib():
         L.orc_fnv_matrix.restype = C.c_uint64
         L.orc_fnv_matrix.argtypes = [u32p, C.c_uint32, C.c_uint32, C.c_uint32]
         L.orc_gemm_u32.argtypes = [C.c_uint32] * 4 + [u32p, C.c_uint32, u32p, C.c_uint32, u32p, C.c_uint32, C.c_int]
+        u64p_ = C.POINTER(C.c_uint64)
+        L.orc_gemm_u64.argtypes = [C.c_uint64] + [C.c_uint32] * 3 + [u64p_, C.c_uint32, u64p_, C.c_uint32, u64p_,
+                                                                       C.c_uint32, C.c_int]
         L.orc_rref_u32.restype = C.c_int64
         L.orc_rref_u32.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, u32p, C.c_uint32, u32p]
         L.orc_det_u32.restype = C.c_int64
@@ -106,6 +109,7 @@ def ref():
         L.ref_transpose_u32.argtypes = [u32, u32, u32p, u32, u32p, u32]
         L.ref_canonicalise_u32.argtypes = [u32] * 3 + [u32p, u32]
         L.ref_canonicalise_acc64_u32.argtypes = [u32] * 3 + [u64p, u32, u32p, u32]
+        L.ref_gemm_u64.argtypes = [C.c_uint64, u32, u32, u32, u64p, u32, u64p, u32, u64p, u32, C.c_int]
         _REF = L
     return _REF
 
@@ -373,3 +377,32 @@ def ref_canonicalise_acc64(p: int, acc) -> np.ndarray:
     d = np.zeros((r, c), np.uint32)
     _chk(ref().ref_canonicalise_acc64_u32(p, r, c, acc.ctypes.data_as(C.POINTER(C.c_uint64)), c, _p(d), c), "ref")
     return d
+
+
+# ---- u64 residues ------------------------------------------------------------------
+def _u64a(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def _p64(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint64))
+
+
+def gemm_u64(p: int, A, B, C_=None, op: int = 0) -> np.ndarray:
+    """C op= A*B mod p over u64 residues (restatement, oracle.c orc_gemm_u64)."""
+    A, B = _u64a(A), _u64a(B)
+    m, k = A.shape
+    n = B.shape[1]
+    Cm = np.zeros((m, n), np.uint64) if C_ is None else _u64a(C_).copy()
+    _chk(lib().orc_gemm_u64(p, m, n, k, _p64(A), max(k, 1), _p64(B), max(n, 1), _p64(Cm), max(n, 1), op))
+    return Cm
+
+
+def ref_gemm_u64(p: int, A, B, C_=None, op: int = 0) -> np.ndarray:
+    """The reference's kernels::gemm<uint64_t> (oracle/_ref)."""
+    A, B = _u64a(A), _u64a(B)
+    m, k = A.shape
+    n = B.shape[1]
+    Cm = np.zeros((m, n), np.uint64) if C_ is None else _u64a(C_).copy()
+    _chk(ref().ref_gemm_u64(p, m, n, k, _p64(A), max(k, 1), _p64(B), max(n, 1), _p64(Cm), max(n, 1), op), "ref")
+    return Cm

@@ -102,6 +102,29 @@ int orc_gemm_u32(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t 
     return 0;
 }
 
+/* C op= A*B mod p over u64 residues, any 2 <= p < 2^64 (engine::kernels::gemm
+ * <uint64_t>, src/ModArithmetic/Kernels.h:178-185; the u64 regime of
+ * ModCtx<uint64_t>, ModCtx.h:226-248): each product reduced with a 128-bit
+ * remainder, summed mod p.  Canonical inputs. */
+int orc_gemm_u64(uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t *A, uint32_t lda,
+                 const uint64_t *B, uint32_t ldb, uint64_t *C, uint32_t ldc, int op) {
+    if (p < 2 || op < 0 || op > 2) return -1;
+    for (uint32_t i = 0; i < m; ++i)
+        for (uint32_t j = 0; j < n; ++j) {
+            unsigned __int128 s = 0;
+            for (uint32_t t = 0; t < k; ++t) {
+                s += (unsigned __int128)A[(size_t)i * lda + t] * B[(size_t)t * ldb + j] % p;
+                if (s >= p) s -= p;
+            }
+            const uint64_t r = (uint64_t)s;
+            uint64_t *c = C + (size_t)i * ldc + j;
+            if (op == 0) *c = r;
+            else if (op == 1) { const unsigned __int128 x = (unsigned __int128)*c + r; *c = (uint64_t)(x >= p ? x - p : x); }
+            else *c = *c >= r ? *c - r : (uint64_t)((unsigned __int128)*c + p - r);
+        }
+    return 0;
+}
+
 /* ---- RREF over F_p ------------------------------------------------------
  * Gauss-Jordan with the legacy pivot rule (RefLinAlg.cpp rref; DenseElim.h
  * header): leftmost column with a non-zero at or below the current row,

@@ -31,6 +31,8 @@ uint64_t orc_fnv_matrix(const uint32_t *M, uint32_t rows, uint32_t cols, uint32_
  * u64 accumulation over k_max products (ModCtx.h:139-142, 233-235). */
 int orc_gemm_u32(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A, uint32_t lda,
                  const uint32_t *B, uint32_t ldb, uint32_t *C, uint32_t ldc, int op);
+int orc_gemm_u64(uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t *A, uint32_t lda,
+                 const uint64_t *B, uint32_t ldb, uint64_t *C, uint32_t ldc, int op);
 
 /* In-place RREF over F_p (leading 1, zero rows at the bottom); pivot columns
  * ascending into pivots[] (>= min(m,n) entries).  Returns the rank.

@@ -105,6 +105,20 @@ int ref_gemm_u32(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t*
     });
 }
 
+// C op= A*B mod p over u64 residues (ModCtx<uint64_t>: Montgomery for odd
+// p < 2^63, wide otherwise).
+int ref_gemm_u64(uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t* A, uint32_t lda,
+                 const uint64_t* B, uint32_t ldb, uint64_t* C, uint32_t ldc, int op) {
+    return guarded([&] {
+        const ModCtx<uint64_t> ctx(p);
+        const auto gop = op == 0 ? kernels::GemmOp::Set : op == 1 ? kernels::GemmOp::Add : kernels::GemmOp::Sub;
+        DenseBuf<uint64_t> bA(const_cast<uint64_t*>(A), static_cast<size_t>(m) * lda, m, k, Layout::RowMajor, lda);
+        DenseBuf<uint64_t> bB(const_cast<uint64_t*>(B), static_cast<size_t>(k) * ldb, k, n, Layout::RowMajor, ldb);
+        DenseBuf<uint64_t> bC(C, static_cast<size_t>(m) * ldc, m, n, Layout::RowMajor, ldc);
+        kernels::gemm<uint64_t>(ctx, cview(bA), cview(bB), DenseView<uint64_t>(bC), gop);
+    });
+}
+
 // Level-1 / level-2 CPU kernels of the reference, row-major with leading dims.
 // C op= A * B^T with B given n x k.
 int ref_gemm_nt_u32(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A, uint32_t lda,

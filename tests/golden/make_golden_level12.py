@@ -8,7 +8,8 @@ oracle/_ref/libhacsref.so has been built (``make -C oracle ref``):
 The values come from the reference library's level-1 / level-2 kernels
 (drjanosch42/hacs 0.2.1, src/ModArithmetic/Kernels.h:188-259: gemv, gemm_nt,
 axpy, scal, transpose, canonicalise, trmm) on inputs from the reference's
-seeded EngineMatrix generator, stored as FNV-1a-64 checksums (the reference
+seeded EngineMatrix generator, and from its u64 GEMM (kernels::gemm
+<uint64_t>) on seeded numpy inputs (`gemm_u64`), stored as FNV-1a-64 checksums (the reference
 micro bench's checksum).  The `micro_gemv` and `micro_transpose` entries are
 the workloads of the reference's `--bench micro gemv|transpose` (EngineMatrix
 salts 3 / 4 and 5, src/Cuda/CudaBench.cpp:91-135).  The reference's CPU engine
@@ -87,6 +88,20 @@ def main():
             X = L12.trsm_unit(p, T, B, lower)
             assert np.array_equal(O.ref_trmm_unit(p, T, X, lower), B), "reference trmm disagrees"
             out["trsm"].append({"m": m, "n": n, "p": p, "lower": lower, "salts": [14, 15], "fnv": fnv(X)})
+
+    # u64 residues: the reference's kernels::gemm<uint64_t> on seeded numpy inputs; the checksum is the FNV
+    # of the result viewed as u32 words (rows x 2 cols, low word first)
+    out["gemm_u64"] = []
+    for m, n, k, p, op, seed in [(64, 48, 200, 2305843009213693951, 0, 1), (100, 70, 513, 18446744073709551557, 1, 2),
+                                 (33, 129, 1000, 134217757, 2, 3), (40, 40, 64, 1099511627776, 0, 4),
+                                 (57, 31, 300, 9223372036854775837, 2, 5), (20, 20, 20, 2, 1, 6)]:
+        rng = np.random.default_rng(seed)
+        A = rng.integers(0, p, (m, k), dtype=np.uint64)
+        B = rng.integers(0, p, (k, n), dtype=np.uint64)
+        C = rng.integers(0, p, (m, n), dtype=np.uint64)
+        R = O.ref_gemm_u64(p, A, B, C, op)
+        out["gemm_u64"].append({"m": m, "n": n, "k": k, "p": p, "op": op, "seed": seed,
+                                "fnv": fnv(R.view(np.uint32).reshape(m, 2 * n))})
 
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "level12.json")
     with open(path, "w") as f:
