@@ -473,6 +473,15 @@ def gemm64_rate(n, p, steps=3, warmup=2):
     ms = time_device(lambda: eng.gemm_u64_dev(p, A, B, Cm), steps, warmup) / steps
     eng.sync()
     out = {"p": p, "n": n, "ms": ms, "tops": 2.0 * n ** 3 / ms / 1e9}
+    # per-kernel CUDA-event times of one more call (library timer on the launching stream)
+    eng.set_timing(True)
+    eng.timing_reset()
+    eng.gemm_u64_dev(p, A, B, Cm)
+    eng.sync()
+    out["kernels_ms"] = {k: round(eng.kernel_time(k)[0], 4) for k in
+                         ("rns_residue", "rns_crt", "narrow", "widen", "limb_split", "limb_gemm", "simt_gemm")
+                         if eng.kernel_time(k)[1]}
+    eng.set_timing(False)
     plain = load_plain()
     if plain is not None and hasattr(plain, "plain_gemm_u64_dev"):
         Cp = torch.empty_like(Cm)
