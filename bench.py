@@ -14,7 +14,9 @@ the reference CPU engine timed on this host (cpu_baseline), the end-to-end
 rate through the public host-pointer API (pinned host buffers, H2D + D2H
 inside the timed region), SM clocks sampled during the timed region, and the
 8192^3 GEMM at p = 65521 (2 limbs) and p = 2^31 - 19 (4 limbs) next to the
-reference's own CUDA-core GEMM (the plain method) on the same buffers.
+reference's own CUDA-core GEMM (the plain method) on the same buffers, and
+the u64-residue GEMM 2048^3 at p = 2^61 - 1 beside the reference's u64 plain
+method.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl hme|reference]
 
@@ -786,6 +788,7 @@ def main():
         ext.update(extra_ring(eng))
         ext["jobstream_config4"] = extra_jobstream(eng, plain)
         ext["scheduler_config5"] = extra_scheduler(eng)
+        ext["gemm_u64_2048_p2^61-1"] = gemm64_rate(2048, 2**61 - 1)
         line["extras"] = ext
     if rank == 0:
         print(json.dumps(line, default=_json), flush=True)

@@ -14,7 +14,8 @@
 //   2. C_t = A_t B_t mod q_t: t products on the INT8-limb tensor-core GEMM
 //      (two limbs each, 4 limb products: 4t in all, against the 64 an
 //      8-limb u64 split would need);
-//   3. the CRT, element by element: y_t = C_t (M/q_t)^-1 mod q_t gives
+//   3. the CRT, element by element (32-bit arithmetic throughout except the
+//      final reduction): y_t = C_t (M/q_t)^-1 mod q_t gives
 //      X = sum_t y_t M/q_t - w M with w = sum_t y_t / q_t - X/M, and since
 //      X/M < 1/4, w = rint(sum_t y_t / q_t) computed in double precision
 //      (error below 2^-45) is exact.  So X mod p = (sum_t y_t (M/q_t mod p)
@@ -36,27 +37,33 @@ namespace {
 
 constexpr int kMaxRns = 12;
 
-// The primes, the CRT constants and p's constants, passed by value.
+// The primes, the CRT constants and p's constants, passed by value.  All the
+// per-prime arithmetic is 32-bit: the primes are below 2^16, so x mod q_t
+// for x < 2^32 is one 32-bit Barrett step (qm = floor(2^32 / q_t)), and the
+// 64-bit constants enter as 32-bit halves.
 struct RnsPlan {
     int t;
     uint32_t q[kMaxRns];
-    uint64_t qbar[kMaxRns];  // floor(2^64 / q_t): reduce_u64 constant
+    uint32_t qm[kMaxRns];    // floor(2^32 / q_t)
+    uint32_t c32[kMaxRns];   // 2^32 mod q_t
     uint32_t minv[kMaxRns];  // (M / q_t)^-1 mod q_t
     double qinv[kMaxRns];    // 1 / q_t
-    uint64_t wm[kMaxRns];    // (M / q_t) mod p   (times 2^64 mod p when mont)
-    uint64_t mneg;           // (p - M mod p) mod p (times 2^64 mod p when mont)
+    uint32_t wlo[kMaxRns];   // W_t = (M / q_t) mod p (times 2^64 mod p when mont): low and high 32 bits
+    uint32_t whi[kMaxRns];
+    uint32_t nlo, nhi;       // (p - M mod p) mod p (times 2^64 mod p when mont): low and high 32 bits
     uint64_t p;
     uint64_t ninv;           // -p^-1 mod 2^64 (mont)
     int mont;
 };
 
-using u128 = unsigned __int128;
-
-__device__ __forceinline__ void mac128(uint64_t& lo, uint64_t& hi, uint64_t a, uint64_t b) {
-    const uint64_t pl = a * b, ph = __umul64hi(a, b);
-    lo += pl;
-    hi += ph + (lo < pl ? 1u : 0u);
+// x mod q for x < 2^32, q < 2^16, qm = floor(2^32 / q): the quotient estimate
+// floor(x qm / 2^32) is floor(x / q) or one less, so one correction suffices.
+__device__ __forceinline__ uint32_t red32(uint32_t x, uint32_t q, uint32_t qm) {
+    const uint32_t r = x - __umulhi(x, qm) * q;
+    return r >= q ? r - q : r;
 }
+
+using u128 = unsigned __int128;
 
 // (hi 2^64 + lo) 2^-64 mod p for hi 2^64 + lo < p 2^64, p odd and < 2^63
 __device__ __forceinline__ uint64_t redc(uint64_t lo, uint64_t hi, uint64_t p, uint64_t ninv) {
@@ -86,8 +93,13 @@ __global__ void __launch_bounds__(256) rns_residue_kernel(const uint64_t* __rest
     for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
         for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
             const uint64_t x = X[r * ldx + c];
+            const uint32_t xl = static_cast<uint32_t>(x), xh = static_cast<uint32_t>(x >> 32);
             const size_t o = static_cast<size_t>(r) * cols + c;
-            for (int t = 0; t < P.t; ++t) out[t * plane + o] = reduce_u64(x, P.q[t], P.qbar[t]);
+            for (int t = 0; t < P.t; ++t) {
+                // x = xh 2^32 + xl; (xh mod q)(2^32 mod q) + (xl mod q) <= (q-1)^2 + q - 1 < 2^32
+                const uint32_t q = P.q[t], qm = P.qm[t];
+                out[t * plane + o] = red32(red32(xh, q, qm) * P.c32[t] + red32(xl, q, qm), q, qm);
+            }
         }
 }
 
@@ -100,14 +112,21 @@ __global__ void __launch_bounds__(256) rns_crt_kernel(const uint32_t* __restrict
     for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
         for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
             const size_t o = static_cast<size_t>(r) * cols + c;
-            uint64_t lo = 0, hi = 0;
+            // T = sum_t y_t W_t + w N = s0 + s1 2^32 with s0 = sum y (W mod 2^32), s1 = sum y (W >> 32):
+            // each term below 2^48, at most 13 terms, so both sums stay below 2^52
+            uint64_t s0 = 0, s1 = 0;
             double wf = 0.0;
             for (int t = 0; t < P.t; ++t) {
-                const uint32_t y = reduce_u64(static_cast<uint64_t>(R[t * plane + o]) * P.minv[t], P.q[t], P.qbar[t]);
+                const uint32_t y = red32(R[t * plane + o] * P.minv[t], P.q[t], P.qm[t]);  // both < 2^16
                 wf = fma(static_cast<double>(y), P.qinv[t], wf);
-                mac128(lo, hi, y, P.wm[t]);
+                s0 += static_cast<uint64_t>(y) * P.wlo[t];
+                s1 += static_cast<uint64_t>(y) * P.whi[t];
             }
-            mac128(lo, hi, static_cast<uint64_t>(rint(wf)), P.mneg);
+            const uint32_t w = static_cast<uint32_t>(rint(wf));
+            s0 += static_cast<uint64_t>(w) * P.nlo;
+            s1 += static_cast<uint64_t>(w) * P.nhi;
+            const uint64_t lo = s0 + (s1 << 32);
+            const uint64_t hi = (s1 >> 32) + (lo < s0 ? 1u : 0u);
             uint64_t v;
             if constexpr (MONT)
                 v = redc(lo, hi, P.p, P.ninv);
@@ -183,12 +202,17 @@ RnsPlan make_plan(uint64_t p, uint32_t k) {
                 mt_q = static_cast<uint32_t>(static_cast<uint64_t>(mt_q) * (P.q[s] % q) % q);
             }
         P.minv[t] = powmod32(mt_q, q - 2, q);
-        P.qbar[t] = make_mod(q).barrett;
+        P.qm[t] = static_cast<uint32_t>((uint64_t(1) << 32) / q);
+        P.c32[t] = static_cast<uint32_t>((uint64_t(1) << 32) % q);
         P.qinv[t] = 1.0 / static_cast<double>(q);
-        P.wm[t] = P.mont ? mulmod_host(mt_p, r64, p) : mt_p;
+        const uint64_t w = P.mont ? mulmod_host(mt_p, r64, p) : mt_p;
+        P.wlo[t] = static_cast<uint32_t>(w);
+        P.whi[t] = static_cast<uint32_t>(w >> 32);
     }
     const uint64_t neg = m_mod_p ? p - m_mod_p : 0;
-    P.mneg = P.mont ? mulmod_host(neg, r64, p) : neg;
+    const uint64_t nm = P.mont ? mulmod_host(neg, r64, p) : neg;
+    P.nlo = static_cast<uint32_t>(nm);
+    P.nhi = static_cast<uint32_t>(nm >> 32);
     if (P.mont) {
         uint64_t inv = p;  // Newton: p inv == 1 mod 2^64
         for (int i = 0; i < 6; ++i) inv *= 2 - p * inv;
