@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "hme_internal.h"
@@ -85,7 +86,9 @@ __device__ __forceinline__ uint64_t combine64(uint64_t old, uint64_t v, int op, 
     return op == HME_SET ? v : op == HME_ADD ? add_mod64(old, v, p) : sub_mod64(old, v, p);
 }
 
-// out[t][r][c] = X[r][c] mod q_t  (out planes rows x cols, contiguous)
+// out[t][r][c] = X[r][c] mod q_t  (out planes rows x cols, contiguous); NT =
+// the number of primes, so the loop unrolls and the constants are immediates
+template <int NT>
 __global__ void __launch_bounds__(256) rns_residue_kernel(const uint64_t* __restrict__ X, uint64_t ldx, uint32_t rows,
                                                           uint32_t cols, uint32_t* __restrict__ out,
                                                           const __grid_constant__ RnsPlan P) {
@@ -94,30 +97,35 @@ __global__ void __launch_bounds__(256) rns_residue_kernel(const uint64_t* __rest
         for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
             const uint64_t x = X[r * ldx + c];
             const uint32_t xl = static_cast<uint32_t>(x), xh = static_cast<uint32_t>(x >> 32);
-            const size_t o = static_cast<size_t>(r) * cols + c;
-            for (int t = 0; t < P.t; ++t) {
+            uint32_t* dst = out + static_cast<size_t>(r) * cols + c;
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
                 // x = xh 2^32 + xl; (xh mod q)(2^32 mod q) + (xl mod q) <= (q-1)^2 + q - 1 < 2^32
                 const uint32_t q = P.q[t], qm = P.qm[t];
-                out[t * plane + o] = red32(red32(xh, q, qm) * P.c32[t] + red32(xl, q, qm), q, qm);
+                dst[t * plane] = red32(red32(xh, q, qm) * P.c32[t] + red32(xl, q, qm), q, qm);
             }
         }
 }
 
 // C[r][c] op= CRT(R[.][r][c]) mod p
-template <bool MONT>
+template <bool MONT, int NT>
 __global__ void __launch_bounds__(256) rns_crt_kernel(const uint32_t* __restrict__ R, uint32_t rows, uint32_t cols,
                                                       uint64_t* __restrict__ C, uint64_t ldc, int op,
                                                       const __grid_constant__ RnsPlan P) {
     const size_t plane = static_cast<size_t>(rows) * cols;
     for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
         for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
-            const size_t o = static_cast<size_t>(r) * cols + c;
+            const uint32_t* src = R + static_cast<size_t>(r) * cols + c;
             // T = sum_t y_t W_t + w N = s0 + s1 2^32 with s0 = sum y (W mod 2^32), s1 = sum y (W >> 32):
             // each term below 2^48, at most 13 terms, so both sums stay below 2^52
             uint64_t s0 = 0, s1 = 0;
             double wf = 0.0;
-            for (int t = 0; t < P.t; ++t) {
-                const uint32_t y = red32(R[t * plane + o] * P.minv[t], P.q[t], P.qm[t]);  // both < 2^16
+            uint32_t rv[NT];
+#pragma unroll
+            for (int t = 0; t < NT; ++t) rv[t] = src[t * plane];
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                const uint32_t y = red32(rv[t] * P.minv[t], P.q[t], P.qm[t]);  // both < 2^16
                 wf = fma(static_cast<double>(y), P.qinv[t], wf);
                 s0 += static_cast<uint64_t>(y) * P.wlo[t];
                 s1 += static_cast<uint64_t>(y) * P.whi[t];
@@ -157,6 +165,23 @@ __global__ void zero64_kernel(uint64_t* C, uint64_t ldc, uint32_t rows, uint32_t
     for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
         for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x)
             C[r * ldc + c] = 0;
+}
+
+// f(std::integral_constant<int, t>) for the plan's prime count t (5..12: p >= 2^32 needs
+// at least 67 bits of M, and a plan holds at most kMaxRns primes)
+template <class F>
+void with_primes(int t, F&& f) {
+    switch (t) {
+        case 5: f(std::integral_constant<int, 5>{}); break;
+        case 6: f(std::integral_constant<int, 6>{}); break;
+        case 7: f(std::integral_constant<int, 7>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        case 9: f(std::integral_constant<int, 9>{}); break;
+        case 10: f(std::integral_constant<int, 10>{}); break;
+        case 11: f(std::integral_constant<int, 11>{}); break;
+        case 12: f(std::integral_constant<int, 12>{}); break;
+        default: throw Error(HME_EINVAL, "gemm_u64: unsupported prime count");
+    }
 }
 
 dim3 grid2d(uint32_t rows, uint32_t cols, int sms) {
@@ -254,17 +279,25 @@ void gemm_u64_device(hme_ctx* ctx, uint64_t p, uint32_t m, uint32_t n, uint32_t 
     uint32_t* ra = static_cast<uint32_t*>(ctx->ws.get(kSlotRns0, 4 * pa * P.t));
     uint32_t* rb = static_cast<uint32_t*>(ctx->ws.get(kSlotRns1, 4 * pb * P.t));
     uint32_t* rc = static_cast<uint32_t*>(ctx->ws.get(kSlotRns2, 4 * pc * P.t));
-    HME_TIMED(ctx, "rns_residue", rns_residue_kernel<<<grid2d(m, k, sms), 256, 0, ctx->stream>>>(A, lda, m, k, ra, P));
-    HME_TIMED(ctx, "rns_residue", rns_residue_kernel<<<grid2d(k, n, sms), 256, 0, ctx->stream>>>(B, ldb, k, n, rb, P));
+    with_primes(P.t, [&](auto nt) {
+        constexpr int NT = decltype(nt)::value;
+        HME_TIMED(ctx, "rns_residue",
+                  rns_residue_kernel<NT><<<grid2d(m, k, sms), 256, 0, ctx->stream>>>(A, lda, m, k, ra, P));
+        HME_TIMED(ctx, "rns_residue",
+                  rns_residue_kernel<NT><<<grid2d(k, n, sms), 256, 0, ctx->stream>>>(B, ldb, k, n, rb, P));
+    });
     HME_CUDA(cudaGetLastError());
     for (int t = 0; t < P.t; ++t)
         gemm_u32_device(ctx, make_mod(P.q[t]), m, n, k, ra + t * pa, k, rb + t * pb, n, rc + t * pc, n, HME_SET);
-    if (P.mont)
-        HME_TIMED(ctx, "rns_crt", rns_crt_kernel<true><<<grid2d(m, n, sms), 256, 0, ctx->stream>>>(rc, m, n, C, ldc,
-                                                                                                  op, P));
-    else
-        HME_TIMED(ctx, "rns_crt", rns_crt_kernel<false><<<grid2d(m, n, sms), 256, 0, ctx->stream>>>(rc, m, n, C, ldc,
-                                                                                                   op, P));
+    with_primes(P.t, [&](auto nt) {
+        constexpr int NT = decltype(nt)::value;
+        if (P.mont)
+            HME_TIMED(ctx, "rns_crt", rns_crt_kernel<true, NT><<<grid2d(m, n, sms), 256, 0, ctx->stream>>>(
+                                          rc, m, n, C, ldc, op, P));
+        else
+            HME_TIMED(ctx, "rns_crt", rns_crt_kernel<false, NT><<<grid2d(m, n, sms), 256, 0, ctx->stream>>>(
+                                          rc, m, n, C, ldc, op, P));
+    });
     HME_CUDA(cudaGetLastError());
 }
 
