@@ -481,7 +481,7 @@ def gemm64_rate(n, p, steps=3, warmup=2):
     eng.gemm_u64_dev(p, A, B, Cm)
     eng.sync()
     out["kernels_ms"] = {k: round(eng.kernel_time(k)[0], 4) for k in
-                         ("rns_residue", "rns_crt", "narrow", "widen", "limb_split", "limb_gemm", "simt_gemm")
+                         ("rns_split", "rns_crt", "narrow", "widen", "limb_split", "limb_gemm", "simt_gemm")
                          if eng.kernel_time(k)[1]}
     eng.set_timing(False)
     plain = load_plain()

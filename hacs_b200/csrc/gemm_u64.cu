@@ -10,7 +10,8 @@
 // Method (residue number system).  With canonical inputs the exact integer
 // X = sum_k a_ik b_kj lies in [0, k (p-1)^2].  Pick t primes q_0 > q_1 > ...
 // just below 2^16 whose product M exceeds 4 k (p-1)^2.  Then:
-//   1. A_t = A mod q_t, B_t = B mod q_t (one pass over each operand);
+//   1. A_t = A mod q_t, B_t = B mod q_t, written directly as the limb planes
+//      the tensor-core GEMM reads (one pass over each operand for all t);
 //   2. C_t = A_t B_t mod q_t: t products on the INT8-limb tensor-core GEMM
 //      (two limbs each, 4 limb products: 4t in all, against the 64 an
 //      8-limb u64 split would need);
@@ -86,25 +87,105 @@ __device__ __forceinline__ uint64_t combine64(uint64_t old, uint64_t v, int op, 
     return op == HME_SET ? v : op == HME_ADD ? add_mod64(old, v, p) : sub_mod64(old, v, p);
 }
 
-// out[t][r][c] = X[r][c] mod q_t  (out planes rows x cols, contiguous); NT =
-// the number of primes, so the loop unrolls and the constants are immediates
+// x mod q from the 32-bit halves of x: (xh mod q)(2^32 mod q) + (xl mod q)
+// <= (q-1)^2 + q - 1 < 2^32, one more Barrett step
+__device__ __forceinline__ uint32_t res32(uint32_t xh, uint32_t xl, uint32_t q, uint32_t qm, uint32_t c32) {
+    return red32(red32(xh, q, qm) * c32 + red32(xl, q, qm), q, qm);
+}
+
+// The limb planes of A mod every prime, straight from the u64 operand, in the
+// layout the limb GEMM reads (two limbs per prime): prime t's planes start at
+// pa + 2 t a_plane, plane j holds byte j of (a mod q_t), [m][Kp] K-major, zero
+// for k in [K, Kp).  16 k per thread, one 16-byte store per plane.
 template <int NT>
-__global__ void __launch_bounds__(256) rns_residue_kernel(const uint64_t* __restrict__ X, uint64_t ldx, uint32_t rows,
-                                                          uint32_t cols, uint32_t* __restrict__ out,
-                                                          const __grid_constant__ RnsPlan P) {
-    const size_t plane = static_cast<size_t>(rows) * cols;
-    for (uint32_t r = blockIdx.y; r < rows; r += gridDim.y)
-        for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
-            const uint64_t x = X[r * ldx + c];
-            const uint32_t xl = static_cast<uint32_t>(x), xh = static_cast<uint32_t>(x >> 32);
-            uint32_t* dst = out + static_cast<size_t>(r) * cols + c;
+__global__ void __launch_bounds__(256) rns_split_a_kernel(const uint64_t* __restrict__ A, uint64_t lda, uint32_t m,
+                                                          uint32_t k, uint32_t Kp, uint8_t* __restrict__ pa,
+                                                          uint64_t a_plane, const __grid_constant__ RnsPlan P) {
+    const uint32_t kch = Kp >> 4;
+    const size_t total = static_cast<size_t>(m) * kch;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const uint32_t row = static_cast<uint32_t>(idx / kch);
+        const uint32_t k0 = static_cast<uint32_t>(idx - static_cast<size_t>(row) * kch) << 4;
+        const uint64_t* src = A + row * lda + k0;
+        uint32_t xl[16], xh[16];
 #pragma unroll
-            for (int t = 0; t < NT; ++t) {
-                // x = xh 2^32 + xl; (xh mod q)(2^32 mod q) + (xl mod q) <= (q-1)^2 + q - 1 < 2^32
-                const uint32_t q = P.q[t], qm = P.qm[t];
-                dst[t * plane] = red32(red32(xh, q, qm) * P.c32[t] + red32(xl, q, qm), q, qm);
-            }
+        for (int e = 0; e < 16; ++e) {
+            const uint64_t v = k0 + e < k ? src[e] : 0u;
+            xl[e] = static_cast<uint32_t>(v);
+            xh[e] = static_cast<uint32_t>(v >> 32);
         }
+        uint8_t* dst = pa + static_cast<size_t>(row) * Kp + k0;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            uint32_t w0[4] = {0, 0, 0, 0}, w1[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                const uint32_t r = res32(xh[e], xl[e], P.q[t], P.qm[t], P.c32[t]);
+                w0[e >> 2] |= (r & 0xffu) << (8 * (e & 3));
+                w1[e >> 2] |= ((r >> 8) & 0xffu) << (8 * (e & 3));
+            }
+            *reinterpret_cast<uint4*>(dst + 2 * t * a_plane) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+            *reinterpret_cast<uint4*>(dst + (2 * t + 1) * a_plane) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+        }
+    }
+}
+
+// The limb planes of B mod every prime: prime t's planes start at
+// pb + 4 t b_plane, plane (i, j) holds byte j of (256^i (b mod q_t) mod q_t),
+// [n][Kp] K-major (B transposed through shared memory, 64 k x 32 n per tile,
+// 8 k per thread), zero for k in [K, Kp).
+template <int NT>
+__global__ void __launch_bounds__(256) rns_split_b_kernel(const uint64_t* __restrict__ B, uint64_t ldb, uint32_t k,
+                                                          uint32_t n, uint32_t Kp, uint8_t* __restrict__ pb,
+                                                          uint64_t b_plane, const __grid_constant__ RnsPlan P) {
+    __shared__ uint64_t tile[64][33];
+    const uint32_t bk = (Kp + 63) / 64, tiles = bk * ((n + 31) / 32);
+    const uint32_t nn = threadIdx.x >> 3, kc = threadIdx.x & 7;
+    for (uint32_t blk = blockIdx.x; blk < tiles; blk += gridDim.x) {
+        const uint32_t k0 = (blk % bk) * 64, n0 = (blk / bk) * 32;
+        uint64_t v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t t = threadIdx.x + 256 * q, kk = k0 + (t >> 5), c = n0 + (t & 31);
+            v[q] = (kk < k && c < n) ? B[kk * ldb + c] : 0u;
+        }
+        __syncthreads();  // the previous tile is out of shared memory
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t t = threadIdx.x + 256 * q;
+            tile[t >> 5][t & 31] = v[q];
+        }
+        __syncthreads();
+        const uint32_t col = n0 + nn, kb = k0 + kc * 8;
+        if (col >= n || kb >= Kp) continue;
+        uint32_t xl[8], xh[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const uint64_t x = tile[kc * 8 + e][nn];
+            xl[e] = static_cast<uint32_t>(x);
+            xh[e] = static_cast<uint32_t>(x >> 32);
+        }
+        uint8_t* base = pb + static_cast<size_t>(col) * Kp + kb;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const uint32_t q = P.q[t], qm = P.qm[t];
+            uint32_t o[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};  // [2 i + j][word]
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const uint32_t r = res32(xh[e], xl[e], q, qm, P.c32[t]);
+                const uint32_t r2 = red32(r << 8, q, qm);  // 256 r mod q (r < 2^16)
+                const int sh = 8 * (e & 3);
+                o[0][e >> 2] |= (r & 0xffu) << sh;
+                o[1][e >> 2] |= ((r >> 8) & 0xffu) << sh;
+                o[2][e >> 2] |= (r2 & 0xffu) << sh;
+                o[3][e >> 2] |= ((r2 >> 8) & 0xffu) << sh;
+            }
+#pragma unroll
+            for (int ij = 0; ij < 4; ++ij)
+                *reinterpret_cast<uint2*>(base + (4 * t + ij) * b_plane) = make_uint2(o[ij][0], o[ij][1]);
+        }
+    }
 }
 
 // C[r][c] op= CRT(R[.][r][c]) mod p
@@ -275,20 +356,24 @@ void gemm_u64_device(hme_ctx* ctx, uint64_t p, uint32_t m, uint32_t n, uint32_t 
         return;
     }
     const RnsPlan P = make_plan(p, k);
-    const size_t pa = static_cast<size_t>(m) * k, pb = static_cast<size_t>(k) * n, pc = static_cast<size_t>(m) * n;
-    uint32_t* ra = static_cast<uint32_t*>(ctx->ws.get(kSlotRns0, 4 * pa * P.t));
-    uint32_t* rb = static_cast<uint32_t*>(ctx->ws.get(kSlotRns1, 4 * pb * P.t));
+    // each prime's limb planes written straight from the u64 operands, then t limb GEMMs on them
+    const int Kp = limb_kp(k);
+    const uint64_t a_plane = static_cast<uint64_t>(m) * Kp, b_plane = static_cast<uint64_t>(n) * Kp;
+    const size_t pc = static_cast<size_t>(m) * n;
+    uint8_t* pa = static_cast<uint8_t*>(ctx->ws.get(kSlotRns0, 2 * a_plane * P.t));
+    uint8_t* pb = static_cast<uint8_t*>(ctx->ws.get(kSlotRns1, 4 * b_plane * P.t));
     uint32_t* rc = static_cast<uint32_t*>(ctx->ws.get(kSlotRns2, 4 * pc * P.t));
+    const int ga = static_cast<int>(std::min<size_t>((static_cast<size_t>(m) * (Kp / 16) + 255) / 256, sms * 8ull));
+    const int gb = static_cast<int>(std::min<size_t>(static_cast<size_t>((Kp + 63) / 64) * ((n + 31) / 32), sms * 8ull));
     with_primes(P.t, [&](auto nt) {
         constexpr int NT = decltype(nt)::value;
-        HME_TIMED(ctx, "rns_residue",
-                  rns_residue_kernel<NT><<<grid2d(m, k, sms), 256, 0, ctx->stream>>>(A, lda, m, k, ra, P));
-        HME_TIMED(ctx, "rns_residue",
-                  rns_residue_kernel<NT><<<grid2d(k, n, sms), 256, 0, ctx->stream>>>(B, ldb, k, n, rb, P));
+        HME_TIMED(ctx, "rns_split", rns_split_a_kernel<NT><<<ga, 256, 0, ctx->stream>>>(A, lda, m, k, Kp, pa, a_plane, P));
+        HME_TIMED(ctx, "rns_split", rns_split_b_kernel<NT><<<gb, 256, 0, ctx->stream>>>(B, ldb, k, n, Kp, pb, b_plane, P));
     });
     HME_CUDA(cudaGetLastError());
     for (int t = 0; t < P.t; ++t)
-        gemm_u32_device(ctx, make_mod(P.q[t]), m, n, k, ra + t * pa, k, rb + t * pb, n, rc + t * pc, n, HME_SET);
+        gemm_u32_planes(ctx, make_mod(P.q[t]), m, n, k, Kp, pa + 2 * t * a_plane, a_plane, pb + 4 * t * b_plane,
+                        rc + t * pc, n, HME_SET);
     with_primes(P.t, [&](auto nt) {
         constexpr int NT = decltype(nt)::value;
         if (P.mont)

@@ -203,6 +203,12 @@ void gemm_u32_host(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, ui
                    size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int variant);
 void simt_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
                           size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int tile);
+// The limb GEMM on planes that are already split (A: [L][m][Kp] with a_plane
+// bytes between limb planes; B: [L][L][n][Kp], byte j of 256^i * B mod p,
+// K-major), K padded to limb_kp(k) with zeros; the shape heuristic's tile.
+int limb_kp(uint32_t k);
+void gemm_u32_planes(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, int Kp, uint8_t* pa,
+                     uint64_t a_plane, uint8_t* pb, uint32_t* C, size_t ldc, int op);
 // The shape heuristic (the method without a learned model).
 int gemm_default_variant(const hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n);
 // The scheduler's choice for one product (sched.cu), and its tear-down.

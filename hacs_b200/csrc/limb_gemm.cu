@@ -474,6 +474,14 @@ int gemm_default_variant(const hme_ctx* ctx, const ModParams& mp, uint32_t m, ui
     return 4 * tiles < 3 * static_cast<size_t>(ctx->num_sms) ? kVariantNarrow : kVariantWide;
 }
 
+int limb_kp(uint32_t k) { return static_cast<int>((k + kblock_for(k) - 1) / kblock_for(k) * kblock_for(k)); }
+
+void gemm_u32_planes(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, int Kp, uint8_t* pa,
+                     uint64_t a_plane, uint8_t* pb, uint32_t* C, size_t ldc, int op) {
+    const bool narrow = gemm_default_variant(ctx, mp, m, n) == kVariantNarrow;
+    launch_gemm_variant(ctx, mp, narrow, m, n, k, Kp, pa, a_plane, pb, C, ldc, op, true);
+}
+
 void gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
                      size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op) {
     int v = ctx->fixed_variant;
