@@ -121,6 +121,47 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+class GpuLocalCpus:
+    """Bind the process to the CPUs of the GPU's own NUMA node (NVML's CPU
+    affinity of the device, read only) for the duration of a block, so that
+    pinned host buffers allocated inside it sit next to the GPU's PCIe root;
+    the previous affinity is restored on exit.  A no-op where NVML or the
+    affinity call is not available.  `note` says what was applied."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.saved = None
+        self.note = "default affinity"
+
+    def __enter__(self):
+        try:
+            import pynvml
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            pynvml.nvmlInit()
+            try:
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+                words = pynvml.nvmlDeviceGetCpuAffinity(h, 64)
+            finally:
+                pynvml.nvmlShutdown()
+            local = {64 * i + b for i, w in enumerate(words) for b in range(64) if (int(w) >> b) & 1}
+            allowed = os.sched_getaffinity(0)
+            use = local & allowed
+            if use and use != allowed:
+                self.saved = allowed
+                os.sched_setaffinity(0, use)
+                self.note = f"GPU-local CPUs ({len(use)} of {len(allowed)}) while allocating and timing"
+        except Exception:
+            self.saved = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.saved is not None:
+            os.sched_setaffinity(0, self.saved)
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -731,20 +772,21 @@ def main():
     ops = 2.0 * n ** 3
     value = ops * args.steps * ws / (t_max / 1e3) / 1e12
 
-    # ---- end to end through the host-pointer API (pinned buffers) ----
-    A_pin = torch.from_numpy(A_h.view(np.int32)).pin_memory().numpy().view(np.uint32)
-    B_pin = torch.from_numpy(B_h.view(np.int32)).pin_memory().numpy().view(np.uint32)
-    C_pin = torch.empty((n, n), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
-    for _ in range(3):
-        eng.gemm(p, A_pin, B_pin, out=C_pin)
-    barrier(ws)
-    e2e_s = 0.0
-    for _ in range(args.steps):
-        flush()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        eng.gemm(p, A_pin, B_pin, out=C_pin)  # synchronous: H2D copies, split, GEMM, D2H copy
-        e2e_s += time.perf_counter() - t0
+    # ---- end to end through the host-pointer API (pinned buffers on the GPU's NUMA node) ----
+    with GpuLocalCpus(local) as numa:
+        A_pin = torch.from_numpy(A_h.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        B_pin = torch.from_numpy(B_h.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        C_pin = torch.empty((n, n), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+        for _ in range(3):
+            eng.gemm(p, A_pin, B_pin, out=C_pin)
+        barrier(ws)
+        e2e_s = 0.0
+        for _ in range(args.steps):
+            flush()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.gemm(p, A_pin, B_pin, out=C_pin)  # synchronous: H2D copies, split, GEMM, D2H copy
+            e2e_s += time.perf_counter() - t0
     barrier(ws)
     e2e_s = max_over_ranks(e2e_s, ws)
     e2e_ok = gen.fnv_matrix(C_pin) == 0x572E8347446366C6
@@ -770,7 +812,7 @@ def main():
                    "k": n, "p": p, "limbs": L, "parallelism": f"replicas x{ws}", "l2": "flushed before every step",
                    "checksum_ok": bool(ok)},
         "e2e": {"value": ops * args.steps * ws / e2e_s / 1e12, "unit": UNIT, "h2d_bytes_per_step": 8 * n * n,
-                "d2h_bytes_per_step": 4 * n * n, "api": "hme_gemm_u32 (host pointers, pinned)",
+                "d2h_bytes_per_step": 4 * n * n, "api": "hme_gemm_u32 (host pointers, pinned)", "host_numa": numa.note,
                 "checksum_ok": bool(e2e_ok)},
         "gpu_launches": launches,
         "roofline": roof,
