@@ -267,7 +267,7 @@ def test_vector_paths_on_aligned_views(engine, p):
     engine.canonicalise_acc64_dev(p, a, d)
     engine.sync()
     assert np.array_equal(_host(d), L12.canonicalise_acc64(p, acc))
-    for m, k in [(1, 4), (65, 8192), (1000, 516)]:
+    for m, k in [(1, 4), (65, 8192), (1000, 516), (3, 50000), (2, 50001)]:  # the last two: x not staged
         A_h, x_h, y0 = _rand(rng, p, (m, k)), _rand(rng, p, k), _rand(rng, p, m)
         y = _dev(y0.reshape(1, m))[0]
         engine.gemv_dev(p, _dev(A_h), _dev(x_h.reshape(1, k))[0], y, hacs_b200.ADD)
