@@ -15,6 +15,10 @@ device-pointer variants over torch CUDA tensors:
   ``Engine.solve_multi_rhs(p, B, Y)``        engine::elim::solve_multi_rhs (DenseElim.h:191-197)
   ``Engine.howell(ell, k, A)``               elim::howell / ring2k::howell / ring3k::howell (ENGINE_API.md Sec. 13.5)
   ``Engine.smith(ell, k, A)``                ring2k::smith / ring3k::smith valuations (Ring2k.h:702, Ring3k.h:100)
+  ``Engine.gemm_u64(p, A, B, C=None, op)``   engine::kernels::gemm<uint64_t> (any modulus below 2^64)
+  ``Engine.gemv_dev / axpy_dev / scal_dev / copy_dev / transpose_dev / fill_dev / axpy_identity_dev /
+  gather_dev / canonicalise_dev / canonicalise_acc64_dev / trsm_unit_dev / gemm_nt_dev /
+  schur_update_dev``                         engine::cuda level-1/2 ops (CudaKernels.h:120-247)
 
 Every call goes to libhme; there is no CPU fallback.
 """
