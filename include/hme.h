@@ -103,8 +103,9 @@ HME_API int hme_gemm_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, u
  * Method: p < 2^32 runs the u32 limb GEMM directly; larger p runs t limb GEMMs
  * modulo primes below 2^16 (t chosen so that their product exceeds
  * 4 k (p-1)^2) and reconstructs each entry by the Chinese remainder theorem,
- * reduced mod p once (Montgomery for odd p < 2^63).  Device workspace: 12 t
- * (mk + kn + mn) bytes (t <= 12).
+ * reduced mod p once (Montgomery for odd p < 2^63).  Device workspace:
+ * t (2 m Kp + 4 n Kp + 4 m n) bytes, Kp = k rounded up to 32 or 128, t <= 12
+ * (p < 2^32: 4 (mk + kn + mn) bytes plus the u32 GEMM's planes).
  * hme_gemm_u64: host pointers (synchronous); hme_gemm_u64_dev: device
  * pointers, asynchronous on the context's stream. */
 HME_API int hme_gemm_u64(hme_ctx *ctx, uint64_t p, uint32_t m, uint32_t n, uint32_t k, const uint64_t *A, size_t lda,
