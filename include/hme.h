@@ -104,7 +104,7 @@ HME_API int hme_gemm_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, u
  * modulo primes below 2^16 (t chosen so that their product exceeds
  * 4 k (p-1)^2) and reconstructs each entry by the Chinese remainder theorem,
  * reduced mod p once (Montgomery for odd p < 2^63).  Device workspace:
- * t (2 m Kp + 4 n Kp + 4 m n) bytes, Kp = k rounded up to 32 or 128, t <= 12
+ * t (2 m Kp + 4 n Kp + 4 m n) bytes, Kp = k rounded up to 32, 64 or a multiple of 128, t <= 12
  * (p < 2^32: 4 (mk + kn + mn) bytes plus the u32 GEMM's planes).
  * hme_gemm_u64: host pointers (synchronous); hme_gemm_u64_dev: device
  * pointers, asynchronous on the context's stream. */
