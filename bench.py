@@ -46,6 +46,16 @@ METRIC = "mod-p GEMM Tops/s (C = A*B mod p, bit-exact)"
 UNIT = "Tops/s"
 L2_FLUSH_BYTES = 256 << 20
 PEAK_FALLBACK_BF16_TFLOPS = 1590.0
+DATA_HEAD = "synthetic (reference splitmix64 EngineMatrix, salts 0x01/0x02)"
+
+
+def head_config(n: int, p: int, ws: int, checksum_ok: bool) -> dict:
+    """The headline workload's config (the same dict on both arms)."""
+    from hacs_b200 import limbs_for
+
+    return {"workload": f"GEMM {n}^3 p={p} (config 1: --bench micro gemm {n} {n} {p})", "m": n, "n": n,
+            "k": n, "p": p, "limbs": limbs_for(p), "parallelism": f"replicas x{ws}",
+            "l2": "flushed before every step", "checksum_ok": checksum_ok}
 
 
 def _json(o):
@@ -203,10 +213,28 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def cpu_info() -> dict:
+    """Model name and the SIMD flags the reference's kernels dispatch on, from /proc/cpuinfo."""
+    model, flags = "unknown", set()
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name") and model == "unknown":
+                model = line.split(":", 1)[1].strip()
+            elif line.startswith("flags") and not flags:
+                flags = set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    isa = [f for f in ("avx2", "avx512f", "avx512dq", "avx512bw", "avx512vl", "avx512_vnni", "avx512ifma")
+           if f in flags]
+    return {"cpu_model": model, "isa": isa, "host_threads": host_threads()}
+
+
 def cpu_gemm_rate(p: int, n: int, budget_s: float = 10.0, min_reps: int = 3):
-    """The reference's CPU engine (oracle/_ref, kernels::gemm<uint32_t> over row
-    blocks on all host threads) on the headline GEMM; falls back to the
-    oracle's C port (one thread) when the reference library is not built."""
+    """The reference's CPU engine (oracle/_ref) on the headline GEMM through its
+    own multi-thread path: one Recorder::gemm node compiled and run by the
+    tape Executor on a ThreadPool of all host threads (Recorder.h:147,
+    Executor.h:79); falls back to the oracle's C port (one thread) when the
+    reference library is not built."""
     import oracle as O
     from hacs_b200 import gen
 
@@ -214,9 +242,18 @@ def cpu_gemm_rate(p: int, n: int, budget_s: float = 10.0, min_reps: int = 3):
     B = gen.engine_matrix(n, n, p, 0x02)
     if O.ref_available():
         thr = host_threads()
-        kind = "reference"
-        fn = lambda: O.ref_gemm(p, A, B, threads=thr)  # noqa: E731
-        sample_n = n
+        C0, _ = O.ref_tape_gemm(p, A, B, threads=thr, reps=1)  # warm: pool start, program compile
+        t0 = time.perf_counter()
+        reps, secs = 0, 0.0
+        while reps < min_reps or time.perf_counter() - t0 < budget_s:
+            _, s1 = O.ref_tape_gemm(p, A, B, threads=thr, reps=2)
+            secs += 2 * s1
+            reps += 2
+        ok = O.fnv_matrix(C0) == 0x572E8347446366C6
+        return {"value": 2.0 * n ** 3 * reps / secs / 1e12, "unit": UNIT, "cores": thr, "kind": "reference",
+                "sample": f"{reps} x GEMM {n}^3 p={p} (EngineMatrix salts 1/2) through tape::Recorder::gemm + "
+                          f"Executor::run on a {thr}-worker pool, {secs:.1f} s of runs",
+                "checksum_ok": bool(ok), **cpu_info()}
     else:
         thr = 1
         kind = "port"
@@ -245,27 +282,31 @@ def run_reference(args):
     A = gen.engine_matrix(n, n, p, 0x01)
     B = gen.engine_matrix(n, n, p, 0x02)
     if O.ref_available():
+        # the reference's own multi-thread GEMM path: a tape program of one Recorder::gemm node run by
+        # the Executor on a pool of all host threads; one program run per step
         thr, kind = host_threads(), "reference"
-        step = lambda: O.ref_gemm(p, A, B, threads=thr)  # noqa: E731
+        how = "tape::Recorder::gemm + Executor::run"
+        for _ in range(args.warmup):
+            O.ref_tape_gemm(p, A, B, threads=thr, reps=1)
+        C_, s1 = O.ref_tape_gemm(p, A, B, threads=thr, reps=args.steps)
+        dt = s1 * args.steps
     else:
-        thr, kind = 1, "port"
-        step = lambda: O.gemm(p, A, B)  # noqa: E731
-    for _ in range(args.warmup):
-        step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        C_ = step()
-    dt = time.perf_counter() - t0
-    ok = gen.fnv_matrix(C_) == 0x572E8347446366C6
+        thr, kind, how = 1, "port", "oracle C port"
+        for _ in range(args.warmup):
+            O.gemm(p, A, B)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            C_ = O.gemm(p, A, B)
+        dt = time.perf_counter() - t0
+    ok = O.fnv_matrix(C_) == 0x572E8347446366C6
     val = 2.0 * n ** 3 * args.steps / dt / 1e12
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (reference splitmix64 EngineMatrix)",
-        "config": {"workload": f"GEMM {n}^3 p={p} (config 1)", "m": n, "n": n, "k": n, "p": p,
-                   "checksum_ok": ok},
+        "vs_baseline": None, "dtype": "u32", "data": DATA_HEAD,
+        "config": head_config(n, p, ws, bool(ok)),
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": thr, "kind": kind,
-                         "sample": f"{args.steps} x GEMM {n}^3 p={p} on {thr} host threads"},
+                         "sample": f"{args.steps} x GEMM {n}^3 p={p} on {thr} host threads ({how})", **cpu_info()},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line, default=_json), flush=True)
@@ -349,10 +390,32 @@ def _golden():
     return json.load(open(path)) if os.path.exists(path) else {}
 
 
+def int8_peak_tops():
+    pk, src = peaks()
+    return 2.0 * float(pk["bf16_tflops"]), f"2 x {src} bf16 dense TFLOP/s (INT8 dense rate = 2 x bf16 on B200)"
+
+
+def hbm_peak_gbs():
+    pk, src = peaks()
+    return float(pk["hbm_gbs"]), f"{src} copy bandwidth"
+
+
+def kernel_breakdown(eng, names):
+    """{name: [total ms, launches]} of the library's per-kernel CUDA-event timer."""
+    out = {}
+    for nm in names:
+        ms, c = eng.kernel_time(nm)
+        if c:
+            out[nm] = [round(ms, 4), int(c)]
+    return out
+
+
 def extra_rref(eng, reps=3):
-    """Config 2: RREF + rank + det of RankedMatrix(4096, 4096, 3900, 2^31 - 19), device-resident."""
+    """Config 2: RREF + rank + det of RankedMatrix(4096, 4096, 3900, 2^31 - 19), device-resident;
+    beside it the reference's elim::rref under the tape's host elimination hook on all host threads."""
     import torch
 
+    import oracle as O
     from hacs_b200 import gen
 
     g = _golden().get("config2", {})
@@ -371,17 +434,59 @@ def extra_rref(eng, reps=3):
         times.append(time.perf_counter() - t0)
     t = min(times[1:])
     ok = gen.fnv_matrix(A.cpu().numpy().view(np.uint32)) == int(g.get("rref_fnv", "0x0"), 16)
-    work = n * n * r - (n + n) * r * r / 2 + r ** 3 / 3 + r * r * (n - r) / 2
-    return {"workload": "RREF/rank/det 4096^2 rank 3900 p=2^31-19 (config 2)", "ms": t * 1e3, "rank": int(len(piv)),
-            "modmac_per_s": work / t, "checksum_ok_vs_reference": bool(ok)}
+    # per-kernel device times of one more RREF (CUDA events around each launch)
+    A.copy_(A0)
+    eng.set_timing(True)
+    eng.timing_reset()
+    eng.rref_dev(p, A)
+    eng.sync()
+    kern = kernel_breakdown(eng, ["panel_factor", "limb_split", "limb_gemm", "trsm", "row_permute", "tri_inv",
+                                  "gather_cols", "assemble_rref", "gather", "copy"])
+    eng.set_timing(False)
+    lu = n * n * r - (n + n) * r * r / 2 + r ** 3 / 3
+    back = r * r * (n - r) / 2
+    work = lu + back
+    peak, psrc = int8_peak_tops()
+    hbm, hsrc = hbm_peak_gbs()
+    # tensor part: every modMAC of the LU and the back substitution is L^2 = 16 int8 limb products (2 ops each)
+    achieved = 16 * 2 * work / t / 1e12
+    gemm_ms = kern.get("limb_gemm", [0, 0])[0]
+    panel_ms = kern.get("panel_factor", [0, 0])[0]
+    panel_bytes = 8.0 * n * 64 * (n // 64)  # read + write of the active rows of every 64-column panel (upper bound m)
+    out = {"workload": "RREF/rank/det 4096^2 rank 3900 p=2^31-19 (config 2)", "ms": t * 1e3, "rank": int(len(piv)),
+           "modmac_per_s": work / t, "checksum_ok_vs_reference": bool(ok), "kernels_ms": kern,
+           "roofline": {"bound": "tensor (trailing updates) / latency (panels)", "achieved_int8_tops": achieved,
+                        "peak": peak, "unit": "TOPS", "frac": achieved / peak, "peak_source": psrc,
+                        "algorithmic": f"LU {lu:.3e} + back substitution {back:.3e} modMAC, 32 int8 ops each",
+                        "limb_gemm_int8_tops": (32 * work / (gemm_ms / 1e3) / 1e12) if gemm_ms else None,
+                        "panel_share": panel_ms / max(1e-9, sum(v[0] for v in kern.values())),
+                        "panel_gbs": (panel_bytes / (panel_ms / 1e3) / 1e9) if panel_ms else None,
+                        "panel_hbm_frac": (panel_bytes / (panel_ms / 1e3) / 1e9 / hbm) if panel_ms else None,
+                        "hbm_peak_source": hsrc}}
+    if O.ref_available():
+        thr = host_threads()
+        Ah = A0.cpu().numpy().view(np.uint32).copy()
+        t0 = time.perf_counter()
+        Rr, pr = O.ref_rref_par(p, Ah, threads=thr)
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value_ms": tc * 1e3, "modmac_per_s": work / tc, "cores": thr, "kind": "reference",
+                               "sample": "the full config: elim::rref under tape::ScopedHostElimHook on a "
+                                         f"{thr}-worker consumer pool, one run",
+                               "checksum_ok": bool(O.fnv_matrix(Rr) == int(g.get("rref_fnv", "0x0"), 16)),
+                               **cpu_info()}
+        out["speedup_vs_cpu"] = tc / t
+    return out
 
 
 def extra_ring(eng, reps=3):
-    """Config 3: Howell over Z/2^16 and Smith over Z/3^10 of planted 2048^2 U*D*V."""
+    """Config 3: Howell over Z/2^16 and Smith over Z/3^10 of planted 2048^2 U*D*V; beside each
+    the reference's ring2k::howell / ring3k::smith under smithpar::ScopedEnable on all host threads."""
+    import oracle as O
     from hacs_b200 import gen
 
     g = _golden().get("config3", {})
     out = {}
+    peak, psrc = int8_peak_tops()
     for (ell, k, kind) in [(2, 16, "howell"), (3, 10, "smith"), (2, 16, "smith"), (3, 10, "howell")]:
         M, e = gen.planted_udv(2048, ell, k, 0x33)
         fn = (lambda: eng.howell(ell, k, M)) if kind == "howell" else (lambda: eng.smith(ell, k, M))
@@ -396,35 +501,66 @@ def extra_ring(eng, reps=3):
             ok = gen.fnv_matrix(res[0]) == int(c.get("howell_fnv", "0x0"), 16)
         else:
             ok = list(res) == c.get("sigma")
-        out[f"{kind}_2048_{ell}^{k}"] = {"ms": min(ts) * 1e3, "bit_exact_vs_reference": bool(ok),
-                                        "api": "host pointers (H2D + D2H inside)"}
+        t = min(ts)
+        n = 2048
+        work = n ** 3 / 3.0
+        # limb products per multiply-add mod ell^k: 4 for 2^16 (two limbs) and for 3^10 (two limbs)
+        achieved = 4 * 2 * work / t / 1e12
+        rec = {"ms": t * 1e3, "bit_exact_vs_reference": bool(ok), "api": "host pointers (H2D + D2H inside)",
+               "roofline": {"bound": "tensor (trailing updates) / latency (panels, Howell pass)",
+                            "achieved_int8_tops": achieved, "peak": peak, "unit": "TOPS", "frac": achieved / peak,
+                            "peak_source": psrc, "algorithmic": "n^3/3 multiply-adds mod ell^k, 4 limb products each"}}
+        if O.ref_available() and (ell, kind) in ((2, "howell"), (3, "smith")):
+            thr = host_threads()
+            t0 = time.perf_counter()
+            if kind == "howell":
+                H, _, _ = O.ref_howell_2k(k, M, threads=thr)
+                cok = gen.fnv_matrix(H) == int(c.get("howell_fnv", "0x0"), 16)
+                what = "ring2k::howell<Traits<uint32_t>>"
+            else:
+                sg = O.ref_smith_3k(k, M, threads=thr)
+                cok = list(sg) == c.get("sigma")
+                what = "ring3k::smith"
+            tc = time.perf_counter() - t0
+            rec["cpu_baseline"] = {"value_ms": tc * 1e3, "cores": thr, "kind": "reference",
+                                   "sample": f"the full config: {what} under smithpar::ScopedEnable, one run",
+                                   "checksum_ok": bool(cok), **cpu_info()}
+            rec["speedup_vs_cpu"] = tc / t
+        out[f"{kind}_2048_{ell}^{k}"] = rec
     return out
 
 
+def cpu_job_rate(stream_s, fam, p, sa, sb, idx, threads):
+    """The reference CPU engine on the jobs `idx` of the stream (kernels::gemm + column_rank_profile per
+    job, one job per worker process, spawn pool of `threads`); returns (jobs/s, seconds, results)."""
+    import multiprocessing as mp
+
+    import oracle as O
+
+    tasks = [(int(j), int(stream_s[j]), int(fam[j]), int(p[j]), int(sa[j]), int(sb[j])) for j in idx]
+    tasks.sort(key=lambda t: -t[1])
+    with mp.get_context("spawn").Pool(threads) as pool:
+        pool.map(O.ref_job, tasks[-threads:])  # warm the workers (library load)
+        t0 = time.perf_counter()
+        res = pool.map(O.ref_job, tasks, chunksize=1)
+        dt = time.perf_counter() - t0
+    return len(tasks) / dt, dt, {j: (r, f) for j, r, f in res}
+
+
 def extra_jobstream(eng, plain, n_jobs=10000, sample=500):
-    """Config 4: the 10,000-job stream (GEMM + rank per job, sides 16..1024), batched,
-    next to one-launch-per-job plain dispatch (the reference's CUDA-core GEMM plus a
-    per-job device rank) on the first `sample` jobs."""
+    """Config 4: the 10,000-job stream (GEMM + rank per job, sides 16..1024), batched, checked job by job
+    against the reference CPU engine's results (tests/golden/jobs10000.json); beside it one-launch-per-job
+    plain dispatch and the reference CPU engine, both on a strided sample of `sample` jobs."""
     import ctypes as C_
 
     import torch
 
     import hacs_b200
-    from hacs_b200 import gen
+    import oracle as O
+    from hacs_b200 import stream
 
-    s, fam, p, sa, sb = gen.job_stream(n_jobs)
-    tot = int((s * s).sum())
-    bufA = torch.empty(tot, dtype=torch.int32, device="cuda")
-    bufB, bufC = torch.empty_like(bufA), torch.empty_like(bufA)
-    jobs, specs, off = [], [], 0
-    for j in range(n_jobs):
-        n = int(s[j])
-        A, B, Cm = (b[off:off + n * n].view(n, n) for b in (bufA, bufB, bufC))
-        off += n * n
-        jobs.append({"p": int(p[j]), "A": A, "B": B, "C": Cm})
-        specs += [(A, int(p[j]), int(fam[j]), int(sa[j])), (B, int(p[j]), int(fam[j]), int(sb[j]))]
-    eng.gen_jobs_dev(specs)
-    arr = eng._jobs(jobs)
+    st = stream.DeviceStream(n_jobs)
+    arr = eng._jobs(st.jobs)
 
     def batched(nj, a):
         ranks = np.zeros(nj, np.uint32)
@@ -433,37 +569,91 @@ def extra_jobstream(eng, plain, n_jobs=10000, sample=500):
         hacs_b200.check(eng._lib.hme_batch_gemm_rank_u32_dev(eng._h, nj, a, ranks.ctypes.data_as(C_.POINTER(C_.c_uint32))))
         return time.perf_counter() - t0, ranks
 
+    eng.gen_jobs_dev(st.specs)
     batched(n_jobs, arr)  # warm: workspace growth, module load
-    eng.gen_jobs_dev(specs)
+    eng.gen_jobs_dev(st.specs)
     t_all, ranks = batched(n_jobs, arr)
+    work = st.work_modmac()
     out = {"workload": f"{n_jobs} jobs GEMM + rank mod p in {{65521, 2^31-19}}, sides log-uniform 16..1024 (config 4)",
-           "jobs_per_s": n_jobs / t_all, "s": t_all, "modmac_gemm": float((s.astype(np.float64) ** 3).sum())}
-    eng.gen_jobs_dev(specs)
-    sub = eng._jobs(jobs[:sample])
-    t_b, r_b = batched(sample, sub)
-    out["sample_jobs"] = sample
-    out["sample_batched_jobs_per_s"] = sample / t_b
+           "jobs_per_s": n_jobs / t_all, "s": t_all, "modmac_gemm": work}
+    # parity: every rank and every C checksum against the reference's own results
+    gold = stream.golden_jobs()
+    eng.gen_jobs_dev(st.specs)
+    hacs_b200.check(eng._lib.hme_batch_gemm_u32_dev(eng._h, n_jobs, arr))
+    eng.sync()
+    fnvs = st.job_checksums()
+    if gold is not None and len(gold[0]) == n_jobs:
+        out["ranks_equal_vs_reference"] = bool(np.array_equal(ranks.astype(np.int64), gold[0]))
+        out["c_fnv_equal_vs_reference"] = bool(fnvs == gold[1])
+        out["parity_source"] = "tests/golden/jobs10000.json (reference kernels::gemm + elim::column_rank_profile)"
+    # roofline: GEMM + rank at the limb GEMM's INT8 rate; a rank of an s x s job is ~ s^3/3 multiply-adds
+    limbs2 = np.where(st.p == 65521, 4, 16).astype(np.float64)
+    s3 = st.s.astype(np.float64) ** 3
+    int8_ops = float((limbs2 * 2 * (s3 + s3 / 3)).sum())
+    peak, psrc = int8_peak_tops()
+    out["roofline"] = {"bound": "tensor (GEMMs, trailing updates) / latency (panels)",
+                       "achieved_int8_tops": int8_ops / t_all / 1e12, "peak": peak, "unit": "TOPS",
+                       "frac": int8_ops / t_all / 1e12 / peak, "peak_source": psrc,
+                       "algorithmic": "sum_j L_j^2 * 2 * (s_j^3 + s_j^3 / 3) int8 ops (GEMM + rank)"}
+    # strided sample: every (n_jobs / sample)-th job
+    idx = np.arange(0, n_jobs, max(1, n_jobs // sample))[:sample]
+    sub_jobs = [st.jobs[j] for j in idx]
+    sub_specs = [st.specs[2 * j + t] for j in idx for t in (0, 1)]
+    eng.gen_jobs_dev(sub_specs)
+    t_b, r_b = batched(len(idx), eng._jobs(sub_jobs))
+    out["sample_jobs"] = int(len(idx))
+    out["sample"] = f"every {max(1, n_jobs // sample)}th job of the stream"
+    out["sample_batched_jobs_per_s"] = len(idx) / t_b
     if plain is not None:
-        eng.gen_jobs_dev(specs[: 2 * sample])
+        # (a) one plain CUDA-core GEMM launch per job (the reference's cuda::gemm) + this library's
+        #     single-job device rank, synchronised per job
+        eng.gen_jobs_dev(sub_specs)
         eng.use_torch_stream()
-        st = torch.cuda.current_stream().cuda_stream
-        r2 = np.zeros(sample, np.uint32)
+        cst = torch.cuda.current_stream().cuda_stream
+        r2 = np.zeros(len(idx), np.uint32)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for j in range(sample):
-            jb = jobs[j]
+        for t, jb in enumerate(sub_jobs):
             n = jb["C"].shape[0]
             if plain.plain_gemm_u32_dev(jb["p"], n, n, n, jb["A"].data_ptr(), n, jb["B"].data_ptr(), n,
-                                        jb["C"].data_ptr(), n, 0, st) != 0:
+                                        jb["C"].data_ptr(), n, 0, cst) != 0:
                 raise RuntimeError(plain.plain_last_error().decode())
             rr = np.zeros(1, np.uint32)
             hacs_b200.check(eng._lib.hme_batch_rank_u32_dev(eng._h, 1, eng._jobs([jb]),
                                                             rr.ctypes.data_as(C_.POINTER(C_.c_uint32))))
-            r2[j] = rr[0]
+            r2[t] = rr[0]
         t_p = time.perf_counter() - t0
-        out["sample_plain_dispatch_jobs_per_s"] = sample / t_p
+        out["sample_plain_dispatch_jobs_per_s"] = len(idx) / t_p
         out["speedup_vs_plain_dispatch"] = t_p / t_b
-        out["ranks_equal"] = bool((r2 == r_b).all() and (r_b == ranks[:sample]).all())
+        # (b) the reference's own path for p > 127: one plain GEMM launch per job, C back to the host,
+        #     elim::column_rank_profile on the host (the reference has no device rank at these p)
+        if O.ref_available():
+            eng.gen_jobs_dev(sub_specs)
+            r3 = np.zeros(len(idx), np.uint32)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for t, jb in enumerate(sub_jobs):
+                n = jb["C"].shape[0]
+                if plain.plain_gemm_u32_dev(jb["p"], n, n, n, jb["A"].data_ptr(), n, jb["B"].data_ptr(), n,
+                                            jb["C"].data_ptr(), n, 0, cst) != 0:
+                    raise RuntimeError(plain.plain_last_error().decode())
+                Ch = jb["C"].cpu().numpy().view(np.uint32)
+                r3[t] = len(O.ref_rank_profile(jb["p"], Ch))
+            t_r = time.perf_counter() - t0
+            out["sample_reference_path_jobs_per_s"] = len(idx) / t_r
+            out["speedup_vs_reference_path"] = t_r / t_b
+            out["reference_path"] = "cuda::gemm per job (plain, sm_100a) + C to host + elim::column_rank_profile"
+        eng.use_own_stream()
+        out["sample_ranks_equal_plain"] = bool((r2 == r_b).all())
+    if O.ref_available():
+        thr = host_threads()
+        rate, tc, res = cpu_job_rate(st.s, st.fam, st.p, st.seed_a, st.seed_b, idx, thr)
+        out["cpu_baseline"] = {"value_jobs_per_s": rate, "cores": thr, "kind": "reference",
+                               "sample": f"{len(idx)} jobs (every {max(1, n_jobs // sample)}th), kernels::gemm + "
+                                         f"elim::column_rank_profile per job on a {thr}-process pool, {tc:.1f} s",
+                               "ranks_equal": bool(all(res[int(j)][0] == int(r_b[t]) for t, j in enumerate(idx))),
+                               **cpu_info()}
+        out["speedup_vs_cpu"] = (n_jobs / t_all) / rate
     return out
 
 
@@ -807,10 +997,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32 residues (u8 limbs x u8 -> s32 tensor-core accumulation)",
-        "data": "synthetic (reference splitmix64 EngineMatrix, salts 0x01/0x02)",
-        "config": {"workload": f"GEMM {n}^3 p={p} (config 1: --bench micro gemm {n} {n} {p})", "m": n, "n": n,
-                   "k": n, "p": p, "limbs": L, "parallelism": f"replicas x{ws}", "l2": "flushed before every step",
-                   "checksum_ok": bool(ok)},
+        "data": DATA_HEAD,
+        "config": head_config(n, p, ws, bool(ok)),
         "e2e": {"value": ops * args.steps * ws / e2e_s / 1e12, "unit": UNIT, "h2d_bytes_per_step": 8 * n * n,
                 "d2h_bytes_per_step": 4 * n * n, "api": "hme_gemm_u32 (host pointers, pinned)", "host_numa": numa.note,
                 "checksum_ok": bool(e2e_ok)},

@@ -10,17 +10,21 @@
 // row) because it is also the cheapest to find in parallel (a min over rows).
 //
 // Blocked right-looking LU, panels of `bw` columns:
-//   1. panel_factor_kernel: one cooperative launch factors A[r0:m, c0:c0+bw)
-//      with one bounded grid barrier per column.  Pivot rows are not swapped
-//      during the panel; they leave the active set.  Each CTA owns a slice of
-//      rows; before every barrier each CTA publishes its topmost candidate row
-//      for the next column (values into a parity-double-buffered slot, index
-//      by atomicMin), so after the barrier every CTA knows the pivot row and
-//      has its values without a second barrier.  Multipliers are stored in the
-//      pivot columns of the active rows (packed L).
+//   1. panel_cluster_kernel: the panel's active rows A[r0:m, c0:c0+bw) sit in
+//      the shared memory of one thread-block cluster (up to 16 CTAs); per
+//      column each CTA pushes its best (valuation, row) key and that row to
+//      every CTA through distributed shared memory, one cluster barrier, a
+//      warp min of the keys; fraction-free row updates, unit scales undone
+//      once per panel.  Panels too tall for one cluster take
+//      panel_factor_kernel instead: one cooperative launch over all SMs with
+//      one bounded grid barrier per column.  Either way pivot rows are not
+//      swapped during the panel (they leave the active set) and multipliers
+//      are stored in the pivot columns of the active rows (packed L).
 //   2. the panel's pivot rows move to rows r0 .. r0+k-1 in pivot order (columns
 //      >= c0; columns left of the panel of non-U rows hold dead multipliers).
-//   3. U12 = L11^-1 A12: L11 inverted in shared memory, then one limb GEMM.
+//   3. U12 = L11^-1 A12 in place: trsm_unit_lower_kernel, one warp per column
+//      of A12 holding its k rows in registers (forward substitution with
+//      shuffles), L11 in shared memory.
 //   4. A22 -= L21 * U12: the INT8-limb tcgen05 GEMM (Sub), K = k pivots.
 // Then RREF = U1^-1 U on the free columns only (the pivot columns of the RREF
 // are the identity): every diagonal block of U1 is inverted in shared memory
@@ -892,10 +896,13 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     }
     const int lu_cols = ring && ring->lu_cols > 0 ? std::min(ring->lu_cols, n) : n;
 
-    static std::once_flag attr_once;
-    static int cluster_cap = 0;  // largest cluster the panel kernel can be launched with (0: none)
-    std::call_once(attr_once, [] {
-        cudaFuncSetAttribute(panel_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax);
+    static OncePerDevice attr;
+    // per device: the largest cluster the panel kernel can be launched with (0: none)
+    static int cluster_caps[OncePerDevice::kMaxDevices] = {};
+    attr.run([](int dev) {
+        int& cluster_cap = cluster_caps[dev];
+        cluster_cap = 0;
+        HME_CUDA(cudaFuncSetAttribute(panel_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax));
         bool attrs_ok = true;
         for (const void* fn : {reinterpret_cast<const void*>(panel_cluster_kernel<kArithPow2, 512>),
                                reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont31, 512>),
@@ -929,11 +936,12 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         }
         cudaGetLastError();  // a refused query leaves no error behind
         const int smem2 = sizeof(uint32_t) * (2 * kMaxPanel * kMaxPanel + kMaxPanel);
-        cudaFuncSetAttribute(tri_inv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
-        cudaFuncSetAttribute(tri_inv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
-        cudaFuncSetAttribute(trsm_unit_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(trsm_smem_bytes(kMaxPanel)));
+        HME_CUDA(cudaFuncSetAttribute(tri_inv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2));
+        HME_CUDA(cudaFuncSetAttribute(tri_inv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2));
+        HME_CUDA(cudaFuncSetAttribute(trsm_unit_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(trsm_smem_bytes(kMaxPanel))));
     });
+    const int cluster_cap = cluster_caps[ctx->device];
 
     // device scratch
     const int grid_cap = std::max(1, std::min(ctx->num_sms, opt.panel_ctas > 0 ? opt.panel_ctas : ctx->num_sms));

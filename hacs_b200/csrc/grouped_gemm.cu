@@ -250,10 +250,10 @@ size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 template <int L, int BN, int KB>
 void ensure_grouped_attr() {
-    static std::once_flag once;
-    std::call_once(once, [] {
-        cudaFuncSetAttribute(grouped_limb_gemm_kernel<L, BN, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             Cfg<L, BN, KB>::SMEM);
+    static OncePerDevice attr;
+    attr.run([](int) {
+        HME_CUDA(cudaFuncSetAttribute(grouped_limb_gemm_kernel<L, BN, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      Cfg<L, BN, KB>::SMEM));
     });
 }
 

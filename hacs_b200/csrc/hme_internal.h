@@ -3,7 +3,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -177,6 +179,31 @@ inline int guard(F&& f) {
         return HME_EINVAL;
     }
 }
+
+// Kernel attributes (the dynamic shared-memory limit, cluster permissions)
+// belong to one device: a process that drives several GPUs must set them on
+// each.  OncePerDevice runs its set-up once per device id on the calling
+// thread's current device; a set-up that throws is retried on the next call.
+class OncePerDevice {
+  public:
+    static constexpr int kMaxDevices = 64;
+    template <class F>
+    void run(F&& f) {
+        int dev = 0;
+        HME_CUDA(cudaGetDevice(&dev));
+        HME_REQUIRE(dev >= 0 && dev < kMaxDevices, "device id out of range");
+        const uint64_t bit = uint64_t(1) << dev;
+        if (done_.load(std::memory_order_acquire) & bit) return;
+        std::lock_guard<std::mutex> lock(mu_);
+        if (done_.load(std::memory_order_relaxed) & bit) return;
+        f(dev);
+        done_.fetch_or(bit, std::memory_order_release);
+    }
+
+  private:
+    std::mutex mu_;
+    std::atomic<uint64_t> done_{0};
+};
 
 // Deterministic primality for 32-bit moduli (Miller-Rabin, bases 2, 7, 61).
 bool is_prime_u32(uint32_t p);

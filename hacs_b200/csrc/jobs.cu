@@ -848,16 +848,16 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
     HME_CUDA(cudaMemcpyAsync(d_maps, maps.data(), sizeof(CUtensorMap) * 2 * ng, cudaMemcpyHostToDevice, ctx->stream));
 
     // ---- launch shapes of a round (fixed)
-    static std::once_flag once;
-    std::call_once(once, [] {
-        cudaFuncSetAttribute(batch_panel_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
-        cudaFuncSetAttribute(batch_panel_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
-        cudaFuncSetAttribute(batch_panel_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
-        cudaFuncSetAttribute(batch_panel_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem);
-        cudaFuncSetAttribute(batch_linv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(batch_linv_smem(kMaxBw)));
-        cudaFuncSetAttribute(batch_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(batch_apply_smem(kMaxBw)));
+    static OncePerDevice attr;
+    attr.run([](int) {
+        HME_CUDA(cudaFuncSetAttribute(batch_panel_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem));
+        HME_CUDA(cudaFuncSetAttribute(batch_panel_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem));
+        HME_CUDA(cudaFuncSetAttribute(batch_panel_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem));
+        HME_CUDA(cudaFuncSetAttribute(batch_panel_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem));
+        HME_CUDA(cudaFuncSetAttribute(batch_linv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(batch_linv_smem(kMaxBw))));
+        HME_CUDA(cudaFuncSetAttribute(batch_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(batch_apply_smem(kMaxBw))));
     });
     size_t bucket_smem[kBuckets2];
     int bucket_grid[kBuckets2];

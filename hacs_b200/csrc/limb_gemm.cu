@@ -332,9 +332,10 @@ void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint
                  uint8_t* planesA, uint64_t a_plane, uint8_t* planesB, uint32_t* C, size_t ldc, int op,
                  bool pdl) {
     using CF = Cfg<L, BN, KB>;
-    static std::once_flag attr_once;
-    std::call_once(attr_once, [] {
-        cudaFuncSetAttribute(limb_gemm_kernel<L, BN, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM);
+    static OncePerDevice attr;
+    attr.run([](int) {
+        HME_CUDA(cudaFuncSetAttribute(limb_gemm_kernel<L, BN, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      CF::SMEM));
     });
     CUtensorMap tmA, tmB;
     {
@@ -738,10 +739,19 @@ extern "C" HME_API int hme_gemm_u32_dev_noalloc(uint32_t p, uint32_t m, uint32_t
         if (m == 0 || n == 0) return HME_OK;
         HME_REQUIRE(C != nullptr && ldc >= n, "gemm: bad C");
         HME_REQUIRE(k == 0 || (A && B && lda >= k && ldb >= n), "gemm: bad A/B");
+        cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+        {
+            // the call waits for its stream and reads the error word back: neither may happen inside a capture
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            const cudaError_t e = cudaStreamIsCapturing(st, &cs);
+            if (e != cudaSuccess) cudaGetLastError();
+            HME_REQUIRE(e == cudaSuccess && cs == cudaStreamCaptureStatusNone,
+                        "hme_gemm_u32_dev_noalloc: cannot be called while a stream capture is in progress (it "
+                        "synchronises its stream)");
+        }
         int dev = 0;
         HME_CUDA(cudaGetDevice(&dev));
         const NoAllocDevice& d = noalloc_setup(dev);
-        cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
         HME_CUDA(cudaMemsetAsync(d.err, 0, sizeof(int), st));
         if (k == 0) {
             if (op == HME_SET)

@@ -293,10 +293,10 @@ struct DevBuf {
 };
 
 void fwd_bwd(hme_mlp* mlp, const float* dX, const float* dY, const int* didx, int n, int total) {
-    static std::once_flag once;
-    std::call_once(once, [] {
-        cudaFuncSetAttribute(mlp_fwd_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(fwd_bwd_smem()));
+    static OncePerDevice attr;
+    attr.run([](int) {
+        HME_CUDA(cudaFuncSetAttribute(mlp_fwd_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(fwd_bwd_smem())));
     });
     hme_ctx* ctx = mlp->ctx;
     HME_CUDA(cudaMemsetAsync(mlp->G, 0, sizeof(float) * kParams, ctx->stream));

@@ -2,9 +2,10 @@
  *
  * Drop-in device layer for the matrix engine of drjanosch42/hacs 0.2.1.  Each
  * entry point names the reference interface it replaces (file:line in the
- * reference tree); INTEGRATION.md shows the C++ shim that installs these
- * behind the reference's own seams (the device RREF hook, the micro-bench GPU
- * hooks, the tape's device kernels, the Z/2^k and Z/3^k Smith / Howell calls).
+ * reference tree); the C++ seam files under integration/ install these behind
+ * the reference's own seams (the device RREF hook, the Z/2^k device LU table,
+ * the micro-bench GPU hooks, the tape's device kernels, the Z/2^k and Z/3^k
+ * Smith / Howell calls).
  *
  * Conventions (the reference's, ENGINE_API.md Sec. 1-5):
  *   - matrices are row-major uint32 with an explicit leading dimension in
@@ -345,8 +346,10 @@ HME_API int hme_sched_plan(hme_ctx *ctx, hme_mlp *mlp, uint32_t n, const uint32_
  * final.  The planes of one call, L*m*Kp + L*L*n*Kp bytes (each rounded up
  * to 256; Kp = k rounded up to 16; L limbs as above), must fit 32 MiB, else
  * HME_EINVAL before anything runs.  The first call on a device does that
- * device's set-up (scratch address lookup, kernel attributes); make it
- * before any stream capture.  All calls share the one scratch array: calls
+ * device's set-up (scratch address lookup, kernel attributes).  The call
+ * synchronises its stream, so it cannot run while any stream is being
+ * captured into a CUDA graph: it then returns HME_EINVAL before doing
+ * anything.  All calls share the one scratch array: calls
  * that overlap on the GPU race and give wrong results, so serialise them.
  * No counterpart in the reference: an addition of this library. */
 HME_API int hme_gemm_u32_dev_noalloc(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t *A, size_t lda,

@@ -23,6 +23,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _ORC = None
 _REF = None
+# Where the reference's sources lie (only the build of oracle/_ref reads them).
+REFERENCE = os.environ.get("HACS_REFERENCE", "/root/reference")
 
 u32p = C.POINTER(C.c_uint32)
 
@@ -31,9 +33,9 @@ def build(with_ref: bool | None = None) -> None:
     """Compile liboracle.so, and the reference library when its sources exist."""
     subprocess.check_call(["make", "-s", "-C", HERE], stdout=subprocess.DEVNULL)
     if with_ref is None:
-        with_ref = os.path.isdir("/root/reference/src/ModArithmetic")
+        with_ref = os.path.isdir(os.path.join(REFERENCE, "src", "ModArithmetic"))
     if with_ref:
-        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref"], stdout=subprocess.DEVNULL)
+        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={REFERENCE}"], stdout=subprocess.DEVNULL)
 
 
 def _p(a: np.ndarray):
@@ -110,6 +112,10 @@ def ref():
         L.ref_canonicalise_u32.argtypes = [u32] * 3 + [u32p, u32]
         L.ref_canonicalise_acc64_u32.argtypes = [u32] * 3 + [u64p, u32, u32p, u32]
         L.ref_gemm_u64.argtypes = [C.c_uint64, u32, u32, u32, u64p, u32, u64p, u32, u64p, u32, C.c_int]
+        if hasattr(L, "ref_tape_gemm_u32"):
+            L.ref_tape_gemm_u32.argtypes = [u32] * 4 + [u32p, u32p, u32p, C.c_int, C.c_int,
+                                                        C.POINTER(C.c_double)]
+            L.ref_rref_par_u32.argtypes = [u32, u32, u32, u32p, u32, u32p, u32p, C.c_int]
         _REF = L
     return _REF
 
@@ -237,6 +243,43 @@ def ref_rref(p: int, A):
     rank = C.c_uint32(0)
     _chk(ref().ref_rref_u32(p, m, n, _p(R), n, _p(piv), C.byref(rank)), "ref")
     return R, piv[: rank.value].copy()
+
+
+def ref_tape_gemm(p: int, A, B, threads: int = 1, reps: int = 1):
+    """C = A*B mod p through the reference's tape (Recorder::gemm, compile, Executor::run on a
+    pool of `threads` workers, run `reps` times); returns (C, mean seconds per run)."""
+    A, B = _u32(A), _u32(B)
+    m, k = A.shape
+    n = B.shape[1]
+    Cm = np.zeros((m, n), np.uint32)
+    secs = C.c_double(0.0)
+    _chk(ref().ref_tape_gemm_u32(p, m, n, k, _p(A), _p(B), _p(Cm), threads, reps, C.byref(secs)), "ref")
+    return Cm, secs.value
+
+
+def ref_rref_par(p: int, A, threads: int = 1):
+    """elim::rref under the tape's host elimination hook on a pool of `threads` workers."""
+    R = _u32(A).copy()
+    m, n = R.shape
+    piv = np.zeros(max(1, min(m, n)), np.uint32)
+    rank = C.c_uint32(0)
+    _chk(ref().ref_rref_par_u32(p, m, n, _p(R), n, _p(piv), C.byref(rank), threads), "ref")
+    return R, piv[: rank.value].copy()
+
+
+def ref_job(spec):
+    """One job of the batched stream on the reference CPU engine, one thread:
+    spec = (j, side, family, p, seed_a, seed_b); A, B from gen.job_matrix,
+    C = kernels::gemm(A, B), rank = |elim::column_rank_profile(C)|.  Returns
+    (j, rank, FNV-1a-64 of C).  A module-level function so that process pools
+    (started with spawn) can run it."""
+    from hacs_b200 import gen
+
+    j, s, fam, p, sa, sb = spec
+    A = gen.job_matrix(s, s, p, fam, sa)
+    B = gen.job_matrix(s, s, p, fam, sb)
+    Cm = ref_gemm(p, A, B)
+    return j, len(ref_rank_profile(p, Cm)), fnv_matrix(Cm)
 
 
 def ref_rank_profile(p: int, A):

@@ -19,6 +19,11 @@
 //   ring2k::howell / smith              src/ModArithmetic/Binary/Ring2k.h:702, :960
 //   ring3k::smith / howell              src/ModArithmetic/Binary/Ring3k.h:100-101
 //   smithpar::ScopedEnable              src/ModArithmetic/Binary/SmithPar.h:160
+//   tape::Recorder::gemm + Executor::run src/Engine/Recorder.h:147, Executor.h:79 (the reference's
+//                                       multi-thread GEMM path, EngineCoreScalingValidation.cpp:87-98)
+//   tape::ScopedHostElimHook            src/Engine/EngineRuntime.h:260 (host eliminations split over
+//                                       the consumer pool, ENGINE_API.md:1047-1059)
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <exception>
@@ -35,6 +40,11 @@
 #include "Binary/Ring2k.h"
 #include "Binary/Ring3k.h"
 #include "Binary/SmithPar.h"
+#include "Engine/EngineRuntime.h"
+#include "Engine/Executor.h"
+#include "Engine/Passes.h"
+#include "Engine/Recorder.h"
+#include "Engine/ThreadPool.h"
 
 using namespace engine;
 
@@ -334,6 +344,48 @@ int ref_howell_3k_u32(uint32_t kexp, uint32_t m, uint32_t n, const uint32_t* A, 
             pivot_v[i] = r.pivot_v[i];
             for (uint32_t j = 0; j < n; ++j) H[static_cast<size_t>(i) * n + j] = r.H.at(i, j);
         }
+    });
+}
+
+// C = A*B mod p (row-major, dense) through the reference's tape: one Recorder::gemm node, compiled,
+// then run `reps` times by an Executor on a ThreadPool of `threads` workers (the executor tiles the
+// node's C over the pool).  *seconds = the mean wall time of one Executor::run.
+int ref_tape_gemm_u32(uint32_t p, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A, const uint32_t* B,
+                      uint32_t* C, int threads, int reps, double* seconds) {
+    return guarded([&] {
+        const ModCtx<uint32_t> ctx(p);
+        DenseBuf<uint32_t> bA = wrap(const_cast<uint32_t*>(A), m, k, k);
+        DenseBuf<uint32_t> bB = wrap(const_cast<uint32_t*>(B), k, n, n);
+        DenseBuf<uint32_t> bC = wrap(C, m, n, n);
+        tape::ThreadPool pool(static_cast<uint32_t>(threads < 1 ? 1 : threads));
+        tape::Executor<uint32_t> ex(&pool);
+        tape::Recorder<uint32_t> rec(ctx);
+        const tape::BufId a = rec.input(cview(bA)), b = rec.input(cview(bB)), c = rec.output(DenseView<uint32_t>(bC));
+        rec.gemm(rec.whole(a), rec.whole(b), rec.whole(c), kernels::GemmOp::Set);
+        tape::Program<uint32_t> prog = rec.finish();
+        tape::compile(prog, tape::PassOptions());
+        const tape::Bindings<uint32_t> bind = rec.bindings();
+        const int r = reps < 1 ? 1 : reps;
+        const auto t0 = std::chrono::steady_clock::now();
+        for (int i = 0; i < r; ++i) ex.run(prog, bind);
+        const auto t1 = std::chrono::steady_clock::now();
+        *seconds = std::chrono::duration<double>(t1 - t0).count() / r;
+    });
+}
+
+// elim::rref of A (in place) with the host elimination hook of the tape bound to a pool of `threads`
+// workers: the reference's multi-thread host elimination.
+int ref_rref_par_u32(uint32_t p, uint32_t m, uint32_t n, uint32_t* A, uint32_t lda, uint32_t* pivots,
+                     uint32_t* rank, int threads) {
+    return guarded([&] {
+        const ModCtx<uint32_t> ctx(p);
+        DenseBuf<uint32_t> a = wrap(A, m, n, lda);
+        tape::ThreadPool pool(static_cast<uint32_t>(threads < 1 ? 1 : threads));
+        tape::ScopedConsumerPool scp(&pool);
+        tape::ScopedHostElimHook hook;
+        const elim::RrefResult r = elim::rref<uint32_t>(ctx, DenseView<uint32_t>(a));
+        *rank = r.rank;
+        for (uint32_t i = 0; i < r.rank; ++i) pivots[i] = r.pivots[i];
     });
 }
 

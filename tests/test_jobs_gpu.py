@@ -118,3 +118,52 @@ def test_batch_rank_wide_panels_and_tall_jobs(engine):
     torch.cuda.synchronize()
     ranks = engine.batch_rank_dev(jobs)
     assert list(ranks) == want
+
+
+def test_config4_full_stream_matches_reference(engine):
+    """All 10,000 jobs of the config-4 stream at full size (sides up to 1024),
+    generated on the device: every job's C checksum and every rank against the
+    reference CPU engine's own results (tests/golden/jobs10000.json, made by
+    tests/golden/make_golden_jobs.py from kernels::gemm and
+    elim::column_rank_profile).  The GEMMs and the ranks are checked apart
+    (the rank destroys C), then once more through the one-call GEMM + rank."""
+    from hacs_b200 import stream
+
+    gold = stream.golden_jobs()
+    assert gold is not None, "tests/golden/jobs10000.json is missing"
+    want_rank, want_fnv = gold
+    st = stream.DeviceStream(len(want_rank))
+    engine.use_own_stream()
+    engine.gen_jobs_dev(st.specs)
+    engine.batch_gemm_dev(st.jobs)
+    engine.sync()
+    got_fnv = st.job_checksums()
+    bad = [j for j in range(st.n_jobs) if got_fnv[j] != want_fnv[j]]
+    assert not bad, f"{len(bad)} jobs' C differ from the reference, first {bad[:5]}"
+    ranks = engine.batch_rank_dev(st.jobs)
+    bad = np.nonzero(ranks != want_rank)[0]
+    assert bad.size == 0, f"{bad.size} ranks differ from the reference, first {bad[:5].tolist()}"
+    engine.gen_jobs_dev(st.specs)
+    ranks = engine.batch_gemm_rank_dev(st.jobs)
+    assert np.array_equal(ranks, want_rank)
+
+
+def test_batch_mixed_with_jobs_taller_than_one_panel_cta(engine):
+    """Stream jobs mixed with jobs of more than 1024 rows (those take the
+    single-matrix elimination inside the batched call): GEMM + rank of every
+    job against the oracle."""
+    import torch
+
+    s, fam, p, sa, sb = gen.job_stream(12)
+    sides = [int(min(x, 300)) for x in s[:10]] + [1100, 1150]
+    jobs, want = [], []
+    for j, n in enumerate(sides):
+        pj = int(p[j % len(p)])
+        f = int(fam[j % len(fam)])
+        Ah = gen.job_matrix(n, n, pj, f, int(sa[j]))
+        Bh = gen.job_matrix(n, n, pj, f, int(sb[j]))
+        want.append(len(O.rref(pj, O.gemm(pj, Ah, Bh))[1]))
+        jobs.append({"p": pj, "A": _dev(Ah), "B": _dev(Bh), "C": torch.zeros((n, n), dtype=torch.int32, device="cuda")})
+    torch.cuda.synchronize()
+    ranks = engine.batch_gemm_rank_dev(jobs)
+    assert list(ranks) == want

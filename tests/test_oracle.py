@@ -126,3 +126,29 @@ def test_oracle_planted_mistake_is_caught():
     A[5, 7] = (A[5, 7] + 1) % case["p"]
     Rr, piv = O.rref(case["p"], A)
     assert fnv(Rr) != case["rref_fnv"]
+
+
+def test_job_stream_golden_pins_restatement():
+    """The config-4 golden file (the reference engine's rank and C checksum of
+    every job) agrees with the oracle's C restatement on a strided sample of
+    the stream's smaller jobs."""
+    import json
+
+    from hacs_b200 import gen
+
+    path = os.path.join(os.path.dirname(__file__), "golden", "jobs10000.json")
+    d = json.load(open(path))
+    assert d["n_jobs"] == len(d["rank"]) == len(d["c_fnv"]) == 10000
+    s, fam, p, sa, sb = gen.job_stream(10000)
+    checked = 0
+    for j in range(0, 10000, 97):
+        n = int(s[j])
+        if n > 160:
+            continue
+        A = gen.job_matrix(n, n, int(p[j]), int(fam[j]), int(sa[j]))
+        B = gen.job_matrix(n, n, int(p[j]), int(fam[j]), int(sb[j]))
+        Cm = O.gemm(int(p[j]), A, B)
+        assert O.fnv_matrix(Cm) == int(d["c_fnv"][j], 16), j
+        assert len(O.rref(int(p[j]), Cm)[1]) == d["rank"][j], j
+        checked += 1
+    assert checked >= 40

@@ -35,7 +35,11 @@ def _rand(g, shape, p):
 @pytest.mark.parametrize("p,shape,op", [(65521, (1024, 1024, 1024), SET),
                                         (2147483629, (300, 200, 500), ADD),
                                         (251, (129, 700, 64), SUB),
-                                        (16777213, (64, 96, 1200), SET)])
+                                        (16777213, (64, 96, 1200), SET),
+                                        # k beyond one exact K chunk (8192 at four limbs): the chunk loop runs
+                                        # twice, the second chunk accumulating on the first
+                                        (2147483629, (64, 64, 9000), SET),
+                                        (2147483629, (64, 64, 9000), SUB)])
 def test_noalloc_matches_regular_entry_point_twice(p, shape, op):
     import torch
 
@@ -72,3 +76,26 @@ def test_noalloc_rejects_oversized_product():
     assert rc == _lib.HME_EINVAL
     assert "32 MiB" in _lib.lib().hme_last_error().decode()
     assert int(Cm[0, 0]) == 7  # nothing ran
+
+
+def test_noalloc_refuses_stream_capture():
+    """The entry point waits for its stream before it returns, which a stream
+    being captured into a CUDA graph cannot do: it refuses the call up front
+    and leaves the capture intact."""
+    import torch
+
+    p = 65521
+    A = torch.ones((32, 32), dtype=torch.int32, device="cuda")
+    B = torch.ones((32, 32), dtype=torch.int32, device="cuda")
+    Cm = torch.zeros((32, 32), dtype=torch.int32, device="cuda")
+    st = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph, stream=st):
+        Cm.add_(1)
+        rc = _noalloc(p, A, B, Cm, SET, st.cuda_stream)
+    assert rc == _lib.HME_EINVAL
+    assert "capture" in _lib.lib().hme_last_error().decode()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert int(Cm[0, 0]) == 1  # the captured work ran; the refused call did not
