@@ -111,6 +111,28 @@ PROTOTYPES.update({
     "hme_mlp_predict_bf16": (C.c_int, [vp, u32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "hme_sched_plan": (C.c_int, [vp, vp, u32, u32p, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                  C.POINTER(C.c_int)]),
+    "hme_batch_gemm_u32_dev_plan": (C.c_int, [vp, u32, C.POINTER(HmeJob), C.POINTER(C.c_int)]),
+    "hme_batch_gemm_rank_u32_dev_plan": (C.c_int, [vp, u32, C.POINTER(HmeJob), C.POINTER(C.c_int), u32p]),
+    "hme_autotune_batch": (C.c_int, [vp, u32, u32, u32, u32, u32, C.c_int, C.POINTER(C.c_float)]),
+})
+
+
+class HmeR2kStep(C.Structure):
+    """struct hme_r2k_step_args (include/hme.h)."""
+    _fields_ = [("m", u32), ("r", u32), ("np", u32), ("pc0", u32), ("pc1", u32), ("panel", vp), ("ldp", sz),
+                ("swaps", u32p), ("nswaps", u32), ("L", vp), ("ldl", sz), ("u0", u32), ("la0", u32), ("la1", u32),
+                ("w", u32)]
+
+
+PROTOTYPES.update({
+    "hme_r2k_plan": (u32, [C.c_int, u32, u32, u32, u32, C.c_uint64]),
+    "hme_r2k_session_bytes": (sz, [u32, u32, u32, u32]),
+    "hme_r2k_open": (C.c_int, [C.c_int, u32, u32, u32, u32, C.POINTER(vp)]),
+    "hme_r2k_put": (C.c_int, [vp, vp, sz, u32, u32, u32, u32]),
+    "hme_r2k_get": (C.c_int, [vp, vp, sz, u32, u32, u32, u32]),
+    "hme_r2k_step": (C.c_int, [vp, C.POINTER(HmeR2kStep)]),
+    "hme_r2k_fetch": (C.c_int, [vp, vp, sz]),
+    "hme_r2k_close": (C.c_int, [vp]),
 })
 
 _lib = None

@@ -269,7 +269,7 @@ void launch_grouped(hme_ctx* ctx, const ModParams& mp, const GroupedProblem* d_p
 }
 
 template <int L>
-void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs_in) {
+void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs_in, int bn_choice) {
     std::vector<GemmJob> jobs;
     jobs.reserve(jobs_in.size());
     for (const GemmJob& j : jobs_in) {
@@ -284,7 +284,7 @@ void run_grouped(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& 
     constexpr int BNn = L == 1 ? 128 : L == 2 ? 64 : 32;
     size_t tiles_wide = 0;
     for (const GemmJob& j : jobs) tiles_wide += static_cast<size_t>((j.M + kBM - 1) / kBM) * ((j.N + BNw - 1) / BNw);
-    const bool narrow = tiles_wide < static_cast<size_t>(ctx->num_sms);
+    const bool narrow = bn_choice == 1 || (bn_choice < 0 && tiles_wide < static_cast<size_t>(ctx->num_sms));
     const int BN = narrow ? BNn : BNw;
     // k-block: the narrowest swizzle row (32, 64 or 128 bytes) that holds every
     // K of the launch (the rank rounds' updates have K = the round's pivots), so
@@ -472,12 +472,12 @@ void grouped_launch_device_tables(hme_ctx* ctx, const ModParams& mp, const Group
     }
 }
 
-void grouped_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs) {
+void grouped_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs, int bn_choice) {
     switch (mp.limbs) {
-        case 1: run_grouped<1>(ctx, mp, jobs); break;
-        case 2: run_grouped<2>(ctx, mp, jobs); break;
-        case 3: run_grouped<3>(ctx, mp, jobs); break;
-        default: run_grouped<4>(ctx, mp, jobs); break;
+        case 1: run_grouped<1>(ctx, mp, jobs, bn_choice); break;
+        case 2: run_grouped<2>(ctx, mp, jobs, bn_choice); break;
+        case 3: run_grouped<3>(ctx, mp, jobs, bn_choice); break;
+        default: run_grouped<4>(ctx, mp, jobs, bn_choice); break;
     }
 }
 

@@ -62,8 +62,15 @@ struct GemmJob {
 // C_j op= A_j * B_j mod mp.p for every job (device pointers), in one split
 // launch and one persistent tensor-core launch on ctx->stream; returns after
 // the launches are enqueued and their host-side tables consumed.  K_j must fit
-// one exact-accumulation chunk (limb_k_chunk).
-void grouped_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs);
+// one exact-accumulation chunk (limb_k_chunk).  bn_choice: the tile width,
+// 0 wide (L * BN close to 256), 1 half-width, -1 wide unless the launch's
+// wide tiles leave SMs idle.
+void grouped_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs,
+                             int bn_choice = -1);
+// The same products on the CUDA cores: one launch over every tile of every
+// job (TILE x TILE tiles, tile 32 or 64), exact u64 accumulation; returns after
+// the launch is enqueued and its tables are on the device.
+void batch_simt_gemm_device(hme_ctx* ctx, const ModParams& mp, const std::vector<GemmJob>& jobs, int tile);
 
 // A device matrix of a batch (rank jobs).
 struct BatchMatrix {

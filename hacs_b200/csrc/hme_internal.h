@@ -236,10 +236,21 @@ void simt_gemm_u32_device(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_
 int limb_kp(uint32_t k);
 void gemm_u32_planes(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, int Kp, uint8_t* pa,
                      uint64_t a_plane, uint8_t* pb, uint32_t* C, size_t ldc, int op);
+// C op= A*B mod 2^32 (native wraparound u32 arithmetic, any u32 words) on the
+// same limb-split + tcgen05 kernels: with the modulus constants p = 0 and
+// Barrett m = 0 every reduction of the split and the epilogue is the
+// truncation to 32 bits (x - mulhi(x, 0) * 0 = x), and 256^i * B "mod p" is
+// B << 8i truncated, so sum_j 256^j D_j truncated is A*B mod 2^32.  Device
+// pointers, on ctx->stream.
+void gemm_u32_wrap_device(hme_ctx* ctx, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A, size_t lda,
+                          const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op);
 // The shape heuristic (the method without a learned model).
 int gemm_default_variant(const hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n);
 // The scheduler's choice for one product (sched.cu), and its tear-down.
 int sched_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k);
+// The learned plan's decision for one product's shape class, or -1 when the
+// plan holds none (sched.cu).
+int sched_planned_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k);
 void sched_release(hme_ctx* ctx);
 
 }  // namespace hme

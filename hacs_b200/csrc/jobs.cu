@@ -980,23 +980,39 @@ void check_job(const hme_job& j) {
     HME_REQUIRE(j.k == 0 || j.m == 0 || j.n == 0 || (j.A && j.B && j.lda >= j.k && j.ldb >= j.n), "job: bad A / B");
 }
 
-void batch_gemm(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs) {
-    // one grouped launch per modulus; a K beyond the exact-accumulation chunk takes the single-job path
+// The GEMM phase of a batch.  Every job's schedule is one of the GEMM variants
+// (GemmVariant: tensor-core wide / half-width tiles, CUDA-core 32 / 64 tiles):
+// from `variants` when given (-1 = the batch rule), else from the context: a
+// pinned variant, or under the learned policy the planner's decision for the
+// job's shape class (unplanned shapes: the batch rule).  The batch rule is one
+// tensor-core launch with wide tiles unless the launch's wide tiles leave SMs
+// idle.  Jobs run as one launch per (modulus, schedule) group, so a schedule
+// changes only the launch a job's tiles belong to, never a residue.
+constexpr int kBatchRule = -1;
+
+void batch_gemm(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs, const int* variants = nullptr) {
     std::vector<uint32_t> mods;
     for (uint32_t t = 0; t < njobs; ++t) {
         check_job(jobs[t]);
+        if (variants) HME_REQUIRE(variants[t] >= kBatchRule && variants[t] < kGemmVariants, "job: unknown variant");
         if (std::find(mods.begin(), mods.end(), jobs[t].p) == mods.end()) mods.push_back(jobs[t].p);
     }
     for (uint32_t p : mods) {
         const ModParams mp = make_mod(p);
-        std::vector<GemmJob> g;
+        // groups: the batch rule, then one per variant
+        std::vector<GemmJob> g[1 + kGemmVariants];
         for (uint32_t t = 0; t < njobs; ++t) {
             const hme_job& j = jobs[t];
             if (j.p != p || j.m == 0 || j.n == 0) continue;
             if (j.k == 0 || j.k > limb_k_chunk(mp.limbs)) {
+                // a K beyond the exact-accumulation chunk takes the single-job path
                 gemm_u32_device(ctx, mp, j.m, j.n, j.k, j.A, j.lda, j.B, j.ldb, j.C, j.ldc, HME_SET);
                 continue;
             }
+            int v = kBatchRule;
+            if (variants) v = variants[t];
+            else if (ctx->fixed_variant >= 0) v = ctx->fixed_variant;
+            else if (ctx->sched_policy == 1) v = sched_planned_variant(ctx, mp, j.m, j.n, j.k);
             GemmJob x;
             x.M = j.m;
             x.N = j.n;
@@ -1008,9 +1024,13 @@ void batch_gemm(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs) {
             x.C = j.C;
             x.ldc = j.ldc;
             x.op = HME_SET;
-            g.push_back(x);
+            g[v + 1].push_back(x);
         }
-        grouped_gemm_u32_device(ctx, mp, g);
+        grouped_gemm_u32_device(ctx, mp, g[0], -1);
+        grouped_gemm_u32_device(ctx, mp, g[1 + kVariantWide], 0);
+        grouped_gemm_u32_device(ctx, mp, g[1 + kVariantNarrow], 1);
+        batch_simt_gemm_device(ctx, mp, g[1 + kVariantSimt32], 32);
+        batch_simt_gemm_device(ctx, mp, g[1 + kVariantSimt64], 64);
     }
 }
 
@@ -1054,6 +1074,65 @@ int hme_batch_gemm_rank_u32_dev(hme_ctx* ctx, uint32_t njobs, const hme_job* job
         bind(ctx);
         batch_gemm(ctx, njobs, jobs);
         batch_rank(ctx, njobs, jobs, ranks);
+    });
+}
+
+int hme_batch_gemm_u32_dev_plan(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs, const int* variants) {
+    return guard([&] {
+        HME_REQUIRE(ctx && (njobs == 0 || jobs), "null argument");
+        bind(ctx);
+        batch_gemm(ctx, njobs, jobs, variants);
+        check_device_error(ctx);
+    });
+}
+
+int hme_batch_gemm_rank_u32_dev_plan(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs, const int* variants,
+                                     uint32_t* ranks) {
+    return guard([&] {
+        HME_REQUIRE(ctx && (njobs == 0 || (jobs && ranks)), "null argument");
+        bind(ctx);
+        batch_gemm(ctx, njobs, jobs, variants);
+        batch_rank(ctx, njobs, jobs, ranks);
+    });
+}
+
+int hme_autotune_batch(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, uint32_t count, int reps,
+                       float* ms) {
+    return guard([&] {
+        HME_REQUIRE(ctx && ms && p >= 2 && m && n && k && count, "autotune_batch: bad arguments");
+        bind(ctx);
+        const size_t ea = static_cast<size_t>(m) * k, eb = static_cast<size_t>(k) * n, ec = static_cast<size_t>(m) * n;
+        uint32_t* AB = static_cast<uint32_t*>(ctx->ws.get(kSlotSched0, sizeof(uint32_t) * (ea + eb) * count));
+        uint32_t* Cs = static_cast<uint32_t*>(ctx->ws.get(kSlotSched1, sizeof(uint32_t) * ec * count));
+        // operand values do not change any variant's timing; fill with a residue pattern
+        HME_CUDA(cudaMemsetAsync(AB, 0x11, sizeof(uint32_t) * (ea + eb) * count, ctx->stream));
+        std::vector<hme_job> jobs(count);
+        for (uint32_t t = 0; t < count; ++t) {
+            jobs[t] = hme_job{p, m, n, k, AB + t * (ea + eb), k, AB + t * (ea + eb) + ea, n, Cs + t * ec, n};
+        }
+        cudaEvent_t e0, e1;
+        HME_CUDA(cudaEventCreate(&e0));
+        HME_CUDA(cudaEventCreate(&e1));
+        std::vector<int> var(count);
+        for (int v = 0; v < kGemmVariants; ++v) {
+            std::fill(var.begin(), var.end(), v);
+            std::vector<float> t;
+            batch_gemm(ctx, count, jobs.data(), var.data());  // warm
+            for (int r = 0; r < std::max(1, reps); ++r) {
+                HME_CUDA(cudaEventRecord(e0, ctx->stream));
+                batch_gemm(ctx, count, jobs.data(), var.data());
+                HME_CUDA(cudaEventRecord(e1, ctx->stream));
+                HME_CUDA(cudaEventSynchronize(e1));
+                float x = 0.f;
+                HME_CUDA(cudaEventElapsedTime(&x, e0, e1));
+                t.push_back(x);
+            }
+            std::sort(t.begin(), t.end());
+            ms[v] = t[t.size() / 2] / static_cast<float>(count);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        check_device_error(ctx);
     });
 }
 

@@ -524,6 +524,34 @@ void gemm_u32_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n,
                         ldc, op, true);
 }
 
+void gemm_u32_wrap_device(hme_ctx* ctx, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A, size_t lda,
+                          const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op) {
+    HME_REQUIRE(op == HME_SET || op == HME_ADD || op == HME_SUB, "gemm: op must be HME_SET, HME_ADD or HME_SUB");
+    HME_REQUIRE(m < (1u << 30) && n < (1u << 30) && k < (1u << 30), "gemm: dimension too large");
+    if (m == 0 || n == 0) return;
+    HME_REQUIRE(ldc >= n, "gemm: ldc < n");
+    if (k == 0) {
+        if (op == HME_SET) {
+            HME_TIMED(ctx, "fill_zero",
+                      fill_zero_kernel<<<std::min<size_t>(1024, (static_cast<size_t>(m) * n + 255) / 256), 256, 0,
+                                         ctx->stream>>>(C, ldc, m, n));
+            HME_CUDA(cudaGetLastError());
+        }
+        return;
+    }
+    HME_REQUIRE(A && B && C && lda >= k && ldb >= n, "gemm: bad operands");
+    ModParams mp;  // p = 0, m = 0: every reduction is the truncation to 32 bits
+    mp.p = 0;
+    mp.limbs = 4;
+    mp.barrett = 0;
+    const int Kp = static_cast<int>((k + kblock_for(k) - 1) / kblock_for(k) * kblock_for(k));
+    uint8_t* pa = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesA, static_cast<size_t>(4) * m * Kp));
+    uint8_t* pb = static_cast<uint8_t*>(ctx->ws.get(kSlotPlanesB, static_cast<size_t>(16) * n * Kp));
+    launch_split(ctx, mp, m, n, k, Kp, A, lda, B, ldb, pa, 0, pb, true, true);
+    launch_gemm_variant(ctx, mp, gemm_default_variant(ctx, mp, m, n) == kVariantNarrow, m, n, k, Kp, pa,
+                        static_cast<uint64_t>(Kp) * m, pb, C, ldc, op, true);
+}
+
 void gemm_u32_host(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k, const uint32_t* A,
                    size_t lda, const uint32_t* B, size_t ldb, uint32_t* C, size_t ldc, int op, int variant) {
     // Pipeline over row chunks of A and C (multiples of the 128-row tile, 1 to

@@ -234,6 +234,13 @@ ShapeKey shape_key(uint32_t m, uint32_t n, uint32_t k, uint32_t limbs) {
 
 }  // namespace
 
+int sched_planned_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k) {
+    if (!ctx->sched_table) return -1;
+    const PlanTable& t = *static_cast<PlanTable*>(ctx->sched_table);
+    auto it = t.find(shape_key(m, n, k, mp.limbs));
+    return it == t.end() ? -1 : it->second;
+}
+
 int sched_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k) {
     if (ctx->sched_policy == 1 && ctx->sched_table) {
         const PlanTable& t = *static_cast<PlanTable*>(ctx->sched_table);

@@ -290,6 +290,16 @@ typedef struct hme_gen_spec {
     uint64_t seed;
 } hme_gen_spec;
 HME_API int hme_batch_gemm_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs);
+/* The same with every job's GEMM schedule given: variants[j] is one of the
+ * GEMM variants below (0, 1 tensor-core wide / half-width tiles; 2, 3
+ * CUDA-core 32 / 64 tiles) or -1 (the batch rule: one tensor-core launch per
+ * modulus, wide tiles unless they leave SMs idle); variants = NULL takes the
+ * context's scheduler (a pinned variant, else under the learned policy the
+ * planner's decision per job's shape class, else the batch rule).  Jobs run as
+ * one launch per (modulus, schedule) group; no schedule changes a residue. */
+HME_API int hme_batch_gemm_u32_dev_plan(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, const int *variants);
+HME_API int hme_batch_gemm_rank_u32_dev_plan(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, const int *variants,
+                                             uint32_t *ranks);
 HME_API int hme_batch_rank_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, uint32_t *ranks);
 HME_API int hme_batch_gemm_rank_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, uint32_t *ranks);
 HME_API int hme_gen_jobs_u32_dev(hme_ctx *ctx, uint32_t nmat, const hme_gen_spec *specs);
@@ -323,6 +333,12 @@ HME_API int hme_gemm_u32_dev_variant(hme_ctx *ctx, int variant, uint32_t p, uint
 HME_API int hme_ctx_set_gemm_variant(hme_ctx *ctx, int variant);
 HME_API int hme_ctx_set_sched_policy(hme_ctx *ctx, int policy);
 HME_API int hme_autotune_gemm(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, int reps, float *ms);
+/* The exhaustive autotuner of the batched stream: a batch of `count` jobs of
+ * one shape run with every job on each variant in turn
+ * (hme_batch_gemm_u32_dev_plan); ms[v] = median batch time / count, the
+ * per-job device time of variant v inside a batch. */
+HME_API int hme_autotune_batch(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, uint32_t count, int reps,
+                               float *ms);
 HME_API int hme_mlp_param_count(void);
 HME_API int hme_mlp_create(hme_ctx *ctx, uint64_t seed, hme_mlp **out);
 HME_API int hme_mlp_destroy(hme_mlp *mlp);
@@ -334,6 +350,64 @@ HME_API int hme_mlp_train(hme_mlp *mlp, uint32_t n, const float *X, const float 
 HME_API int hme_mlp_predict_bf16(hme_mlp *mlp, uint32_t n, const float *X, float *Y);
 HME_API int hme_sched_plan(hme_ctx *ctx, hme_mlp *mlp, uint32_t n, const uint32_t *shapes, const float *density,
                            const float *norm, int *variants);
+
+/* ---- device-resident blocked LU over Z/2^32 and Z/2^64 (ring2k device ops) ----
+ * The session behind engine::ring2k::device::Ops (src/ModArithmetic/Binary/
+ * Ring2kDevice.h:64-83, installed by src/hacs/Integral/Descent/
+ * DescentSmithGpu.cpp:160-178; its device side in the reference is
+ * engine::cuda::ring2k, src/Cuda/CudaRing2k.h:27-45).  ring2k::echelon_blocked
+ * (Ring2k.h:539-695, driver Ring2kDeviceLU.h) factors each panel on the host
+ * and hands the device one step per panel; every entry is an exact value of
+ * Z/2^W (W = 8 * elem), bit-identical to the host LU.
+ *
+ * hme_r2k_plan: the column window cw for an m x n matrix of elem-byte entries
+ *   (4 or 8) with this panel width: n when the session fits the device's free
+ *   memory (less a reserve of max(1 GiB, 2 % of the card), capped at vram_cap
+ *   bytes when non-zero), a multiple of panel below n (tiled), or 0 (decline:
+ *   the host LU runs).  Ops::plan.
+ * hme_r2k_session_bytes: device bytes of a session (window, L store, planes).
+ * hme_r2k_open: a session on `device` for m rows and a window of cw columns
+ *   (Ops::open); its own stream pair and pinned staging.
+ * hme_r2k_put / hme_r2k_get: synchronous copies between a host block (ld ldh
+ *   elements) and the window's rows [r0, r0+rows) x columns [c0, c0+cols)
+ *   (Ops::put / Ops::get).
+ * hme_r2k_step: one panel step (Ops::step with StepArgs, Ring2kDevice.h:49-62):
+ *   the factored panel (rows r .. m-1, columns [pc0, pc1), ld ldp; NULL = none)
+ *   written into the window; the nswaps row pairs of `swaps` exchanged in order
+ *   on every other window column of [0, w); the unit-lower solve with L's rows
+ *   0 .. np-1 (L row 0 = matrix row r, ld ldl) on the pivot rows, columns
+ *   [u0, w); C -= L21 U12 on rows r+np .. m-1, columns [u0, w); lookahead: rows
+ *   r+np .. m-1 of the columns [la0, la1) are read back once updated (empty
+ *   when la0 == la1).  w = 0 means the session's cw.  The host buffers are
+ *   copied before the call returns; the device work is asynchronous.
+ * hme_r2k_fetch: waits for the last step's lookahead block and copies it to a
+ *   host block (ld ldh elements) (Ops::fetch).
+ * hme_r2k_close: frees the session; reports a device-side timeout seen in it
+ *   (Ops::close). */
+typedef struct hme_r2k hme_r2k;
+typedef struct hme_r2k_step_args {
+    uint32_t m;
+    uint32_t r, np;
+    uint32_t pc0, pc1;
+    const void *panel;
+    size_t ldp;
+    const uint32_t *swaps;
+    uint32_t nswaps;
+    const void *L;
+    size_t ldl;
+    uint32_t u0;
+    uint32_t la0, la1;
+    uint32_t w;
+} hme_r2k_step_args;
+HME_API uint32_t hme_r2k_plan(int device, uint32_t elem, uint32_t m, uint32_t n, uint32_t panel, uint64_t vram_cap);
+HME_API size_t hme_r2k_session_bytes(uint32_t elem, uint32_t m, uint32_t cw, uint32_t panel);
+HME_API int hme_r2k_open(int device, uint32_t elem, uint32_t m, uint32_t cw, uint32_t panel, hme_r2k **out);
+HME_API int hme_r2k_put(hme_r2k *s, const void *host, size_t ldh, uint32_t r0, uint32_t rows, uint32_t c0,
+                        uint32_t cols);
+HME_API int hme_r2k_get(hme_r2k *s, void *host, size_t ldh, uint32_t r0, uint32_t rows, uint32_t c0, uint32_t cols);
+HME_API int hme_r2k_step(hme_r2k *s, const hme_r2k_step_args *a);
+HME_API int hme_r2k_fetch(hme_r2k *s, void *host, size_t ldh);
+HME_API int hme_r2k_close(hme_r2k *s);
 
 /* The GEMM above (same kernels, same result bits) for callers that cannot
  * allocate device memory when they call it -- a plugin inside another runtime

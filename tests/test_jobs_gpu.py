@@ -167,3 +167,60 @@ def test_batch_mixed_with_jobs_taller_than_one_panel_cta(engine):
     torch.cuda.synchronize()
     ranks = engine.batch_gemm_rank_dev(jobs)
     assert list(ranks) == want
+
+
+def test_batch_plan_variants_match_oracle(engine):
+    """Every job of a batch on an explicit GEMM schedule (tensor-core wide /
+    half-width tiles, CUDA-core 32 / 64 tiles, or the batch rule), mixed in one
+    call over two moduli: C and the ranks bit-exact against the oracle, and the
+    same for every schedule (a schedule changes only the launch a job runs in)."""
+    import ctypes as C_
+
+    import torch
+
+    from hacs_b200 import _lib
+
+    shapes = [(16, 16, 16), (37, 20, 53), (128, 128, 128), (200, 150, 90), (300, 300, 300), (64, 500, 40),
+              (513, 257, 129), (90, 90, 5), (1, 1, 1), (700, 33, 640)]
+    jobs, want_c, want_r, hjobs = [], [], [], []
+    for t, (m, k, n) in enumerate(shapes * 2):
+        p = (65521, 2147483629)[t % 2]
+        fam = (t // 3) % 2
+        A = gen.job_matrix(m, k, p, fam, 3000 + t)
+        B = gen.job_matrix(k, n, p, fam, 4000 + t)
+        Cw = O.gemm(p, A, B)
+        want_c.append(Cw)
+        want_r.append(len(O.rref(p, Cw)[1]))
+        jobs.append({"p": p, "A": _dev(A), "B": _dev(B), "C": torch.zeros((m, n), dtype=torch.int32, device="cuda")})
+    arr = engine._jobs(jobs)
+    L = _lib.lib()
+    for rot in range(5):
+        var = np.array([((t + rot) % 5) - 1 for t in range(len(jobs))], dtype=np.int32)
+        for j in jobs:
+            j["C"].zero_()
+        torch.cuda.synchronize()
+        rc = L.hme_batch_gemm_u32_dev_plan(engine._h, len(jobs), arr, var.ctypes.data_as(C_.POINTER(C_.c_int)))
+        assert rc == 0, L.hme_last_error().decode()
+        for j, Cw in zip(jobs, want_c):
+            assert np.array_equal(j["C"].cpu().numpy().view(np.uint32), Cw), (rot, j["C"].shape)
+    ranks = np.zeros(len(jobs), np.uint32)
+    var = np.array([(t % 5) - 1 for t in range(len(jobs))], dtype=np.int32)
+    rc = L.hme_batch_gemm_rank_u32_dev_plan(engine._h, len(jobs), arr, var.ctypes.data_as(C_.POINTER(C_.c_int)),
+                                            ranks.ctypes.data_as(C_.POINTER(C_.c_uint32)))
+    assert rc == 0, L.hme_last_error().decode()
+    assert list(ranks) == want_r
+    bad = np.full(len(jobs), 7, np.int32)
+    assert L.hme_batch_gemm_u32_dev_plan(engine._h, len(jobs), arr, bad.ctypes.data_as(C_.POINTER(C_.c_int))) == \
+        _lib.HME_EINVAL
+
+
+def test_batch_autotuner_times_every_variant(engine):
+    import ctypes as C_
+
+    from hacs_b200 import _lib
+
+    ms = np.zeros(4, np.float32)
+    for (p, m, n, k, count) in [(65521, 32, 32, 32, 64), (2147483629, 256, 256, 256, 4)]:
+        rc = _lib.lib().hme_autotune_batch(engine._h, p, m, n, k, count, 3, ms.ctypes.data_as(C_.POINTER(C_.c_float)))
+        assert rc == 0, _lib.lib().hme_last_error().decode()
+        assert np.all(ms > 0) and np.all(np.isfinite(ms))
