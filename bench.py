@@ -657,36 +657,97 @@ def extra_jobstream(eng, plain, n_jobs=10000, sample=500):
     return out
 
 
-def extra_scheduler(eng, n_stream=50000, sample=2000):
-    """Config 5: the trained MLP (committed weights, trained on this engine's own
-    autotuner timings) plans a 50,000-job stream drawn from the configurations'
-    mix with one BF16 inference launch; on a sample, the chosen variants' device
-    times against the exhaustive autotuner's best (regret) and the heuristic."""
-    from hacs_b200 import sched
+def serve_stream(eng, ms, plan, warm: bool = False):
+    """Serve the mixed stream in its chunks with per-job GEMM schedules `plan`
+    (hme_batch_gemm_rank_u32_dev_plan); returns (seconds inside the calls, ranks)."""
+    import ctypes as C_
 
-    if not os.path.exists(sched.WEIGHTS):
-        return {"unavailable": "no trained weights in the package"}
+    import torch
+
+    import hacs_b200
+
+    ranks = np.zeros(ms.n_jobs, np.uint32)
+    total = 0.0
+    for c0, c1 in ms.chunks():
+        jobs, specs = ms.device_chunk(c0, c1)
+        eng.gen_jobs_dev(specs)
+        arr = eng._jobs(jobs)
+        var = np.ascontiguousarray(plan[c0:c1], dtype=np.int32)
+        out = np.zeros(c1 - c0, np.uint32)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hacs_b200.check(eng._lib.hme_batch_gemm_rank_u32_dev_plan(eng._h, c1 - c0, arr,
+                                                                  var.ctypes.data_as(C_.POINTER(C_.c_int)),
+                                                                  out.ctypes.data_as(C_.POINTER(C_.c_uint32))))
+        total += time.perf_counter() - t0
+        ranks[c0:c1] = out
+        if warm:
+            break
+    return total, ranks
+
+
+def extra_scheduler(eng, n_stream=50000):
+    """Config 5: the 50,000-job mixed stream (stream.MixedStream: config-4 jobs, config-2 rank-deficient
+    products, config-1 products) served end to end through the batched GEMM + rank call under three plans of
+    per-job GEMM schedules: the learned planner's (the MLP trained on this engine's batch autotuner timings,
+    one BF16 inference launch for the whole stream), the batch rule (the method without the network) and the
+    exhaustive batch autotuner's best per shape class.  Ranks are checked across plans and against the
+    reference / the construction."""
+    from hacs_b200 import sched, stream
+
+    if not os.path.exists(sched.BATCH_WEIGHTS):
+        return {"unavailable": "no trained batch-planner weights in the package"}
+    ms = stream.MixedStream(n_stream)
+    shapes, dens = ms.shapes(), ms.density()
     mlp = sched.MLP(eng)
-    mlp.load()
-    shapes, dens = sched.sample_shapes(n_stream, seed=2027)
+    mlp.load(sched.BATCH_WEIGHTS)
     mlp.plan(shapes[:64], dens[:64])  # warm
     t0 = time.perf_counter()
-    plan = mlp.plan(shapes, dens)
+    learned = mlp.plan(shapes, dens)
     t_plan = time.perf_counter() - t0
-    T = np.stack([sched.autotune(eng, *shapes[i]) for i in range(sample)])
-    F = sched.raw_features(shapes[:sample, 0], shapes[:sample, 1], shapes[:sample, 2], shapes[:sample, 3],
-                           dens[:sample])
-    heur = sched.heuristic_choice(F)
-    rows = np.arange(sample)
-    out = {"workload": f"{n_stream}-job mixed stream (configs 1-4 shapes), MLP plan; regret on {sample} jobs "
-                       "against the exhaustive autotuner (config 5)",
-           "plan_ms": t_plan * 1e3, "plan_jobs_per_s": n_stream / t_plan,
-           "regret_mlp": sched.regret(T, plan[:sample]), "regret_heuristic": sched.regret(T, heur),
-           "sample_jobs_per_s_mlp": sample / (T[rows, plan[:sample]].sum() / 1e3),
-           "sample_jobs_per_s_heuristic": sample / (T[rows, heur].sum() / 1e3),
-           "sample_jobs_per_s_best": sample / (T.min(1).sum() / 1e3),
-           "variant_share": np.bincount(plan, minlength=sched.N_VARIANTS).tolist()}
     mlp.close()
+    # the exhaustive autotuner: every variant timed inside a batch, once per shape class of the stream
+    t0 = time.perf_counter()
+    first = {}
+    for t in range(ms.n_jobs):
+        first.setdefault(sched.shape_class(*shapes[t]), t)
+    T = {key: sched.autotune_batch(eng, *shapes[t]) for key, t in first.items()}
+    t_tune = time.perf_counter() - t0
+    keys = [sched.shape_class(*row) for row in shapes]
+    best = np.array([int(np.argmin(T[k])) for k in keys], np.int32)
+    rule = np.full(ms.n_jobs, sched.BATCH_RULE, np.int32)
+    serve_stream(eng, ms, rule, warm=True)  # workspace growth, module load
+    res = {}
+    for name, plan in (("heuristic", rule), ("learned", learned), ("autotuner_best", best)):
+        ts, rk = [], None
+        for _ in range(2):
+            t, r = serve_stream(eng, ms, plan)
+            ts.append(t)
+            if rk is not None:
+                assert np.array_equal(rk, r)
+            rk = r
+        res[name] = (min(ts), rk)
+    t_h, r_h = res["heuristic"]
+    t_l, r_l = res["learned"]
+    t_b, r_b = res["autotuner_best"]
+    per_job = np.array([T[k] for k in keys])  # per-job batch times of every variant, by class
+    rows = np.arange(ms.n_jobs)
+    out = {"workload": f"{ms.n_jobs}-job mixed stream (config-4 jobs incl. all 10,000 of config 4, config-2 "
+                       "rank-deficient products at 2^31-19, config-1 1024^3 products), GEMM + rank per job, "
+                       f"served in chunks of {ms.chunk} (config 5)",
+           "jobs_per_s_served": {"learned": ms.n_jobs / t_l, "heuristic": ms.n_jobs / t_h,
+                                 "autotuner_best": ms.n_jobs / t_b},
+           "served_s": {"learned": t_l, "heuristic": t_h, "autotuner_best": t_b},
+           "regret_served_learned": (t_l - t_b) / t_b, "regret_served_heuristic": (t_h - t_b) / t_b,
+           "learned_vs_heuristic": t_h / t_l,
+           "regret_per_job_model_learned": float(np.mean((per_job[rows, learned] - per_job.min(1)) / per_job.min(1))),
+           "plan_ms": t_plan * 1e3, "autotune_s": t_tune, "shape_classes": len(first),
+           "variant_share_learned": np.bincount(learned, minlength=sched.N_VARIANTS).tolist(),
+           "variant_share_best": np.bincount(best, minlength=sched.N_VARIANTS).tolist(),
+           "ranks_equal_across_plans": bool(np.array_equal(r_h, r_l) and np.array_equal(r_h, r_b)),
+           "rank_checks": ms.check_ranks(r_l),
+           "planner": "MLP 5-64-64-64-4 (hand-written FP32 training / BF16 inference kernels) trained on "
+                      "hme_autotune_batch timings (python -m hacs_b200.sched_train --batch)"}
     return out
 
 

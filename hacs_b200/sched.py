@@ -23,6 +23,10 @@ from ._lib import check
 DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 WEIGHTS = os.path.join(DATA, "sched_mlp.npz")
 TIMINGS = os.path.join(DATA, "sched_timings.npz")
+# the batched stream's planner: trained on per-job times inside batches (hme_autotune_batch)
+BATCH_WEIGHTS = os.path.join(DATA, "sched_batch_mlp.npz")
+BATCH_TIMINGS = os.path.join(DATA, "sched_batch_timings.npz")
+BATCH_RULE = -1
 N_VARIANTS = 4
 VARIANT_NAMES = ("tensor-wide", "tensor-narrow", "simt-32", "simt-64")
 
@@ -188,6 +192,66 @@ def autotune(engine, p, m, n, k, reps: int = 3) -> np.ndarray:
     ms = np.zeros(N_VARIANTS, np.float32)
     check(_lib.lib().hme_autotune_gemm(engine._h, int(p), int(m), int(n), int(k), reps, ms.ctypes.data_as(_fp)))
     return ms
+
+
+def batch_count(m, n, k, work: float = 2.0 ** 27, cap: int = 256) -> int:
+    """Jobs of one shape timed together by the batch autotuner: about `work`
+    multiply-adds per batch, at least one job, at most `cap`."""
+    return int(max(1, min(cap, work // max(1, int(m) * int(n) * int(k)))))
+
+
+def autotune_batch(engine, p, m, n, k, count=None, reps: int = 3) -> np.ndarray:
+    """Per-job device time (ms) of every GEMM variant inside a batch of `count`
+    jobs of this shape (hme_autotune_batch)."""
+    ms = np.zeros(N_VARIANTS, np.float32)
+    c = batch_count(m, n, k) if count is None else int(count)
+    check(_lib.lib().hme_autotune_batch(engine._h, int(p), int(m), int(n), int(k), c, reps, ms.ctypes.data_as(_fp)))
+    return ms
+
+
+def shape_class(p, m, n, k) -> tuple:
+    """Quarter-octave class of a product's shape and its limb count (the key of
+    the engine's plan table, sched.cu shape_key)."""
+    q = lambda x: int(np.rint(4.0 * np.log2(max(1, int(x)))))  # noqa: E731
+    p = int(p)
+    L = 1 if p <= 256 else 2 if p <= 65536 else 3 if p <= (1 << 24) else 4
+    return (q(m), q(n), q(k), L)
+
+
+def sample_stream_shapes(n: int, seed: int = 11):
+    """Seeded job shapes of the batched stream's mix (stream.MixedStream): config-4
+    jobs (squares 16..1024, p in {65521, 2^31 - 19}, dense or banded), config-2
+    products (s x r times r x s, s 64..1024, r = s - s // 20, p = 2^31 - 19) and
+    config-1 cubes (128..1024 at 65521).  Rows (p, m, n, k), density."""
+    rng = np.random.default_rng(seed)
+    kind = rng.choice(3, size=n, p=[0.6, 0.25, 0.15])
+    P = np.zeros(n, np.int64)
+    S = np.zeros((n, 3), np.int64)
+    dens = np.ones(n)
+    for i in range(n):
+        if kind[i] == 0:
+            s = int(np.rint(16 * 64 ** rng.random()))
+            P[i] = (65521, 2147483629)[rng.integers(0, 2)]
+            S[i] = (s, s, s)
+            dens[i] = (1.0, 0.05)[rng.integers(0, 2)]
+        elif kind[i] == 1:
+            s = int(np.rint(64 * 16 ** rng.random()))
+            P[i] = 2147483629
+            S[i] = (s, s, s - s // 20)
+        else:
+            s = int(np.rint(128 * 8 ** rng.random()))
+            P[i] = 65521
+            S[i] = (s, s, s)
+    return np.column_stack([P, S]).astype(np.uint32), dens
+
+
+def collect_batch(engine, n: int, seed: int = 11, reps: int = 3):
+    """Time every variant inside batches on n seeded stream shapes: (shapes, density, per-job ms)."""
+    shapes, dens = sample_stream_shapes(n, seed)
+    T = np.zeros((n, N_VARIANTS), np.float32)
+    for i, (p, m, nn, k) in enumerate(shapes):
+        T[i] = autotune_batch(engine, p, m, nn, k, reps=reps)
+    return shapes, dens, T
 
 
 def collect(engine, n: int, seed: int = 11, reps: int = 3):

@@ -1,6 +1,6 @@
 """Collect autotuner timings on this GPU and train the scheduler MLP.
 
-    python -m hacs_b200.sched_train [--shapes 20000] [--reps 3] [--epochs 300]
+    python -m hacs_b200.sched_train [--shapes 20000] [--reps 3] [--epochs 300] [--batch]
 
 Times every GEMM variant on `--shapes` seeded shapes from the configurations'
 mix with the exhaustive autotuner (hme_autotune_gemm), trains the MLP on the
@@ -8,6 +8,11 @@ GPU (hme_mlp_train: the library's FP32 forward / backward / Adam kernels) on
 80 % of them, reports the BF16-inference regret against the autotuner's best on
 the other 20 % next to the shape heuristic's, and writes
 hacs_b200/data/sched_timings.npz and hacs_b200/data/sched_mlp.npz.
+
+--batch trains the batched stream's planner instead: every variant is timed
+per job inside a batch of same-shape jobs (hme_autotune_batch, the cost a job
+adds to a batched call), written to sched_batch_timings.npz and
+sched_batch_mlp.npz; the method without the network is the batch rule.
 """
 import argparse
 import json
@@ -30,17 +35,21 @@ def main():
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--reuse", action="store_true", help="train on the existing timing file")
+    ap.add_argument("--batch", action="store_true", help="the batched stream's planner (per-job times in batches)")
     args = ap.parse_args()
+    timings = sched.BATCH_TIMINGS if args.batch else sched.TIMINGS
+    weights = sched.BATCH_WEIGHTS if args.batch else sched.WEIGHTS
     eng = hacs_b200.Engine(0)
-    if args.reuse and os.path.exists(sched.TIMINGS):
-        d = np.load(sched.TIMINGS)
+    if args.reuse and os.path.exists(timings):
+        d = np.load(timings)
         shapes, dens, T = d["shapes"], d["density"], d["ms"]
     else:
         t0 = time.time()
-        shapes, dens, T = sched.collect(eng, args.shapes, args.seed, args.reps)
+        collect = sched.collect_batch if args.batch else sched.collect
+        shapes, dens, T = collect(eng, args.shapes, args.seed, args.reps)
         print(f"timed {len(shapes)} shapes x {sched.N_VARIANTS} variants in {time.time() - t0:.1f} s", flush=True)
         os.makedirs(sched.DATA, exist_ok=True)
-        np.savez_compressed(sched.TIMINGS, shapes=shapes, density=dens, ms=T)
+        np.savez_compressed(timings, shapes=shapes, density=dens, ms=T)
     F = sched.raw_features(shapes[:, 0], shapes[:, 1], shapes[:, 2], shapes[:, 3], dens)
     n = len(F)
     cut = int(0.8 * n)
@@ -48,11 +57,11 @@ def main():
     t0 = time.time()
     loss = mlp.fit(F[:cut], T[:cut], epochs=args.epochs, batch=256, lr=2e-3)
     tt = time.time() - t0
-    mlp.save(sched.WEIGHTS)
+    mlp.save(weights)
     ch = mlp.choose(F[cut:])
     rep = {"train_shapes": cut, "test_shapes": n - cut, "train_loss": loss, "train_s": tt,
            "regret_mlp": sched.regret(T[cut:], ch),
-           "regret_heuristic": sched.regret(T[cut:], sched.heuristic_choice(F[cut:])),
+           "regret_heuristic": (None if args.batch else sched.regret(T[cut:], sched.heuristic_choice(F[cut:]))),
            "regret_always_wide": sched.regret(T[cut:], np.zeros(n - cut, int)),
            "variant_share_best": np.bincount(T[cut:].argmin(1), minlength=4).tolist(),
            "variant_share_mlp": np.bincount(ch, minlength=4).tolist()}

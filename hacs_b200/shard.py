@@ -65,3 +65,44 @@ def run_sharded(n_jobs: int, costs: Sequence[float], run: Callable[[list[int]], 
     for r in range(world):
         out[shards[r]] = parts[r]
     return out
+
+
+# ---- one large GEMM split by rows of C ------------------------------------------------------
+def row_blocks(m: int, world: int, align: int = 128) -> list[tuple[int, int]]:
+    """Rank r's rows [r0, r1) of an m-row product: contiguous blocks in rank
+    order whose boundaries fall on multiples of `align` (the limb GEMM's 128-row
+    tile), block sizes differing by at most one tile.  Deterministic, so every
+    rank computes the same split without communication."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    tiles = -(-m // align)
+    out, t0 = [], 0
+    for r in range(world):
+        t1 = t0 + tiles // world + (1 if r < tiles % world else 0)
+        out.append((min(m, t0 * align), min(m, t1 * align)))
+        t0 = t1
+    return out
+
+
+def gemm_row_split(gemm: Callable, p: int, A, B, rank: int, world: int, group=None, align: int = 128):
+    """C = A B mod p with C's rows split over the ranks (A's row block local,
+    B replicated, no reduction since every C row has one owner).  Rank r computes its block with gemm(p, A[r0:r1], B) on its own
+    device, then the blocks are all-gathered (torch.distributed, NCCL for CUDA
+    tensors, gloo for CPU ones) so every rank returns the whole C.  A and B are
+    torch tensors on this rank's device; gemm returns the block as a tensor."""
+    import torch
+
+    blocks = row_blocks(int(A.shape[0]), world, align)
+    r0, r1 = blocks[rank]
+    n = int(B.shape[1])
+    Cb = gemm(p, A[r0:r1], B) if r1 > r0 else torch.empty((0, n), dtype=A.dtype, device=A.device)
+    if world == 1:
+        return Cb
+    import torch.distributed as dist
+
+    mx = max(b1 - b0 for b0, b1 in blocks)
+    pad = torch.zeros((mx, n), dtype=Cb.dtype, device=Cb.device)
+    pad[: r1 - r0] = Cb
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    return torch.cat([parts[r][: b1 - b0] for r, (b0, b1) in enumerate(blocks)], dim=0)

@@ -115,8 +115,9 @@ def test_session_rejects_bad_steps():
 def test_plan_windows():
     L = _lib.lib()
     assert L.hme_r2k_plan(0, 4, 2048, 2048, 128, 0) == 2048  # resident
-    cap = L.hme_r2k_session_bytes(4, 4096, 0, 128) + 4096 * 4 * 1024  # room for ~1024 columns
+    base = L.hme_r2k_session_bytes(4, 4096, 0, 128)
+    cap = base + 8 * (L.hme_r2k_session_bytes(4, 4096, 1024, 128) - base)  # room for 8192 window columns
     cw = L.hme_r2k_plan(0, 4, 4096, 100000, 128, cap)
-    assert 0 < cw < 100000 and cw % 128 == 0
+    assert cw == 8192
     assert L.hme_r2k_plan(0, 3, 64, 64, 16, 0) == 0  # elem must be 4 or 8
     assert L.hme_r2k_plan(0, 4, 4096, 100000, 128, 1 << 20) == 0  # too little memory: decline

@@ -88,3 +88,65 @@ def test_two_gloo_ranks_gather_equals_single_run():
     assert all(pr.exitcode == 0 for pr in procs)
     want = _run_jobs(list(range(N_JOBS)))
     assert got == want
+
+
+def test_row_blocks_cover_and_align():
+    from hacs_b200.shard import row_blocks
+
+    for m in (1, 127, 128, 1000, 8192, 8200):
+        for world in (1, 2, 3, 8):
+            b = row_blocks(m, world)
+            assert b[0][0] == 0 and b[-1][1] == m
+            assert all(b[i][1] == b[i + 1][0] for i in range(world - 1))
+            assert all(r0 % 128 == 0 or r0 == m for r0, _ in b)
+            sizes = [-(-(r1 - r0) // 128) for r0, r1 in b]
+            assert max(sizes) - min(sizes) <= 1
+
+
+def _gemm_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+
+    import torch
+
+    import oracle
+    from hacs_b200.shard import gemm_row_split
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        p = 2147483629
+        A = torch.from_numpy(gen.engine_matrix(300, 70, p, 0x01).view(np.int32))
+        B = torch.from_numpy(gen.engine_matrix(70, 90, p, 0x02).view(np.int32))
+
+        def block_gemm(pp, Ab, Bb):  # each rank's own product of its row block (the oracle stands in for a GPU)
+            Cb = oracle.gemm(pp, Ab.numpy().view(np.uint32), Bb.numpy().view(np.uint32))
+            return torch.from_numpy(Cb.view(np.int32))
+
+        C = gemm_row_split(block_gemm, p, A, B, rank, world)
+        q.put((rank, C.numpy().view(np.uint32).tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_row_split_gemm_equals_single_product():
+    """A 300-row product split over two ranks (blocks of 128-row tiles: 256 + 44
+    rows), all-gathered: every rank holds the whole C, equal to one product."""
+    import oracle
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gemm_worker, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    try:
+        got = dict(q.get(timeout=120) for _ in range(2))
+    finally:
+        for pr in procs:
+            pr.join(timeout=60)
+    assert all(pr.exitcode == 0 for pr in procs)
+    p = 2147483629
+    want = oracle.gemm(p, gen.engine_matrix(300, 70, p, 0x01), gen.engine_matrix(70, 90, p, 0x02))
+    for r in range(2):
+        assert np.array_equal(np.array(got[r], dtype=np.uint32), want)
