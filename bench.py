@@ -949,6 +949,93 @@ def run_case(args):
     return 0
 
 
+def multi_gpu_extras(eng, ws, rank, local):
+    """The paths that shard across N GPUs (one process per GPU), timed on the device as the max over ranks:
+    one 8192^3 GEMM split by rows of C (A's row block and B on every rank, C all-gathered over NCCL; no
+    reduction), and the 10,000-job stream split by predicted cost (each rank one batched call on its share;
+    ranks gathered on the host).  Every rank takes the same collective steps in the same order."""
+    import ctypes as C_
+
+    import torch
+    import torch.distributed as dist
+
+    import hacs_b200
+    from hacs_b200 import shard, stream
+
+    out = {}
+    for p in (65521, 2147483629):
+        n = 8192
+        g = torch.Generator(device="cuda").manual_seed(p)
+        A = torch.randint(0, p, (n, n), dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
+        B = torch.randint(0, p, (n, n), dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
+        blocks = shard.row_blocks(n, ws)
+        r0, r1 = blocks[rank]
+        Cb = torch.empty((r1 - r0, n), dtype=torch.int32, device="cuda")
+
+        def block_gemm(pp, Ab, Bb):
+            eng.gemm_dev(pp, Ab, Bb, Cb)
+            return Cb
+
+        for _ in range(2):  # warm: workspace, modules, NCCL channels
+            shard.gemm_row_split(block_gemm, p, A, B, rank, ws)
+        torch.cuda.synchronize()
+        dist.barrier()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        eng.gemm_dev(p, A[r0:r1], B, Cb)
+        e1.record()
+        C = shard.gemm_row_split(lambda pp, Ab, Bb: Cb, p, A, B, rank, ws)  # the gather of the computed blocks
+        e2.record()
+        torch.cuda.synchronize()
+        t_gemm = max_over_ranks(e0.elapsed_time(e1), ws)
+        t_all = max_over_ranks(e0.elapsed_time(e2), ws)
+        ok = None
+        if rank == 0:
+            Cf = torch.empty_like(C)
+            eng.gemm_dev(p, A, B, Cf)
+            torch.cuda.synchronize()
+            ok = bool(torch.equal(Cf, C))
+        out[f"gemm_{n}_rowsplit_p{p}"] = {
+            "ranks": ws, "rows_per_rank": [b1 - b0 for b0, b1 in blocks], "ms_gemm_max": t_gemm,
+            "ms_with_allgather_max": t_all, "tops_gemm": 2.0 * n ** 3 / t_gemm / 1e9,
+            "tops_with_allgather": 2.0 * n ** 3 / t_all / 1e9, "bit_exact_vs_one_gpu": ok}
+        del A, B, Cb, C
+        torch.cuda.empty_cache()
+    # the job stream, sharded by predicted cost
+    from hacs_b200 import gen
+
+    s = gen.job_stream(10000)[0]
+    shards = shard.shard_jobs(shard.job_cost(s, s, s), ws)
+    st = stream.DeviceStream(10000, indices=shards[rank])
+    arr = eng._jobs(st.jobs)
+    ranks = np.zeros(max(1, st.n_jobs), np.uint32)
+
+    def call():
+        hacs_b200.check(eng._lib.hme_batch_gemm_rank_u32_dev(eng._h, st.n_jobs, arr,
+                                                             ranks.ctypes.data_as(C_.POINTER(C_.c_uint32))))
+
+    eng.gen_jobs_dev(st.specs)
+    call()  # warm
+    eng.gen_jobs_dev(st.specs)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    call()
+    t_rank = time.perf_counter() - t0
+    t_max = max_over_ranks(t_rank, ws)
+    parts = [None] * ws if rank == 0 else None
+    dist.gather_object(ranks[: st.n_jobs].tolist(), parts, dst=0)
+    rec = {"ranks": ws, "jobs_per_rank": [len(x) for x in shards], "s_max": t_max, "jobs_per_s": 10000 / t_max}
+    if rank == 0:
+        allr = np.full(10000, -1, np.int64)
+        for r in range(ws):
+            allr[shards[r]] = parts[r]
+        gold = stream.golden_jobs()
+        rec["ranks_equal_vs_reference"] = bool(gold is not None and np.array_equal(allr, gold[0]))
+    out["jobstream_config4_sharded"] = rec
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1069,7 +1156,9 @@ def main():
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_gemm_rate(p, n)
     line["clocks"] = clk.summary()
-    if not args.no_extras:
+    if not args.no_extras and ws > 1:
+        line["extras"] = multi_gpu_extras(eng, ws, rank, local)
+    elif not args.no_extras:
         plain = load_plain()
         ext = {}
         for pp in (65521, 2147483629):

@@ -124,6 +124,19 @@ class HmeR2kStep(C.Structure):
                 ("w", u32)]
 
 
+u64 = C.c_uint64
+PROTOTYPES.update({
+    "hme_axpy_u64_dev": (C.c_int, [vp, u64, u64, u32, u32, vp, sz, sz, vp, sz, sz, C.c_int]),
+    "hme_scal_u64_dev": (C.c_int, [vp, u64, u64, u32, u32, vp, sz, sz]),
+    "hme_copy_u64_dev": (C.c_int, [vp, u32, u32, vp, sz, sz, vp, sz, sz]),
+    "hme_transpose_u64_dev": (C.c_int, [vp, u32, u32, vp, sz, sz, vp, sz, sz]),
+    "hme_fill_u64_dev": (C.c_int, [vp, u32, u32, vp, sz, sz, u64]),
+    "hme_axpy_identity_u64_dev": (C.c_int, [vp, u64, u64, u32, u32, vp, sz, sz, C.c_int]),
+    "hme_gather_u64_dev": (C.c_int, [vp, u64, u64, u64, vp, u32, u32, sz, sz, u32, vp, vp, u32, u32, vp, sz, sz,
+                                     C.c_int]),
+    "hme_canonicalise_u64_dev": (C.c_int, [vp, u64, u32, u32, vp, sz, sz]),
+})
+
 PROTOTYPES.update({
     "hme_r2k_plan": (u32, [C.c_int, u32, u32, u32, u32, C.c_uint64]),
     "hme_r2k_session_bytes": (sz, [u32, u32, u32, u32]),

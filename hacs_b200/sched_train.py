@@ -36,9 +36,14 @@ def main():
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--reuse", action="store_true", help="train on the existing timing file")
     ap.add_argument("--batch", action="store_true", help="the batched stream's planner (per-job times in batches)")
+    ap.add_argument("--out-dir", default=None, help="write the timing and weight files here (default: the package)")
     args = ap.parse_args()
     timings = sched.BATCH_TIMINGS if args.batch else sched.TIMINGS
     weights = sched.BATCH_WEIGHTS if args.batch else sched.WEIGHTS
+    if args.out_dir:
+        os.makedirs(args.out_dir, exist_ok=True)
+        timings = os.path.join(args.out_dir, os.path.basename(timings))
+        weights = os.path.join(args.out_dir, os.path.basename(weights))
     eng = hacs_b200.Engine(0)
     if args.reuse and os.path.exists(timings):
         d = np.load(timings)
@@ -48,7 +53,7 @@ def main():
         collect = sched.collect_batch if args.batch else sched.collect
         shapes, dens, T = collect(eng, args.shapes, args.seed, args.reps)
         print(f"timed {len(shapes)} shapes x {sched.N_VARIANTS} variants in {time.time() - t0:.1f} s", flush=True)
-        os.makedirs(sched.DATA, exist_ok=True)
+        os.makedirs(os.path.dirname(timings), exist_ok=True)
         np.savez_compressed(timings, shapes=shapes, density=dens, ms=T)
     F = sched.raw_features(shapes[:, 0], shapes[:, 1], shapes[:, 2], shapes[:, 3], dens)
     n = len(F)

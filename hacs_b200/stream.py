@@ -23,13 +23,19 @@ GOLDEN_JOBS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__fil
 
 
 class DeviceStream:
-    def __init__(self, n_jobs: int, salt: int = 0x44, first: int = 0):
+    """Jobs [first, first + n_jobs) of the stream, or the jobs `indices` of its
+    first n_jobs (one rank's share of a sharded stream)."""
+
+    def __init__(self, n_jobs: int, salt: int = 0x44, first: int = 0, indices=None):
         import torch
 
         s, fam, p, sa, sb = gen.job_stream(first + n_jobs, salt)
-        self.s, self.fam, self.p = s[first:], fam[first:], p[first:]
-        self.seed_a, self.seed_b = sa[first:], sb[first:]
-        self.n_jobs = n_jobs
+        sel = np.arange(first, first + n_jobs) if indices is None else np.asarray(indices, dtype=np.int64)
+        self.s, self.fam, self.p = s[sel], fam[sel], p[sel]
+        self.seed_a, self.seed_b = sa[sel], sb[sel]
+        self.indices = sel
+        self.n_jobs = len(sel)
+        n_jobs = self.n_jobs
         sq = self.s * self.s
         self.offsets = np.concatenate([[0], np.cumsum(sq)]).astype(np.int64)
         tot = int(self.offsets[-1])

@@ -174,6 +174,33 @@ HME_API int hme_canonicalise_acc64_u32_dev(hme_ctx *ctx, uint32_t p, uint32_t ro
 HME_API int hme_trsm_unit_u32_dev(hme_ctx *ctx, uint32_t p, int lower, uint32_t m, uint32_t n, const uint32_t *T,
                                   size_t ldt, uint32_t *B, size_t ldb);
 
+/* The same level-1 operations over u64 residues (2 <= p < 2^64; entries and
+ * scalars canonical below p), the uint64_t instantiations of
+ * engine::cuda::axpy / scal / copy / transpose / fill / axpy_identity /
+ * gather / canonicalise (src/Cuda/CudaKernels.h:194-234, bodies
+ * cuda_kernels.cu:986-1088): products formed in 128 bits and reduced once;
+ * the lazy form of hme_canonicalise_u64_dev needs 2p <= 2^64.  The u64 GEMM
+ * is hme_gemm_u64_dev. */
+HME_API int hme_axpy_u64_dev(hme_ctx *ctx, uint64_t p, uint64_t alpha, uint32_t rows, uint32_t cols,
+                             const uint64_t *x, size_t x_rs, size_t x_cs, uint64_t *y, size_t y_rs, size_t y_cs,
+                             int subtract);
+HME_API int hme_scal_u64_dev(hme_ctx *ctx, uint64_t p, uint64_t alpha, uint32_t rows, uint32_t cols, uint64_t *x,
+                             size_t rs, size_t cs);
+HME_API int hme_copy_u64_dev(hme_ctx *ctx, uint32_t rows, uint32_t cols, const uint64_t *src, size_t s_rs,
+                             size_t s_cs, uint64_t *dst, size_t d_rs, size_t d_cs);
+HME_API int hme_transpose_u64_dev(hme_ctx *ctx, uint32_t rows_dst, uint32_t cols_dst, const uint64_t *src,
+                                  size_t s_rs, size_t s_cs, uint64_t *dst, size_t d_rs, size_t d_cs);
+HME_API int hme_fill_u64_dev(hme_ctx *ctx, uint32_t rows, uint32_t cols, uint64_t *x, size_t rs, size_t cs,
+                             uint64_t value);
+HME_API int hme_axpy_identity_u64_dev(hme_ctx *ctx, uint64_t p, uint64_t alpha, uint32_t rows, uint32_t cols,
+                                      uint64_t *y, size_t rs, size_t cs, int subtract);
+HME_API int hme_gather_u64_dev(hme_ctx *ctx, uint64_t p, uint64_t alpha, uint64_t beta, const uint64_t *a,
+                               uint32_t a_rows, uint32_t a_cols, size_t a_rs, size_t a_cs, uint32_t row_off,
+                               const uint32_t *cols, const uint32_t *rows, uint32_t c_rows, uint32_t c_cols,
+                               uint64_t *c, size_t c_rs, size_t c_cs, int accumulate);
+HME_API int hme_canonicalise_u64_dev(hme_ctx *ctx, uint64_t p, uint32_t rows, uint32_t cols, uint64_t *v, size_t rs,
+                                     size_t cs);
+
 /* ---- elimination over F_p (p prime, p < 2^32) --------------------------------
  * Device-resident blocked LU: a cooperative panel kernel (pivot = leftmost
  * column with a non-zero in the Schur complement, topmost such row), row

@@ -107,3 +107,47 @@ def gemm_nt(p: int, A, B, C, op: int) -> np.ndarray:
     """C op= A B^T with B given n x k (CudaKernels.h:126-129)."""
     return gemm(p, np.ascontiguousarray(A, np.uint32), np.ascontiguousarray(np.asarray(B, np.uint32).T),
                 np.asarray(C, np.uint32), op)
+
+
+# ---- the u64 element type (any modulus below 2^64): exact Python integers ----------------------
+def _obj(a) -> np.ndarray:
+    return np.asarray(a, dtype=np.uint64).astype(object)
+
+
+def axpy64(p: int, alpha: int, x, y, subtract: bool) -> np.ndarray:
+    """y +/- alpha x mod p over u64 residues (kernels::axpy<uint64_t>, the uint64_t twin of the above)."""
+    v = (_obj(y) - alpha * _obj(x)) % p if subtract else (_obj(y) + alpha * _obj(x)) % p
+    return v.astype(np.uint64)
+
+
+def scal64(p: int, alpha: int, x) -> np.ndarray:
+    return ((alpha * _obj(x)) % p).astype(np.uint64)
+
+
+def axpy_identity64(p: int, alpha: int, y, subtract: bool) -> np.ndarray:
+    out = _obj(y)
+    n = min(out.shape)
+    for i in range(n):
+        out[i, i] = (out[i, i] - alpha) % p if subtract else (out[i, i] + alpha) % p
+    return out.astype(np.uint64)
+
+
+def gather64(p: int, alpha: int, beta: int, a, row_off: int, cols, c, accumulate: bool, rows=None) -> np.ndarray:
+    c = _obj(c)
+    nr, nc = c.shape
+    r = list(range(nr)) if rows is None else [int(x) for x in rows]
+    col = list(range(nc)) if cols is None else [int(x) for x in cols]
+    A = None if a is None else _obj(a)
+    out = np.empty((nr, nc), dtype=object)
+    for i in range(nr):
+        for t in range(nc):
+            v = alpha if row_off + r[i] == col[t] else 0
+            if A is not None:
+                v = (v + beta * A[r[i], col[t]]) % p
+            out[i, t] = (c[i, t] + v) % p if accumulate else v
+    return out.astype(np.uint64)
+
+
+def canonicalise64(p: int, v) -> np.ndarray:
+    v = _obj(v)
+    return np.where(v >= p, v - p, v).astype(np.uint64)
