@@ -35,6 +35,7 @@ PROTOTYPES = {
     "hme_ctx_set_stream": (C.c_int, [vp, vp]),
     "hme_ctx_own_stream": (vp, [vp]),
     "hme_ctx_sync": (C.c_int, [vp]),
+    "hme_ctx_set_workspace_retain": (C.c_int, [vp, C.c_int]),
     "hme_ctx_launches": (C.c_uint64, [vp]),
     "hme_ctx_set_timing": (C.c_int, [vp, C.c_int]),
     "hme_ctx_kernel_time": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),

@@ -19,7 +19,8 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 void* Workspace::get(int slot, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (size[slot] < bytes) {
-        if (ptr[slot]) HME_CUDA(cudaFree(ptr[slot]));
+        if (ptr[slot] && retain) retired.push_back(ptr[slot]);
+        else if (ptr[slot]) HME_CUDA(cudaFree(ptr[slot]));
         ptr[slot] = nullptr;
         size[slot] = 0;
         // grow with headroom so a sequence of slightly larger calls does not reallocate every time
@@ -36,6 +37,8 @@ void Workspace::release() {
         ptr[s] = nullptr;
         size[s] = 0;
     }
+    for (void* q : retired) cudaFree(q);
+    retired.clear();
 }
 
 cudaEvent_t KernelTimer::take() {
@@ -156,6 +159,13 @@ int hme_ctx_set_stream(hme_ctx* ctx, void* stream) {
 }
 
 void* hme_ctx_own_stream(const hme_ctx* ctx) { return ctx ? static_cast<void*>(ctx->own_stream) : nullptr; }
+
+int hme_ctx_set_workspace_retain(hme_ctx* ctx, int on) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        ctx->ws.retain = on != 0;
+    });
+}
 
 int hme_ctx_sync(hme_ctx* ctx) {
     return guard([&] {

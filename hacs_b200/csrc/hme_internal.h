@@ -78,6 +78,10 @@ struct Workspace {
     static constexpr int kSlots = 32;
     void* ptr[kSlots] = {};
     size_t size[kSlots] = {};
+    // keep a slot's previous allocation alive when it grows (freed by release()), so that CUDA
+    // graphs captured with the old pointers stay valid (hme_ctx_set_workspace_retain)
+    bool retain = false;
+    std::vector<void*> retired;
     void* get(int slot, size_t bytes);
     void release();
 };

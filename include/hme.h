@@ -60,6 +60,12 @@ HME_API int hme_ctx_destroy(hme_ctx *ctx);
  * created and uses until this is called. */
 HME_API int hme_ctx_set_stream(hme_ctx *ctx, void *cuda_stream);
 HME_API void *hme_ctx_own_stream(const hme_ctx *ctx);
+/* Keep (on != 0) every device workspace allocation of the context alive until
+ * hme_ctx_destroy, also after a larger call replaced it: kernels captured in a
+ * CUDA graph keep the pointers of the workspace they were captured with, so a
+ * caller that replays graphs of this context's asynchronous entry points turns
+ * this on (the tape's device layer does).  Off by default. */
+HME_API int hme_ctx_set_workspace_retain(hme_ctx *ctx, int on);
 /* Wait for the context's stream; reports a device-side timeout as HME_ETIMEOUT. */
 HME_API int hme_ctx_sync(hme_ctx *ctx);
 /* Kernel launches issued by this library on the context so far (a counter). */

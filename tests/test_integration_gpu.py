@@ -26,3 +26,22 @@ def test_reference_callers_through_hme_seams():
     out = r.stdout + r.stderr
     assert r.returncode == 0, out[-6000:]
     assert "0 failed" in out
+
+
+TAPE = os.path.join(ROOT, "oracle", "_ref", "seams", "tape_check")
+
+
+def test_reference_tape_on_the_hme_device_layer():
+    """The reference's tape -- Recorder, compile, Executor and DeviceBackend compiled
+    unchanged from its sources -- linked against integration/HmeEngineCuda.cpp (the
+    reference's engine::cuda layer over libhme) in place of the reference's
+    libEngineCuda: u32 and u64 programs (GEMM, Schur update, AXPY, SCAL, TRANSPOSE,
+    row-list GATHER; row- and column-major operands) on the device, the second run
+    from a captured CUDA graph, equal entry for entry to the CPU run; one program
+    under the executor's own device verify twin."""
+    if not os.path.exists(TAPE):
+        pytest.skip("the tape check is built only where the reference sources are present")
+    r = subprocess.run([TAPE], capture_output=True, text=True, timeout=900)
+    out = r.stdout + r.stderr
+    assert r.returncode == 0, out[-6000:]
+    assert "0 failed" in out
