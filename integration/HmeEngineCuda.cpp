@@ -14,8 +14,8 @@
 //     first laid out row-major in scratch by hme's copy / transpose), gemv, axpy, scal, copy,
 //     transpose, fill, axpy_identity, gather, canonicalise (both forms), trsm_unit.  u64: the
 //     residue-number-system GEMM (hme_gemm_u64_dev) and the u64 level-1 operations; gemv is a
-//     one-column GEMM.  GemmBatch: one grouped launch (hme_batch_gemm_u32_dev) for a Set batch
-//     of row-contiguous u32 instances outside a capture, else one GEMM per instance.
+//     one-column GEMM.  GemmBatch: one GEMM per instance (capturable; hme's grouped launch for
+//     uneven batches is the batched stream's API, which synchronises the host).
 //   * imma_rref (the reference's device RREF for p <= 127): hme's device elimination, for every
 //     field p < 2^32; pivot_rows (the row rank profile) is the column rank profile of A^T.
 //
@@ -91,33 +91,66 @@ const Avail& avail() {
 }
 
 std::atomic<uint64_t> g_launches{0}, g_gemms{0}, g_batched{0};
+cudaStream_t st(Stream s) { return static_cast<cudaStream_t>(s.h); }
 thread_local int t_capturing = 0;
 thread_local const char* t_tag = "";
 std::atomic<bool> g_ctx_created{false};
 
-// One hme context per (host thread, stream), on the engine's device: work on different streams
-// runs concurrently, so each stream needs its own workspace; within a stream the calls are
-// ordered.  The contexts keep every workspace allocation alive (hme_ctx_set_workspace_retain), so
-// a graph captured with a workspace pointer stays valid after a later, larger call grew it.
+// One hme context per host thread, on the engine's device, its stream set to the caller's for each
+// call.  The calls of one thread share the context's workspace, so they are chained across streams:
+// before a call on stream s, s waits for the thread's previous call (an event recorded after it on
+// whichever stream it ran), and the call records that event again.  Events and waits are captured
+// into a graph like any launch, and the chain restarts at every capture's begin and end (a wait
+// never crosses a capture boundary).  Every workspace allocation stays alive
+// (hme_ctx_set_workspace_retain), so the workspace a graph was captured with stays valid after a
+// later, larger call grew it; the direct first run of a program grows the workspace to what its
+// captured replays need, so no allocation happens inside a capture.
 struct ThreadHme {
-    std::unordered_map<void*, hme_ctx*> by_stream;
+    hme_ctx* h = nullptr;
+    cudaEvent_t done = nullptr;  // recorded after the thread's last call
+    void* last = nullptr;        // the stream it was recorded on
+    bool valid = false;
     ~ThreadHme() {
-        for (auto& kv : by_stream) hme_ctx_destroy(kv.second);
+        if (done) cudaEventDestroy(done);
+        if (h) hme_ctx_destroy(h);
     }
 };
-hme_ctx* hme_on(Stream s) {
+ThreadHme& thread_hme() {
     thread_local ThreadHme t;
-    hme_ctx*& h = t.by_stream[s.h];
-    if (!h) {
-        chk(hme_ctx_create(env_device(), &h), "hme_ctx_create");
-        chk(hme_ctx_set_workspace_retain(h, 1), "hme_ctx_set_workspace_retain");
-        chk(hme_ctx_set_stream(h, s.h), "hme_ctx_set_stream");
-    }
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    return h;
+    return t;
 }
+void chain_restart() { thread_hme().valid = false; }
 
-cudaStream_t st(Stream s) { return static_cast<cudaStream_t>(s.h); }
+// A call of the thread's hme context on stream s: ordered after the thread's previous call.
+class HmeCall {
+  public:
+    explicit HmeCall(Stream s) : t_(thread_hme()), s_(s) {
+        if (!t_.h) {
+            chk(hme_ctx_create(env_device(), &t_.h), "hme_ctx_create");
+            chk(hme_ctx_set_workspace_retain(t_.h, 1), "hme_ctx_set_workspace_retain");
+            cu(cudaEventCreateWithFlags(&t_.done, cudaEventDisableTiming), "cudaEventCreate");
+        }
+        if (t_.valid && t_.last != s.h) cu(cudaStreamWaitEvent(st(s), t_.done, 0), "cudaStreamWaitEvent");
+        chk(hme_ctx_set_stream(t_.h, s.h), "hme_ctx_set_stream");
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+    }
+    ~HmeCall() {
+        if (cudaEventRecord(t_.done, st(s_)) == cudaSuccess) {
+            t_.last = s_.h;
+            t_.valid = true;
+        } else {
+            cudaGetLastError();
+            t_.valid = false;
+        }
+        // between calls the context holds its own stream, never a caller's (which may be destroyed)
+        hme_ctx_set_stream(t_.h, hme_ctx_own_stream(t_.h));
+    }
+    hme_ctx* ctx() const { return t_.h; }
+
+  private:
+    ThreadHme& t_;
+    Stream s_;
+};
 
 }  // namespace
 
@@ -408,6 +441,13 @@ struct GraphCapture::Impl {
 GraphCapture::GraphCapture() : impl_(new Impl()) {}
 GraphCapture::~GraphCapture() {
     if (impl_) {
+        if (impl_->capturing) {  // abandoned mid-capture (an exception): end it, discard the graph
+            cudaGraph_t g = nullptr;
+            if (cudaStreamEndCapture(impl_->stream, &g) == cudaSuccess && g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            --t_capturing;
+            chain_restart();
+        }
         if (impl_->exec) cudaGraphExecDestroy(impl_->exec);
         if (impl_->graph) cudaGraphDestroy(impl_->graph);
         delete impl_;
@@ -416,6 +456,7 @@ GraphCapture::~GraphCapture() {
 void GraphCapture::begin(Stream s) {
     if (impl_->capturing) throw CudaError("GraphCapture::begin: already capturing");
     impl_->stream = st(s);
+    chain_restart();
     cu(cudaStreamBeginCapture(impl_->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     impl_->capturing = true;
     ++t_capturing;
@@ -424,6 +465,7 @@ void GraphCapture::end() {
     if (!impl_->capturing) throw CudaError("GraphCapture::end: not capturing");
     impl_->capturing = false;
     --t_capturing;
+    chain_restart();
     cudaGraph_t g = nullptr;
     cu(cudaStreamEndCapture(impl_->stream, &g), "cudaStreamEndCapture");
     if (impl_->exec) cudaGraphExecDestroy(impl_->exec);
@@ -519,7 +561,8 @@ void gemm_views(const ModCtx<Elt>& ctx, DeviceView<const Elt> A, DeviceView<cons
     if (C.empty()) return;
     if (windows_overlap(A, DeviceView<const Elt>(C)) || windows_overlap(B, DeviceView<const Elt>(C)))
         throw std::logic_error("gemm: C overlaps an operand");
-    hme_ctx* h = hme_on(s);
+    HmeCall hc(s);
+    hme_ctx* h = hc.ctx();
     g_gemms.fetch_add(1, std::memory_order_relaxed);
     const uint32_t m = C.rows, n = C.cols, k = A.cols;
     // u32 with B stored column-contiguous: hme's C op= A B^T on B as given
@@ -579,7 +622,8 @@ void gemv(const ModCtx<Elt>& ctx, DeviceView<const Elt> A, DeviceView<const Elt>
     if (x.cols != 1 || y.cols != 1 || A.cols != x.rows || A.rows != y.rows) throw std::logic_error("gemv: shape mismatch");
     if (y.rows == 0) return;
     if constexpr (sizeof(Elt) == 4) {
-        chk(hme_gemv_u32_dev(hme_on(s), ctx.p, A.rows, A.cols, A.base, A.rs, A.cs, x.base, x.rs, y.base, y.rs,
+        HmeCall hc(s);
+        chk(hme_gemv_u32_dev(hc.ctx(), ctx.p, A.rows, A.cols, A.base, A.rs, A.cs, x.base, x.rs, y.base, y.rs,
                              op_of(op)), "hme_gemv_u32_dev");
     } else {
         gemm_views<Elt>(ctx, A, x, y, op, s);  // a one-column GEMM
@@ -590,53 +634,53 @@ template <class Elt>
 void axpy(const ModCtx<Elt>& ctx, Elt alpha, DeviceView<const Elt> x, DeviceView<Elt> y, bool subtract, Stream s) {
     if (x.rows != y.rows || x.cols != y.cols) throw std::logic_error("axpy: shape mismatch");
     if constexpr (sizeof(Elt) == 4)
-        chk(hme_axpy_u32_dev(hme_on(s), ctx.p, alpha, y.rows, y.cols, x.base, x.rs, x.cs, y.base, y.rs, y.cs,
+        chk(hme_axpy_u32_dev(HmeCall(s).ctx(), ctx.p, alpha, y.rows, y.cols, x.base, x.rs, x.cs, y.base, y.rs, y.cs,
                              subtract), "hme_axpy_u32_dev");
     else
-        chk(hme_axpy_u64_dev(hme_on(s), ctx.p, alpha, y.rows, y.cols, x.base, x.rs, x.cs, y.base, y.rs, y.cs,
+        chk(hme_axpy_u64_dev(HmeCall(s).ctx(), ctx.p, alpha, y.rows, y.cols, x.base, x.rs, x.cs, y.base, y.rs, y.cs,
                              subtract), "hme_axpy_u64_dev");
 }
 
 template <class Elt>
 void scal(const ModCtx<Elt>& ctx, Elt alpha, DeviceView<Elt> x, Stream s) {
     if constexpr (sizeof(Elt) == 4)
-        chk(hme_scal_u32_dev(hme_on(s), ctx.p, alpha, x.rows, x.cols, x.base, x.rs, x.cs), "hme_scal_u32_dev");
+        chk(hme_scal_u32_dev(HmeCall(s).ctx(), ctx.p, alpha, x.rows, x.cols, x.base, x.rs, x.cs), "hme_scal_u32_dev");
     else
-        chk(hme_scal_u64_dev(hme_on(s), ctx.p, alpha, x.rows, x.cols, x.base, x.rs, x.cs), "hme_scal_u64_dev");
+        chk(hme_scal_u64_dev(HmeCall(s).ctx(), ctx.p, alpha, x.rows, x.cols, x.base, x.rs, x.cs), "hme_scal_u64_dev");
 }
 
 template <class Elt>
 void copy(DeviceView<const Elt> src, DeviceView<Elt> dst, Stream s) {
     if (src.rows != dst.rows || src.cols != dst.cols) throw std::logic_error("copy: shape mismatch");
-    copy_any<Elt>(hme_on(s), src, dst);
+    copy_any<Elt>(HmeCall(s).ctx(), src, dst);
 }
 
 template <class Elt>
 void transpose(DeviceView<const Elt> src, DeviceView<Elt> dst, Stream s) {
     if (src.rows != dst.cols || src.cols != dst.rows) throw std::logic_error("transpose: shape mismatch");
     if constexpr (sizeof(Elt) == 4)
-        chk(hme_transpose_u32_dev(hme_on(s), dst.rows, dst.cols, src.base, src.rs, src.cs, dst.base, dst.rs, dst.cs),
+        chk(hme_transpose_u32_dev(HmeCall(s).ctx(), dst.rows, dst.cols, src.base, src.rs, src.cs, dst.base, dst.rs, dst.cs),
             "hme_transpose_u32_dev");
     else
-        chk(hme_transpose_u64_dev(hme_on(s), dst.rows, dst.cols, src.base, src.rs, src.cs, dst.base, dst.rs, dst.cs),
+        chk(hme_transpose_u64_dev(HmeCall(s).ctx(), dst.rows, dst.cols, src.base, src.rs, src.cs, dst.base, dst.rs, dst.cs),
             "hme_transpose_u64_dev");
 }
 
 template <class Elt>
 void fill(DeviceView<Elt> x, Elt value, Stream s) {
     if constexpr (sizeof(Elt) == 4)
-        chk(hme_fill_u32_dev(hme_on(s), x.rows, x.cols, x.base, x.rs, x.cs, value), "hme_fill_u32_dev");
+        chk(hme_fill_u32_dev(HmeCall(s).ctx(), x.rows, x.cols, x.base, x.rs, x.cs, value), "hme_fill_u32_dev");
     else
-        chk(hme_fill_u64_dev(hme_on(s), x.rows, x.cols, x.base, x.rs, x.cs, value), "hme_fill_u64_dev");
+        chk(hme_fill_u64_dev(HmeCall(s).ctx(), x.rows, x.cols, x.base, x.rs, x.cs, value), "hme_fill_u64_dev");
 }
 
 template <class Elt>
 void axpy_identity(const ModCtx<Elt>& ctx, Elt alpha, DeviceView<Elt> y, bool subtract, Stream s) {
     if constexpr (sizeof(Elt) == 4)
-        chk(hme_axpy_identity_u32_dev(hme_on(s), ctx.p, alpha, y.rows, y.cols, y.base, y.rs, y.cs, subtract),
+        chk(hme_axpy_identity_u32_dev(HmeCall(s).ctx(), ctx.p, alpha, y.rows, y.cols, y.base, y.rs, y.cs, subtract),
             "hme_axpy_identity_u32_dev");
     else
-        chk(hme_axpy_identity_u64_dev(hme_on(s), ctx.p, alpha, y.rows, y.cols, y.base, y.rs, y.cs, subtract),
+        chk(hme_axpy_identity_u64_dev(HmeCall(s).ctx(), ctx.p, alpha, y.rows, y.cols, y.base, y.rs, y.cs, subtract),
             "hme_axpy_identity_u64_dev");
 }
 
@@ -645,11 +689,11 @@ void gather(const ModCtx<Elt>& ctx, Elt alpha, Elt beta, DeviceView<const Elt> a
             const uint32_t* cols, DeviceView<Elt> c, bool accumulate, Stream s, const uint32_t* rows) {
     const bool have_a = !a.empty();
     if constexpr (sizeof(Elt) == 4)
-        chk(hme_gather_u32_dev(hme_on(s), ctx.p, alpha, beta, have_a ? a.base : nullptr, a.rows, a.cols, a.rs, a.cs,
+        chk(hme_gather_u32_dev(HmeCall(s).ctx(), ctx.p, alpha, beta, have_a ? a.base : nullptr, a.rows, a.cols, a.rs, a.cs,
                                row_off, cols, rows, c.rows, c.cols, c.base, c.rs, c.cs, accumulate),
             "hme_gather_u32_dev");
     else
-        chk(hme_gather_u64_dev(hme_on(s), ctx.p, alpha, beta, have_a ? a.base : nullptr, a.rows, a.cols, a.rs, a.cs,
+        chk(hme_gather_u64_dev(HmeCall(s).ctx(), ctx.p, alpha, beta, have_a ? a.base : nullptr, a.rows, a.cols, a.rs, a.cs,
                                row_off, cols, rows, c.rows, c.cols, c.base, c.rs, c.cs, accumulate),
             "hme_gather_u64_dev");
 }
@@ -657,13 +701,13 @@ void gather(const ModCtx<Elt>& ctx, Elt alpha, Elt beta, DeviceView<const Elt> a
 template <class Elt>
 void canonicalise(const ModCtx<Elt>& ctx, DeviceView<Elt> v, Stream s) {
     if constexpr (sizeof(Elt) == 4)
-        chk(hme_canonicalise_u32_dev(hme_on(s), ctx.p, v.rows, v.cols, v.base, v.rs, v.cs), "hme_canonicalise_u32_dev");
+        chk(hme_canonicalise_u32_dev(HmeCall(s).ctx(), ctx.p, v.rows, v.cols, v.base, v.rs, v.cs), "hme_canonicalise_u32_dev");
     else
-        chk(hme_canonicalise_u64_dev(hme_on(s), ctx.p, v.rows, v.cols, v.base, v.rs, v.cs), "hme_canonicalise_u64_dev");
+        chk(hme_canonicalise_u64_dev(HmeCall(s).ctx(), ctx.p, v.rows, v.cols, v.base, v.rs, v.cs), "hme_canonicalise_u64_dev");
 }
 
 void canonicalise(const ModCtx<uint32_t>& ctx, DeviceView<const uint64_t> acc, DeviceView<uint32_t> dst, Stream s) {
-    chk(hme_canonicalise_acc64_u32_dev(hme_on(s), ctx.p, dst.rows, dst.cols, acc.base, acc.rs, acc.cs, dst.base,
+    chk(hme_canonicalise_acc64_u32_dev(HmeCall(s).ctx(), ctx.p, dst.rows, dst.cols, acc.base, acc.rs, acc.cs, dst.base,
                                        dst.rs, dst.cs), "hme_canonicalise_acc64_u32_dev");
 }
 
@@ -675,7 +719,8 @@ void trsm_unit(const ModCtx<Elt>& ctx, DeviceView<const Elt> T, DeviceView<Elt> 
         const bool lower = T.structure == Structure::LowerUnitri;
         if (!lower && T.structure != Structure::UpperUnitri)
             throw std::logic_error("trsm_unit: T must be LowerUnitri or UpperUnitri");
-        hme_ctx* h = hme_on(s);
+        HmeCall hc(s);
+        hme_ctx* h = hc.ctx();
         size_t ldt;
         const Elt* t = row_major(h, T, 0, ldt);
         if (B.cs == 1) {
@@ -736,16 +781,9 @@ template <class Elt>
 void GemmBatch<Elt>::run(const ModCtx<Elt>& ctx, GemmOp op, Stream s, int, int, void*, size_t) const {
     if (entries_.empty() || m_ == 0 || n_ == 0) return;
     g_batched.fetch_add(entries_.size(), std::memory_order_relaxed);
-    if constexpr (sizeof(Elt) == 4) {
-        if (op == GemmOp::Set && a_cs_ == 1 && b_cs_ == 1 && c_cs_ == 1 && k_ > 0 && !capturing_now()) {
-            std::vector<hme_job> jobs(entries_.size());
-            for (size_t t = 0; t < entries_.size(); ++t)
-                jobs[t] = hme_job{ctx.p, m_, n_, k_, entries_[t].A, a_rs_, entries_[t].B, b_rs_, entries_[t].C, c_rs_};
-            chk(hme_batch_gemm_u32_dev(hme_on(s), static_cast<uint32_t>(jobs.size()), jobs.data()),
-                "hme_batch_gemm_u32_dev");
-            return;
-        }
-    }
+    // One GEMM per instance, in both of DeviceBackend's modes (direct launches and graph capture), so
+    // the captured run uses exactly the workspace the direct run grew.  (hme's grouped launch for
+    // uneven batches, hme_batch_gemm_u32_dev, synchronises the host and is not capturable.)
     for (const GemmBatchEntry<Elt>& e : entries_)
         gemm_views<Elt>(ctx, DeviceView<const Elt>(e.A, a_rs_, a_cs_, m_, k_),
                         DeviceView<const Elt>(e.B, b_rs_, b_cs_, k_, n_), DeviceView<Elt>(e.C, c_rs_, c_cs_, m_, n_),
@@ -774,7 +812,8 @@ ImmaRrefResult imma_rref(const ModCtx<uint32_t>& ctx, uint32_t m, uint32_t n, co
         for (uint32_t i = 0; i < nr; ++i)
             for (uint32_t j = 0; j < n; ++j) A[(static_cast<size_t>(r0) + i) * n + j] = v.at(i, j);
     }
-    hme_ctx* h = hme_on(Stream{nullptr});
+    HmeCall hc(Stream{nullptr});
+    hme_ctx* h = hc.ctx();
     // the row rank profile: the column rank profile of A^T
     std::vector<uint32_t> At(static_cast<size_t>(n) * m);
     for (uint32_t i = 0; i < m; ++i)

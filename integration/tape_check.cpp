@@ -9,6 +9,7 @@
 // Built by integration/Makefile; run by tests/test_integration_gpu.py.
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <random>
 #include <string>
 #include <vector>
@@ -88,7 +89,7 @@ void run_case(Case<Elt>& c, const ModCtx<Elt>& ctx, Executor<Elt>& ex, DevicePol
     rec.schur_update(rec.whole(e), rec.whole(f), rec.whole(bd));
     rec.axpy(alpha, rec.whole(bc), rec.whole(bd));
     rec.scal(beta, rec.whole(bd));
-    rec.transpose(rec.whole(bc), rec.whole(bt));
+    rec.transpose(rec.view(bc, 0, c.C.rows, 0, c.C.cols, /*transposed=*/true), rec.whole(bt));
     std::vector<uint32_t> rows, cols;
     for (uint32_t i = 0; i < c.G.rows; ++i) rows.push_back((7 * i + 3) % c.C.rows);
     for (uint32_t t = 0; t < c.G.cols; ++t) cols.push_back((5 * t + 1) % c.C.cols);
@@ -102,23 +103,31 @@ void run_case(Case<Elt>& c, const ModCtx<Elt>& ctx, Executor<Elt>& ex, DevicePol
     for (int r = 0; r < runs; ++r) ex.run(prog, bind);
 }
 
+// graphs: 0 = direct launches only (ENGINE_CUDA_GRAPH=0, one run); 1 = the default (the second run
+// of a program captured and replayed; three runs)
 template <class Elt>
 void check_program(const char* name, Elt p, uint32_t m, uint32_t k, uint32_t n, uint32_t k2, Layout lay,
-                   uint64_t seed, bool verify = false) {
+                   uint64_t seed, int graphs, bool verify = false) {
+    setenv("ENGINE_CUDA_GRAPH", graphs ? "1" : "0", 1);
     const ModCtx<Elt> ctx(p);
     ThreadPool pool(4);
     Executor<Elt> dev_ex(&pool), host_ex(&pool);
     dev_ex.set_verify_device(verify);
     Case<Elt> d = make_case<Elt>(p, m, k, n, k2, lay, seed), h = make_case<Elt>(p, m, k, n, k2, lay, seed);
-    const uint64_t gpu0 = dev_ex.device_stats().gpu_nodes;
-    run_case<Elt>(d, ctx, dev_ex, DevicePolicy::Gpu, 2);
+    const std::string tag = std::string(name) + (graphs ? " [graph replay]" : " [direct]");
+    try {
+        run_case<Elt>(d, ctx, dev_ex, DevicePolicy::Gpu, graphs ? 3 : 1);
+    } catch (const std::exception& e) {
+        check(false, tag + ": " + e.what());
+        return;
+    }
     const auto& ds = dev_ex.device_stats();
     run_case<Elt>(h, ctx, host_ex, DevicePolicy::Cpu, 1);
-    check(ds.gpu_nodes > gpu0 && ds.graph_launches > 0,
-          std::string(name) + ": GPU nodes ran (" + std::to_string(ds.gpu_nodes - gpu0) + "), the second run from a "
-              "captured graph (" + std::to_string(ds.graph_launches) + " graph launches)");
+    check(ds.gpu_nodes > 0 && (graphs == 0 || ds.graph_launches > 0),
+          tag + ": GPU nodes ran (" + std::to_string(ds.gpu_nodes) + "), graph launches " +
+              std::to_string(ds.graph_launches));
     check(same(d.C, h.C) && same(d.D, h.D) && same(d.T, h.T) && same(d.G, h.G),
-          std::string(name) + ": GEMM, Schur update, AXPY, SCAL, TRANSPOSE and GATHER outputs equal the CPU run's");
+          tag + ": GEMM, Schur update, AXPY, SCAL, TRANSPOSE and GATHER outputs equal the CPU run's");
 }
 
 }  // namespace
@@ -129,16 +138,18 @@ int main() {
         return 1;
     }
     try {
-        check_program<uint32_t>("u32 p=2^31-19 row-major 300x200x250", 2147483629u, 300, 200, 250, 64,
-                                Layout::RowMajor, 1);
-        check_program<uint32_t>("u32 p=65521 column-major operands 257x130x300", 65521u, 257, 130, 300, 33,
-                                Layout::ColMajor, 2);
-        check_program<uint64_t>("u64 p=2^61-1 row-major 160x90x120", (uint64_t(1) << 61) - 1, 160, 90, 120, 40,
-                                Layout::RowMajor, 3);
-        check_program<uint64_t>("u64 p=2^64-59 column-major operands 96x70x64",
-                                static_cast<uint64_t>(-59), 96, 70, 64, 17, Layout::ColMajor, 4);
+        for (int graphs : {0, 1}) {
+            check_program<uint32_t>("u32 p=2^31-19 row-major 300x200x250", 2147483629u, 300, 200, 250, 64,
+                                    Layout::RowMajor, 1, graphs);
+            check_program<uint32_t>("u32 p=65521 column-major operands 257x130x300", 65521u, 257, 130, 300, 33,
+                                    Layout::ColMajor, 2, graphs);
+            check_program<uint64_t>("u64 p=2^61-1 row-major 160x90x120", (uint64_t(1) << 61) - 1, 160, 90, 120, 40,
+                                    Layout::RowMajor, 3, graphs);
+            check_program<uint64_t>("u64 p=2^64-59 column-major operands 96x70x64", static_cast<uint64_t>(-59), 96,
+                                    70, 64, 17, Layout::ColMajor, 4, graphs);
+        }
         check_program<uint32_t>("u32 p=4294967291 with the executor's device verify twin", 4294967291u, 200, 180,
-                                150, 48, Layout::RowMajor, 5, true);
+                                150, 48, Layout::RowMajor, 5, 0, true);
         const cuda::LaunchStats ls = cuda::launch_stats();
         check(ls.gemm_launches > 0, "engine::cuda GEMMs served by libhme: " + std::to_string(ls.gemm_launches));
     } catch (const std::exception& e) {
