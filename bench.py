@@ -807,8 +807,10 @@ def run_case(args):
 
         n, r, p = int(parts[1]), int(parts[2]), int(parts[3])
         eng = hacs_b200.Engine(0)
-        if len(parts) > 4:  # rref:<n>:<rank>:<p>:<panel>:<rows per CTA> (tuning: no value changes)
+        if len(parts) > 4:  # rref:<n>:<rank>:<p>:<panel>:<rows per CTA>[:<lookahead 0|1>] (tuning only)
             eng.set_elim_options(panel=int(parts[4]), rows_per_cta=int(parts[5]) if len(parts) > 5 else 0)
+        if len(parts) > 6:
+            eng.set_elim_lookahead(parts[6] != "0")
         L, R = gen.ranked_factors(n, n, r, p)
         A = eng.gemm(p, L, R)
         t0 = time.perf_counter()

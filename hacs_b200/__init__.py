@@ -308,6 +308,10 @@ class Engine:
     def set_elim_options(self, panel: int = 0, rows_per_cta: int = 0, panel_ctas: int = 0, back_block: int = 0):
         check(self._lib.hme_ctx_set_elim_options(self._h, panel, rows_per_cta, panel_ctas, back_block))
 
+    def set_elim_lookahead(self, on: bool) -> None:
+        """Factor the next LU panel on a second stream during the current trailing update (tuning only)."""
+        check(self._lib.hme_ctx_set_elim_lookahead(self._h, 1 if on else 0))
+
     def set_panel_kernel(self, mode: int) -> None:
         """LU panel kernel: 0 automatic, 1 cooperative grid kernel, 2 thread-block cluster kernel,
         3 cluster kernel with 1024 threads per CTA."""

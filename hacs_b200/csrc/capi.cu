@@ -144,6 +144,12 @@ int hme_ctx_destroy(hme_ctx* ctx) {
         for (cudaEvent_t e : ctx->pipe_ev) cudaEventDestroy(e);
         if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
         if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
+        if (ctx->aux_stream) {
+            cudaStreamSynchronize(ctx->aux_stream);
+            cudaStreamDestroy(ctx->aux_stream);
+        }
+        for (cudaEvent_t e : ctx->elim_ev) cudaEventDestroy(e);
+        if (ctx->elim_pinned) cudaFreeHost(ctx->elim_pinned);
         if (ctx->d_err) cudaFree(ctx->d_err);
         if (ctx->h_err) cudaFreeHost(ctx->h_err);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

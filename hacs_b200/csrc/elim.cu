@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstring>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -943,50 +944,67 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     });
     const int cluster_cap = cluster_caps[ctx->device];
 
-    // device scratch
+    // device scratch: two sets (by panel parity), so that the next panel, factored ahead on the
+    // second stream, never writes the pivot lists the current panel's update still reads
     const int grid_cap = std::max(1, std::min(ctx->num_sms, opt.panel_ctas > 0 ? opt.panel_ctas : ctx->num_sms));
     struct Scratch {
         unsigned long long piv_slot[kMaxPanel];
         int pivot_rows[kMaxPanel];
         int pivot_cols[kMaxPanel];
         int k;
+        int err;  // the device error word as of the panel's end
         unsigned bar[2];
     };
+    const size_t scratch_bytes = (sizeof(Scratch) + 255) / 256 * 256;
     const size_t cand_bytes = sizeof(uint32_t) * 2 * static_cast<size_t>(grid_cap) * kMaxPanel;
-    const size_t perm_bytes = sizeof(int) * static_cast<size_t>(m);
-    uint8_t* base = static_cast<uint8_t*>(ctx->ws.get(kSlotElim0, sizeof(Scratch) + 256 + cand_bytes + perm_bytes + 256));
-    Scratch* d_s = reinterpret_cast<Scratch*>(base);
-    uint32_t* d_cand = reinterpret_cast<uint32_t*>(base + (sizeof(Scratch) + 255) / 256 * 256);
-    int* d_perm = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(d_cand) + cand_bytes);
-    HME_CUDA(cudaMemsetAsync(d_s->bar, 0, sizeof(unsigned) * 2, ctx->stream));
+    const size_t perm_bytes = (sizeof(int) * static_cast<size_t>(m) + 255) / 256 * 256;
+    uint8_t* base = static_cast<uint8_t*>(
+        ctx->ws.get(kSlotElim0, 2 * (scratch_bytes + cand_bytes) + 2 * perm_bytes + 256));
+    Scratch* d_sb[2] = {reinterpret_cast<Scratch*>(base), reinterpret_cast<Scratch*>(base + scratch_bytes)};
+    uint32_t* d_candb[2] = {reinterpret_cast<uint32_t*>(base + 2 * scratch_bytes),
+                            reinterpret_cast<uint32_t*>(base + 2 * scratch_bytes + cand_bytes)};
+    int* d_permb[2] = {reinterpret_cast<int*>(base + 2 * (scratch_bytes + cand_bytes)),
+                       reinterpret_cast<int*>(base + 2 * (scratch_bytes + cand_bytes) + perm_bytes)};
+    HME_CUDA(cudaMemsetAsync(d_sb[0]->bar, 0, sizeof(unsigned) * 2, ctx->stream));
+    HME_CUDA(cudaMemsetAsync(d_sb[1]->bar, 0, sizeof(unsigned) * 2, ctx->stream));
+    // pinned copies of the two scratch sets (the host reads a panel's pivots without waiting for
+    // the other stream's work), the second stream and the events of the lookahead
+    // (and two pinned permutation buffers: the host queues a panel's update behind the previous
+    // one's without waiting for it)
+    const size_t pinned_bytes = 2 * sizeof(Scratch) + 2 * sizeof(int) * static_cast<size_t>(m);
+    if (ctx->elim_pinned_bytes < pinned_bytes) {
+        if (ctx->elim_pinned) {
+            HME_CUDA(cudaDeviceSynchronize());
+            HME_CUDA(cudaFreeHost(ctx->elim_pinned));
+            ctx->elim_pinned = nullptr;
+            ctx->elim_pinned_bytes = 0;
+        }
+        HME_CUDA(cudaMallocHost(&ctx->elim_pinned, pinned_bytes));
+        ctx->elim_pinned_bytes = pinned_bytes;
+    }
+    Scratch* h_sb = static_cast<Scratch*>(ctx->elim_pinned);
+    int* h_permb[2] = {reinterpret_cast<int*>(h_sb + 2), reinterpret_cast<int*>(h_sb + 2) + m};
+    if (!ctx->aux_stream) {
+        // the lookahead panel's stream at the highest priority: its cluster takes SMs as they free up
+        int lo = 0, hi = 0;
+        HME_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        HME_CUDA(cudaStreamCreateWithPriority(&ctx->aux_stream, cudaStreamNonBlocking, hi));
+    }
+    while (ctx->elim_ev.size() < 3) {
+        cudaEvent_t e;
+        HME_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->elim_ev.push_back(e);
+    }
+    cudaEvent_t ev_next = ctx->elim_ev[0], ev_panel[2] = {ctx->elim_ev[1], ctx->elim_ev[2]};
+    const cudaStream_t s_main = ctx->stream, s_aux = ctx->aux_stream;
+    // lookahead only where it can overlap: the cluster kernel (a few SMs), and not while the
+    // per-kernel timer is on (its events assume one stream)
+    const bool allow_lookahead = !opt.no_lookahead && !ctx->timer.on;
 
-    std::vector<int> pivots;
-    pivots.reserve(std::min(m, n));
-    std::vector<int> perm_host;
-    int r0 = 0;
-    Scratch h_s;
-    for (int c0 = 0; c0 < lu_cols && r0 < m; c0 += bw) {
-        const int w = std::min(bw, lu_cols - c0);
-        HME_CUDA(cudaMemsetAsync(d_s->piv_slot, 0x7f, sizeof(unsigned long long) * kMaxPanel, ctx->stream));
-        PanelArgs pa{};
-        pa.A = A;
-        pa.ld = ld;
-        pa.m = m;
-        pa.c0 = c0;
-        pa.bw = w;
-        pa.r0 = r0;
-        pa.R = rg;
-        pa.piv_slot = d_s->piv_slot;
-        pa.cand = d_cand;
-        pa.pivot_rows = d_s->pivot_rows;
-        pa.pivot_cols = d_s->pivot_cols;
-        pa.k_out = &d_s->k;
-        pa.bar = d_s->bar;
-        pa.err = ctx->d_err;
-        const int rows = m - r0;
-        // the cluster kernel when the active rows fit the shared memory of one cluster:
-        // the cluster doubles (up to the largest the device runs) until each CTA
-        // holds at most rows_per_cta rows, and further while a slice does not fit
+    // The cluster kernel when the active rows fit the shared memory of one cluster: the cluster
+    // doubles (up to the largest the device runs) until each CTA holds at most rows_per_cta rows,
+    // and further while a slice does not fit.  Returns the cluster size, 0 for the grid kernel.
+    auto cluster_size = [&](int rows, int w) -> int {
         int cs = 0;
         if (opt.panel_kernel != 1 && cluster_cap > 0) {
             const size_t want = static_cast<size_t>(std::max(1, opt.rows_per_cta > 0 ? opt.rows_per_cta : 32));
@@ -1000,6 +1018,33 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             while (c < cluster_cap && (rpc_of(c) > want || !fits(c))) c *= 2;
             if (fits(c)) cs = c;
         }
+        return cs;
+    };
+
+    // The panel [c0, c0 + w) of the active rows [r0, m) on `st`: its pivots and the error word
+    // land in h_sb[par] and ev_panel[par] is recorded.  Returns the cluster size (0: grid kernel).
+    auto launch_panel = [&](int c0, int w, int r0, int par, cudaStream_t st) -> int {
+        Scratch* d_s = d_sb[par];
+        const cudaStream_t saved = ctx->stream;
+        ctx->stream = st;  // HME_TIMED brackets the launch on the launching stream
+        HME_CUDA(cudaMemsetAsync(d_s->piv_slot, 0x7f, sizeof(unsigned long long) * kMaxPanel, st));
+        PanelArgs pa{};
+        pa.A = A;
+        pa.ld = ld;
+        pa.m = m;
+        pa.c0 = c0;
+        pa.bw = w;
+        pa.r0 = r0;
+        pa.R = rg;
+        pa.piv_slot = d_s->piv_slot;
+        pa.cand = d_candb[par];
+        pa.pivot_rows = d_s->pivot_rows;
+        pa.pivot_cols = d_s->pivot_cols;
+        pa.k_out = &d_s->k;
+        pa.bar = d_s->bar;
+        pa.err = ctx->d_err;
+        const int rows = m - r0;
+        const int cs = cluster_size(rows, w);
         HME_REQUIRE(opt.panel_kernel < 2 || cs > 0, "elim: the panel does not fit one cluster");
         if (cs > 0) {
             const int rpc = static_cast<int>((static_cast<size_t>(rows) + cs - 1) / cs);
@@ -1007,7 +1052,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             cfg.gridDim = dim3(cs);
             cfg.blockDim = dim3(kClusterThreads);
             cfg.dynamicSmemBytes = cluster_smem_bytes(rpc, w);
-            cfg.stream = ctx->stream;
+            cfg.stream = st;
             cudaLaunchAttribute at[1];
             at[0].id = cudaLaunchAttributeClusterDimension;
             at[0].val.clusterDim.x = cs;
@@ -1044,15 +1089,35 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             void* args[] = {&pa, &smem_rows};
             HME_TIMED(ctx, "panel_factor",
                       HME_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(panel_factor_kernel), want_grid,
-                                                           kPanelThreads, args, dyn, ctx->stream)));
+                                                           kPanelThreads, args, dyn, st)));
         }
-        HME_CUDA(cudaMemcpyAsync(&h_s, d_s, sizeof(Scratch), cudaMemcpyDeviceToHost, ctx->stream));
-        check_device_error(ctx);  // synchronises
+        // the panel's error word next to its pivots, then the pivots to pinned memory
+        HME_CUDA(cudaMemcpyAsync(&d_s->err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToDevice, st));
+        HME_CUDA(cudaMemcpyAsync(&h_sb[par], d_s, sizeof(Scratch), cudaMemcpyDeviceToHost, st));
+        HME_CUDA(cudaEventRecord(ev_panel[par], st));
+        ctx->stream = saved;
+        return cs;
+    };
+
+    std::vector<int> pivots;
+    pivots.reserve(std::min(m, n));
+    std::vector<int> perm_host;
+    int r0 = 0;
+    int par = 0;
+    bool launched = false;  // the panel at c0 was already factored ahead (on the second stream)
+    for (int c0 = 0; c0 < lu_cols && r0 < m; c0 += bw) {
+        const int w = std::min(bw, lu_cols - c0);
+        if (!launched) launch_panel(c0, w, r0, par, s_main);
+        launched = false;
+        HME_CUDA(cudaEventSynchronize(ev_panel[par]));
+        const Scratch& h_s = h_sb[par];
+        if (h_s.err != 0) check_device_error(ctx);  // reports the timeout (and clears the word)
         const int k = h_s.k;
-        if (k == 0) continue;
+        if (k == 0) continue;  // no pivot in the panel: nothing moved, the next panel starts at r0
         for (int t = 0; t < k; ++t) pivots.push_back(h_s.pivot_cols[t]);
 
         // (2) pivot rows first, in pivot order, the other active rows after them in order
+        const int rows = m - r0;
         perm_host.assign(rows, 0);
         {
             std::vector<char> is_piv(rows, 0);
@@ -1075,40 +1140,73 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         }
         bool identity = true;
         for (int i = 0; i < rows && identity; ++i) identity = perm_host[i] == r0 + i;
-        const int cols_right = n - c0;
         if (!identity) {
-            HME_CUDA(cudaMemcpyAsync(d_perm, perm_host.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, ctx->stream));
-            uint32_t* tmp = static_cast<uint32_t*>(ctx->ws.get(kSlotElim1, sizeof(uint32_t) * static_cast<size_t>(rows) * cols_right));
-            const int g = grid_1d(static_cast<size_t>(rows) * cols_right, ctx->num_sms);
-            HME_TIMED(ctx, "row_permute", gather_rows_kernel<<<g, 256, 0, ctx->stream>>>(A, ld, d_perm, rows, c0, cols_right, tmp));
-            HME_TIMED(ctx, "row_permute", scatter_rows_kernel<<<g, 256, 0, ctx->stream>>>(A, ld, r0, rows, c0, cols_right, tmp));
-            HME_CUDA(cudaGetLastError());
+            // pinned by parity: the copy of the panel two steps back has long completed (the host
+            // waited for this panel, which follows that panel's update on the main stream)
+            std::memcpy(h_permb[par], perm_host.data(), sizeof(int) * rows);
+            HME_CUDA(cudaMemcpyAsync(d_permb[par], h_permb[par], sizeof(int) * rows, cudaMemcpyHostToDevice, s_main));
         }
-        // pivot columns of this panel, on the device (reuse the pivot_cols slot)
+        int* d_perm = d_permb[par];
         const int c1 = c0 + w;
-        const int trail = n - c1;
         const int below = m - r0 - k;
-        if (trail > 0) {
-            // (3) U12 = L11^-1 A12 in place: forward substitution, one warp per column
+        const int* d_pcols = d_sb[par]->pivot_cols;
+        // the update of columns [ca, cb): row permutation (from c0 on), U12 = L11^-1 A12, A22 -= L21 U12
+        uint32_t* L21 = nullptr;
+        auto update = [&](int ca, int cb, int sm_cap) {
+            if (cb <= ca) return;
+            if (!identity) {
+                const int cols = cb - ca;
+                uint32_t* tmp = static_cast<uint32_t*>(ctx->ws.get(kSlotElim1, sizeof(uint32_t) * static_cast<size_t>(rows) * (n - c0)));
+                const int g = grid_1d(static_cast<size_t>(rows) * cols, ctx->num_sms);
+                HME_TIMED(ctx, "row_permute", gather_rows_kernel<<<g, 256, 0, s_main>>>(A, ld, d_perm, rows, ca, cols, tmp));
+                HME_TIMED(ctx, "row_permute", scatter_rows_kernel<<<g, 256, 0, s_main>>>(A, ld, r0, rows, ca, cols, tmp));
+                HME_CUDA(cudaGetLastError());
+            }
+            const int ua = std::max(ca, c1);
+            if (cb <= ua) return;
+            const int cols = cb - ua;
             if (k > 1) {
-                const int g = (trail + kTrsmCols - 1) / kTrsmCols;
-                HME_TIMED(ctx, "trsm", trsm_unit_lower_kernel<<<g, 32 * kTrsmCols, trsm_smem_bytes(k), ctx->stream>>>(
-                                           A, ld, r0, d_s->pivot_cols, k, c1, trail, p, mp.barrett));
+                const int g = (cols + kTrsmCols - 1) / kTrsmCols;
+                HME_TIMED(ctx, "trsm", trsm_unit_lower_kernel<<<g, 32 * kTrsmCols, trsm_smem_bytes(k), s_main>>>(
+                                           A, ld, r0, d_pcols, k, ua, cols, p, mp.barrett));
                 HME_CUDA(cudaGetLastError());
             }
-            // (4) A22 -= L21 * U12
             if (below > 0) {
-                uint32_t* L21 = static_cast<uint32_t*>(ctx->ws.get(kSlotElim2, sizeof(uint32_t) * static_cast<size_t>(below) * k));
-                HME_TIMED(ctx, "gather_cols",
-                          gather_cols_kernel<<<grid_1d(static_cast<size_t>(below) * k, ctx->num_sms), 256, 0, ctx->stream>>>(
-                              A, ld, r0 + k, below, d_s->pivot_cols, k, L21));
-                HME_CUDA(cudaGetLastError());
-                gemm_u32_device(ctx, mp, below, trail, k, L21, k, A + static_cast<size_t>(r0) * ld + c1, ld,
-                                A + static_cast<size_t>(r0 + k) * ld + c1, ld, HME_SUB);
+                if (!L21) {
+                    L21 = static_cast<uint32_t*>(ctx->ws.get(kSlotElim2, sizeof(uint32_t) * static_cast<size_t>(below) * k));
+                    HME_TIMED(ctx, "gather_cols",
+                              gather_cols_kernel<<<grid_1d(static_cast<size_t>(below) * k, ctx->num_sms), 256, 0, s_main>>>(
+                                  A, ld, r0 + k, below, d_pcols, k, L21));
+                    HME_CUDA(cudaGetLastError());
+                }
+                ctx->gemm_sm_cap = sm_cap;
+                gemm_u32_device(ctx, mp, below, cols, k, L21, k, A + static_cast<size_t>(r0) * ld + ua, ld,
+                                A + static_cast<size_t>(r0 + k) * ld + ua, ld, HME_SUB);
+                ctx->gemm_sm_cap = 0;
             }
+        };
+        const int nw = std::min(bw, lu_cols - c1);
+        // lookahead only when the next panel runs on the cluster kernel (a few SMs beside the GEMM;
+        // the cooperative grid kernel would wait for the whole device anyway)
+        const bool next = allow_lookahead && c1 < lu_cols && below > 0 && nw > 0 && cluster_size(below, nw) > 0;
+        if (next) {
+            // LOOKAHEAD: the next panel's columns first; that panel is factored on the second stream
+            // while the rest of this update runs here, the GEMM leaving the cluster's SMs free
+            update(c0, c1 + nw, 0);
+            HME_CUDA(cudaEventRecord(ev_next, s_main));
+            HME_CUDA(cudaStreamWaitEvent(s_aux, ev_next, 0));
+            const int cs_next = launch_panel(c1, nw, r0 + k, par ^ 1, s_aux);
+            update(c1 + nw, n, cs_next > 0 ? std::max(1, ctx->num_sms - cs_next) : 0);
+            launched = true;
+        } else {
+            update(c0, n, 0);
         }
+        // the main stream's later work (the next panel's update) follows the lookahead panel
+        if (launched) HME_CUDA(cudaStreamWaitEvent(s_main, ev_panel[par ^ 1], 0));
         r0 += k;
+        par ^= 1;
     }
+    HME_CUDA(cudaStreamSynchronize(s_aux));
     res.rank = r0;
     res.pivots = pivots;
 

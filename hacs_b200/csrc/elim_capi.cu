@@ -138,6 +138,13 @@ int hme_ctx_set_panel_kernel(hme_ctx* ctx, int mode) {
     });
 }
 
+int hme_ctx_set_elim_lookahead(hme_ctx* ctx, int on) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr, "null context");
+        opts(ctx).no_lookahead = on == 0;
+    });
+}
+
 int hme_rref_u32_dev(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t* A, size_t lda, uint32_t* pivots,
                      uint32_t* rank) {
     return guard([&] {

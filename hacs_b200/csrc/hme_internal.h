@@ -97,6 +97,7 @@ struct ElimOptions {
     int back_block = 128;   // block of the RREF backward substitution
     bool want_diag = false; // return the U diagonal (determinant)
     int panel_kernel = 0;   // 0 automatic, 1 cooperative grid kernel, 2 cluster kernel where the panel fits
+    bool no_lookahead = false;  // factor each panel only after the previous update (no second stream)
 };
 
 // Optional per-kernel CUDA-event timing (bench / profiling use): when enabled,
@@ -134,6 +135,11 @@ struct hme_ctx {
     int fixed_variant = -1;          // >= 0: every GEMM of this context uses that variant
     int sched_policy = 0;            // 0 shape heuristic, 1 learned planner table
     void* sched_table = nullptr;     // planner decisions by shape class (sched.cu)
+    int gemm_sm_cap = 0;             // > 0: persistent GEMM grids use at most this many SMs
+    cudaStream_t aux_stream = nullptr;   // elimination: the lookahead panel's stream (created on first use)
+    void* elim_pinned = nullptr;         // elimination: pinned copies of the panel scratch, permutations
+    size_t elim_pinned_bytes = 0;
+    std::vector<cudaEvent_t> elim_ev;    // elimination: lookahead events
 };
 
 // Bracket one kernel launch with timing events when the context's timer is on.

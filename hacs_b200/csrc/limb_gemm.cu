@@ -364,7 +364,7 @@ void launch_gemm(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint
     g.group_m = 16;
     g.err = ctx->d_err;
     const int total = g.tiles_m * g.tiles_n;
-    const int grid = std::min(total, ctx->num_sms);
+    const int grid = std::min(total, ctx->gemm_sm_cap > 0 ? std::min(ctx->gemm_sm_cap, ctx->num_sms) : ctx->num_sms);
     const uint32_t chunk = limb_k_chunk(L);
     for (uint32_t kb0 = 0; kb0 < k; kb0 += chunk) {
         const uint32_t kc = std::min(chunk, k - kb0);

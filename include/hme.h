@@ -265,6 +265,11 @@ HME_API int hme_inverse_u32(hme_ctx *ctx, uint32_t p, uint32_t n, const uint32_t
 HME_API int hme_solve_u32(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t nb, uint32_t ny, const uint32_t *B,
                           size_t ldb, const uint32_t *Y, size_t ldy, uint32_t *X, size_t ldx);
 HME_API int hme_ctx_set_elim_options(hme_ctx *ctx, int panel, int rows_per_cta, int panel_ctas, int back_block);
+/* hme_ctx_set_elim_lookahead: on (the default) factors the next panel on a
+ * second stream while the rest of the current panel's trailing update runs
+ * (its GEMM leaving the panel's SMs free); off factors each panel after the
+ * whole update.  Tuning only: no setting changes a value. */
+HME_API int hme_ctx_set_elim_lookahead(hme_ctx *ctx, int on);
 HME_API int hme_ctx_set_panel_kernel(hme_ctx *ctx, int mode);
 
 /* ---- Howell and Smith forms over Z/ell^k (ell prime, ell^k < 2^32) ----------
