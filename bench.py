@@ -438,10 +438,12 @@ def extra_rref(eng, reps=3):
     A.copy_(A0)
     eng.set_timing(True)
     eng.timing_reset()
+    b0, s0 = eng.elim_panel_stats()
     eng.rref_dev(p, A)
     eng.sync()
-    kern = kernel_breakdown(eng, ["panel_factor", "limb_split", "limb_gemm", "trsm", "row_permute", "tri_inv",
-                                  "gather_cols", "assemble_rref", "gather", "copy"])
+    b1, s1 = eng.elim_panel_stats()
+    kern = kernel_breakdown(eng, ["panel_block", "panel_w", "panel_factor", "limb_split", "limb_gemm", "trsm", "row_permute",
+                                  "tri_inv", "gather_cols", "assemble_rref", "gather", "copy"])
     eng.set_timing(False)
     lu = n * n * r - (n + n) * r * r / 2 + r ** 3 / 3
     back = r * r * (n - r) / 2
@@ -451,10 +453,11 @@ def extra_rref(eng, reps=3):
     # tensor part: every modMAC of the LU and the back substitution is L^2 = 16 int8 limb products (2 ops each)
     achieved = 16 * 2 * work / t / 1e12
     gemm_ms = kern.get("limb_gemm", [0, 0])[0]
-    panel_ms = kern.get("panel_factor", [0, 0])[0]
+    panel_ms = kern.get("panel_factor", [0, 0])[0] + kern.get("panel_block", [0, 0])[0]
     panel_bytes = 8.0 * n * 64 * (n // 64)  # read + write of the active rows of every 64-column panel (upper bound m)
     out = {"workload": "RREF/rank/det 4096^2 rank 3900 p=2^31-19 (config 2)", "ms": t * 1e3, "rank": int(len(piv)),
            "modmac_per_s": work / t, "checksum_ok_vs_reference": bool(ok), "kernels_ms": kern,
+           "panels": {"settled_by_top_block": b1 - b0, "searched": s1 - s0},
            "roofline": {"bound": "tensor (trailing updates) / latency (panels)", "achieved_int8_tops": achieved,
                         "peak": peak, "unit": "TOPS", "frac": achieved / peak, "peak_source": psrc,
                         "algorithmic": f"LU {lu:.3e} + back substitution {back:.3e} modMAC, 32 int8 ops each",

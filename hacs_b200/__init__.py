@@ -313,9 +313,16 @@ class Engine:
         check(self._lib.hme_ctx_set_elim_lookahead(self._h, 1 if on else 0))
 
     def set_panel_kernel(self, mode: int) -> None:
-        """LU panel kernel: 0 automatic, 1 cooperative grid kernel, 2 thread-block cluster kernel,
-        3 cluster kernel with 1024 threads per CTA."""
+        """LU panel kernel: 0 automatic (over a field the top-block path first, then a searching
+        kernel), 1 cooperative grid kernel, 2 thread-block cluster kernel, 3 cluster kernel with
+        1024 threads per CTA."""
         check(self._lib.hme_ctx_set_panel_kernel(self._h, mode))
+
+    def elim_panel_stats(self) -> tuple[int, int]:
+        """(panels settled by the top-block path, panels factored by a searching kernel) so far."""
+        b, s = C.c_uint64(0), C.c_uint64(0)
+        check(self._lib.hme_ctx_elim_panel_stats(self._h, C.byref(b), C.byref(s)))
+        return b.value, s.value
 
     def rref(self, p: int, A):
         """(RREF(A), pivot columns): the reference's elim::rref result."""

@@ -54,6 +54,7 @@ PROTOTYPES = {
     "hme_ctx_set_elim_options": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "hme_ctx_set_panel_kernel": (C.c_int, [vp, C.c_int]),
     "hme_ctx_set_elim_lookahead": (C.c_int, [vp, C.c_int]),
+    "hme_ctx_elim_panel_stats": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "hme_howell_u32": (C.c_int, [vp, u32, u32, u32, u32, u32p, sz, u32p, sz, u32p, u32p, u32p]),
     "hme_smith_u32": (C.c_int, [vp, u32, u32, u32, u32, u32p, sz, u32p, u32p]),
     "hme_gemm_u32": (C.c_int, [vp, u32, u32, u32, u32, u32p, sz, u32p, sz, u32p, sz, C.c_int]),

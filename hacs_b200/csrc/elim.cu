@@ -172,6 +172,7 @@ struct PanelArgs {
     int* k_out;          // out: pivots found
     unsigned* bar;       // [2]: arrival count, generation
     int* err;
+    const int* skip;     // non-null and non-zero: the panel is settled already (top-block path)
 };
 
 // Bounded grid-wide barrier for a cooperative launch (all CTAs co-resident).
@@ -222,6 +223,8 @@ __global__ void __launch_bounds__(kPanelThreads) panel_factor_kernel(const Panel
     __shared__ unsigned long long s_piv;
     __shared__ uint32_t s_inv, s_div;
 
+    // settled by the top-block path: the same in every CTA, before any grid barrier
+    if (a.skip != nullptr && *a.skip != 0) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int active_rows = a.m - a.r0;
     const int rpc = (active_rows + gridDim.x - 1) / gridDim.x;
@@ -465,6 +468,48 @@ __device__ __forceinline__ uint32_t ff_update(uint32_t w, uint32_t y, uint32_t x
     }
 }
 
+// The scale tables of a fraction-free factorization with k pivots, raw pivots
+// s_w[0..k): s_inv[t] = w_t^-1 and s_sinv[t] = S_t^-1 = prod_{s<t} (w_s rho)^-1
+// for t <= kMaxPanel (rho = 2^-32 for the Montgomery forms, else 1).  Called by
+// every thread of the CTA; ends with a CTA barrier.
+template <int ARITH>
+__device__ void ff_scale_tables(int k, const uint32_t* s_w, uint32_t* s_inv, uint32_t* s_sinv, const Ring& R) {
+    const int lane = threadIdx.x & 31;
+    for (int t = threadIdx.x; t < k; t += blockDim.x) s_inv[t] = unit_inverse(s_w[t], R);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const uint32_t q = R.q;
+        const uint64_t bm = R.barrett;
+        const uint32_t one = 1u % q;
+        // rho^-1 = 2^32 mod q (Montgomery) or 1
+        const uint32_t rinv = ARITH == kArithPow2 ? one : mont_mul(R.mont_r2, 1u, q, R.mont_qinv);
+        uint32_t f[kMaxPanel / 32];
+        uint32_t run = one;
+#pragma unroll
+        for (int e = 0; e < kMaxPanel / 32; ++e) {
+            const int t = lane * (kMaxPanel / 32) + e;
+            f[e] = t < k ? mod_mul(s_inv[t], rinv, q, bm) : one;
+            run = mod_mul(run, f[e], q, bm);
+        }
+        // inclusive scan of the lane products, then exclusive per element
+        uint32_t incl = run;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl = mod_mul(incl, y, q, bm);
+        }
+        uint32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) ex = one;
+#pragma unroll
+        for (int e = 0; e < kMaxPanel / 32; ++e) {
+            s_sinv[lane * (kMaxPanel / 32) + e] = ex;
+            ex = mod_mul(ex, f[e], q, bm);
+        }
+        if (lane == 31) s_sinv[kMaxPanel] = ex;
+    }
+    __syncthreads();
+}
+
 template <int ARITH, int NT>
 __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(const PanelArgs a) {
     extern __shared__ __align__(16) uint32_t s_dyn[];
@@ -476,6 +521,8 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(const PanelArgs a)
     __shared__ uint32_t s_sinv[kMaxPanel + 1];                // S_t^-1
     __shared__ int s_colstep[kMaxPanel];                      // step t of pivot column c0 + j; else -1 - pivots left of it
 
+    // settled by the top-block path: the same in every CTA, before any cluster barrier
+    if (a.skip != nullptr && *a.skip != 0) return;
     const uint32_t crank = cluster_ctarank(), csize = cluster_nctarank();
     const int rows = a.m - a.r0;
     const int rpc = (rows + static_cast<int>(csize) - 1) / static_cast<int>(csize);
@@ -604,39 +651,7 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(const PanelArgs a)
     if (pend_col >= 0) S[pend_col * rs + li] = pend_xp;
 
     // ---- back to the classical values: w_t^-1 and S_t^-1 = prod_{s<t} w_s^-1 rho^-1
-    for (int t = tid; t < k; t += NT) s_inv[t] = unit_inverse(s_w[t], a.R);
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t q = a.R.q;
-        const uint64_t bm = a.R.barrett;
-        const uint32_t one = 1u % q;
-        // rho^-1 = 2^32 mod q (Montgomery) or 1
-        const uint32_t rinv = ARITH == kArithPow2 ? one : mont_mul(a.R.mont_r2, 1u, q, a.R.mont_qinv);
-        uint32_t f[kMaxPanel / 32];
-        uint32_t run = one;
-#pragma unroll
-        for (int e = 0; e < kMaxPanel / 32; ++e) {
-            const int t = lane * (kMaxPanel / 32) + e;
-            f[e] = t < k ? mod_mul(s_inv[t], rinv, q, bm) : one;
-            run = mod_mul(run, f[e], q, bm);
-        }
-        // inclusive scan of the lane products, then exclusive per element
-        uint32_t incl = run;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
-            if (lane >= off) incl = mod_mul(incl, y, q, bm);
-        }
-        uint32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) ex = one;
-#pragma unroll
-        for (int e = 0; e < kMaxPanel / 32; ++e) {
-            s_sinv[lane * (kMaxPanel / 32) + e] = ex;
-            ex = mod_mul(ex, f[e], q, bm);
-        }
-        if (lane == 31) s_sinv[kMaxPanel] = ex;
-    }
-    __syncthreads();
+    ff_scale_tables<ARITH>(k, s_w, s_inv, s_sinv, a.R);
     if (has_row) {
         const int st = s_step[li];
         const int tau = st ? st - 1 : k;  // the step that froze this row's scale
@@ -655,6 +670,344 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(const PanelArgs a)
         for (int j = lane; j < bw; j += 32) dst[j] = S[j * rs + r];
     }
     if (crank == 0 && tid == 0) *a.k_out = k;
+}
+
+// ---- the top-block path of a field panel ---------------------------------------
+// At step t of a panel the pivot is the topmost active row with a non-zero in
+// column c0 + t.  If the first t steps took rows r0 .. r0+t-1, row r0 + t is
+// the topmost active row, so it is the pivot exactly when its entry (after the
+// first t steps) is non-zero -- and those entries depend only on the top
+// rows.  Hence: when the nb x w top block B = A[r0 : r0+nb, c0 : c0+w) (nb =
+// min(w, m - r0)) factors with non-zero diagonal entries, the panel's pivots
+// are (r0 + t, c0 + t), t < nb, the same as the search finds, with no row
+// moved.  The packed LU of the block is unique for that pivot sequence, and
+// the rest of the elimination step is one product:
+//   [A12; A22] += [L^-1 - I; -A21 B^-1] A12
+// gives U12 = L^-1 A12 in the top rows and the Schur complement A22 - A21 B^-1
+// A12 below (B = L U, nb = w whenever rows remain below).  When a diagonal
+// entry is zero, nothing is written and the searching kernel factors the panel.
+struct BlockArgs {
+    uint32_t* A;
+    uint64_t ld;
+    int m, r0, c0, w;
+    Ring R;
+    int* pivot_rows;  // [w] out
+    int* pivot_cols;  // [w] out
+    int* k_out;       // out
+    int* ok;          // out: 1 when the top block settled the panel, else 0
+    uint32_t* linv;   // out: L^-1 - I (nb x nb, row-major)
+    uint32_t* binv;   // out: B^-1 (w x w, row-major) when rows remain below the block
+    int* err;         // device error word (a wavefront wait that runs out)
+};
+constexpr int kBlockThreads = 1024;
+
+__host__ __device__ constexpr int block_stride(int nb, int w) { return (w + nb) | 1; }
+__host__ __device__ constexpr size_t block_smem_bytes(int nb, int w) {
+    return sizeof(uint32_t) * static_cast<size_t>(nb) * block_stride(nb, w);  // T = [B | I], nb x (w + nb)
+}
+
+// x * y for the back substitution: y in Montgomery form (y 2^32 mod q) for odd
+// q, so one Montgomery reduction gives x y mod q; plain for q = 2^k.
+template <int ARITH>
+__device__ __forceinline__ uint32_t mul_mform(uint32_t x, uint32_t ym, const Ring& R) {
+    if constexpr (ARITH == kArithPow2) return (x * ym) & (R.q - 1u);
+    else return mont_mul(x, ym, R.q, R.mont_qinv);
+}
+
+// Row flags of a wavefront inside one CTA: one mbarrier per row, expecting
+// the 32 arrivals of the warp that owns the row.  publish_row: every lane
+// arrives (release: its shared-memory stores of the row are visible to a
+// waiter).  wait_row: every lane waits for the phase (acquire), suspended in
+// hardware rather than spinning on issue slots, with the bounded wait of
+// mbar_wait: when it runs out the CTA's abort flag and the device error word
+// are set, every later wait returns at once, and it returns false.
+__device__ __forceinline__ void publish_row(uint64_t* bars, int row) { mbar_arrive(&bars[row]); }
+
+__device__ __forceinline__ bool wait_row(uint64_t* bars, int row, volatile int* abort, int* err) {
+    const bool ok = mbar_wait(&bars[row], 0, abort, err, DERR_WAIT_ROW);
+    return __all_sync(0xffffffffu, ok) != 0;
+}
+
+// One CTA: the top block's elimination as two row wavefronts (warps over rows,
+// each row in the registers of its warp, lanes over columns).
+// (1) Forward, on [B | I] without a search (row t pivots at step t): row i
+// applies the fraction-free updates of pivot rows 0 .. i-1 in order, each as
+// soon as that row is published -- the same operations in the same order as a
+// step-by-step elimination, so the same values -- then checks its own pivot
+// and is published.  Rows leave the multipliers, U and, in the right half,
+// L^-1, each scaled by the unit its steps accumulated; the classical values
+// are restored as in the cluster kernel.  Row i's right half is zero beyond
+// column w + i, and pivot row s's beyond w + s, so row i touches columns
+// s+1 .. w+s and w+i at step s.
+// (2) With rows below: B^-1 = U^-1 L^-1 by a backward wavefront on [U | L^-1]
+// (rows scaled by the inverse diagonal, U's part kept in Montgomery form):
+// row r subtracts U'[r][t] X[t] for t = w-1 .. r+1 as those rows are published.
+// WMAX (64 or 128) bounds w.
+template <int ARITH, int WMAX>
+__global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockArgs a) {
+    extern __shared__ __align__(16) uint32_t s_blk[];
+    __shared__ uint32_t s_w[kMaxPanel], s_inv[kMaxPanel], s_sinv[kMaxPanel + 1], s_dinv[kMaxPanel],
+        s_dinvm[kMaxPanel];
+    __shared__ __align__(8) uint64_t s_fwd[kMaxPanel], s_bwd[kMaxPanel];  // row mbarriers
+    __shared__ int s_fail, s_abort;
+    const int w = a.w, nb = min(w, a.m - a.r0), ts = block_stride(nb, w), wide = w + nb;
+    uint32_t* T = s_blk;  // [nb][ts]: [B | I]; row i written once it is final
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = kBlockThreads / 32;
+    constexpr int CI = 2 * WMAX / 32;  // column slots of [B | I] per lane
+    constexpr int CW = WMAX / 32;      // slots of the pivot index
+    const uint32_t one = 1u % a.R.q;
+    uint64_t* fwd = s_fwd;
+    uint64_t* bwd = s_bwd;
+    volatile int* abort_flag = &s_abort;
+    for (int i = tid; i < kMaxPanel; i += kBlockThreads) {
+        mbar_init(&s_fwd[i], 32);
+        mbar_init(&s_bwd[i], 32);
+    }
+    if (tid == 0) {
+        s_fail = 0;
+        s_abort = 0;
+    }
+    fence_mbar_init();
+    __syncthreads();
+    for (int i = warp; i < nb; i += NW) {
+        uint32_t y[CI];
+        const uint32_t* src = a.A + static_cast<size_t>(a.r0 + i) * a.ld + a.c0;
+#pragma unroll
+        for (int c = 0; c < CI; ++c) {
+            const int j = lane + 32 * c;
+            y[c] = j < w ? src[j] : (j == w + i ? one : 0u);
+        }
+        bool live = true;
+#pragma unroll
+        for (int sc = 0; sc < CW; ++sc) {
+            for (int sl = 0; sl < 32 && live; ++sl) {
+                const int s = 32 * sc + sl;
+                if (s >= i) {
+                    live = false;  // leaves both loops: this row's steps are done
+                    break;
+                }
+                if (!wait_row(fwd, s, abort_flag, a.err)) break;
+                const uint32_t xn = ff_negate<ARITH>(__shfl_sync(0xffffffffu, y[sc], sl), a.R);
+                const uint32_t ws = T[s * ts + s];
+#pragma unroll
+                for (int c = 0; c < CI; ++c) {
+                    const int j = lane + 32 * c;
+                    if (j > s && (j <= w + s || j == w + i) && j < wide)
+                        y[c] = ff_update<ARITH>(ws, y[c], xn, T[s * ts + j], a.R);
+                }
+            }
+        }
+        // the pivot of step i: column i of this row
+        uint32_t pv = y[0];
+#pragma unroll
+        for (int c = 1; c < CW; ++c)
+            if ((i >> 5) == c) pv = y[c];
+        pv = __shfl_sync(0xffffffffu, pv, i & 31);
+        if (pv == 0 && lane == 0) s_fail = 1;
+#pragma unroll
+        for (int c = 0; c < CI; ++c) {
+            const int j = lane + 32 * c;
+            if (j < wide) T[i * ts + j] = y[c];
+        }
+        publish_row(fwd, i);
+    }
+    __syncthreads();
+    if (s_fail || s_abort) {
+        if (tid == 0) *a.ok = 0;
+        return;
+    }
+    if (tid < nb) s_w[tid] = T[tid * ts + tid];
+    __syncthreads();
+    ff_scale_tables<ARITH>(nb, s_w, s_inv, s_sinv, a.R);
+    // row r froze at step r: a multiplier of step j < r takes w_j^-1, the rest (U, L^-1) S_r^-1
+    for (int r = warp; r < nb; r += NW)
+        for (int j = lane; j < wide; j += 32) {
+            const uint32_t f = j < r ? s_inv[j] : s_sinv[r];
+            T[r * ts + j] = mod_mul(T[r * ts + j], f, a.R.q, a.R.barrett);
+        }
+    __syncthreads();
+    for (int r = warp; r < nb; r += NW) {
+        uint32_t* dst = a.A + static_cast<size_t>(a.r0 + r) * a.ld + a.c0;
+        for (int j = lane; j < w; j += 32) dst[j] = T[r * ts + j];
+        for (int j = lane; j < nb; j += 32) {
+            const uint32_t v = T[r * ts + w + j];
+            a.linv[static_cast<size_t>(r) * nb + j] = j == r ? mod_sub(v, one, a.R.q) : v;
+        }
+    }
+    if (tid < nb) {
+        a.pivot_rows[tid] = a.r0 + tid;
+        a.pivot_cols[tid] = a.c0 + tid;
+    }
+    if (tid == 0) {
+        *a.k_out = nb;
+        *a.ok = 1;
+    }
+    if (nb < w || a.m - a.r0 == nb) return;  // no row below the block: B^-1 is not needed
+    // ---- B^-1: [U | L^-1] rows times the inverse diagonal (U's part into Montgomery form)
+    if (tid < w) {
+        const uint32_t d = unit_inverse(T[tid * ts + tid], a.R);
+        s_dinv[tid] = d;
+        const uint32_t r32 = ARITH == kArithPow2 ? one : mont_mul(a.R.mont_r2, 1u, a.R.q, a.R.mont_qinv);  // 2^32 mod q
+        s_dinvm[tid] = mod_mul(d, r32, a.R.q, a.R.barrett);
+    }
+    __syncthreads();
+    for (int r = warp; r < w; r += NW)
+        for (int j = r + 1 + lane; j < wide; j += 32)
+            T[r * ts + j] = mod_mul(T[r * ts + j], j < w ? s_dinvm[r] : s_dinv[r], a.R.q, a.R.barrett);
+    __syncthreads();
+    // backward wavefront: warp k takes rows w-1-k, w-1-k-32, ...
+    for (int r = w - 1 - warp; r >= 0; r -= NW) {
+        uint32_t x[CW];
+#pragma unroll
+        for (int c = 0; c < CW; ++c) {
+            const int j = lane + 32 * c;
+            x[c] = j < w ? T[r * ts + w + j] : 0u;
+        }
+        for (int t = w - 1; t > r; --t) {
+            if (!wait_row(bwd, t, abort_flag, a.err)) break;
+            const uint32_t um = T[r * ts + t];
+            if (um == 0) continue;
+#pragma unroll
+            for (int c = 0; c < CW; ++c) {
+                const int j = lane + 32 * c;
+                if (j < w) x[c] = mod_sub(x[c], mul_mform<ARITH>(T[t * ts + w + j], um, a.R), a.R.q);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CW; ++c) {
+            const int j = lane + 32 * c;
+            if (j < w) T[r * ts + w + j] = x[c];
+        }
+        publish_row(bwd, r);
+    }
+    __syncthreads();
+    if (s_abort) {  // the device error word is set; the host reports it
+        if (tid == 0) *a.ok = 0;
+        return;
+    }
+    for (int r = warp; r < w; r += NW)
+        for (int j = lane; j < w; j += 32) a.binv[static_cast<size_t>(r) * w + j] = T[r * ts + w + j];
+}
+
+// The left factor of the fused update, W ((m - r0) x nb, row-major, ld nb):
+// rows t < nb are L^-1 - I; a row x below the block becomes -x B^-1 (x = the
+// row's panel columns).  A warp takes four rows at once, lanes over output
+// columns; each dot product runs exactly in a 96-bit carry chain (nb <= 128
+// products below 2^64) and is reduced once.
+constexpr int kWRows = 32;
+constexpr int kWRowsPerWarp = 4;
+
+__device__ __forceinline__ void mac96(uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t x, uint32_t y) {
+    asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+        "addc.u32 %2, %2, 0;"
+        : "+r"(a0), "+r"(a1), "+r"(a2)
+        : "r"(x), "r"(y));
+}
+
+template <int WMAX>
+__global__ void __launch_bounds__(256) panel_w_kernel(const uint32_t* __restrict__ A, uint64_t ld, int r0, int m,
+                                                      int c0, int nb, const uint32_t* __restrict__ linv,
+                                                      const uint32_t* __restrict__ binv, uint32_t q,
+                                                      uint64_t barrett, uint32_t* __restrict__ W) {
+    extern __shared__ __align__(16) uint32_t s_wk[];
+    const int rb = r0 + static_cast<int>(blockIdx.x) * kWRows;  // first row of this CTA
+    const int nr = min(kWRows, m - rb);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = 256 / 32;
+    static_assert(NW * kWRowsPerWarp == kWRows, "one pass of the warps covers the CTA's rows");
+    // the top rows: L^-1 - I
+    for (int r = warp; r < nr; r += NW) {
+        const int row = rb + r;
+        if (row >= r0 + nb) break;
+        for (int j = lane; j < nb; j += 32)
+            W[static_cast<size_t>(row - r0) * nb + j] = linv[static_cast<size_t>(row - r0) * nb + j];
+    }
+    if (rb + nr <= r0 + nb) return;  // no row below the block in this CTA (uniform)
+    uint32_t* Bi = s_wk;                                   // [nb][nb]
+    uint32_t* Xr = s_wk + static_cast<size_t>(nb) * nb;    // [kWRows][nb]
+    constexpr int CS = WMAX / 32;
+    {
+        // B^-1 in 16-byte pieces (its buffer is 16-byte aligned), all loads of a thread in flight at once
+        const int n4 = (nb * nb) >> 2;
+        const uint4* b4 = reinterpret_cast<const uint4*>(binv);
+        uint4* d4 = reinterpret_cast<uint4*>(Bi);
+        constexpr int P = 4;
+        for (int base = 0; base < n4; base += 256 * P) {
+            uint4 v[P];
+#pragma unroll
+            for (int e = 0; e < P; ++e) {
+                const int idx = base + tid + 256 * e;
+                if (idx < n4) v[e] = b4[idx];
+            }
+#pragma unroll
+            for (int e = 0; e < P; ++e) {
+                const int idx = base + tid + 256 * e;
+                if (idx < n4) d4[idx] = v[e];
+            }
+        }
+        for (int idx = 4 * n4 + tid; idx < nb * nb; idx += 256) Bi[idx] = binv[idx];
+    }
+    {
+        // this warp's four rows (zero for top rows and rows past the end)
+        const int rl0 = warp * kWRowsPerWarp;
+        uint32_t v[kWRowsPerWarp][CS];
+#pragma unroll
+        for (int i = 0; i < kWRowsPerWarp; ++i) {
+            const int row = rb + rl0 + i;
+            const bool below = rl0 + i < nr && row >= r0 + nb;
+            const uint32_t* src = A + static_cast<size_t>(below ? row : r0) * ld + c0;
+#pragma unroll
+            for (int c = 0; c < CS; ++c) {
+                const int j = lane + 32 * c;
+                v[i][c] = below && j < nb ? src[j] : 0u;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kWRowsPerWarp; ++i)
+#pragma unroll
+            for (int c = 0; c < CS; ++c) {
+                const int j = lane + 32 * c;
+                if (j < nb) Xr[(rl0 + i) * nb + j] = v[i][c];
+            }
+    }
+    __syncthreads();
+    uint32_t a0[kWRowsPerWarp][CS], a1[kWRowsPerWarp][CS], a2[kWRowsPerWarp][CS];
+#pragma unroll
+    for (int i = 0; i < kWRowsPerWarp; ++i)
+#pragma unroll
+        for (int c = 0; c < CS; ++c) a0[i][c] = a1[i][c] = a2[i][c] = 0;
+    const int rl = warp * kWRowsPerWarp;  // this warp's rows: rl .. rl + 3 of the CTA
+    for (int t = 0; t < nb; ++t) {
+        uint32_t bt[CS];
+#pragma unroll
+        for (int c = 0; c < CS; ++c) {
+            const int j = lane + 32 * c;
+            bt[c] = j < nb ? Bi[t * nb + j] : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < kWRowsPerWarp; ++i) {
+            const uint32_t x = Xr[(rl + i) * nb + t];
+#pragma unroll
+            for (int c = 0; c < CS; ++c) mac96(a0[i][c], a1[i][c], a2[i][c], x, bt[c]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kWRowsPerWarp; ++i) {
+        const int row = rb + rl + i;
+        if (rl + i >= nr || row < r0 + nb) continue;
+        uint32_t* dst = W + static_cast<size_t>(row - r0) * nb;
+#pragma unroll
+        for (int c = 0; c < CS; ++c) {
+            const int j = lane + 32 * c;
+            if (j < nb) {
+                const uint64_t h = reduce_u64((static_cast<uint64_t>(a2[i][c]) << 32) | a1[i][c], q, barrett);
+                const uint32_t v = static_cast<uint32_t>(reduce_u64((h << 32) | a0[i][c], q, barrett));
+                dst[j] = v == 0 ? 0u : q - v;
+            }
+        }
+    }
 }
 
 // ---- row permutation of columns [c0, n) for rows [r0, m) -------------------------
@@ -904,6 +1257,19 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         int& cluster_cap = cluster_caps[dev];
         cluster_cap = 0;
         HME_CUDA(cudaFuncSetAttribute(panel_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax));
+        {
+            const int bsm = static_cast<int>(block_smem_bytes(kMaxPanel, kMaxPanel));
+            for (const void* fn : {reinterpret_cast<const void*>(panel_block_kernel<kArithPow2, 64>),
+                                   reinterpret_cast<const void*>(panel_block_kernel<kArithMont31, 64>),
+                                   reinterpret_cast<const void*>(panel_block_kernel<kArithMont32, 64>),
+                                   reinterpret_cast<const void*>(panel_block_kernel<kArithPow2, 128>),
+                                   reinterpret_cast<const void*>(panel_block_kernel<kArithMont31, 128>),
+                                   reinterpret_cast<const void*>(panel_block_kernel<kArithMont32, 128>)})
+                HME_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bsm));
+            const int wsm = static_cast<int>(sizeof(uint32_t) * (kMaxPanel * kMaxPanel + kWRows * kMaxPanel));
+            HME_CUDA(cudaFuncSetAttribute(panel_w_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
+            HME_CUDA(cudaFuncSetAttribute(panel_w_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
+        }
         bool attrs_ok = true;
         for (const void* fn : {reinterpret_cast<const void*>(panel_cluster_kernel<kArithPow2, 512>),
                                reinterpret_cast<const void*>(panel_cluster_kernel<kArithMont31, 512>),
@@ -952,19 +1318,25 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         int pivot_rows[kMaxPanel];
         int pivot_cols[kMaxPanel];
         int k;
-        int err;  // the device error word as of the panel's end
+        int err;       // the device error word as of the panel's end
+        int block_ok;  // the top-block path settled the panel
         unsigned bar[2];
     };
     const size_t scratch_bytes = (sizeof(Scratch) + 255) / 256 * 256;
     const size_t cand_bytes = sizeof(uint32_t) * 2 * static_cast<size_t>(grid_cap) * kMaxPanel;
     const size_t perm_bytes = (sizeof(int) * static_cast<size_t>(m) + 255) / 256 * 256;
+    const size_t uinv_bytes = 2 * sizeof(uint32_t) * kMaxPanel * kMaxPanel;  // L^-1 - I, B^-1
     uint8_t* base = static_cast<uint8_t*>(
-        ctx->ws.get(kSlotElim0, 2 * (scratch_bytes + cand_bytes) + 2 * perm_bytes + 256));
+        ctx->ws.get(kSlotElim0, 2 * (scratch_bytes + cand_bytes) + 2 * perm_bytes + 2 * uinv_bytes + 256));
+    // the L21 / W slot at its largest (every panel's rows x pivots fits), so no panel regrows it
+    ctx->ws.get(kSlotElim2, sizeof(uint32_t) * static_cast<size_t>(m) * bw);
     Scratch* d_sb[2] = {reinterpret_cast<Scratch*>(base), reinterpret_cast<Scratch*>(base + scratch_bytes)};
     uint32_t* d_candb[2] = {reinterpret_cast<uint32_t*>(base + 2 * scratch_bytes),
                             reinterpret_cast<uint32_t*>(base + 2 * scratch_bytes + cand_bytes)};
     int* d_permb[2] = {reinterpret_cast<int*>(base + 2 * (scratch_bytes + cand_bytes)),
                        reinterpret_cast<int*>(base + 2 * (scratch_bytes + cand_bytes) + perm_bytes)};
+    uint32_t* d_uinvb[2] = {reinterpret_cast<uint32_t*>(base + 2 * (scratch_bytes + cand_bytes + perm_bytes)),
+                            reinterpret_cast<uint32_t*>(base + 2 * (scratch_bytes + cand_bytes + perm_bytes) + uinv_bytes)};
     HME_CUDA(cudaMemsetAsync(d_sb[0]->bar, 0, sizeof(unsigned) * 2, ctx->stream));
     HME_CUDA(cudaMemsetAsync(d_sb[1]->bar, 0, sizeof(unsigned) * 2, ctx->stream));
     // pinned copies of the two scratch sets (the host reads a panel's pivots without waiting for
@@ -1023,6 +1395,9 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
 
     // The panel [c0, c0 + w) of the active rows [r0, m) on `st`: its pivots and the error word
     // land in h_sb[par] and ev_panel[par] is recorded.  Returns the cluster size (0: grid kernel).
+    // the top-block path: in automatic mode, over a field
+    const bool use_block = opt.panel_kernel == 0 && rg.k == 1;
+    bool block_tried[2] = {false, false};
     auto launch_panel = [&](int c0, int w, int r0, int par, cudaStream_t st) -> int {
         Scratch* d_s = d_sb[par];
         const cudaStream_t saved = ctx->stream;
@@ -1044,6 +1419,44 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         pa.bar = d_s->bar;
         pa.err = ctx->d_err;
         const int rows = m - r0;
+        // the top-block path first (fields only: a ring pivot needs the minimal valuation over all
+        // rows); the searching kernel below runs only when it did not settle the panel
+        block_tried[par] = use_block;
+        if (use_block) {
+            const int nb = std::min(w, rows);
+            BlockArgs ba{};
+            ba.A = A;
+            ba.ld = ld;
+            ba.m = m;
+            ba.r0 = r0;
+            ba.c0 = c0;
+            ba.w = w;
+            ba.R = rg;
+            ba.pivot_rows = d_s->pivot_rows;
+            ba.pivot_cols = d_s->pivot_cols;
+            ba.k_out = &d_s->k;
+            ba.ok = &d_s->block_ok;
+            ba.linv = d_uinvb[par];
+            ba.binv = d_uinvb[par] + kMaxPanel * kMaxPanel;
+            ba.err = ctx->d_err;
+            const size_t bsm = block_smem_bytes(nb, w);
+            auto launch_block = [&](auto kern) {
+                HME_TIMED(ctx, "panel_block", kern<<<1, kBlockThreads, bsm, st>>>(ba));
+            };
+            const bool w64 = w <= 64;
+            if (rg.ell == 2) {
+                if (w64) launch_block(panel_block_kernel<kArithPow2, 64>);
+                else launch_block(panel_block_kernel<kArithPow2, 128>);
+            } else if (p < (1u << 31)) {
+                if (w64) launch_block(panel_block_kernel<kArithMont31, 64>);
+                else launch_block(panel_block_kernel<kArithMont31, 128>);
+            } else {
+                if (w64) launch_block(panel_block_kernel<kArithMont32, 64>);
+                else launch_block(panel_block_kernel<kArithMont32, 128>);
+            }
+            HME_CUDA(cudaGetLastError());
+            pa.skip = &d_s->block_ok;
+        }
         const int cs = cluster_size(rows, w);
         HME_REQUIRE(opt.panel_kernel < 2 || cs > 0, "elim: the panel does not fit one cluster");
         if (cs > 0) {
@@ -1112,14 +1525,19 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         HME_CUDA(cudaEventSynchronize(ev_panel[par]));
         const Scratch& h_s = h_sb[par];
         if (h_s.err != 0) check_device_error(ctx);  // reports the timeout (and clears the word)
+        if (block_tried[par] && h_s.block_ok) ++ctx->elim_block_panels;
+        else ++ctx->elim_search_panels;
         const int k = h_s.k;
         if (k == 0) continue;  // no pivot in the panel: nothing moved, the next panel starts at r0
         for (int t = 0; t < k; ++t) pivots.push_back(h_s.pivot_cols[t]);
 
-        // (2) pivot rows first, in pivot order, the other active rows after them in order
+        // (2) pivot rows first, in pivot order, the other active rows after them in order; the
+        // identity when the pivots are rows r0 .. r0+k-1 in order (then nothing moves)
         const int rows = m - r0;
-        perm_host.assign(rows, 0);
-        {
+        bool identity = true;
+        for (int t = 0; t < k && identity; ++t) identity = h_s.pivot_rows[t] == r0 + t;
+        if (!identity) {
+            perm_host.assign(rows, 0);
             std::vector<char> is_piv(rows, 0);
             for (int t = 0; t < k; ++t) {
                 perm_host[t] = h_s.pivot_rows[t];
@@ -1128,19 +1546,23 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             int q = k;
             for (int i = 0; i < rows; ++i)
                 if (!is_piv[i]) perm_host[q++] = r0 + i;
-            // permutation parity: inversions of the sequence (rows relative to r0)
+            // permutation parity: the sequence is the pivot rows p_0 .. p_k-1 (relative to r0), then
+            // the other rows ascending, so its inversions are the pivot pairs out of order plus, per
+            // pivot p_t, the other rows below it (p_t minus the pivots below it): O(k^2), not O(rows)
             long long inv = 0;
-            std::vector<int> bit(rows + 1, 0);
-            for (int t = rows - 1; t >= 0; --t) {
-                int x = perm_host[t] - r0 + 1;
-                for (int y = x - 1; y > 0; y -= y & -y) inv += bit[y];
-                for (int y = x; y <= rows; y += y & -y) bit[y] += 1;
+            for (int t = 0; t < k; ++t) {
+                const int pt = h_s.pivot_rows[t] - r0;
+                int below_piv = 0;
+                for (int u = 0; u < k; ++u) {
+                    const int pu = h_s.pivot_rows[u] - r0;
+                    if (pu < pt) {
+                        ++below_piv;
+                        if (u > t) ++inv;  // p_t before p_u in the sequence, p_t > p_u
+                    }
+                }
+                inv += pt - below_piv;
             }
             if (inv & 1) res.sign_negative = !res.sign_negative;
-        }
-        bool identity = true;
-        for (int i = 0; i < rows && identity; ++i) identity = perm_host[i] == r0 + i;
-        if (!identity) {
             // pinned by parity: the copy of the panel two steps back has long completed (the host
             // waited for this panel, which follows that panel's update on the main stream)
             std::memcpy(h_permb[par], perm_host.data(), sizeof(int) * rows);
@@ -1152,8 +1574,36 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         const int* d_pcols = d_sb[par]->pivot_cols;
         // the update of columns [ca, cb): row permutation (from c0 on), U12 = L11^-1 A12, A22 -= L21 U12
         uint32_t* L21 = nullptr;
+        const bool blk = block_tried[par] && h_s.block_ok;
+        uint32_t* Wf = nullptr;
         auto update = [&](int ca, int cb, int sm_cap) {
             if (cb <= ca) return;
+            if (blk) {
+                // settled by the top block (no row moved): [A12; A22] += W A12, W = [L^-1 - I; -A21 B^-1],
+                // on a tensor-core variant (it reads A12 through its limb planes, so C may alias it)
+                const int ua = std::max(ca, c1);
+                if (cb <= ua) return;
+                if (!Wf) {
+                    Wf = static_cast<uint32_t*>(ctx->ws.get(kSlotElim2, sizeof(uint32_t) * static_cast<size_t>(rows) * k));
+                    const int g = (rows + kWRows - 1) / kWRows;
+                    const size_t wsm = sizeof(uint32_t) * (static_cast<size_t>(k) * k + static_cast<size_t>(kWRows) * k);
+                    const uint32_t* linv = d_uinvb[par];
+                    const uint32_t* binv = d_uinvb[par] + kMaxPanel * kMaxPanel;
+                    if (k <= 64)
+                        HME_TIMED(ctx, "panel_w", panel_w_kernel<64><<<g, 256, wsm, s_main>>>(
+                                                      A, ld, r0, m, c0, k, linv, binv, p, mp.barrett, Wf));
+                    else
+                        HME_TIMED(ctx, "panel_w", panel_w_kernel<128><<<g, 256, wsm, s_main>>>(
+                                                      A, ld, r0, m, c0, k, linv, binv, p, mp.barrett, Wf));
+                    HME_CUDA(cudaGetLastError());
+                }
+                ctx->gemm_sm_cap = sm_cap;
+                uint32_t* C12 = A + static_cast<size_t>(r0) * ld + ua;
+                gemm_u32_variant(ctx, mp, rows, cb - ua, k, Wf, k, C12, ld, C12, ld, HME_ADD,
+                                 gemm_default_variant(ctx, mp, rows, cb - ua));
+                ctx->gemm_sm_cap = 0;
+                return;
+            }
             if (!identity) {
                 const int cols = cb - ca;
                 uint32_t* tmp = static_cast<uint32_t*>(ctx->ws.get(kSlotElim1, sizeof(uint32_t) * static_cast<size_t>(rows) * (n - c0)));

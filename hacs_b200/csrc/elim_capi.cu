@@ -138,6 +138,14 @@ int hme_ctx_set_panel_kernel(hme_ctx* ctx, int mode) {
     });
 }
 
+int hme_ctx_elim_panel_stats(const hme_ctx* ctx, uint64_t* block_panels, uint64_t* search_panels) {
+    return guard([&] {
+        HME_REQUIRE(ctx != nullptr && block_panels != nullptr && search_panels != nullptr, "null argument");
+        *block_panels = ctx->elim_block_panels;
+        *search_panels = ctx->elim_search_panels;
+    });
+}
+
 int hme_ctx_set_elim_lookahead(hme_ctx* ctx, int on) {
     return guard([&] {
         HME_REQUIRE(ctx != nullptr, "null context");

@@ -140,6 +140,8 @@ struct hme_ctx {
     void* elim_pinned = nullptr;         // elimination: pinned copies of the panel scratch, permutations
     size_t elim_pinned_bytes = 0;
     std::vector<cudaEvent_t> elim_ev;    // elimination: lookahead events
+    uint64_t elim_block_panels = 0;      // field panels settled by the top-block path
+    uint64_t elim_search_panels = 0;     // panels factored by a searching kernel
 };
 
 // Bracket one kernel launch with timing events when the context's timer is on.

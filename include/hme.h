@@ -243,8 +243,11 @@ HME_API int hme_canonicalise_u64_dev(hme_ctx *ctx, uint64_t p, uint32_t rows, ui
  *   kernel, cap on its grid, block of the backward substitution (0 = default).
  *   Tuning only: no option changes a value.
  * hme_ctx_set_panel_kernel: which kernel factors the LU panels: 0 automatic
- *   (the thread-block-cluster kernel whenever the panel's active rows fit the
- *   shared memory of one cluster, else the cooperative grid kernel), 1 always
+ *   (over a field, the top-block path first: when the panel's top rows factor
+ *   with non-zero diagonal entries they are its pivots and no search runs;
+ *   otherwise, and over Z/ell^k, the thread-block-cluster kernel whenever the
+ *   panel's active rows fit the shared memory of one cluster, else the
+ *   cooperative grid kernel), 1 always
  *   the grid kernel, 2 the cluster kernel (HME_EINVAL from a factorisation
  *   whose panel does not fit), 3 the cluster kernel with 1024 threads per CTA
  *   (2 uses 512 while a CTA holds at most 512 rows).  Tuning only: every mode
@@ -271,6 +274,12 @@ HME_API int hme_ctx_set_elim_options(hme_ctx *ctx, int panel, int rows_per_cta, 
  * whole update.  Tuning only: no setting changes a value. */
 HME_API int hme_ctx_set_elim_lookahead(hme_ctx *ctx, int on);
 HME_API int hme_ctx_set_panel_kernel(hme_ctx *ctx, int mode);
+/* hme_ctx_elim_panel_stats: panels of this context's eliminations so far that
+ * the top-block path settled (mode 0 over a field: the nb x w top block of the
+ * panel factors with non-zero diagonal entries, so the pivots are its rows in
+ * order and the rows below take x U^-1), and panels that a searching kernel
+ * factored. */
+HME_API int hme_ctx_elim_panel_stats(const hme_ctx *ctx, uint64_t *block_panels, uint64_t *search_panels);
 
 /* ---- Howell and Smith forms over Z/ell^k (ell prime, ell^k < 2^32) ----------
  * Input canonical in [0, ell^k) (else HME_EINVAL, the reference's entry check).

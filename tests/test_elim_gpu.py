@@ -205,3 +205,62 @@ def test_panel_kernels_agree_ring(engine, ell, k):
             assert np.array_equal(engine.smith(ell, k, A), want_s), (ell, k, mode)
     finally:
         engine.set_panel_kernel(0)
+
+
+@pytest.mark.parametrize("p", [2, 3, 65521, 2147483629, 4294967291])
+def test_top_block_path(engine, p):
+    """Over a field, a panel whose top rows factor with non-zero diagonal
+    entries is settled without a search (its pivots are those rows in order,
+    the rows below take x U^-1); a zero on that diagonal sends the panel to the
+    searching kernel.  Both kinds of panel, at several panel widths, give the
+    oracle's RREF and pivots, and the context's counters see both paths."""
+    rng = np.random.default_rng(p % 1013)
+    b0, s0 = engine.elim_panel_stats()
+    cases = []
+    cases.append(_rand(rng, (300, 300), p))                 # generic: every panel settled by its top block
+    cases.append(_ranked(rng, 260, 300, 200, p))            # rank-deficient: the last panels search
+    A = _rand(rng, (200, 190), p)
+    A[4, :] = A[2, :]                                       # step 4 of panel 0 meets a zero: search
+    A[0, 0] = 0                                             # and the very first entry is zero
+    cases.append(A)
+    A = _rand(rng, (150, 400), p)
+    A[70:90, 64:128] = 0                                    # a zero block inside panel 1's top rows
+    cases.append(A)
+    cases.append(_rand(rng, (40, 300), p))                  # fewer active rows than the panel width
+    try:
+        for panel in (0, 8, 33, 100, 128):
+            engine.set_elim_options(panel, 0, 0, 0)
+            for A in cases:
+                R1, p1 = engine.rref(p, A)
+                R2, p2 = O.rref(p, A)
+                assert np.array_equal(p1, p2), (p, A.shape, panel)
+                assert np.array_equal(R1, R2), (p, A.shape, panel)
+            n = 97
+            M = _rand(rng, (n, n), p)
+            assert engine.det(p, M) == O.det(p, M), (p, panel)
+    finally:
+        engine.set_elim_options()
+    b1, s1 = engine.elim_panel_stats()
+    assert b1 > b0 and s1 > s0, (b0, b1, s0, s1)
+
+
+def test_top_block_path_ring_and_forced_modes(engine):
+    """The ring forms (minimal-valuation pivots) and the forced kernel modes never
+    take the top-block path."""
+    rng = np.random.default_rng(5)
+    A = rng.integers(0, 2 ** 16, (200, 180), dtype=np.uint64).astype(np.uint32)
+    b0, _ = engine.elim_panel_stats()
+    H, piv, pv = engine.howell(2, 16, A)
+    want = O.howell(2, 16, A)
+    assert np.array_equal(H, want[0]) and np.array_equal(piv, want[1])
+    try:
+        for mode in (1, 2, 3):
+            engine.set_panel_kernel(mode)
+            B = _rand(rng, (150, 150), 65521)
+            R1, p1 = engine.rref(65521, B)
+            R2, p2 = O.rref(65521, B)
+            assert np.array_equal(R1, R2) and np.array_equal(p1, p2)
+    finally:
+        engine.set_panel_kernel(0)
+    b1, _ = engine.elim_panel_stats()
+    assert b1 == b0
