@@ -695,23 +695,31 @@ struct BlockArgs {
     int* pivot_cols;  // [w] out
     int* k_out;       // out
     int* ok;          // out: 1 when the top block settled the panel, else 0
-    uint32_t* linv;   // out: L^-1 - I (nb x nb, row-major)
-    uint32_t* binv;   // out: B^-1 (w x w, row-major) when rows remain below the block
+    uint32_t* lm;     // out: L's strict lower part, Montgomery form (nb x nb, row-major, zero elsewhere)
+    uint32_t* um;     // out: U's strict upper part, Montgomery form (nb x nb, row-major, zero elsewhere)
+    uint32_t* dm;     // out: U's inverse diagonal, Montgomery form (nb)
     int* err;         // device error word (a wavefront wait that runs out)
 };
 constexpr int kBlockThreads = 1024;
 
-__host__ __device__ constexpr int block_stride(int nb, int w) { return (w + nb) | 1; }
+__host__ __device__ constexpr int block_stride(int w) { return w | 1; }
 __host__ __device__ constexpr size_t block_smem_bytes(int nb, int w) {
-    return sizeof(uint32_t) * static_cast<size_t>(nb) * block_stride(nb, w);  // T = [B | I], nb x (w + nb)
+    return sizeof(uint32_t) * static_cast<size_t>(nb) * block_stride(w);  // T = B, nb x w
 }
 
-// x * y for the back substitution: y in Montgomery form (y 2^32 mod q) for odd
-// q, so one Montgomery reduction gives x y mod q; plain for q = 2^k.
+// x * y with y in the Montgomery form (y 2^32 mod q) for odd q: one Montgomery
+// reduction gives x y mod q; plain products for q = 2^k.
 template <int ARITH>
 __device__ __forceinline__ uint32_t mul_mform(uint32_t x, uint32_t ym, const Ring& R) {
     if constexpr (ARITH == kArithPow2) return (x * ym) & (R.q - 1u);
     else return mont_mul(x, ym, R.q, R.mont_qinv);
+}
+
+// x -> its Montgomery form x 2^32 mod q (unchanged for q = 2^k)
+template <int ARITH>
+__device__ __forceinline__ uint32_t to_mform(uint32_t x, const Ring& R) {
+    if constexpr (ARITH == kArithPow2) return x;
+    else return mont_mul(x, R.mont_r2, R.q, R.mont_qinv);
 }
 
 // Row flags of a wavefront inside one CTA: one mbarrier per row, expecting
@@ -728,42 +736,27 @@ __device__ __forceinline__ bool wait_row(uint64_t* bars, int row, volatile int* 
     return __all_sync(0xffffffffu, ok) != 0;
 }
 
-// One CTA: the top block's elimination as two row wavefronts (warps over rows,
-// each row in the registers of its warp, lanes over columns).
-// (1) Forward, on [B | I] without a search (row t pivots at step t): row i
-// applies the fraction-free updates of pivot rows 0 .. i-1 in order, each as
-// soon as that row is published -- the same operations in the same order as a
-// step-by-step elimination, so the same values -- then checks its own pivot
-// and is published.  Rows leave the multipliers, U and, in the right half,
-// L^-1, each scaled by the unit its steps accumulated; the classical values
-// are restored as in the cluster kernel.  Row i's right half is zero beyond
-// column w + i, and pivot row s's beyond w + s, so row i touches columns
-// s+1 .. w+s and w+i at step s.
-// (2) With rows below: B^-1 = U^-1 L^-1 by a backward wavefront on [U | L^-1]
-// (rows scaled by the inverse diagonal, U's part kept in Montgomery form):
-// row r subtracts U'[r][t] X[t] for t = w-1 .. r+1 as those rows are published.
-// WMAX (64 or 128) bounds w.
+// One CTA: the LU of the top block as a row wavefront (warps over rows, each
+// row in the registers of its warp, lanes over columns): row i applies the
+// fraction-free updates of pivot rows 0 .. i-1 in order, each as soon as that
+// row is published -- the operations of a step-by-step elimination in the same
+// order, so the same values -- then checks its pivot (column i) and is
+// published.  The classical values are restored as in the cluster kernel and
+// written back; L, U and U's inverse diagonal go out in Montgomery form for
+// the row solves of panel_w_kernel.  WMAX (64 or 128) bounds w.
 template <int ARITH, int WMAX>
 __global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockArgs a) {
     extern __shared__ __align__(16) uint32_t s_blk[];
-    __shared__ uint32_t s_w[kMaxPanel], s_inv[kMaxPanel], s_sinv[kMaxPanel + 1], s_dinv[kMaxPanel],
-        s_dinvm[kMaxPanel];
-    __shared__ __align__(8) uint64_t s_fwd[kMaxPanel], s_bwd[kMaxPanel];  // row mbarriers
+    __shared__ uint32_t s_w[kMaxPanel], s_inv[kMaxPanel], s_sinv[kMaxPanel + 1];
+    __shared__ __align__(8) uint64_t s_fwd[kMaxPanel];  // row mbarriers
     __shared__ int s_fail, s_abort;
-    const int w = a.w, nb = min(w, a.m - a.r0), ts = block_stride(nb, w), wide = w + nb;
-    uint32_t* T = s_blk;  // [nb][ts]: [B | I]; row i written once it is final
+    const int w = a.w, nb = min(w, a.m - a.r0), ts = block_stride(w);
+    uint32_t* T = s_blk;  // [nb][ts]: row i written once it is final
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = kBlockThreads / 32;
-    constexpr int CI = 2 * WMAX / 32;  // column slots of [B | I] per lane
-    constexpr int CW = WMAX / 32;      // slots of the pivot index
-    const uint32_t one = 1u % a.R.q;
-    uint64_t* fwd = s_fwd;
-    uint64_t* bwd = s_bwd;
+    constexpr int CW = WMAX / 32;  // column slots per lane
     volatile int* abort_flag = &s_abort;
-    for (int i = tid; i < kMaxPanel; i += kBlockThreads) {
-        mbar_init(&s_fwd[i], 32);
-        mbar_init(&s_bwd[i], 32);
-    }
+    for (int i = tid; i < kMaxPanel; i += kBlockThreads) mbar_init(&s_fwd[i], 32);
     if (tid == 0) {
         s_fail = 0;
         s_abort = 0;
@@ -771,12 +764,12 @@ __global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockA
     fence_mbar_init();
     __syncthreads();
     for (int i = warp; i < nb; i += NW) {
-        uint32_t y[CI];
+        uint32_t y[CW];
         const uint32_t* src = a.A + static_cast<size_t>(a.r0 + i) * a.ld + a.c0;
 #pragma unroll
-        for (int c = 0; c < CI; ++c) {
+        for (int c = 0; c < CW; ++c) {
             const int j = lane + 32 * c;
-            y[c] = j < w ? src[j] : (j == w + i ? one : 0u);
+            y[c] = j < w ? src[j] : 0u;
         }
         bool live = true;
 #pragma unroll
@@ -787,30 +780,28 @@ __global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockA
                     live = false;  // leaves both loops: this row's steps are done
                     break;
                 }
-                if (!wait_row(fwd, s, abort_flag, a.err)) break;
+                if (!wait_row(s_fwd, s, abort_flag, a.err)) break;
                 const uint32_t xn = ff_negate<ARITH>(__shfl_sync(0xffffffffu, y[sc], sl), a.R);
                 const uint32_t ws = T[s * ts + s];
 #pragma unroll
-                for (int c = 0; c < CI; ++c) {
+                for (int c = 0; c < CW; ++c) {
                     const int j = lane + 32 * c;
-                    if (j > s && (j <= w + s || j == w + i) && j < wide)
-                        y[c] = ff_update<ARITH>(ws, y[c], xn, T[s * ts + j], a.R);
+                    if (32 * c + 31 > s && j > s && j < w) y[c] = ff_update<ARITH>(ws, y[c], xn, T[s * ts + j], a.R);
                 }
             }
         }
-        // the pivot of step i: column i of this row
-        uint32_t pv = y[0];
+        uint32_t pv = y[0];  // the pivot of step i: column i of this row
 #pragma unroll
         for (int c = 1; c < CW; ++c)
             if ((i >> 5) == c) pv = y[c];
         pv = __shfl_sync(0xffffffffu, pv, i & 31);
         if (pv == 0 && lane == 0) s_fail = 1;
 #pragma unroll
-        for (int c = 0; c < CI; ++c) {
+        for (int c = 0; c < CW; ++c) {
             const int j = lane + 32 * c;
-            if (j < wide) T[i * ts + j] = y[c];
+            if (j < w) T[i * ts + j] = y[c];
         }
-        publish_row(fwd, i);
+        publish_row(s_fwd, i);
     }
     __syncthreads();
     if (s_fail || s_abort) {
@@ -820,192 +811,167 @@ __global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockA
     if (tid < nb) s_w[tid] = T[tid * ts + tid];
     __syncthreads();
     ff_scale_tables<ARITH>(nb, s_w, s_inv, s_sinv, a.R);
-    // row r froze at step r: a multiplier of step j < r takes w_j^-1, the rest (U, L^-1) S_r^-1
-    for (int r = warp; r < nb; r += NW)
-        for (int j = lane; j < wide; j += 32) {
-            const uint32_t f = j < r ? s_inv[j] : s_sinv[r];
-            T[r * ts + j] = mod_mul(T[r * ts + j], f, a.R.q, a.R.barrett);
-        }
-    __syncthreads();
+    // row r froze at step r: a multiplier of step j < r takes w_j^-1, the rest (U) S_r^-1
     for (int r = warp; r < nb; r += NW) {
         uint32_t* dst = a.A + static_cast<size_t>(a.r0 + r) * a.ld + a.c0;
-        for (int j = lane; j < w; j += 32) dst[j] = T[r * ts + j];
-        for (int j = lane; j < nb; j += 32) {
-            const uint32_t v = T[r * ts + w + j];
-            a.linv[static_cast<size_t>(r) * nb + j] = j == r ? mod_sub(v, one, a.R.q) : v;
+        for (int j = lane; j < w; j += 32) {
+            const uint32_t v = mod_mul(T[r * ts + j], j < r ? s_inv[j] : s_sinv[r], a.R.q, a.R.barrett);
+            dst[j] = v;
+            if (j < nb) {
+                a.lm[static_cast<size_t>(r) * nb + j] = j < r ? to_mform<ARITH>(v, a.R) : 0u;
+                a.um[static_cast<size_t>(r) * nb + j] = j > r ? to_mform<ARITH>(v, a.R) : 0u;
+            }
+            if (j == r) T[r * ts + r] = v;  // the classical diagonal, for its inverse below
         }
     }
     if (tid < nb) {
         a.pivot_rows[tid] = a.r0 + tid;
         a.pivot_cols[tid] = a.c0 + tid;
     }
+    __syncthreads();
+    if (tid < nb) a.dm[tid] = to_mform<ARITH>(unit_inverse(T[tid * ts + tid], a.R), a.R);
     if (tid == 0) {
         *a.k_out = nb;
         *a.ok = 1;
     }
-    if (nb < w || a.m - a.r0 == nb) return;  // no row below the block: B^-1 is not needed
-    // ---- B^-1: [U | L^-1] rows times the inverse diagonal (U's part into Montgomery form)
-    if (tid < w) {
-        const uint32_t d = unit_inverse(T[tid * ts + tid], a.R);
-        s_dinv[tid] = d;
-        const uint32_t r32 = ARITH == kArithPow2 ? one : mont_mul(a.R.mont_r2, 1u, a.R.q, a.R.mont_qinv);  // 2^32 mod q
-        s_dinvm[tid] = mod_mul(d, r32, a.R.q, a.R.barrett);
-    }
-    __syncthreads();
-    for (int r = warp; r < w; r += NW)
-        for (int j = r + 1 + lane; j < wide; j += 32)
-            T[r * ts + j] = mod_mul(T[r * ts + j], j < w ? s_dinvm[r] : s_dinv[r], a.R.q, a.R.barrett);
-    __syncthreads();
-    // backward wavefront: warp k takes rows w-1-k, w-1-k-32, ...
-    for (int r = w - 1 - warp; r >= 0; r -= NW) {
-        uint32_t x[CW];
-#pragma unroll
-        for (int c = 0; c < CW; ++c) {
-            const int j = lane + 32 * c;
-            x[c] = j < w ? T[r * ts + w + j] : 0u;
-        }
-        for (int t = w - 1; t > r; --t) {
-            if (!wait_row(bwd, t, abort_flag, a.err)) break;
-            const uint32_t um = T[r * ts + t];
-            if (um == 0) continue;
-#pragma unroll
-            for (int c = 0; c < CW; ++c) {
-                const int j = lane + 32 * c;
-                if (j < w) x[c] = mod_sub(x[c], mul_mform<ARITH>(T[t * ts + w + j], um, a.R), a.R.q);
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < CW; ++c) {
-            const int j = lane + 32 * c;
-            if (j < w) T[r * ts + w + j] = x[c];
-        }
-        publish_row(bwd, r);
-    }
-    __syncthreads();
-    if (s_abort) {  // the device error word is set; the host reports it
-        if (tid == 0) *a.ok = 0;
-        return;
-    }
-    for (int r = warp; r < w; r += NW)
-        for (int j = lane; j < w; j += 32) a.binv[static_cast<size_t>(r) * w + j] = T[r * ts + w + j];
 }
 
 // The left factor of the fused update, W ((m - r0) x nb, row-major, ld nb):
-// rows t < nb are L^-1 - I; a row x below the block becomes -x B^-1 (x = the
-// row's panel columns).  A warp takes four rows at once, lanes over output
-// columns; each dot product runs exactly in a 96-bit carry chain (nb <= 128
-// products below 2^64) and is reduced once.
+// row t < nb is e_t L^-1 - e_t; a row x below the block becomes -x B^-1 =
+// -(x U^-1) L^-1.  Both by substitution on the row, lanes over columns: the
+// forward solve y U = x (y_s = (x_s - sum_{t<s} y_t U[t][s]) / U[s][s]) and
+// the backward solve z L = y (z_i = y_i - sum_{t>i} z_t L[t][i], unit
+// diagonal).  A warp carries four rows at once; L, U and U's inverse diagonal
+// come in Montgomery form, so each product is one Montgomery reduction.
 constexpr int kWRows = 32;
 constexpr int kWRowsPerWarp = 4;
 
-__device__ __forceinline__ void mac96(uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t x, uint32_t y) {
-    asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
-        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
-        "addc.u32 %2, %2, 0;"
-        : "+r"(a0), "+r"(a1), "+r"(a2)
-        : "r"(x), "r"(y));
-}
-
-template <int WMAX>
+template <int ARITH, int WMAX>
 __global__ void __launch_bounds__(256) panel_w_kernel(const uint32_t* __restrict__ A, uint64_t ld, int r0, int m,
-                                                      int c0, int nb, const uint32_t* __restrict__ linv,
-                                                      const uint32_t* __restrict__ binv, uint32_t q,
-                                                      uint64_t barrett, uint32_t* __restrict__ W) {
+                                                      int c0, int nb, const uint32_t* __restrict__ lm,
+                                                      const uint32_t* __restrict__ um,
+                                                      const uint32_t* __restrict__ dm, const Ring R,
+                                                      uint32_t* __restrict__ W) {
     extern __shared__ __align__(16) uint32_t s_wk[];
+    uint32_t* Ls = s_wk;                                          // [nb][nb]
+    uint32_t* Us = s_wk + ((static_cast<size_t>(nb) * nb + 3) & ~size_t(3));  // [nb][nb], 16-byte aligned
+    __shared__ uint32_t s_dm[kMaxPanel];
     const int rb = r0 + static_cast<int>(blockIdx.x) * kWRows;  // first row of this CTA
     const int nr = min(kWRows, m - rb);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = 256 / 32;
     static_assert(NW * kWRowsPerWarp == kWRows, "one pass of the warps covers the CTA's rows");
-    // the top rows: L^-1 - I
-    for (int r = warp; r < nr; r += NW) {
-        const int row = rb + r;
-        if (row >= r0 + nb) break;
-        for (int j = lane; j < nb; j += 32)
-            W[static_cast<size_t>(row - r0) * nb + j] = linv[static_cast<size_t>(row - r0) * nb + j];
-    }
-    if (rb + nr <= r0 + nb) return;  // no row below the block in this CTA (uniform)
-    uint32_t* Bi = s_wk;                                   // [nb][nb]
-    uint32_t* Xr = s_wk + static_cast<size_t>(nb) * nb;    // [kWRows][nb]
     constexpr int CS = WMAX / 32;
+    const bool any_below = rb + nr > r0 + nb;  // uniform: U is needed
     {
-        // B^-1 in 16-byte pieces (its buffer is 16-byte aligned), all loads of a thread in flight at once
+        // L (and U when rows below) in 16-byte pieces (the buffers are 16-byte aligned)
         const int n4 = (nb * nb) >> 2;
-        const uint4* b4 = reinterpret_cast<const uint4*>(binv);
-        uint4* d4 = reinterpret_cast<uint4*>(Bi);
-        constexpr int P = 4;
-        for (int base = 0; base < n4; base += 256 * P) {
-            uint4 v[P];
+        for (int base = 0; base < n4; base += 256 * 4) {
+            uint4 v[4], u[4];
 #pragma unroll
-            for (int e = 0; e < P; ++e) {
+            for (int e = 0; e < 4; ++e) {
                 const int idx = base + tid + 256 * e;
-                if (idx < n4) v[e] = b4[idx];
+                if (idx < n4) {
+                    v[e] = reinterpret_cast<const uint4*>(lm)[idx];
+                    if (any_below) u[e] = reinterpret_cast<const uint4*>(um)[idx];
+                }
             }
 #pragma unroll
-            for (int e = 0; e < P; ++e) {
+            for (int e = 0; e < 4; ++e) {
                 const int idx = base + tid + 256 * e;
-                if (idx < n4) d4[idx] = v[e];
+                if (idx < n4) {
+                    reinterpret_cast<uint4*>(Ls)[idx] = v[e];
+                    if (any_below) reinterpret_cast<uint4*>(Us)[idx] = u[e];
+                }
             }
         }
-        for (int idx = 4 * n4 + tid; idx < nb * nb; idx += 256) Bi[idx] = binv[idx];
-    }
-    {
-        // this warp's four rows (zero for top rows and rows past the end)
-        const int rl0 = warp * kWRowsPerWarp;
-        uint32_t v[kWRowsPerWarp][CS];
-#pragma unroll
-        for (int i = 0; i < kWRowsPerWarp; ++i) {
-            const int row = rb + rl0 + i;
-            const bool below = rl0 + i < nr && row >= r0 + nb;
-            const uint32_t* src = A + static_cast<size_t>(below ? row : r0) * ld + c0;
-#pragma unroll
-            for (int c = 0; c < CS; ++c) {
-                const int j = lane + 32 * c;
-                v[i][c] = below && j < nb ? src[j] : 0u;
-            }
+        for (int idx = 4 * n4 + tid; idx < nb * nb; idx += 256) {
+            Ls[idx] = lm[idx];
+            if (any_below) Us[idx] = um[idx];
         }
-#pragma unroll
-        for (int i = 0; i < kWRowsPerWarp; ++i)
-#pragma unroll
-            for (int c = 0; c < CS; ++c) {
-                const int j = lane + 32 * c;
-                if (j < nb) Xr[(rl0 + i) * nb + j] = v[i][c];
-            }
+        for (int t = tid; t < nb; t += 256) s_dm[t] = dm[t];
     }
-    __syncthreads();
-    uint32_t a0[kWRowsPerWarp][CS], a1[kWRowsPerWarp][CS], a2[kWRowsPerWarp][CS];
+    const int rl = warp * kWRowsPerWarp;  // this warp's rows: rb + rl .. rb + rl + 3
+    uint32_t a4[kWRowsPerWarp][CS];
 #pragma unroll
-    for (int i = 0; i < kWRowsPerWarp; ++i)
-#pragma unroll
-        for (int c = 0; c < CS; ++c) a0[i][c] = a1[i][c] = a2[i][c] = 0;
-    const int rl = warp * kWRowsPerWarp;  // this warp's rows: rl .. rl + 3 of the CTA
-    for (int t = 0; t < nb; ++t) {
-        uint32_t bt[CS];
+    for (int i = 0; i < kWRowsPerWarp; ++i) {
+        const int row = rb + rl + i;
+        const bool below = rl + i < nr && row >= r0 + nb;
+        const uint32_t* src = A + static_cast<size_t>(below ? row : r0) * ld + c0;
 #pragma unroll
         for (int c = 0; c < CS; ++c) {
             const int j = lane + 32 * c;
-            bt[c] = j < nb ? Bi[t * nb + j] : 0u;
+            a4[i][c] = below && j < nb ? src[j] : 0u;
         }
+    }
+    __syncthreads();
+    if (any_below) {
+        // forward solve y U = x: at step s, y_s = x_s / U[s][s] is final; columns j > s take -y_s U[s][j]
 #pragma unroll
-        for (int i = 0; i < kWRowsPerWarp; ++i) {
-            const uint32_t x = Xr[(rl + i) * nb + t];
+        for (int sc = 0; sc < CS; ++sc) {
+            for (int sl = 0; sl < 32; ++sl) {
+                const int s = 32 * sc + sl;
+                if (s >= nb) break;
+                const uint32_t ds = s_dm[s];
+                uint32_t ys[kWRowsPerWarp];
 #pragma unroll
-            for (int c = 0; c < CS; ++c) mac96(a0[i][c], a1[i][c], a2[i][c], x, bt[c]);
+                for (int i = 0; i < kWRowsPerWarp; ++i) {
+                    ys[i] = mul_mform<ARITH>(__shfl_sync(0xffffffffu, a4[i][sc], sl), ds, R);
+                    if (lane == sl) a4[i][sc] = ys[i];
+                }
+#pragma unroll
+                for (int c = sc; c < CS; ++c) {
+                    const int j = lane + 32 * c;
+                    const uint32_t u = j > s && j < nb ? Us[s * nb + j] : 0u;
+#pragma unroll
+                    for (int i = 0; i < kWRowsPerWarp; ++i)
+                        a4[i][c] = mod_sub(a4[i][c], mul_mform<ARITH>(ys[i], u, R), R.q);
+                }
+            }
+        }
+    }
+    // the top rows start the backward solve from e_t
+    const uint32_t one = 1u % R.q;
+#pragma unroll
+    for (int i = 0; i < kWRowsPerWarp; ++i) {
+        const int t = rb + rl + i - r0;
+        if (t < nb) {
+#pragma unroll
+            for (int c = 0; c < CS; ++c) a4[i][c] = lane + 32 * c == t ? one : 0u;
+        }
+    }
+    // backward solve z L = y: at step t (nb-1 down to 1), z_t = y_t is final; columns j < t take -z_t L[t][j]
+#pragma unroll
+    for (int sc = CS - 1; sc >= 0; --sc) {
+        for (int sl = 31; sl >= 0; --sl) {
+            const int t = 32 * sc + sl;
+            if (t >= nb || t == 0) continue;
+            uint32_t zt[kWRowsPerWarp];
+#pragma unroll
+            for (int i = 0; i < kWRowsPerWarp; ++i) zt[i] = __shfl_sync(0xffffffffu, a4[i][sc], sl);
+#pragma unroll
+            for (int c = 0; c <= sc; ++c) {
+                const int j = lane + 32 * c;
+                const uint32_t l = j < t ? Ls[t * nb + j] : 0u;
+#pragma unroll
+                for (int i = 0; i < kWRowsPerWarp; ++i)
+                    a4[i][c] = mod_sub(a4[i][c], mul_mform<ARITH>(zt[i], l, R), R.q);
+            }
         }
     }
 #pragma unroll
     for (int i = 0; i < kWRowsPerWarp; ++i) {
         const int row = rb + rl + i;
-        if (rl + i >= nr || row < r0 + nb) continue;
-        uint32_t* dst = W + static_cast<size_t>(row - r0) * nb;
+        if (rl + i >= nr) continue;
+        const int t = row - r0;
+        uint32_t* dst = W + static_cast<size_t>(t) * nb;
 #pragma unroll
         for (int c = 0; c < CS; ++c) {
             const int j = lane + 32 * c;
-            if (j < nb) {
-                const uint64_t h = reduce_u64((static_cast<uint64_t>(a2[i][c]) << 32) | a1[i][c], q, barrett);
-                const uint32_t v = static_cast<uint32_t>(reduce_u64((h << 32) | a0[i][c], q, barrett));
-                dst[j] = v == 0 ? 0u : q - v;
-            }
+            if (j >= nb) continue;
+            const uint32_t v = a4[i][c];
+            if (t < nb) dst[j] = j == t ? mod_sub(v, one, R.q) : v;  // e_t L^-1 - e_t
+            else dst[j] = v == 0 ? 0u : R.q - v;                     // -x B^-1
         }
     }
 }
@@ -1266,9 +1232,14 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
                                    reinterpret_cast<const void*>(panel_block_kernel<kArithMont31, 128>),
                                    reinterpret_cast<const void*>(panel_block_kernel<kArithMont32, 128>)})
                 HME_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bsm));
-            const int wsm = static_cast<int>(sizeof(uint32_t) * (kMaxPanel * kMaxPanel + kWRows * kMaxPanel));
-            HME_CUDA(cudaFuncSetAttribute(panel_w_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
-            HME_CUDA(cudaFuncSetAttribute(panel_w_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
+            const int wsm = static_cast<int>(2 * sizeof(uint32_t) * kMaxPanel * kMaxPanel);
+            for (const void* fn : {reinterpret_cast<const void*>(panel_w_kernel<kArithPow2, 64>),
+                                   reinterpret_cast<const void*>(panel_w_kernel<kArithMont31, 64>),
+                                   reinterpret_cast<const void*>(panel_w_kernel<kArithMont32, 64>),
+                                   reinterpret_cast<const void*>(panel_w_kernel<kArithPow2, 128>),
+                                   reinterpret_cast<const void*>(panel_w_kernel<kArithMont31, 128>),
+                                   reinterpret_cast<const void*>(panel_w_kernel<kArithMont32, 128>)})
+                HME_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
         }
         bool attrs_ok = true;
         for (const void* fn : {reinterpret_cast<const void*>(panel_cluster_kernel<kArithPow2, 512>),
@@ -1325,7 +1296,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     const size_t scratch_bytes = (sizeof(Scratch) + 255) / 256 * 256;
     const size_t cand_bytes = sizeof(uint32_t) * 2 * static_cast<size_t>(grid_cap) * kMaxPanel;
     const size_t perm_bytes = (sizeof(int) * static_cast<size_t>(m) + 255) / 256 * 256;
-    const size_t uinv_bytes = 2 * sizeof(uint32_t) * kMaxPanel * kMaxPanel;  // L^-1 - I, B^-1
+    const size_t uinv_bytes = sizeof(uint32_t) * (2 * kMaxPanel * kMaxPanel + kMaxPanel);  // L, U, U's inverse diagonal
     uint8_t* base = static_cast<uint8_t*>(
         ctx->ws.get(kSlotElim0, 2 * (scratch_bytes + cand_bytes) + 2 * perm_bytes + 2 * uinv_bytes + 256));
     // the L21 / W slot at its largest (every panel's rows x pivots fits), so no panel regrows it
@@ -1436,8 +1407,9 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             ba.pivot_cols = d_s->pivot_cols;
             ba.k_out = &d_s->k;
             ba.ok = &d_s->block_ok;
-            ba.linv = d_uinvb[par];
-            ba.binv = d_uinvb[par] + kMaxPanel * kMaxPanel;
+            ba.lm = d_uinvb[par];
+            ba.um = d_uinvb[par] + kMaxPanel * kMaxPanel;
+            ba.dm = d_uinvb[par] + 2 * kMaxPanel * kMaxPanel;
             ba.err = ctx->d_err;
             const size_t bsm = block_smem_bytes(nb, w);
             auto launch_block = [&](auto kern) {
@@ -1586,15 +1558,24 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
                 if (!Wf) {
                     Wf = static_cast<uint32_t*>(ctx->ws.get(kSlotElim2, sizeof(uint32_t) * static_cast<size_t>(rows) * k));
                     const int g = (rows + kWRows - 1) / kWRows;
-                    const size_t wsm = sizeof(uint32_t) * (static_cast<size_t>(k) * k + static_cast<size_t>(kWRows) * k);
-                    const uint32_t* linv = d_uinvb[par];
-                    const uint32_t* binv = d_uinvb[par] + kMaxPanel * kMaxPanel;
-                    if (k <= 64)
-                        HME_TIMED(ctx, "panel_w", panel_w_kernel<64><<<g, 256, wsm, s_main>>>(
-                                                      A, ld, r0, m, c0, k, linv, binv, p, mp.barrett, Wf));
-                    else
-                        HME_TIMED(ctx, "panel_w", panel_w_kernel<128><<<g, 256, wsm, s_main>>>(
-                                                      A, ld, r0, m, c0, k, linv, binv, p, mp.barrett, Wf));
+                    const size_t wsm = 2 * sizeof(uint32_t) * ((static_cast<size_t>(k) * k + 3) & ~size_t(3));
+                    const uint32_t* lmp = d_uinvb[par];
+                    const uint32_t* ump = d_uinvb[par] + kMaxPanel * kMaxPanel;
+                    const uint32_t* dmp = d_uinvb[par] + 2 * kMaxPanel * kMaxPanel;
+                    auto launch_w = [&](auto kern) {
+                        HME_TIMED(ctx, "panel_w", kern<<<g, 256, wsm, s_main>>>(A, ld, r0, m, c0, k, lmp, ump, dmp, rg, Wf));
+                    };
+                    const bool w64 = k <= 64;
+                    if (rg.ell == 2) {
+                        if (w64) launch_w(panel_w_kernel<kArithPow2, 64>);
+                        else launch_w(panel_w_kernel<kArithPow2, 128>);
+                    } else if (p < (1u << 31)) {
+                        if (w64) launch_w(panel_w_kernel<kArithMont31, 64>);
+                        else launch_w(panel_w_kernel<kArithMont31, 128>);
+                    } else {
+                        if (w64) launch_w(panel_w_kernel<kArithMont32, 64>);
+                        else launch_w(panel_w_kernel<kArithMont32, 128>);
+                    }
                     HME_CUDA(cudaGetLastError());
                 }
                 ctx->gemm_sm_cap = sm_cap;
