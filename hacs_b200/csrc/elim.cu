@@ -698,9 +698,8 @@ struct BlockArgs {
     uint32_t* lm;     // out: L's strict lower part, Montgomery form (nb x nb, row-major, zero elsewhere)
     uint32_t* um;     // out: U's strict upper part, Montgomery form (nb x nb, row-major, zero elsewhere)
     uint32_t* dm;     // out: U's inverse diagonal, Montgomery form (nb)
-    int* err;         // device error word (a wavefront wait that runs out)
 };
-constexpr int kBlockThreads = 1024;
+constexpr int kBlockThreads = 256;
 
 __host__ __device__ constexpr int block_stride(int w) { return w | 1; }
 __host__ __device__ constexpr size_t block_smem_bytes(int nb, int w) {
@@ -722,89 +721,69 @@ __device__ __forceinline__ uint32_t to_mform(uint32_t x, const Ring& R) {
     else return mont_mul(x, R.mont_r2, R.q, R.mont_qinv);
 }
 
-// Row flags of a wavefront inside one CTA: one mbarrier per row, expecting
-// the 32 arrivals of the warp that owns the row.  publish_row: every lane
-// arrives (release: its shared-memory stores of the row are visible to a
-// waiter).  wait_row: every lane waits for the phase (acquire), suspended in
-// hardware rather than spinning on issue slots, with the bounded wait of
-// mbar_wait: when it runs out the CTA's abort flag and the device error word
-// are set, every later wait returns at once, and it returns false.
-__device__ __forceinline__ void publish_row(uint64_t* bars, int row) { mbar_arrive(&bars[row]); }
-
-__device__ __forceinline__ bool wait_row(uint64_t* bars, int row, volatile int* abort, int* err) {
-    const bool ok = mbar_wait(&bars[row], 0, abort, err, DERR_WAIT_ROW);
-    return __all_sync(0xffffffffu, ok) != 0;
-}
-
-// One CTA: the LU of the top block as a row wavefront (warps over rows, each
-// row in the registers of its warp, lanes over columns): row i applies the
-// fraction-free updates of pivot rows 0 .. i-1 in order, each as soon as that
-// row is published -- the operations of a step-by-step elimination in the same
-// order, so the same values -- then checks its pivot (column i) and is
-// published.  The classical values are restored as in the cluster kernel and
-// written back; L, U and U's inverse diagonal go out in Montgomery form for
-// the row solves of panel_w_kernel.  WMAX (64 or 128) bounds w.
+// One CTA: the fraction-free LU of the top block without a search (row t
+// pivots at step t), one CTA barrier per step.  Step t touches only the
+// active block (rows t+1 .. nb-1, columns t+1 .. w-1): warps over rows, lanes
+// over columns, each row's operands loaded before its updates are computed.
+// The classical values are restored as in the cluster kernel and written
+// back; L, U and U's inverse diagonal go out in Montgomery form for the row
+// solves of panel_w_kernel.  WMAX (64 or 128) bounds w.
 template <int ARITH, int WMAX>
 __global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockArgs a) {
     extern __shared__ __align__(16) uint32_t s_blk[];
     __shared__ uint32_t s_w[kMaxPanel], s_inv[kMaxPanel], s_sinv[kMaxPanel + 1];
-    __shared__ __align__(8) uint64_t s_fwd[kMaxPanel];  // row mbarriers
-    __shared__ int s_fail, s_abort;
     const int w = a.w, nb = min(w, a.m - a.r0), ts = block_stride(w);
-    uint32_t* T = s_blk;  // [nb][ts]: row i written once it is final
+    uint32_t* T = s_blk;  // [nb][ts]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = kBlockThreads / 32;
     constexpr int CW = WMAX / 32;  // column slots per lane
-    volatile int* abort_flag = &s_abort;
-    for (int i = tid; i < kMaxPanel; i += kBlockThreads) mbar_init(&s_fwd[i], 32);
-    if (tid == 0) {
-        s_fail = 0;
-        s_abort = 0;
-    }
-    fence_mbar_init();
-    __syncthreads();
-    for (int i = warp; i < nb; i += NW) {
-        uint32_t y[CW];
-        const uint32_t* src = a.A + static_cast<size_t>(a.r0 + i) * a.ld + a.c0;
+    constexpr int RI = WMAX / NW;  // row slots per warp
+    for (int r = warp; r < nb; r += NW) {
+        const uint32_t* src = a.A + static_cast<size_t>(a.r0 + r) * a.ld + a.c0;
 #pragma unroll
         for (int c = 0; c < CW; ++c) {
             const int j = lane + 32 * c;
-            y[c] = j < w ? src[j] : 0u;
+            if (j < w) T[r * ts + j] = src[j];
         }
-        bool live = true;
+    }
+    __syncthreads();
+    bool fail = false;
+    for (int t = 0; t < nb; ++t) {
+        const uint32_t wt = T[t * ts + t];
+        if (wt == 0) {  // the same value in every thread: uniform
+            fail = true;
+            break;
+        }
+        if (tid == 0) s_w[t] = wt;
+        const int jb = t + 1;
+        uint32_t pr[CW];
 #pragma unroll
-        for (int sc = 0; sc < CW; ++sc) {
-            for (int sl = 0; sl < 32 && live; ++sl) {
-                const int s = 32 * sc + sl;
-                if (s >= i) {
-                    live = false;  // leaves both loops: this row's steps are done
-                    break;
-                }
-                if (!wait_row(s_fwd, s, abort_flag, a.err)) break;
-                const uint32_t xn = ff_negate<ARITH>(__shfl_sync(0xffffffffu, y[sc], sl), a.R);
-                const uint32_t ws = T[s * ts + s];
+        for (int c = 0; c < CW; ++c) {
+            const int j = jb + lane + 32 * c;
+            pr[c] = j < w ? T[t * ts + j] : 0u;
+        }
+#pragma unroll 2
+        for (int i = 0; i < RI; ++i) {
+            const int r = jb + warp + NW * i;
+            if (r >= nb) break;  // uniform in the warp
+            const uint32_t xn = ff_negate<ARITH>(T[r * ts + t], a.R);
+            uint32_t y[CW];
 #pragma unroll
-                for (int c = 0; c < CW; ++c) {
-                    const int j = lane + 32 * c;
-                    if (32 * c + 31 > s && j > s && j < w) y[c] = ff_update<ARITH>(ws, y[c], xn, T[s * ts + j], a.R);
-                }
+            for (int c = 0; c < CW; ++c) {
+                const int j = jb + lane + 32 * c;
+                y[c] = j < w ? T[r * ts + j] : 0u;
+            }
+#pragma unroll
+            for (int c = 0; c < CW; ++c) y[c] = ff_update<ARITH>(wt, y[c], xn, pr[c], a.R);
+#pragma unroll
+            for (int c = 0; c < CW; ++c) {
+                const int j = jb + lane + 32 * c;
+                if (j < w) T[r * ts + j] = y[c];
             }
         }
-        uint32_t pv = y[0];  // the pivot of step i: column i of this row
-#pragma unroll
-        for (int c = 1; c < CW; ++c)
-            if ((i >> 5) == c) pv = y[c];
-        pv = __shfl_sync(0xffffffffu, pv, i & 31);
-        if (pv == 0 && lane == 0) s_fail = 1;
-#pragma unroll
-        for (int c = 0; c < CW; ++c) {
-            const int j = lane + 32 * c;
-            if (j < w) T[i * ts + j] = y[c];
-        }
-        publish_row(s_fwd, i);
+        __syncthreads();
     }
-    __syncthreads();
-    if (s_fail || s_abort) {
+    if (fail) {
         if (tid == 0) *a.ok = 0;
         return;
     }
@@ -836,142 +815,200 @@ __global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockA
     }
 }
 
+// Row solves against the factored top block, one warp per row, lanes over
+// columns: the forward solve y U = v (y_s = (v_s - sum_{t<s} y_t U[t][s]) /
+// U[s][s]) and the backward solve z L = y (z_i = y_i - sum_{t>i} z_t L[t][i],
+// unit diagonal).  L, U and U's inverse diagonal come in Montgomery form, so
+// each product is one Montgomery reduction.  panel_binv_kernel runs 2 nb of
+// them: row r of B^-1 = e_r U^-1 L^-1 (when rows remain below the block) and
+// row t of L^-1 (stored as L^-1 - I, the top rows of the update's left
+// factor).  Nothing runs unless the top block settled the panel.
+constexpr int kSolveWarps = 4;
+
+template <int ARITH, int WMAX>
+__global__ void __launch_bounds__(32 * kSolveWarps) panel_binv_kernel(const uint32_t* __restrict__ lm,
+                                                                       const uint32_t* __restrict__ um,
+                                                                       const uint32_t* __restrict__ dm, int nb,
+                                                                       int with_binv, const Ring R,
+                                                                       const int* __restrict__ ok,
+                                                                       uint32_t* __restrict__ binv,
+                                                                       uint32_t* __restrict__ linv) {
+    if (*ok == 0) return;
+    extern __shared__ __align__(16) uint32_t s_sv[];
+    uint32_t* Ls = s_sv;                                                      // [nb][nb]
+    uint32_t* Us = s_sv + ((static_cast<size_t>(nb) * nb + 3) & ~size_t(3));  // [nb][nb]
+    __shared__ uint32_t s_dm[kMaxPanel];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int CS = WMAX / 32;
+    for (int idx = tid; idx < nb * nb; idx += 32 * kSolveWarps) {
+        Ls[idx] = lm[idx];
+        if (with_binv) Us[idx] = um[idx];
+    }
+    for (int t = tid; t < nb; t += 32 * kSolveWarps) s_dm[t] = dm[t];
+    __syncthreads();
+    const int v = static_cast<int>(blockIdx.x) * kSolveWarps + warp;  // virtual row
+    const bool is_binv = v < nb;
+    const int r = is_binv ? v : v - nb;
+    if (r >= nb || (is_binv && !with_binv)) return;  // uniform in the warp; no barrier follows
+    const uint32_t one = 1u % R.q;
+    uint32_t a[CS];
+#pragma unroll
+    for (int c = 0; c < CS; ++c) a[c] = lane + 32 * c == r ? one : 0u;
+    if (is_binv) {
+        // forward solve from e_r: y_s = 0 for s < r
+#pragma unroll
+        for (int sc = 0; sc < CS; ++sc) {
+            for (int sl = 0; sl < 32; ++sl) {
+                const int s = 32 * sc + sl;
+                if (s >= nb) break;
+                if (s < r) continue;
+                const uint32_t ys = mul_mform<ARITH>(__shfl_sync(0xffffffffu, a[sc], sl), s_dm[s], R);
+                if (lane == sl) a[sc] = ys;
+#pragma unroll
+                for (int c = sc; c < CS; ++c) {
+                    const int j = lane + 32 * c;
+                    const uint32_t u = j > s && j < nb ? Us[s * nb + j] : 0u;
+                    a[c] = mod_sub(a[c], mul_mform<ARITH>(ys, u, R), R.q);
+                }
+            }
+        }
+    }
+    // backward solve z L = y
+#pragma unroll
+    for (int sc = CS - 1; sc >= 0; --sc) {
+        for (int sl = 31; sl >= 0; --sl) {
+            const int t = 32 * sc + sl;
+            if (t >= nb || t == 0) continue;
+            const uint32_t zt = __shfl_sync(0xffffffffu, a[sc], sl);
+#pragma unroll
+            for (int c = 0; c <= sc; ++c) {
+                const int j = lane + 32 * c;
+                const uint32_t l = j < t ? Ls[t * nb + j] : 0u;
+                a[c] = mod_sub(a[c], mul_mform<ARITH>(zt, l, R), R.q);
+            }
+        }
+    }
+    uint32_t* dst = (is_binv ? binv : linv) + static_cast<size_t>(r) * nb;
+#pragma unroll
+    for (int c = 0; c < CS; ++c) {
+        const int j = lane + 32 * c;
+        if (j < nb) dst[j] = !is_binv && j == r ? mod_sub(a[c], one, R.q) : a[c];
+    }
+}
+
 // The left factor of the fused update, W ((m - r0) x nb, row-major, ld nb):
-// row t < nb is e_t L^-1 - e_t; a row x below the block becomes -x B^-1 =
-// -(x U^-1) L^-1.  Both by substitution on the row, lanes over columns: the
-// forward solve y U = x (y_s = (x_s - sum_{t<s} y_t U[t][s]) / U[s][s]) and
-// the backward solve z L = y (z_i = y_i - sum_{t>i} z_t L[t][i], unit
-// diagonal).  A warp carries four rows at once; L, U and U's inverse diagonal
-// come in Montgomery form, so each product is one Montgomery reduction.
+// rows t < nb are L^-1 - I (from panel_binv_kernel); a row x below the block
+// becomes -x B^-1 (x = the row's panel columns).  A warp takes four rows at
+// once, lanes over output columns; each dot product runs exactly in a 96-bit
+// carry chain (nb <= 128 products below 2^64) and is reduced once.
 constexpr int kWRows = 32;
 constexpr int kWRowsPerWarp = 4;
 
-template <int ARITH, int WMAX>
+__device__ __forceinline__ void mac96(uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t x, uint32_t y) {
+    asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+        "addc.u32 %2, %2, 0;"
+        : "+r"(a0), "+r"(a1), "+r"(a2)
+        : "r"(x), "r"(y));
+}
+
+template <int WMAX>
 __global__ void __launch_bounds__(256) panel_w_kernel(const uint32_t* __restrict__ A, uint64_t ld, int r0, int m,
-                                                      int c0, int nb, const uint32_t* __restrict__ lm,
-                                                      const uint32_t* __restrict__ um,
-                                                      const uint32_t* __restrict__ dm, const Ring R,
-                                                      uint32_t* __restrict__ W) {
+                                                      int c0, int nb, const uint32_t* __restrict__ linv,
+                                                      const uint32_t* __restrict__ binv, uint32_t q,
+                                                      uint64_t barrett, uint32_t* __restrict__ W) {
     extern __shared__ __align__(16) uint32_t s_wk[];
-    uint32_t* Ls = s_wk;                                          // [nb][nb]
-    uint32_t* Us = s_wk + ((static_cast<size_t>(nb) * nb + 3) & ~size_t(3));  // [nb][nb], 16-byte aligned
-    __shared__ uint32_t s_dm[kMaxPanel];
     const int rb = r0 + static_cast<int>(blockIdx.x) * kWRows;  // first row of this CTA
     const int nr = min(kWRows, m - rb);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = 256 / 32;
     static_assert(NW * kWRowsPerWarp == kWRows, "one pass of the warps covers the CTA's rows");
     constexpr int CS = WMAX / 32;
-    const bool any_below = rb + nr > r0 + nb;  // uniform: U is needed
-    {
-        // L (and U when rows below) in 16-byte pieces (the buffers are 16-byte aligned)
-        const int n4 = (nb * nb) >> 2;
-        for (int base = 0; base < n4; base += 256 * 4) {
-            uint4 v[4], u[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int idx = base + tid + 256 * e;
-                if (idx < n4) {
-                    v[e] = reinterpret_cast<const uint4*>(lm)[idx];
-                    if (any_below) u[e] = reinterpret_cast<const uint4*>(um)[idx];
-                }
-            }
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int idx = base + tid + 256 * e;
-                if (idx < n4) {
-                    reinterpret_cast<uint4*>(Ls)[idx] = v[e];
-                    if (any_below) reinterpret_cast<uint4*>(Us)[idx] = u[e];
-                }
-            }
-        }
-        for (int idx = 4 * n4 + tid; idx < nb * nb; idx += 256) {
-            Ls[idx] = lm[idx];
-            if (any_below) Us[idx] = um[idx];
-        }
-        for (int t = tid; t < nb; t += 256) s_dm[t] = dm[t];
+    // the top rows: L^-1 - I
+    for (int r = warp; r < nr; r += NW) {
+        const int row = rb + r;
+        if (row >= r0 + nb) break;
+        for (int j = lane; j < nb; j += 32)
+            W[static_cast<size_t>(row - r0) * nb + j] = linv[static_cast<size_t>(row - r0) * nb + j];
     }
-    const int rl = warp * kWRowsPerWarp;  // this warp's rows: rb + rl .. rb + rl + 3
-    uint32_t a4[kWRowsPerWarp][CS];
+    if (rb + nr <= r0 + nb) return;  // no row below the block in this CTA (uniform)
+    uint32_t* Bi = s_wk;                                   // [nb][nb]
+    uint32_t* Xr = s_wk + ((static_cast<size_t>(nb) * nb + 3) & ~size_t(3));  // [kWRows][nb]
+    {
+        // B^-1 in 16-byte pieces (its buffer is 16-byte aligned), four loads of a thread in flight
+        const int n4 = (nb * nb) >> 2;
+        const uint4* b4 = reinterpret_cast<const uint4*>(binv);
+        uint4* d4 = reinterpret_cast<uint4*>(Bi);
+        for (int base = 0; base < n4; base += 256 * 4) {
+            uint4 v[4];
 #pragma unroll
-    for (int i = 0; i < kWRowsPerWarp; ++i) {
-        const int row = rb + rl + i;
-        const bool below = rl + i < nr && row >= r0 + nb;
-        const uint32_t* src = A + static_cast<size_t>(below ? row : r0) * ld + c0;
+            for (int e = 0; e < 4; ++e) {
+                const int idx = base + tid + 256 * e;
+                if (idx < n4) v[e] = b4[idx];
+            }
 #pragma unroll
-        for (int c = 0; c < CS; ++c) {
-            const int j = lane + 32 * c;
-            a4[i][c] = below && j < nb ? src[j] : 0u;
+            for (int e = 0; e < 4; ++e) {
+                const int idx = base + tid + 256 * e;
+                if (idx < n4) d4[idx] = v[e];
+            }
         }
+        for (int idx = 4 * n4 + tid; idx < nb * nb; idx += 256) Bi[idx] = binv[idx];
+    }
+    const int rl = warp * kWRowsPerWarp;  // this warp's rows: rl .. rl + 3 of the CTA
+    {
+        uint32_t v[kWRowsPerWarp][CS];
+#pragma unroll
+        for (int i = 0; i < kWRowsPerWarp; ++i) {
+            const int row = rb + rl + i;
+            const bool below = rl + i < nr && row >= r0 + nb;
+            const uint32_t* src = A + static_cast<size_t>(below ? row : r0) * ld + c0;
+#pragma unroll
+            for (int c = 0; c < CS; ++c) {
+                const int j = lane + 32 * c;
+                v[i][c] = below && j < nb ? src[j] : 0u;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kWRowsPerWarp; ++i)
+#pragma unroll
+            for (int c = 0; c < CS; ++c) {
+                const int j = lane + 32 * c;
+                if (j < nb) Xr[(rl + i) * nb + j] = v[i][c];
+            }
     }
     __syncthreads();
-    if (any_below) {
-        // forward solve y U = x: at step s, y_s = x_s / U[s][s] is final; columns j > s take -y_s U[s][j]
+    uint32_t a0[kWRowsPerWarp][CS], a1[kWRowsPerWarp][CS], a2[kWRowsPerWarp][CS];
 #pragma unroll
-        for (int sc = 0; sc < CS; ++sc) {
-            for (int sl = 0; sl < 32; ++sl) {
-                const int s = 32 * sc + sl;
-                if (s >= nb) break;
-                const uint32_t ds = s_dm[s];
-                uint32_t ys[kWRowsPerWarp];
+    for (int i = 0; i < kWRowsPerWarp; ++i)
 #pragma unroll
-                for (int i = 0; i < kWRowsPerWarp; ++i) {
-                    ys[i] = mul_mform<ARITH>(__shfl_sync(0xffffffffu, a4[i][sc], sl), ds, R);
-                    if (lane == sl) a4[i][sc] = ys[i];
-                }
+        for (int c = 0; c < CS; ++c) a0[i][c] = a1[i][c] = a2[i][c] = 0;
+    for (int t = 0; t < nb; ++t) {
+        uint32_t bt[CS];
 #pragma unroll
-                for (int c = sc; c < CS; ++c) {
-                    const int j = lane + 32 * c;
-                    const uint32_t u = j > s && j < nb ? Us[s * nb + j] : 0u;
-#pragma unroll
-                    for (int i = 0; i < kWRowsPerWarp; ++i)
-                        a4[i][c] = mod_sub(a4[i][c], mul_mform<ARITH>(ys[i], u, R), R.q);
-                }
-            }
+        for (int c = 0; c < CS; ++c) {
+            const int j = lane + 32 * c;
+            bt[c] = j < nb ? Bi[t * nb + j] : 0u;
         }
-    }
-    // the top rows start the backward solve from e_t
-    const uint32_t one = 1u % R.q;
 #pragma unroll
-    for (int i = 0; i < kWRowsPerWarp; ++i) {
-        const int t = rb + rl + i - r0;
-        if (t < nb) {
+        for (int i = 0; i < kWRowsPerWarp; ++i) {
+            const uint32_t x = Xr[(rl + i) * nb + t];
 #pragma unroll
-            for (int c = 0; c < CS; ++c) a4[i][c] = lane + 32 * c == t ? one : 0u;
-        }
-    }
-    // backward solve z L = y: at step t (nb-1 down to 1), z_t = y_t is final; columns j < t take -z_t L[t][j]
-#pragma unroll
-    for (int sc = CS - 1; sc >= 0; --sc) {
-        for (int sl = 31; sl >= 0; --sl) {
-            const int t = 32 * sc + sl;
-            if (t >= nb || t == 0) continue;
-            uint32_t zt[kWRowsPerWarp];
-#pragma unroll
-            for (int i = 0; i < kWRowsPerWarp; ++i) zt[i] = __shfl_sync(0xffffffffu, a4[i][sc], sl);
-#pragma unroll
-            for (int c = 0; c <= sc; ++c) {
-                const int j = lane + 32 * c;
-                const uint32_t l = j < t ? Ls[t * nb + j] : 0u;
-#pragma unroll
-                for (int i = 0; i < kWRowsPerWarp; ++i)
-                    a4[i][c] = mod_sub(a4[i][c], mul_mform<ARITH>(zt[i], l, R), R.q);
-            }
+            for (int c = 0; c < CS; ++c) mac96(a0[i][c], a1[i][c], a2[i][c], x, bt[c]);
         }
     }
 #pragma unroll
     for (int i = 0; i < kWRowsPerWarp; ++i) {
         const int row = rb + rl + i;
-        if (rl + i >= nr) continue;
-        const int t = row - r0;
-        uint32_t* dst = W + static_cast<size_t>(t) * nb;
+        if (rl + i >= nr || row < r0 + nb) continue;
+        uint32_t* dst = W + static_cast<size_t>(row - r0) * nb;
 #pragma unroll
         for (int c = 0; c < CS; ++c) {
             const int j = lane + 32 * c;
-            if (j >= nb) continue;
-            const uint32_t v = a4[i][c];
-            if (t < nb) dst[j] = j == t ? mod_sub(v, one, R.q) : v;  // e_t L^-1 - e_t
-            else dst[j] = v == 0 ? 0u : R.q - v;                     // -x B^-1
+            if (j < nb) {
+                const uint64_t h = reduce_u64((static_cast<uint64_t>(a2[i][c]) << 32) | a1[i][c], q, barrett);
+                const uint32_t v = static_cast<uint32_t>(reduce_u64((h << 32) | a0[i][c], q, barrett));
+                dst[j] = v == 0 ? 0u : q - v;
+            }
         }
     }
 }
@@ -1232,14 +1269,17 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
                                    reinterpret_cast<const void*>(panel_block_kernel<kArithMont31, 128>),
                                    reinterpret_cast<const void*>(panel_block_kernel<kArithMont32, 128>)})
                 HME_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bsm));
-            const int wsm = static_cast<int>(2 * sizeof(uint32_t) * kMaxPanel * kMaxPanel);
-            for (const void* fn : {reinterpret_cast<const void*>(panel_w_kernel<kArithPow2, 64>),
-                                   reinterpret_cast<const void*>(panel_w_kernel<kArithMont31, 64>),
-                                   reinterpret_cast<const void*>(panel_w_kernel<kArithMont32, 64>),
-                                   reinterpret_cast<const void*>(panel_w_kernel<kArithPow2, 128>),
-                                   reinterpret_cast<const void*>(panel_w_kernel<kArithMont31, 128>),
-                                   reinterpret_cast<const void*>(panel_w_kernel<kArithMont32, 128>)})
-                HME_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
+            const int wsm = static_cast<int>(sizeof(uint32_t) * (kMaxPanel * kMaxPanel + kWRows * kMaxPanel));
+            HME_CUDA(cudaFuncSetAttribute(panel_w_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
+            HME_CUDA(cudaFuncSetAttribute(panel_w_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
+            const int ssm = static_cast<int>(2 * sizeof(uint32_t) * kMaxPanel * kMaxPanel);
+            for (const void* fn : {reinterpret_cast<const void*>(panel_binv_kernel<kArithPow2, 64>),
+                                   reinterpret_cast<const void*>(panel_binv_kernel<kArithMont31, 64>),
+                                   reinterpret_cast<const void*>(panel_binv_kernel<kArithMont32, 64>),
+                                   reinterpret_cast<const void*>(panel_binv_kernel<kArithPow2, 128>),
+                                   reinterpret_cast<const void*>(panel_binv_kernel<kArithMont31, 128>),
+                                   reinterpret_cast<const void*>(panel_binv_kernel<kArithMont32, 128>)})
+                HME_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, ssm));
         }
         bool attrs_ok = true;
         for (const void* fn : {reinterpret_cast<const void*>(panel_cluster_kernel<kArithPow2, 512>),
@@ -1296,7 +1336,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     const size_t scratch_bytes = (sizeof(Scratch) + 255) / 256 * 256;
     const size_t cand_bytes = sizeof(uint32_t) * 2 * static_cast<size_t>(grid_cap) * kMaxPanel;
     const size_t perm_bytes = (sizeof(int) * static_cast<size_t>(m) + 255) / 256 * 256;
-    const size_t uinv_bytes = sizeof(uint32_t) * (2 * kMaxPanel * kMaxPanel + kMaxPanel);  // L, U, U's inverse diagonal
+    const size_t uinv_bytes = sizeof(uint32_t) * (4 * kMaxPanel * kMaxPanel + kMaxPanel);  // L, U, B^-1, L^-1 - I, 1/diag U
     uint8_t* base = static_cast<uint8_t*>(
         ctx->ws.get(kSlotElim0, 2 * (scratch_bytes + cand_bytes) + 2 * perm_bytes + 2 * uinv_bytes + 256));
     // the L21 / W slot at its largest (every panel's rows x pivots fits), so no panel regrows it
@@ -1409,8 +1449,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             ba.ok = &d_s->block_ok;
             ba.lm = d_uinvb[par];
             ba.um = d_uinvb[par] + kMaxPanel * kMaxPanel;
-            ba.dm = d_uinvb[par] + 2 * kMaxPanel * kMaxPanel;
-            ba.err = ctx->d_err;
+            ba.dm = d_uinvb[par] + 4 * kMaxPanel * kMaxPanel;
             const size_t bsm = block_smem_bytes(nb, w);
             auto launch_block = [&](auto kern) {
                 HME_TIMED(ctx, "panel_block", kern<<<1, kBlockThreads, bsm, st>>>(ba));
@@ -1427,6 +1466,30 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
                 else launch_block(panel_block_kernel<kArithMont32, 128>);
             }
             HME_CUDA(cudaGetLastError());
+            {
+                // B^-1 (when rows remain below) and L^-1 - I by row solves, one warp per row
+                const int with_binv = rows > nb ? 1 : 0;
+                const int gs = (2 * nb + kSolveWarps - 1) / kSolveWarps;
+                const size_t ssm = 2 * sizeof(uint32_t) * ((static_cast<size_t>(nb) * nb + 3) & ~size_t(3));
+                uint32_t* sb = d_uinvb[par];
+                auto launch_solve = [&](auto kern) {
+                    HME_TIMED(ctx, "panel_block", kern<<<gs, 32 * kSolveWarps, ssm, st>>>(
+                                                      sb, sb + kMaxPanel * kMaxPanel, sb + 4 * kMaxPanel * kMaxPanel, nb,
+                                                      with_binv, rg, &d_s->block_ok, sb + 2 * kMaxPanel * kMaxPanel,
+                                                      sb + 3 * kMaxPanel * kMaxPanel));
+                };
+                if (rg.ell == 2) {
+                    if (w64) launch_solve(panel_binv_kernel<kArithPow2, 64>);
+                    else launch_solve(panel_binv_kernel<kArithPow2, 128>);
+                } else if (p < (1u << 31)) {
+                    if (w64) launch_solve(panel_binv_kernel<kArithMont31, 64>);
+                    else launch_solve(panel_binv_kernel<kArithMont31, 128>);
+                } else {
+                    if (w64) launch_solve(panel_binv_kernel<kArithMont32, 64>);
+                    else launch_solve(panel_binv_kernel<kArithMont32, 128>);
+                }
+                HME_CUDA(cudaGetLastError());
+            }
             pa.skip = &d_s->block_ok;
         }
         const int cs = cluster_size(rows, w);
@@ -1558,24 +1621,16 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
                 if (!Wf) {
                     Wf = static_cast<uint32_t*>(ctx->ws.get(kSlotElim2, sizeof(uint32_t) * static_cast<size_t>(rows) * k));
                     const int g = (rows + kWRows - 1) / kWRows;
-                    const size_t wsm = 2 * sizeof(uint32_t) * ((static_cast<size_t>(k) * k + 3) & ~size_t(3));
-                    const uint32_t* lmp = d_uinvb[par];
-                    const uint32_t* ump = d_uinvb[par] + kMaxPanel * kMaxPanel;
-                    const uint32_t* dmp = d_uinvb[par] + 2 * kMaxPanel * kMaxPanel;
-                    auto launch_w = [&](auto kern) {
-                        HME_TIMED(ctx, "panel_w", kern<<<g, 256, wsm, s_main>>>(A, ld, r0, m, c0, k, lmp, ump, dmp, rg, Wf));
-                    };
-                    const bool w64 = k <= 64;
-                    if (rg.ell == 2) {
-                        if (w64) launch_w(panel_w_kernel<kArithPow2, 64>);
-                        else launch_w(panel_w_kernel<kArithPow2, 128>);
-                    } else if (p < (1u << 31)) {
-                        if (w64) launch_w(panel_w_kernel<kArithMont31, 64>);
-                        else launch_w(panel_w_kernel<kArithMont31, 128>);
-                    } else {
-                        if (w64) launch_w(panel_w_kernel<kArithMont32, 64>);
-                        else launch_w(panel_w_kernel<kArithMont32, 128>);
-                    }
+                    const size_t wsm = sizeof(uint32_t) * (((static_cast<size_t>(k) * k + 3) & ~size_t(3)) +
+                                                           static_cast<size_t>(kWRows) * k);
+                    const uint32_t* binv = d_uinvb[par] + 2 * kMaxPanel * kMaxPanel;
+                    const uint32_t* linv = d_uinvb[par] + 3 * kMaxPanel * kMaxPanel;
+                    if (k <= 64)
+                        HME_TIMED(ctx, "panel_w", panel_w_kernel<64><<<g, 256, wsm, s_main>>>(
+                                                      A, ld, r0, m, c0, k, linv, binv, p, mp.barrett, Wf));
+                    else
+                        HME_TIMED(ctx, "panel_w", panel_w_kernel<128><<<g, 256, wsm, s_main>>>(
+                                                      A, ld, r0, m, c0, k, linv, binv, p, mp.barrett, Wf));
                     HME_CUDA(cudaGetLastError());
                 }
                 ctx->gemm_sm_cap = sm_cap;

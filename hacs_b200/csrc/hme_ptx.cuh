@@ -27,7 +27,6 @@ enum DeviceErr : int {
     DERR_TMEM_ADDR = 6,       // tensor-memory allocation returned an unusable address
     DERR_GRID_BARRIER = 7,    // a cooperative kernel's grid barrier waited too long
     DERR_LAUNCH_SHAPE = 8,    // a kernel found its launch shape outside what it supports and did nothing
-    DERR_WAIT_ROW = 9,        // a warp of a row wavefront waited too long for an earlier row
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
