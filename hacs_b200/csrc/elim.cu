@@ -9,7 +9,12 @@
 // anyway (leftmost column with a non-zero in the Schur complement, topmost such
 // row) because it is also the cheapest to find in parallel (a min over rows).
 //
-// Blocked right-looking LU, panels of `bw` columns:
+// Blocked right-looking LU, panels of `bw` columns.  Over a field the panel
+// first takes the top-block path (panel_block_kernel, panel_binv_kernel,
+// panel_w_kernel; the reasoning is at their definitions): when the panel's top
+// bw rows factor with non-zero diagonal entries they are its pivots, no search
+// runs, no row moves, and steps 2-4 below collapse into one limb GEMM
+// [A12; A22] += [L^-1 - I; -A21 B^-1] A12.  Otherwise:
 //   1. panel_cluster_kernel: the panel's active rows A[r0:m, c0:c0+bw) sit in
 //      the shared memory of one thread-block cluster (up to 16 CTAs); per
 //      column each CTA pushes its best (valuation, row) key and that row to
@@ -699,7 +704,7 @@ struct BlockArgs {
     uint32_t* um;     // out: U's strict upper part, Montgomery form (nb x nb, row-major, zero elsewhere)
     uint32_t* dm;     // out: U's inverse diagonal, Montgomery form (nb)
 };
-constexpr int kBlockThreads = 256;
+constexpr int kBlockThreads = 512;
 
 __host__ __device__ constexpr int block_stride(int w) { return w | 1; }
 __host__ __device__ constexpr size_t block_smem_bytes(int nb, int w) {
@@ -727,7 +732,7 @@ __device__ __forceinline__ uint32_t to_mform(uint32_t x, const Ring& R) {
 // over columns, each row's operands loaded before its updates are computed.
 // The classical values are restored as in the cluster kernel and written
 // back; L, U and U's inverse diagonal go out in Montgomery form for the row
-// solves of panel_w_kernel.  WMAX (64 or 128) bounds w.
+// solves of panel_binv_kernel.  WMAX (64 or 128) bounds w.
 template <int ARITH, int WMAX>
 __global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockArgs a) {
     extern __shared__ __align__(16) uint32_t s_blk[];
@@ -750,7 +755,8 @@ __global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockA
     bool fail = false;
     for (int t = 0; t < nb; ++t) {
         const uint32_t wt = T[t * ts + t];
-        if (wt == 0) {  // the same value in every thread: uniform
+        // the pivot must be a unit (over a field: non-zero); the same value in every thread: uniform
+        if (wt == 0 || (a.R.k > 1 && wt % a.R.ell == 0)) {
             fail = true;
             break;
         }
@@ -1407,7 +1413,12 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     // The panel [c0, c0 + w) of the active rows [r0, m) on `st`: its pivots and the error word
     // land in h_sb[par] and ev_panel[par] is recorded.  Returns the cluster size (0: grid kernel).
     // the top-block path: in automatic mode, over a field
-    const bool use_block = opt.panel_kernel == 0 && rg.k == 1;
+    // the top-block path in automatic mode, over fields of at least 256 elements (a random top block
+    // of 64 steps meets a zero pivot with probability about 64/p, so over small fields and over rings,
+    // where a non-unit pivot is as likely, the attempts would mostly fail); after a panel it did not
+    // settle, the next three panels go straight to the search (rank-deficient tails)
+    const bool use_block = opt.panel_kernel == 0 && rg.k == 1 && p >= 256;
+    int block_rest = 0;
     bool block_tried[2] = {false, false};
     auto launch_panel = [&](int c0, int w, int r0, int par, cudaStream_t st) -> int {
         Scratch* d_s = d_sb[par];
@@ -1430,10 +1441,12 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         pa.bar = d_s->bar;
         pa.err = ctx->d_err;
         const int rows = m - r0;
-        // the top-block path first (fields only: a ring pivot needs the minimal valuation over all
-        // rows); the searching kernel below runs only when it did not settle the panel
-        block_tried[par] = use_block;
-        if (use_block) {
+        // the top-block path first; the searching kernel below runs only when the block did not
+        // settle the panel
+        const bool try_block = use_block && block_rest == 0;
+        if (use_block && block_rest > 0) --block_rest;
+        block_tried[par] = try_block;
+        if (try_block) {
             const int nb = std::min(w, rows);
             BlockArgs ba{};
             ba.A = A;
@@ -1562,6 +1575,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         if (h_s.err != 0) check_device_error(ctx);  // reports the timeout (and clears the word)
         if (block_tried[par] && h_s.block_ok) ++ctx->elim_block_panels;
         else ++ctx->elim_search_panels;
+        if (block_tried[par] && !h_s.block_ok) block_rest = 3;
         const int k = h_s.k;
         if (k == 0) continue;  // no pivot in the panel: nothing moved, the next panel starts at r0
         for (int t = 0; t < k; ++t) pivots.push_back(h_s.pivot_cols[t]);
