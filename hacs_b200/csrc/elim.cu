@@ -1420,11 +1420,17 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     const bool use_block = opt.panel_kernel == 0 && rg.k == 1 && p >= 256;
     int block_rest = 0;
     bool block_tried[2] = {false, false};
-    auto launch_panel = [&](int c0, int w, int r0, int par, cudaStream_t st) -> int {
+    // The panel [c0, c0 + w) of the active rows [r0, m) on `st`: the top-block path when it is tried
+    // (the host launches the search afterwards if the block did not settle the panel), else the
+    // searching kernel.  Its pivots and the error word land in h_sb[par] and ev_panel[par] is
+    // recorded.  Returns the cluster size the search takes (0: grid kernel), the SMs a GEMM beside
+    // the panel leaves free.
+    cudaStream_t panel_stream[2] = {s_main, s_main};
+    auto launch_panel = [&](int c0, int w, int r0, int par, cudaStream_t st, bool search_only) -> int {
         Scratch* d_s = d_sb[par];
         const cudaStream_t saved = ctx->stream;
         ctx->stream = st;  // HME_TIMED brackets the launch on the launching stream
-        HME_CUDA(cudaMemsetAsync(d_s->piv_slot, 0x7f, sizeof(unsigned long long) * kMaxPanel, st));
+        panel_stream[par] = st;
         PanelArgs pa{};
         pa.A = A;
         pa.ld = ld;
@@ -1443,8 +1449,8 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
         const int rows = m - r0;
         // the top-block path first; the searching kernel below runs only when the block did not
         // settle the panel
-        const bool try_block = use_block && block_rest == 0;
-        if (use_block && block_rest > 0) --block_rest;
+        const bool try_block = !search_only && use_block && block_rest == 0;
+        if (!search_only && use_block && block_rest > 0) --block_rest;
         block_tried[par] = try_block;
         if (try_block) {
             const int nb = std::min(w, rows);
@@ -1503,11 +1509,12 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
                 }
                 HME_CUDA(cudaGetLastError());
             }
-            pa.skip = &d_s->block_ok;
         }
         const int cs = cluster_size(rows, w);
         HME_REQUIRE(opt.panel_kernel < 2 || cs > 0, "elim: the panel does not fit one cluster");
-        if (cs > 0) {
+        if (try_block) {
+            // no search behind the block: the host relaunches the panel with the search if needed
+        } else if (cs > 0) {
             const int rpc = static_cast<int>((static_cast<size_t>(rows) + cs - 1) / cs);
             cudaLaunchConfig_t cfg{};
             cfg.gridDim = dim3(cs);
@@ -1540,6 +1547,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
                 else launch(panel_cluster_kernel<kArithMont32, 1024>);
             }
         } else {
+            HME_CUDA(cudaMemsetAsync(d_s->piv_slot, 0x7f, sizeof(unsigned long long) * kMaxPanel, st));
             const int rpc_want = std::max(1, opt.rows_per_cta > 0 ? opt.rows_per_cta : 32);
             const int want_grid = std::max(1, std::min(grid_cap, (rows + rpc_want - 1) / rpc_want));
             const int rpc = (rows + want_grid - 1) / want_grid;
@@ -1568,14 +1576,21 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
     bool launched = false;  // the panel at c0 was already factored ahead (on the second stream)
     for (int c0 = 0; c0 < lu_cols && r0 < m; c0 += bw) {
         const int w = std::min(bw, lu_cols - c0);
-        if (!launched) launch_panel(c0, w, r0, par, s_main);
+        if (!launched) launch_panel(c0, w, r0, par, s_main, false);
         launched = false;
         HME_CUDA(cudaEventSynchronize(ev_panel[par]));
+        if (block_tried[par] && !h_sb[par].block_ok) {
+            // the top block did not settle the panel (nothing was written): the search, on the
+            // panel's stream; the main stream's later work waits for it too
+            block_rest = 3;
+            launch_panel(c0, w, r0, par, panel_stream[par], true);
+            if (panel_stream[par] != s_main) HME_CUDA(cudaStreamWaitEvent(s_main, ev_panel[par], 0));
+            HME_CUDA(cudaEventSynchronize(ev_panel[par]));
+        }
         const Scratch& h_s = h_sb[par];
         if (h_s.err != 0) check_device_error(ctx);  // reports the timeout (and clears the word)
-        if (block_tried[par] && h_s.block_ok) ++ctx->elim_block_panels;
+        if (block_tried[par]) ++ctx->elim_block_panels;
         else ++ctx->elim_search_panels;
-        if (block_tried[par] && !h_s.block_ok) block_rest = 3;
         const int k = h_s.k;
         if (k == 0) continue;  // no pivot in the panel: nothing moved, the next panel starts at r0
         for (int t = 0; t < k; ++t) pivots.push_back(h_s.pivot_cols[t]);
@@ -1695,7 +1710,7 @@ ElimResult elim_device(hme_ctx* ctx, const ModParams& mp, uint32_t* A, size_t ld
             update(c0, c1 + nw, 0);
             HME_CUDA(cudaEventRecord(ev_next, s_main));
             HME_CUDA(cudaStreamWaitEvent(s_aux, ev_next, 0));
-            const int cs_next = launch_panel(c1, nw, r0 + k, par ^ 1, s_aux);
+            const int cs_next = launch_panel(c1, nw, r0 + k, par ^ 1, s_aux, false);
             update(c1 + nw, n, cs_next > 0 ? std::max(1, ctx->num_sms - cs_next) : 0);
             launched = true;
         } else {

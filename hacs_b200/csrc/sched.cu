@@ -498,14 +498,17 @@ int hme_mlp_predict_bf16(hme_mlp* m, uint32_t n, const float* X, float* Y) {
         bind(m->ctx);
         if (n == 0) return;
         hme_ctx* ctx = m->ctx;
-        DevBuf dX(sizeof(float) * n * kIn), dY(sizeof(float) * n * kOut);
-        HME_CUDA(cudaMemcpyAsync(dX.p, X, sizeof(float) * n * kIn, cudaMemcpyHostToDevice, ctx->stream));
+        // features and scores in the context's scheduler slots: no allocation (and no device-wide
+        // synchronisation of a free) per call
+        float* dX = static_cast<float*>(ctx->ws.get(kSlotSched0, sizeof(float) * n * kIn));
+        float* dY = static_cast<float*>(ctx->ws.get(kSlotSched1, sizeof(float) * n * kOut));
+        HME_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * n * kIn, cudaMemcpyHostToDevice, ctx->stream));
         HME_TIMED(ctx, "mlp_to_bf16", to_bf16_kernel<<<(kParams + 255) / 256, 256, 0, ctx->stream>>>(m->P, m->Q));
         const int grid = std::max(1, std::min(ctx->num_sms * 4, static_cast<int>((n + kWarps - 1) / kWarps)));
         HME_TIMED(ctx, "mlp_predict_bf16",
-                  mlp_predict_bf16_kernel<<<grid, kWarps * 32, 0, ctx->stream>>>(m->Q, dX.as<float>(), n, dY.as<float>()));
+                  mlp_predict_bf16_kernel<<<grid, kWarps * 32, 0, ctx->stream>>>(m->Q, dX, n, dY));
         HME_CUDA(cudaGetLastError());
-        HME_CUDA(cudaMemcpyAsync(Y, dY.p, sizeof(float) * n * kOut, cudaMemcpyDeviceToHost, ctx->stream));
+        HME_CUDA(cudaMemcpyAsync(Y, dY, sizeof(float) * n * kOut, cudaMemcpyDeviceToHost, ctx->stream));
         check_device_error(ctx);
     });
 }
@@ -536,7 +539,8 @@ int hme_sched_plan(hme_ctx* ctx, hme_mlp* m, uint32_t n, const uint32_t* shapes,
                 if (Y[t * kOut + v] < Y[t * kOut + best]) best = v;
             variants[t] = best;
             const uint32_t* s = shapes + 4 * static_cast<size_t>(t);
-            tab[shape_key(s[1], s[2], s[3], make_mod(s[0]).limbs)] = best;
+            const uint32_t limbs = s[0] <= 256u ? 1u : s[0] <= 65536u ? 2u : s[0] <= (1u << 24) ? 3u : 4u;  // as make_mod
+            tab[shape_key(s[1], s[2], s[3], limbs)] = best;
         }
     });
 }
