@@ -121,3 +121,32 @@ def test_gemm_host_pointers_strided_pipeline(engine, p, m, n, k, op):
     check(rc)
     assert np.array_equal(Ch[:, :n], want)
     assert np.array_equal(Ch[:, n:], pad)
+
+
+def test_gemm_and_rref_on_every_visible_device():
+    """Kernel attributes (the large dynamic shared memory of the limb GEMM, the
+    elimination's cluster and block kernels) are set once per device, not once
+    per process: a context on each visible device runs a GEMM and an RREF in the
+    same process, bit-exact (skipped with a single visible device)."""
+    import torch
+
+    import hacs_b200
+
+    n_dev = torch.cuda.device_count()
+    if n_dev < 2:
+        pytest.skip("one visible device")
+    rng = np.random.default_rng(77)
+    p = 2147483629
+    A, B = _rand(rng, (300, 257), p), _rand(rng, (257, 190), p)
+    want = O.gemm(p, A, B)
+    M = _rand(rng, (150, 140), p)
+    want_r, want_p = O.rref(p, M)
+    engines = [hacs_b200.Engine(d) for d in range(n_dev)]
+    try:
+        for e in engines + engines[::-1]:
+            assert np.array_equal(e.gemm(p, A, B), want)
+            R, piv = e.rref(p, M)
+            assert np.array_equal(R, want_r) and np.array_equal(piv, want_p)
+    finally:
+        for e in engines:
+            e.close()
