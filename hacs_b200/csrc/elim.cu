@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(kBlockThreads) panel_block_kernel(const BlockA
             const int j = jb + lane + 32 * c;
             pr[c] = j < w ? T[t * ts + j] : 0u;
         }
-#pragma unroll 2
+#pragma unroll
         for (int i = 0; i < RI; ++i) {
             const int r = jb + warp + NW * i;
             if (r >= nb) break;  // uniform in the warp
