@@ -910,14 +910,6 @@ __global__ void __launch_bounds__(32 * kSolveWarps) panel_binv_kernel(const uint
 constexpr int kWRows = 32;
 constexpr int kWRowsPerWarp = 4;
 
-__device__ __forceinline__ void mac96(uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t x, uint32_t y) {
-    asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
-        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
-        "addc.u32 %2, %2, 0;"
-        : "+r"(a0), "+r"(a1), "+r"(a2)
-        : "r"(x), "r"(y));
-}
-
 template <int WMAX>
 __global__ void __launch_bounds__(256) panel_w_kernel(const uint32_t* __restrict__ A, uint64_t ld, int r0, int m,
                                                       int c0, int nb, const uint32_t* __restrict__ linv,

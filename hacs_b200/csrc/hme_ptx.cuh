@@ -89,6 +89,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
     }
 }
 
+// ---- exact dot products ---------------------------------------------------------
+// (a2:a1:a0) += x * y as one 96-bit unsigned sum (mad.lo.cc / madc.hi.cc / addc):
+// up to 2^32 products below 2^64 stay exact; reduce the sum once at the end.
+__device__ __forceinline__ void mac96(uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t x, uint32_t y) {
+    asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+        "addc.u32 %2, %2, 0;"
+        : "+r"(a0), "+r"(a1), "+r"(a2)
+        : "r"(x), "r"(y));
+}
+
 // ---- L2 prefetch ----------------------------------------------------------------
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));

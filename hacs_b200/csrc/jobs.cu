@@ -326,9 +326,9 @@ struct SolveJob {
 // substitution on e_j, one warp per column, lane l holding rows l, l+32, ...;
 // at step t row t is final and a shuffle broadcasts it), into the job's slot;
 // batch_apply_kernel, one CTA per (job, 32 trailing columns): the product
-// L11^-1 A12 with lane = column and warps over rows, each output a dot
-// product accumulated in 64 bits and reduced once per kmax products -- no
-// sequential dependency, so no idle lanes.
+// L11^-1 A12 with lane = column and warps over rows, each output an exact
+// dot product in a 96-bit sum reduced once -- no sequential dependency, so no
+// idle lanes.
 constexpr int kBatchTrsmCols = 32;
 size_t batch_linv_smem(int k) { return sizeof(uint32_t) * static_cast<size_t>(k) * (k | 1); }
 size_t batch_apply_smem(int k) {
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(256) batch_linv_kernel(const SolveJob* __restr
 
 __global__ void __launch_bounds__(256) batch_apply_kernel(const SolveJob* __restrict__ jobs) {
     extern __shared__ uint32_t smem_ba[];
-    const SolveJob& J = jobs[blockIdx.y];
+    const SolveJob J = jobs[blockIdx.y];
     const int k = J.k;
     // nothing to solve, or no columns for this CTA: the test is the same for the whole CTA
     if (k < 2 || static_cast<int>(blockIdx.x) * kBatchTrsmCols >= J.ntrail) return;
@@ -405,17 +405,13 @@ __global__ void __launch_bounds__(256) batch_apply_kernel(const SolveJob* __rest
         __syncthreads();
         if (lane < nc) {
             for (int r = warp; r < k; r += nw) {
-                uint64_t acc = X[r * xs + lane];  // the unit diagonal
-                uint32_t cnt = 0;
+                // the unit diagonal's term, then r exact products in a 96-bit sum, one reduction
+                uint32_t a0 = X[r * xs + lane], a1 = 0, a2 = 0;
                 const uint32_t* lr = Li + r * ls;
-                for (int s = 0; s < r; ++s) {
-                    acc += static_cast<uint64_t>(lr[s]) * X[s * xs + lane];
-                    if (++cnt == J.kmax) {
-                        acc = reduce_u64(acc, J.p, J.barrett);
-                        cnt = 0;
-                    }
-                }
-                J.A[static_cast<size_t>(J.r0 + r) * J.ld + J.c1 + c0 + lane] = reduce_u64(acc, J.p, J.barrett);
+                for (int s = 0; s < r; ++s) mac96(a0, a1, a2, lr[s], X[s * xs + lane]);
+                const uint64_t h = reduce_u64((static_cast<uint64_t>(a2) << 32) | a1, J.p, J.barrett);
+                J.A[static_cast<size_t>(J.r0 + r) * J.ld + J.c1 + c0 + lane] =
+                    reduce_u64((h << 32) | a0, J.p, J.barrett);
             }
         }
     }
