@@ -1,5 +1,5 @@
 // Inline-PTX building blocks for sm_100a: mbarriers with bounded waits, TMA
-// tensor loads (no multicast anywhere in this library), and the tcgen05
+// tensor loads (each CTA loads only into its own shared memory), and the tcgen05
 // tensor-core / tensor-memory instructions.
 //
 // Every spin on an mbarrier is bounded by wall time (%globaltimer): when the

@@ -23,7 +23,7 @@
 // tensor-core operands), Kp = K rounded up to 16 bytes for TMA strides.
 //
 // Kernel: persistent, one CTA per SM, 10 warps: warp 0 issues TMA loads
-// (128-byte swizzle, no multicast), warp 1 owns tensor memory and issues the
+// (128-byte swizzle, each CTA loads its own tiles), warp 1 owns tensor memory and issues the
 // MMAs, warps 2-9 (two per TMEM lane quarter, alternate 16-column chunks)
 // drain the double-buffered accumulator (2 x L*BN columns of
 // TMEM) into C while the next tile's MMAs run.
