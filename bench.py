@@ -660,9 +660,10 @@ def extra_jobstream(eng, plain, n_jobs=10000, sample=500):
     return out
 
 
-def serve_stream(eng, ms, plan, warm: bool = False):
-    """Serve the mixed stream in its chunks with per-job GEMM schedules `plan`
-    (hme_batch_gemm_rank_u32_dev_plan); returns (seconds inside the calls, ranks)."""
+def serve_stream(eng, ms, plan, rank_plan=None, warm: bool = False):
+    """Serve the mixed stream in its chunks with per-job GEMM schedules `plan` and
+    rank schedules `rank_plan` (hme_batch_gemm_rank_u32_dev_sched; None: the rank
+    rounds' batch rule); returns (seconds inside the calls, ranks)."""
     import ctypes as C_
 
     import torch
@@ -676,12 +677,14 @@ def serve_stream(eng, ms, plan, warm: bool = False):
         eng.gen_jobs_dev(specs)
         arr = eng._jobs(jobs)
         var = np.ascontiguousarray(plan[c0:c1], dtype=np.int32)
+        rvar = np.ascontiguousarray(np.full(c1 - c0, -1) if rank_plan is None else rank_plan[c0:c1], dtype=np.int32)
         out = np.zeros(c1 - c0, np.uint32)
+        ip = C_.POINTER(C_.c_int)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        hacs_b200.check(eng._lib.hme_batch_gemm_rank_u32_dev_plan(eng._h, c1 - c0, arr,
-                                                                  var.ctypes.data_as(C_.POINTER(C_.c_int)),
-                                                                  out.ctypes.data_as(C_.POINTER(C_.c_uint32))))
+        hacs_b200.check(eng._lib.hme_batch_gemm_rank_u32_dev_sched(eng._h, c1 - c0, arr, var.ctypes.data_as(ip),
+                                                                   rvar.ctypes.data_as(ip),
+                                                                   out.ctypes.data_as(C_.POINTER(C_.c_uint32))))
         total += time.perf_counter() - t0
         ranks[c0:c1] = out
         if warm:
@@ -691,15 +694,17 @@ def serve_stream(eng, ms, plan, warm: bool = False):
 
 def extra_scheduler(eng, n_stream=50000):
     """Config 5: the 50,000-job mixed stream (stream.MixedStream: config-4 jobs, config-2 rank-deficient
-    products, config-1 products) served end to end through the batched GEMM + rank call under three plans of
-    per-job GEMM schedules: the learned planner's (the MLP trained on this engine's batch autotuner timings,
-    one BF16 inference launch for the whole stream), the batch rule (the method without the network) and the
-    exhaustive batch autotuner's best per shape class.  Ranks are checked across plans and against the
-    reference / the construction."""
+    products, config-1 products) served end to end through the batched GEMM + rank call under three plans,
+    each a per-job GEMM schedule and a per-job rank-round schedule (trailing-update variant, panel width of
+    the rounds): the learned planners' (two MLPs trained on this engine's batch autotuner timings of the GEMM
+    phase and of the rank rounds, one BF16 inference launch each for the whole stream), the batch rules (the
+    method without the networks) and the exhaustive batch autotuners' best per shape class.  Ranks are
+    checked across plans and against the reference / the construction."""
     from hacs_b200 import sched, stream
 
     if not os.path.exists(sched.BATCH_WEIGHTS):
         return {"unavailable": "no trained batch-planner weights in the package"}
+    have_rank = os.path.exists(sched.RANK_WEIGHTS)
     ms = stream.MixedStream(n_stream)
     shapes, dens = ms.shapes(), ms.density()
     mlp = sched.MLP(eng)
@@ -709,22 +714,36 @@ def extra_scheduler(eng, n_stream=50000):
     learned = mlp.plan(shapes, dens)
     t_plan = time.perf_counter() - t0
     mlp.close()
-    # the exhaustive autotuner: every variant timed inside a batch, once per shape class of the stream
+    rule_rank = np.full(ms.n_jobs, sched.BATCH_RULE, np.int32)
+    learned_rank, t_plan_rank = rule_rank, 0.0
+    if have_rank:
+        mlp_r = sched.MLP(eng)
+        mlp_r.load(sched.RANK_WEIGHTS)
+        mlp_r.plan_rank(shapes[:64], dens[:64])  # warm
+        t0 = time.perf_counter()
+        learned_rank = mlp_r.plan_rank(shapes, dens)
+        t_plan_rank = time.perf_counter() - t0
+        mlp_r.close()
+    # the exhaustive autotuners: every variant timed inside a batch, once per shape class of the stream
     t0 = time.perf_counter()
     first = {}
     for t in range(ms.n_jobs):
         first.setdefault(sched.shape_class(*shapes[t]), t)
     T = {key: sched.autotune_batch(eng, *shapes[t]) for key, t in first.items()}
+    TR = ({key: sched.autotune_batch_rank(eng, *shapes[t], dens[t]) for key, t in first.items()}
+          if have_rank else {})
     t_tune = time.perf_counter() - t0
     keys = [sched.shape_class(*row) for row in shapes]
     best = np.array([int(np.argmin(T[k])) for k in keys], np.int32)
+    best_rank = np.array([int(np.argmin(TR[k])) for k in keys], np.int32) if have_rank else rule_rank
     rule = np.full(ms.n_jobs, sched.BATCH_RULE, np.int32)
     serve_stream(eng, ms, rule, warm=True)  # workspace growth, module load
     res = {}
-    for name, plan in (("heuristic", rule), ("learned", learned), ("autotuner_best", best)):
+    for name, plan, rplan in (("heuristic", rule, rule_rank), ("learned", learned, learned_rank),
+                              ("autotuner_best", best, best_rank)):
         ts, rk = [], None
         for _ in range(2):
-            t, r = serve_stream(eng, ms, plan)
+            t, r = serve_stream(eng, ms, plan, rplan)
             ts.append(t)
             if rk is not None:
                 assert np.array_equal(rk, r)
@@ -744,13 +763,27 @@ def extra_scheduler(eng, n_stream=50000):
            "regret_served_learned": (t_l - t_b) / t_b, "regret_served_heuristic": (t_h - t_b) / t_b,
            "learned_vs_heuristic": t_h / t_l,
            "regret_per_job_model_learned": float(np.mean((per_job[rows, learned] - per_job.min(1)) / per_job.min(1))),
-           "plan_ms": t_plan * 1e3, "autotune_s": t_tune, "shape_classes": len(first),
+           "plan_ms": t_plan * 1e3, "plan_rank_ms": t_plan_rank * 1e3, "autotune_s": t_tune,
+           "shape_classes": len(first),
            "variant_share_learned": np.bincount(learned, minlength=sched.N_VARIANTS).tolist(),
            "variant_share_best": np.bincount(best, minlength=sched.N_VARIANTS).tolist(),
+           "rank_variants": list(sched.RANK_VARIANT_NAMES),
+           "rank_variant_share_learned": np.bincount(np.maximum(learned_rank, 0),
+                                                     minlength=sched.N_RANK_VARIANTS).tolist(),
+           "rank_variant_share_best": np.bincount(np.maximum(best_rank, 0), minlength=sched.N_RANK_VARIANTS).tolist(),
            "ranks_equal_across_plans": bool(np.array_equal(r_h, r_l) and np.array_equal(r_h, r_b)),
            "rank_checks": ms.check_ranks(r_l),
            "planner": "MLP 5-64-64-64-4 (hand-written FP32 training / BF16 inference kernels) trained on "
-                      "hme_autotune_batch timings (python -m hacs_b200.sched_train --batch)"}
+                      "hme_autotune_batch timings (python -m hacs_b200.sched_train --batch); the rank rounds' "
+                      "planner: the same network trained on hme_autotune_batch_rank timings "
+                      "(python -m hacs_b200.sched_train --rank)" + ("" if have_rank else " -- not trained: rule")}
+    if have_rank:
+        per_job_r = np.array([TR[k] for k in keys])
+        out["regret_per_job_model_learned_rank"] = float(np.mean(
+            (per_job_r[rows, learned_rank] - per_job_r.min(1)) / per_job_r.min(1)))
+        rr = sched.rank_rule(shapes[:, 1])
+        out["regret_per_job_model_rule_rank"] = float(np.mean((per_job_r[rows, rr] - per_job_r.min(1)) /
+                                                              per_job_r.min(1)))
     return out
 
 
@@ -842,12 +875,14 @@ def run_case(args):
         eng.close()
         return 0
     if kind == "jobs":
-        # jobs:<count>: the first <count> jobs of the config-4 stream, batched GEMM + rank
+        # jobs:<count>[:<rank schedule>]: the first <count> jobs of the config-4 stream, batched GEMM + rank
+        # (every job's rank rounds on the given schedule, 0..3; default: the batch rule)
         import ctypes as C_
 
-        from hacs_b200 import gen
+        from hacs_b200 import gen, stream
 
         nj = int(parts[1])
+        rv = int(parts[2]) if len(parts) > 2 else -1
         eng = hacs_b200.Engine(0)
         s, fam, pj, sa, sb = gen.job_stream(10000)
         s, fam, pj, sa, sb = s[:nj], fam[:nj], pj[:nj], sa[:nj], sb[:nj]
@@ -862,14 +897,39 @@ def run_case(args):
             specs += [(A, int(pj[j]), int(fam[j]), int(sa[j])), (B, int(pj[j]), int(fam[j]), int(sb[j]))]
         arr = eng._jobs(jobs)
         ranks = np.zeros(nj, np.uint32)
-        t0 = time.perf_counter()
-        for _ in range(max(1, args.warmup + args.steps)):
+        rvar = np.full(nj, rv, np.int32)
+        ip = C_.POINTER(C_.c_int)
+
+        def stream_once():
+            hacs_b200.check(eng._lib.hme_batch_gemm_rank_u32_dev_sched(eng._h, nj, arr, None, rvar.ctypes.data_as(ip),
+                                                                       ranks.ctypes.data_as(C_.POINTER(C_.c_uint32))))
+
+        for _ in range(max(0, args.warmup)):
             eng.gen_jobs_dev(specs)
-            hacs_b200.check(eng._lib.hme_batch_gemm_rank_u32_dev(eng._h, nj, arr,
-                                                                 ranks.ctypes.data_as(C_.POINTER(C_.c_uint32))))
-        dt = (time.perf_counter() - t0) / max(1, args.warmup + args.steps)
-        print(json.dumps(default=_json, obj={"case": args.case, "s_per_stream": dt, "rank_sum": int(ranks.sum())}),
-              flush=True)
+            stream_once()
+        dt = 0.0
+        for _ in range(max(1, args.steps)):
+            eng.gen_jobs_dev(specs)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            stream_once()
+            dt += time.perf_counter() - t0
+        dt /= max(1, args.steps)
+        out = {"case": args.case, "s_per_stream": dt, "jobs_per_s": nj / dt, "rank_sum": int(ranks.sum())}
+        gold = stream.golden_jobs() if nj <= 10000 else None
+        if gold is not None:
+            out["ranks_equal_reference"] = bool(np.array_equal(ranks.astype(np.int64), gold[0][:nj]))
+        # per-kernel device times of one more stream (library timer: rounds launched directly, no graph)
+        eng.set_timing(True)
+        eng.timing_reset()
+        eng.gen_jobs_dev(specs)
+        stream_once()
+        eng.sync()
+        names = ("grouped_gemm", "grouped_split", "batch_panel", "batch_simt_update", "batch_trsm",
+                 "batch_permute", "batch_gather", "rank_post", "rank_plan", "limb_gemm", "simt_gemm")
+        out["kernels_ms"] = {k: round(eng.kernel_time(k)[0], 3) for k in names if eng.kernel_time(k)[1]}
+        eng.set_timing(False)
+        print(json.dumps(default=_json, obj=out), flush=True)
         eng.close()
         return 0
     if kind == "mlp":
@@ -888,6 +948,16 @@ def run_case(args):
         print(json.dumps(default=_json, obj={"case": args.case, "loss": float(loss),
                           "plan_share": np.bincount(plan, minlength=sched.N_VARIANTS).tolist()}), flush=True)
         mlp.close()
+        eng.close()
+        return 0
+    if kind == "sched5":
+        # sched5[:<jobs>]: the config-5 mixed stream served under the learned, batch-rule and autotuned plans
+        # (both phases' schedules), the same figures as the bench line's extras.scheduler_config5
+        torch.cuda.set_stream(torch.cuda.Stream())
+        eng = hacs_b200.Engine(0)
+        eng.use_torch_stream()
+        out = extra_scheduler(eng, int(parts[1]) if len(parts) > 1 else 50000)
+        print(json.dumps(default=_json, obj={"case": args.case, **out}), flush=True)
         eng.close()
         return 0
     if kind == "gemm64":
@@ -1058,7 +1128,8 @@ def main():
                          "U*D*V; jobs:<count> runs W + K batched GEMM + rank streams of the first <count> jobs; "
                          "mlp:<rows> trains the scheduler MLP for K epochs and plans <rows> shapes; level12:<m>:<n>:<p> "
                          "times the device level-1 / level-2 operations on m x n operands; gemm64:<n>:<p> runs the "
-                         "u64-residue GEMM beside the plain method")
+                         "u64-residue GEMM beside the plain method; sched5[:<jobs>] serves the config-5 mixed stream under "
+                         "the learned, batch-rule and autotuned plans")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -442,17 +442,42 @@ class Engine:
         arr = self._jobs(jobs)
         check(self._lib.hme_batch_gemm_u32_dev(self._h, len(jobs), arr))
 
-    def batch_rank_dev(self, jobs) -> np.ndarray:
-        """rank of each C_j over F_{p_j} (destroys C_j)."""
+    @staticmethod
+    def _variants(v, n):
+        if v is None:
+            return None
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=np.int32), (n,)))
+        return a
+
+    def batch_rank_dev(self, jobs, rank_variants=None) -> np.ndarray:
+        """rank of each C_j over F_{p_j} (destroys C_j).  rank_variants: per-job
+        schedules of the rank rounds (0..3, -1 the batch rule; a scalar applies to
+        every job; None: the context's scheduler)."""
         arr = self._jobs(jobs)
         ranks = np.zeros(max(1, len(jobs)), np.uint32)
-        check(self._lib.hme_batch_rank_u32_dev(self._h, len(jobs), arr, _p32(ranks)))
+        rv = self._variants(rank_variants, len(jobs))
+        if rv is None:
+            check(self._lib.hme_batch_rank_u32_dev(self._h, len(jobs), arr, _p32(ranks)))
+        else:
+            check(self._lib.hme_batch_rank_u32_dev_sched(self._h, len(jobs), arr,
+                                                         rv.ctypes.data_as(C.POINTER(C.c_int)), _p32(ranks)))
         return ranks[: len(jobs)].copy()
 
-    def batch_gemm_rank_dev(self, jobs) -> np.ndarray:
+    def batch_gemm_rank_dev(self, jobs, gemm_variants=None, rank_variants=None) -> np.ndarray:
+        """C_j = A_j B_j mod p_j, then rank(C_j): the GEMM phase under per-job GEMM
+        schedules, the rank phase under per-job rank schedules (None: the
+        context's scheduler for that phase)."""
         arr = self._jobs(jobs)
         ranks = np.zeros(max(1, len(jobs)), np.uint32)
-        check(self._lib.hme_batch_gemm_rank_u32_dev(self._h, len(jobs), arr, _p32(ranks)))
+        if gemm_variants is None and rank_variants is None:
+            check(self._lib.hme_batch_gemm_rank_u32_dev(self._h, len(jobs), arr, _p32(ranks)))
+        else:
+            gv = self._variants(gemm_variants, len(jobs))
+            rv = self._variants(rank_variants, len(jobs))
+            ip = C.POINTER(C.c_int)
+            check(self._lib.hme_batch_gemm_rank_u32_dev_sched(
+                self._h, len(jobs), arr, gv.ctypes.data_as(ip) if gv is not None else None,
+                rv.ctypes.data_as(ip) if rv is not None else None, _p32(ranks)))
         return ranks[: len(jobs)].copy()
 
     def gen_jobs_dev(self, specs) -> None:

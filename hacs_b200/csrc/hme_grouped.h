@@ -77,7 +77,23 @@ struct BatchMatrix {
     uint32_t* A = nullptr;
     size_t ld = 0;
     uint32_t m = 0, n = 0, p = 0;
+    int rank_variant = 0;  // the schedule of its rank rounds (RankVariant)
 };
+
+// The schedules of a job's rank rounds: the trailing-update variant (the
+// grouped tensor-core limb GEMM or the CUDA-core update) and the widest last
+// panel (a job whose remaining columns fit it finishes in that one panel, on
+// one CTA, with no trailing update; otherwise its rounds take 32 columns).
+// Every schedule computes the same rank; only the time changes.
+enum RankVariant {
+    kRankTensorLast128 = 0,  // grouped limb GEMM, last panel up to 128 columns (the batch rule)
+    kRankTensorLast32 = 1,   // grouped limb GEMM, 32-column rounds to the end
+    kRankSimtLast128 = 2,    // CUDA-core update, last panel up to 128 columns
+    kRankSimtLast32 = 3,     // CUDA-core update, 32-column rounds to the end
+    kRankVariants = 4
+};
+inline int rank_variant_last(int v) { return v == kRankTensorLast32 || v == kRankSimtLast32 ? 32 : 128; }
+inline bool rank_variant_simt(int v) { return v == kRankSimtLast128 || v == kRankSimtLast32; }
 
 // ranks[j] = rank of mats[j] over F_p (destroys the matrices).
 void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::vector<int>& ranks);

@@ -135,6 +135,7 @@ struct hme_ctx {
     int fixed_variant = -1;          // >= 0: every GEMM of this context uses that variant
     int sched_policy = 0;            // 0 shape heuristic, 1 learned planner table
     void* sched_table = nullptr;     // planner decisions by shape class (sched.cu)
+    void* sched_rank_table = nullptr;  // the rank rounds' planner decisions by shape class (sched.cu)
     int gemm_sm_cap = 0;             // > 0: persistent GEMM grids use at most this many SMs
     cudaStream_t aux_stream = nullptr;   // elimination: the lookahead panel's stream (created on first use)
     void* elim_pinned = nullptr;         // elimination: pinned copies of the panel scratch, permutations
@@ -263,6 +264,8 @@ int sched_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uin
 // The learned plan's decision for one product's shape class, or -1 when the
 // plan holds none (sched.cu).
 int sched_planned_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k);
+// The same for the schedule of a batched job's rank rounds (RankVariant).
+int sched_planned_rank_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k);
 void sched_release(hme_ctx* ctx);
 
 }  // namespace hme

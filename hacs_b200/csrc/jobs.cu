@@ -102,6 +102,8 @@ struct RankDev {
     uint32_t* tmp;        // 64 x n: rows in flight during the row moves
     int* mv;              // 64 sources, then 64 destinations
     uint32_t kmax;        // delayed-reduction bound of p
+    int last_max;         // the job's schedule: the widest last panel (columns; 32 or kMaxBw)
+    int simt;             // the job's schedule: 1 = CUDA-core trailing update, 0 = the grouped limb GEMM
 };
 
 struct RankOut {
@@ -320,6 +322,8 @@ struct SolveJob {
     uint32_t* L21;     // (m - r0 - k) x k
     uint32_t* Linv;    // k x k: L11^-1
     uint32_t kmax;     // products a 64-bit sum starting below p holds before a reduction
+    int simt;          // the trailing update A22 -= L21 U12 on CUDA cores (batch_simt_update_kernel)
+    int simt_base;     // the job's first entry in the round's CUDA-core tile list
 };
 // U12 = L11^-1 A12 for every job with a pivot block, in two launches:
 // batch_linv_kernel, one CTA per job: L11^-1 column by column (forward
@@ -427,6 +431,107 @@ __global__ void batch_gather_l21_kernel(const SolveJob* __restrict__ jobs) {
     }
 }
 
+// The CUDA-core trailing update, for the jobs whose schedule takes it
+// (SolveJob::simt): A22 -= L21 U12 mod p with L21 the compact (below x k)
+// gather and U12 the pivot rows' trailing columns, k <= kRoundBw.  The work
+// is a list of 64 x 64 tiles of A22 built by rank_post_kernel (each job
+// appends its tiles; tile_job[t] = the job, t - simt_base its tile in row-major
+// tile order), taken by a persistent grid, so a large job's tiles spread over
+// the whole GPU and the launch has no idle CTAs for jobs on the other
+// schedule.  A CTA stages the tile's L21 rows and U12 columns in shared
+// memory and gives each thread 4 x 4 outputs (rows ty + 16a, columns tx + 16b,
+// so a half warp writes 16 consecutive words of a row); each output is an
+// exact dot product reduced once: a 64-bit sum when kRoundBw (p - 1)^2 fits
+// 64 bits (one wide multiply-add per product), else a 96-bit sum
+// (mad.lo.cc / madc.hi.cc / addc).  No limb planes, no split, no tensor map.
+constexpr int kSimtTile = 64;
+__host__ __device__ inline int simt_tiles(int rows, int cols) {
+    return ((rows + kSimtTile - 1) / kSimtTile) * ((cols + kSimtTile - 1) / kSimtTile);
+}
+__global__ void __launch_bounds__(256) batch_simt_update_kernel(const SolveJob* __restrict__ jobs,
+                                                                const int* __restrict__ tile_job,
+                                                                const int* __restrict__ count) {
+    __shared__ uint32_t sL[kSimtTile][kRoundBw + 1];
+    __shared__ uint32_t sU[kRoundBw][kSimtTile];
+    const int total = *count;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {  // t is the same for the whole CTA
+        const SolveJob& J = jobs[tile_job[t]];
+        const int k = J.k, below = J.m - J.r0 - k;
+        const int tc = (J.ntrail + kSimtTile - 1) / kSimtTile;
+        const int local = t - J.simt_base;
+        const int i0 = (local / tc) * kSimtTile, j0 = (local % tc) * kSimtTile;
+        const uint32_t* U = J.A + static_cast<size_t>(J.r0) * J.ld + J.c1;
+        uint32_t* A22 = J.A + static_cast<size_t>(J.r0 + k) * J.ld + J.c1;
+        __syncthreads();  // the previous tile's operands are consumed
+        for (int idx = threadIdx.x; idx < kSimtTile * k; idx += blockDim.x) {
+            const int i = idx / k, s = idx - i * k;
+            sL[i][s] = i0 + i < below ? J.L21[static_cast<size_t>(i0 + i) * k + s] : 0u;
+        }
+        for (int idx = threadIdx.x; idx < k * kSimtTile; idx += blockDim.x) {
+            const int s = idx / kSimtTile, j = idx % kSimtTile;
+            sU[s][j] = j0 + j < J.ntrail ? U[static_cast<size_t>(s) * J.ld + j0 + j] : 0u;
+        }
+        __syncthreads();
+        auto sub = [&](int a, int b, uint32_t d) {  // A22(i, j) -= d mod p
+            const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+            if (i >= below || j >= J.ntrail) return;
+            uint32_t* c = A22 + static_cast<size_t>(i) * J.ld + j;
+            const uint32_t x = *c;
+            *c = x >= d ? x - d : x + (J.p - d);
+        };
+        const uint64_t pm1 = J.p - 1u;
+        if (pm1 * pm1 <= ~0ull / kRoundBw) {
+            // k <= kRoundBw products below (p - 1)^2 sum exactly in 64 bits: one wide multiply-add each
+            uint64_t acc[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] = 0u;
+            for (int s = 0; s < k; ++s) {
+                uint32_t l[4], u[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) l[a] = sL[ty + 16 * a][s];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) u[b] = sU[s][tx + 16 * b];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) acc[a][b] += static_cast<uint64_t>(l[a]) * u[b];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) sub(a, b, reduce_u64(acc[a][b], J.p, J.barrett));
+        } else {
+            uint32_t a0[4][4], a1[4][4], a2[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) a0[a][b] = a1[a][b] = a2[a][b] = 0u;
+            for (int s = 0; s < k; ++s) {
+                uint32_t l[4], u[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) l[a] = sL[ty + 16 * a][s];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) u[b] = sU[s][tx + 16 * b];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) mac96(a0[a][b], a1[a][b], a2[a][b], l[a], u[b]);
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const uint64_t h =
+                        reduce_u64((static_cast<uint64_t>(a2[a][b]) << 32) | a1[a][b], J.p, J.barrett);
+                    sub(a, b, reduce_u64((h << 32) | a0[a][b], J.p, J.barrett));
+                }
+        }
+    }
+}
+
 size_t a256(size_t x) { return (x + 255) / 256 * 256; }
 
 // ---- device-driven rounds ----------------------------------------------------------------
@@ -460,7 +565,7 @@ __global__ void rank_plan_kernel(RankDev* __restrict__ devs, int nj, int* __rest
         if (!D.active) continue;
         const int rows = D.J.m - D.J.r0, left = D.J.n - D.J.c0;
         const int wfit = (kRankSmem - rows - 16) / (4 * (rows | 1));
-        const bool last = left <= min(kMaxBw, wfit);
+        const bool last = left <= min(D.last_max, wfit);
         D.J.w = last ? left : min(kRoundBw, wfit);
         const int b = row_class(rows) + (last ? kRowClasses : 0);
         const int idx = atomicAdd(&counters[b], 1);
@@ -475,7 +580,8 @@ __global__ void rank_post_kernel(RankDev* __restrict__ devs, int nj, const RankO
                                  PermJob* __restrict__ perms, SolveJob* __restrict__ solves,
                                  GroupedProblem* __restrict__ gprob, GroupedSplitJob* __restrict__ gsplit,
                                  int* __restrict__ tiles, int* __restrict__ blocks,
-                                 const RankGroup* __restrict__ groups) {
+                                 const RankGroup* __restrict__ groups, int* __restrict__ simt_tile_job,
+                                 int* __restrict__ simt_count) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nj; j += gridDim.x * blockDim.x) {
         RankDev& D = devs[j];
         RankJob& J = D.J;
@@ -486,6 +592,7 @@ __global__ void rank_post_kernel(RankDev* __restrict__ devs, int nj, const RankO
         sj.m = 0;
         sj.r0 = 0;
         sj.ntrail = 0;
+        sj.simt = 0;
         tiles[j] = 0;
         blocks[j] = 0;
         if (!D.active) continue;
@@ -547,6 +654,16 @@ __global__ void rank_post_kernel(RankDev* __restrict__ devs, int nj, const RankO
             sj.L21 = D.L21;
             sj.Linv = D.Linv;
             sj.kmax = D.kmax;
+            sj.simt = D.simt;
+            if (D.simt) {  // the job's tiles join the round's CUDA-core tile list
+                const int nt = simt_tiles(below, ntrail);
+                const int base = atomicAdd(simt_count, nt);
+                sj.simt_base = base;
+                for (int i = 0; i < nt; ++i) simt_tile_job[base + i] = j;
+            }
+        }
+        if (k > 0 && ntrail > 0 && below > 0 && !D.simt) {
+            // the trailing update as the group's grouped limb GEMM: split and GEMM entries
             const RankGroup& G = groups[D.group];
             const int jl = j - G.begin;
             GroupedProblem& gp = gprob[j];
@@ -716,6 +833,8 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
     size_t buf_bytes = 0, plane_bytes = 0;
     std::vector<size_t> off_l21(nj), off_linv(nj), off_tmp(nj), off_mv(nj), g_planes(ng);
     std::vector<size_t> g_tiles(ng, 0), g_blocks(ng, 0);
+    bool any_simt = false;
+    size_t simt_cap = 0;  // CUDA-core tiles the round's list can hold: every such job's first-round tile count
     uint32_t max_n = 0;
     for (int g = 0; g < ng; ++g) {
         const ModParams mp = make_mod(gmod[g]);
@@ -742,6 +861,13 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
             J.out = i;
             D.active = 1;
             D.group = g;
+            D.last_max = rank_variant_last(M.rank_variant);
+            D.simt = rank_variant_simt(M.rank_variant) ? 1 : 0;
+            if (D.simt) {
+                any_simt = true;
+                simt_cap += static_cast<size_t>(simt_tiles(static_cast<int>(M.m), static_cast<int>(M.n)));
+            }
+            max_n = std::max(max_n, M.n);
             D.a_row0 = static_cast<int>(sm);
             D.b_col0 = static_cast<int>(sn);
             sm += M.m;
@@ -762,7 +888,6 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
             const int bn = grouped_bn_wide(L);
             g_tiles[g] += static_cast<size_t>((M.m + limb::kBM - 1) / limb::kBM) * ((M.n + bn - 1) / bn);
             g_blocks[g] += 64 + (M.n + 31) / 32;
-            max_n = std::max(max_n, M.n);
         }
         RankGroup& G = groups[g];
         G.sum_m = sm;
@@ -785,7 +910,8 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
     const size_t o_gprob = take(sizeof(GroupedProblem) * nj), o_gsplit = take(sizeof(GroupedSplitJob) * nj);
     const size_t o_tiles = take(sizeof(int) * nj), o_blocks = take(sizeof(int) * nj);
     const size_t o_lists = take(sizeof(int) * kBuckets2 * static_cast<size_t>(nj));
-    const size_t o_counters = take(sizeof(int) * kBuckets2);
+    const size_t o_counters = take(sizeof(int) * (kBuckets2 + 1));  // the buckets' counts, the CUDA-core tiles'
+    const size_t o_simt = take(sizeof(int) * std::max<size_t>(1, simt_cap));
     const size_t o_groups = take(sizeof(RankGroup) * ng), o_maps = take(sizeof(CUtensorMap) * 2 * ng);
     const size_t o_totals = take(sizeof(int) * 2 * ng);
     std::vector<size_t> o_tp(ng), o_bj(ng);
@@ -806,6 +932,8 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
     int* d_blocks = reinterpret_cast<int*>(tables + o_blocks);
     int* d_lists = reinterpret_cast<int*>(tables + o_lists);
     int* d_counters = reinterpret_cast<int*>(tables + o_counters);
+    int* d_simt_count = d_counters + kBuckets2;
+    int* d_simt_tiles = reinterpret_cast<int*>(tables + o_simt);
     RankGroup* d_groups = reinterpret_cast<RankGroup*>(tables + o_groups);
     CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(tables + o_maps);
     int* d_totals = reinterpret_cast<int*>(tables + o_totals);
@@ -871,11 +999,37 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
         }
         bucket_grid[b] = std::max(1, std::min(nj, ctx->num_sms * std::max(1, occ)));
     }
+    int simt_grid = 1;
+    if (any_simt) {  // persistent: every resident CTA of the GPU, no more than the list can hold
+        int occ = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_simt_update_kernel, 256, 0);
+        simt_grid = static_cast<int>(std::max<size_t>(1, std::min<size_t>(simt_cap, static_cast<size_t>(ctx->num_sms) *
+                                                                                      std::max(1, occ))));
+    }
+    // with per-kernel timing on, every launch stays on the context's stream (the timer's events are there)
+    const bool fork = any_simt && !ctx->timer.on;
+    struct EventPair {
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~EventPair() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } evs;
+    if (fork) {
+        if (!ctx->aux_stream) {
+            int lo = 0, hi = 0;
+            HME_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            HME_CUDA(cudaStreamCreateWithPriority(&ctx->aux_stream, cudaStreamNonBlocking, hi));
+        }
+        HME_CUDA(cudaEventCreateWithFlags(&evs.a, cudaEventDisableTiming));
+        HME_CUDA(cudaEventCreateWithFlags(&evs.b, cudaEventDisableTiming));
+    }
+    const cudaEvent_t ev_fork = evs.a, ev_join = evs.b;
     HME_CUDA(cudaGetLastError());
     const size_t linv_smem = batch_linv_smem(kRoundBw), apply_smem = batch_apply_smem(kRoundBw);
     const int small_grid = std::max(1, std::min((nj + 255) / 256, ctx->num_sms * 8));
     auto round = [&]() {
-        HME_CUDA(cudaMemsetAsync(d_counters, 0, sizeof(int) * kBuckets2, ctx->stream));
+        HME_CUDA(cudaMemsetAsync(d_counters, 0, sizeof(int) * (kBuckets2 + 1), ctx->stream));
         HME_TIMED(ctx, "rank_plan", rank_plan_kernel<<<small_grid, 256, 0, ctx->stream>>>(d_devs, nj, d_lists, d_counters));
         for (int b = 0; b < kBuckets2; ++b) {
             const int* list = d_lists + static_cast<size_t>(b) * nj;
@@ -889,7 +1043,8 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
             }
         }
         HME_TIMED(ctx, "rank_post", rank_post_kernel<<<small_grid, 256, 0, ctx->stream>>>(
-                                         d_devs, nj, d_outs, d_perm, d_solve, d_gprob, d_gsplit, d_tiles, d_blocks, d_groups));
+                                         d_devs, nj, d_outs, d_perm, d_solve, d_gprob, d_gsplit, d_tiles, d_blocks, d_groups,
+                                         d_simt_tiles, d_simt_count));
         HME_TIMED(ctx, "rank_post", rank_scan_kernel<<<ng, 1024, 0, ctx->stream>>>(d_groups, d_tiles, d_blocks, d_gprob,
                                                                                   d_gsplit));
         HME_TIMED(ctx, "rank_post", rank_fill_kernel<<<small_grid, 256, 0, ctx->stream>>>(d_groups, d_devs, nj, d_tiles,
@@ -902,11 +1057,24 @@ void batch_rank_device(hme_ctx* ctx, const std::vector<BatchMatrix>& mats, std::
             HME_TIMED(ctx, "batch_trsm", batch_apply_kernel<<<dim3(32, nb), 256, apply_smem, ctx->stream>>>(d_solve + b0));
             HME_TIMED(ctx, "batch_gather", batch_gather_l21_kernel<<<dim3(8, nb), 256, 0, ctx->stream>>>(d_solve + b0));
         }
+        if (fork) {
+            // the CUDA-core updates on the second stream, beside the grouped split + GEMM of the other
+            // jobs (disjoint jobs, so disjoint data); joined before the round ends
+            HME_CUDA(cudaEventRecord(ev_fork, ctx->stream));
+            HME_CUDA(cudaStreamWaitEvent(ctx->aux_stream, ev_fork, 0));
+            batch_simt_update_kernel<<<simt_grid, 256, 0, ctx->aux_stream>>>(d_solve, d_simt_tiles, d_simt_count);
+            ++ctx->launches;
+            HME_CUDA(cudaEventRecord(ev_join, ctx->aux_stream));
+        } else if (any_simt) {
+            HME_TIMED(ctx, "batch_simt_update",
+                      batch_simt_update_kernel<<<simt_grid, 256, 0, ctx->stream>>>(d_solve, d_simt_tiles, d_simt_count));
+        }
         for (int g = 0; g < ng; ++g) {
             const RankGroup& G = groups[g];
             grouped_launch_device_tables(ctx, make_mod(gmod[g]), d_gsplit + G.begin, G.block_job, G.totals + 1,
                                          d_gprob + G.begin, G.tile_prob, G.totals);
         }
+        if (fork) HME_CUDA(cudaStreamWaitEvent(ctx->stream, ev_join, 0));
         HME_CUDA(cudaGetLastError());
     };
     for (int g = 0; g < ng; ++g) grouped_prepare_device_tables(make_mod(gmod[g]).limbs);
@@ -1030,14 +1198,38 @@ void batch_gemm(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs, const int* va
     }
 }
 
-void batch_rank(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs, uint32_t* ranks) {
+// The batch rule of the rank rounds (the method without the planner): the
+// grouped tensor-core limb GEMM as the trailing update, and one last panel of
+// up to 128 columns only for jobs of at most 128 rows -- a taller job's last
+// panel is a long serial chain on one CTA that every job of the round waits
+// for, so its rounds take 32 columns to the end.
+int rank_rule(uint32_t m) { return m <= 128 ? kRankTensorLast128 : kRankTensorLast32; }
+
+// The rank phase of a batch.  Every job's rank rounds follow one of the
+// RankVariant schedules: from `rank_variants` when given (-1 = the batch rule),
+// else under the learned policy the planner's decision for the job's shape
+// class (unplanned shapes: the batch rule).  A schedule changes which kernels
+// apply a job's trailing updates and how many columns a round takes, never a
+// residue or the rank.
+void batch_rank(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs, uint32_t* ranks,
+                const int* rank_variants = nullptr) {
     std::vector<BatchMatrix> mats(njobs);
     for (uint32_t t = 0; t < njobs; ++t) {
+        if (rank_variants)
+            HME_REQUIRE(rank_variants[t] >= kBatchRule && rank_variants[t] < kRankVariants,
+                        "job: unknown rank schedule");
         mats[t].A = jobs[t].C;
         mats[t].ld = jobs[t].ldc;
         mats[t].m = jobs[t].m;
         mats[t].n = jobs[t].n;
         mats[t].p = jobs[t].p;
+        int v = kBatchRule;
+        if (rank_variants) {
+            v = rank_variants[t];
+        } else if (ctx->sched_policy == 1 && jobs[t].p >= 2) {
+            v = sched_planned_rank_variant(ctx, make_mod(jobs[t].p), jobs[t].m, jobs[t].n, jobs[t].k);
+        }
+        mats[t].rank_variant = v < 0 ? rank_rule(jobs[t].m) : v;
     }
     std::vector<int> r;
     batch_rank_device(ctx, mats, r);
@@ -1089,6 +1281,112 @@ int hme_batch_gemm_rank_u32_dev_plan(hme_ctx* ctx, uint32_t njobs, const hme_job
         bind(ctx);
         batch_gemm(ctx, njobs, jobs, variants);
         batch_rank(ctx, njobs, jobs, ranks);
+    });
+}
+
+int hme_batch_rank_u32_dev_sched(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs, const int* rank_variants,
+                                 uint32_t* ranks) {
+    return guard([&] {
+        HME_REQUIRE(ctx && (njobs == 0 || (jobs && ranks)), "null argument");
+        bind(ctx);
+        batch_rank(ctx, njobs, jobs, ranks, rank_variants);
+    });
+}
+
+int hme_batch_gemm_rank_u32_dev_sched(hme_ctx* ctx, uint32_t njobs, const hme_job* jobs, const int* gemm_variants,
+                                      const int* rank_variants, uint32_t* ranks) {
+    return guard([&] {
+        HME_REQUIRE(ctx && (njobs == 0 || (jobs && ranks)), "null argument");
+        bind(ctx);
+        if (rank_variants)  // every argument checked before anything runs
+            for (uint32_t t = 0; t < njobs; ++t)
+                HME_REQUIRE(rank_variants[t] >= kBatchRule && rank_variants[t] < kRankVariants,
+                            "job: unknown rank schedule");
+        batch_gemm(ctx, njobs, jobs, gemm_variants);
+        batch_rank(ctx, njobs, jobs, ranks, rank_variants);
+    });
+}
+
+int hme_autotune_batch_rank(hme_ctx* ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, float density,
+                            uint32_t count, int reps, float* ms) {
+    return guard([&] {
+        HME_REQUIRE(ctx && ms && m && n && k && count, "autotune_batch_rank: bad arguments");
+        HME_REQUIRE(m <= 1024, "autotune_batch_rank: rows beyond 1024 take the single-matrix elimination");
+        HME_REQUIRE(is_prime_u32(p), "autotune_batch_rank: the modulus must be prime");
+        bind(ctx);
+        // count products C = A B of the stream's construction (banded sparse operands below density 0.5,
+        // dense uniform ones otherwise), so the rounds meet the ranks and pivot patterns such jobs have, and
+        // one anchor: a dense 1024 x 1024 product of full rank on the batch rule, whose rounds run the whole
+        // 34-round sequence as the stream's largest jobs do.  A schedule's cost is its jobs' MARGINAL time
+        // beside the anchor (the batch with them minus the anchor alone): what the jobs add to a stream whose
+        // rounds run anyway, not the latency of a small batch alone.
+        constexpr uint32_t kAnchor = 1024;
+        const size_t ea = static_cast<size_t>(m) * k, eb = static_cast<size_t>(k) * n, ec = static_cast<size_t>(m) * n;
+        const size_t anc = static_cast<size_t>(kAnchor) * kAnchor;
+        const size_t ab_all = (ea + eb) * count + 2 * anc, c_all = ec * count + anc;
+        uint32_t* AB = static_cast<uint32_t*>(ctx->ws.get(kSlotSched0, sizeof(uint32_t) * ab_all));
+        uint32_t* Cs = static_cast<uint32_t*>(ctx->ws.get(kSlotSched1, sizeof(uint32_t) * 2 * c_all));
+        uint32_t* C0 = Cs + c_all;
+        std::vector<GenSpec> specs(2 * static_cast<size_t>(count) + 2);
+        std::vector<hme_job> jobs(count + 1);
+        const int family = density < 0.5f ? 0 : 1;
+        for (uint32_t t = 0; t < count; ++t) {
+            uint32_t* A = AB + t * (ea + eb);
+            uint32_t* B = A + ea;
+            specs[2 * t] = GenSpec{A, k, m, k, p, family, 0x5EED0000ull + 2 * t};
+            specs[2 * t + 1] = GenSpec{B, n, k, n, p, family, 0x5EED0001ull + 2 * t};
+            jobs[t] = hme_job{p, m, n, k, A, k, B, n, C0 + t * ec, n};
+        }
+        uint32_t* Aa = AB + (ea + eb) * count;
+        uint32_t* Ba = Aa + anc;
+        specs[2 * count] = GenSpec{Aa, kAnchor, kAnchor, kAnchor, p, 1, 0xA5C40000ull};
+        specs[2 * count + 1] = GenSpec{Ba, kAnchor, kAnchor, kAnchor, p, 1, 0xA5C40001ull};
+        jobs[count] = hme_job{p, kAnchor, kAnchor, kAnchor, Aa, kAnchor, Ba, kAnchor, C0 + ec * count, kAnchor};
+        gen_jobs_device(ctx, specs);
+        batch_gemm(ctx, count + 1, jobs.data());
+        for (uint32_t t = 0; t <= count; ++t) jobs[t].C = Cs + (jobs[t].C - C0);  // the copies the ranks destroy
+        cudaEvent_t e0, e1;
+        HME_CUDA(cudaEventCreate(&e0));
+        HME_CUDA(cudaEventCreate(&e1));
+        std::vector<int> var(count + 1, kBatchRule);
+        std::vector<uint32_t> rk(count + 1), rk0(count + 1);
+        // the median time of a batched rank of `nj` jobs starting at jobs[j0] (fresh copies every run)
+        auto timed = [&](uint32_t j0, uint32_t nj, bool check) {
+            std::vector<float> t;
+            for (int r = -1; r < std::max(1, reps); ++r) {  // r = -1: warm
+                HME_CUDA(cudaMemcpyAsync(Cs, C0, sizeof(uint32_t) * c_all, cudaMemcpyDeviceToDevice, ctx->stream));
+                HME_CUDA(cudaEventRecord(e0, ctx->stream));
+                batch_rank(ctx, nj, jobs.data() + j0, rk.data(), var.data() + j0);
+                HME_CUDA(cudaEventRecord(e1, ctx->stream));
+                HME_CUDA(cudaEventSynchronize(e1));
+                float x = 0.f;
+                HME_CUDA(cudaEventElapsedTime(&x, e0, e1));
+                if (r >= 0) t.push_back(x);
+                if (check) {
+                    if (rk0[count] == 0) rk0 = rk;  // the anchor's rank is 1024: the first run's ranks are kept
+                    // a schedule changes only the time: the same ranks under every schedule
+                    HME_REQUIRE(rk == rk0, "autotune_batch_rank: schedules disagree on a rank");
+                }
+            }
+            std::sort(t.begin(), t.end());
+            return t[t.size() / 2];
+        };
+        try {
+            const float t_anchor = timed(count, 1, false);
+            for (int v = 0; v < kRankVariants; ++v) {
+                std::fill(var.begin(), var.begin() + count, v);
+                const float tv = timed(0, count + 1, true);
+                // a marginal time at or below the anchor's noise is floored at 1 us per batch
+                ms[v] = std::max(tv - t_anchor, 1e-3f) / static_cast<float>(count);
+            }
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        check_device_error(ctx);
     });
 }
 

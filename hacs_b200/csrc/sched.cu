@@ -241,6 +241,13 @@ int sched_planned_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_
     return it == t.end() ? -1 : it->second;
 }
 
+int sched_planned_rank_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k) {
+    if (!ctx->sched_rank_table) return -1;
+    const PlanTable& t = *static_cast<PlanTable*>(ctx->sched_rank_table);
+    auto it = t.find(shape_key(m, n, k, mp.limbs));
+    return it == t.end() ? -1 : it->second;
+}
+
 int sched_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uint32_t k) {
     if (ctx->sched_policy == 1 && ctx->sched_table) {
         const PlanTable& t = *static_cast<PlanTable*>(ctx->sched_table);
@@ -253,6 +260,8 @@ int sched_variant(hme_ctx* ctx, const ModParams& mp, uint32_t m, uint32_t n, uin
 void sched_release(hme_ctx* ctx) {
     delete static_cast<PlanTable*>(ctx->sched_table);
     ctx->sched_table = nullptr;
+    delete static_cast<PlanTable*>(ctx->sched_rank_table);
+    ctx->sched_rank_table = nullptr;
 }
 
 }  // namespace hme
@@ -314,6 +323,39 @@ void fwd_bwd(hme_mlp* mlp, const float* dX, const float* dY, const int* didx, in
     HME_CUDA(cudaGetLastError());
 }
 
+}  // namespace
+
+namespace {
+// BF16 inference of a planner network over the shapes (p, m, n, k), the
+// arg-min per shape into `variants`, and the decisions recorded by shape class
+// in the context's table `*table` (created on first use).
+void sched_plan_into(hme_ctx* ctx, hme_mlp* m, uint32_t n, const uint32_t* shapes, const float* density,
+                     const float* norm, int* variants, void** table) {
+    if (n == 0) return;
+    // features (log2 m, log2 n, log2 k, log2 p, density), normalised by norm[0..4] (mean), norm[5..9] (std)
+    std::vector<float> X(static_cast<size_t>(n) * kIn), Y(static_cast<size_t>(n) * kOut);
+    for (uint32_t t = 0; t < n; ++t) {
+        const uint32_t* s = shapes + 4 * static_cast<size_t>(t);
+        const float f[kIn] = {std::log2(static_cast<float>(std::max(1u, s[1]))),
+                              std::log2(static_cast<float>(std::max(1u, s[2]))),
+                              std::log2(static_cast<float>(std::max(1u, s[3]))),
+                              std::log2(static_cast<float>(std::max(2u, s[0]))), density ? density[t] : 1.0f};
+        for (int i = 0; i < kIn; ++i) X[t * kIn + i] = (f[i] - norm[i]) / norm[kIn + i];
+    }
+    const int rc = hme_mlp_predict_bf16(m, n, X.data(), Y.data());
+    if (rc != HME_OK) throw Error(rc, hme_last_error());
+    if (!*table) *table = new PlanTable();
+    PlanTable& tab = *static_cast<PlanTable*>(*table);
+    for (uint32_t t = 0; t < n; ++t) {
+        int best = 0;
+        for (int v = 1; v < kOut; ++v)
+            if (Y[t * kOut + v] < Y[t * kOut + best]) best = v;
+        variants[t] = best;
+        const uint32_t* s = shapes + 4 * static_cast<size_t>(t);
+        const uint32_t limbs = s[0] <= 256u ? 1u : s[0] <= 65536u ? 2u : s[0] <= (1u << 24) ? 3u : 4u;  // as make_mod
+        tab[shape_key(s[1], s[2], s[3], limbs)] = best;
+    }
+}
 }  // namespace
 
 extern "C" {
@@ -513,35 +555,22 @@ int hme_mlp_predict_bf16(hme_mlp* m, uint32_t n, const float* X, float* Y) {
     });
 }
 
+
 int hme_sched_plan(hme_ctx* ctx, hme_mlp* m, uint32_t n, const uint32_t* shapes, const float* density,
                    const float* norm, int* variants) {
     return guard([&] {
         HME_REQUIRE(ctx && m && shapes && norm && variants, "null argument");
         bind(ctx);
-        if (n == 0) return;
-        // features (log2 m, log2 n, log2 k, log2 p, density), normalised by norm[0..4] (mean), norm[5..9] (std)
-        std::vector<float> X(static_cast<size_t>(n) * kIn), Y(static_cast<size_t>(n) * kOut);
-        for (uint32_t t = 0; t < n; ++t) {
-            const uint32_t* s = shapes + 4 * static_cast<size_t>(t);
-            const float f[kIn] = {std::log2(static_cast<float>(std::max(1u, s[1]))),
-                                  std::log2(static_cast<float>(std::max(1u, s[2]))),
-                                  std::log2(static_cast<float>(std::max(1u, s[3]))),
-                                  std::log2(static_cast<float>(std::max(2u, s[0]))), density ? density[t] : 1.0f};
-            for (int i = 0; i < kIn; ++i) X[t * kIn + i] = (f[i] - norm[i]) / norm[kIn + i];
-        }
-        const int rc = hme_mlp_predict_bf16(m, n, X.data(), Y.data());
-        if (rc != HME_OK) throw Error(rc, hme_last_error());
-        if (!ctx->sched_table) ctx->sched_table = new PlanTable();
-        PlanTable& tab = *static_cast<PlanTable*>(ctx->sched_table);
-        for (uint32_t t = 0; t < n; ++t) {
-            int best = 0;
-            for (int v = 1; v < kOut; ++v)
-                if (Y[t * kOut + v] < Y[t * kOut + best]) best = v;
-            variants[t] = best;
-            const uint32_t* s = shapes + 4 * static_cast<size_t>(t);
-            const uint32_t limbs = s[0] <= 256u ? 1u : s[0] <= 65536u ? 2u : s[0] <= (1u << 24) ? 3u : 4u;  // as make_mod
-            tab[shape_key(s[1], s[2], s[3], limbs)] = best;
-        }
+        sched_plan_into(ctx, m, n, shapes, density, norm, variants, &ctx->sched_table);
+    });
+}
+
+int hme_sched_plan_rank(hme_ctx* ctx, hme_mlp* m, uint32_t n, const uint32_t* shapes, const float* density,
+                        const float* norm, int* variants) {
+    return guard([&] {
+        HME_REQUIRE(ctx && m && shapes && norm && variants, "null argument");
+        bind(ctx);
+        sched_plan_into(ctx, m, n, shapes, density, norm, variants, &ctx->sched_rank_table);
     });
 }
 

@@ -3,8 +3,13 @@ collection with the exhaustive autotuner, training, planning and regret.
 
 A schedule is a GEMM variant (hme_gemm_u32_dev_variant: 0 limb tcgen05 wide
 tiles, 1 limb tcgen05 half-width tiles, 2 CUDA-core 32 x 32, 3 CUDA-core
-64 x 64).  Every variant computes the same residues, so neither the MLP nor
-the autotuner can change a value -- only the time.  The MLP (5 -> 3 x 64 -> 4,
+64 x 64), and for a batched job's rank rounds a rank schedule (0 / 1 the
+grouped tcgen05 limb GEMM as the trailing update, 2 / 3 the CUDA-core update;
+0 / 2 finish a job in one last panel of up to 128 columns, 1 / 3 take 32-column
+rounds to the end), each picked by its own network of the same shape, trained
+on its own autotuner's timings.  Every
+variant computes the same residues (and ranks), so neither the MLP nor the
+autotuner can change a value -- only the time.  The MLP (5 -> 3 x 64 -> 4,
 hand-written CUDA kernels: FP32 training, BF16 inference) predicts each
 variant's normalised log-time from (log2 m, log2 n, log2 k, log2 p, density);
 the exhaustive autotuner (hme_autotune_gemm) times all variants, supplies the
@@ -26,9 +31,22 @@ TIMINGS = os.path.join(DATA, "sched_timings.npz")
 # the batched stream's planner: trained on per-job times inside batches (hme_autotune_batch)
 BATCH_WEIGHTS = os.path.join(DATA, "sched_batch_mlp.npz")
 BATCH_TIMINGS = os.path.join(DATA, "sched_batch_timings.npz")
+# the rank rounds' planner: trained on per-job rank times inside batches (hme_autotune_batch_rank)
+RANK_WEIGHTS = os.path.join(DATA, "sched_rank_mlp.npz")
+RANK_TIMINGS = os.path.join(DATA, "sched_rank_timings.npz")
 BATCH_RULE = -1
 N_VARIANTS = 4
 VARIANT_NAMES = ("tensor-wide", "tensor-narrow", "simt-32", "simt-64")
+# schedules of a batched job's rank rounds: trailing-update variant, widest last panel (columns)
+N_RANK_VARIANTS = 4
+RANK_VARIANT_NAMES = ("tensor/last-128", "tensor/last-32", "simt/last-128", "simt/last-32")
+
+
+def rank_rule(m) -> np.ndarray:
+    """The rank rounds' batch rule (the method without the planner): schedule 0
+    (tensor-core update, one last panel of up to 128 columns) for jobs of at most
+    128 rows, else 1 (32-column rounds to the end); as jobs.cu rank_rule."""
+    return np.where(np.asarray(m) <= 128, 0, 1).astype(np.int32)
 
 _fp = C.POINTER(C.c_float)
 
@@ -142,6 +160,20 @@ class MLP:
                                        v.ctypes.data_as(C.POINTER(C.c_int))))
         return v[:n]
 
+    def plan_rank(self, shapes, density=None) -> np.ndarray:
+        """hme_sched_plan_rank: the same for the rank rounds' schedules (a network
+        trained on hme_autotune_batch_rank timings); records the decisions in the
+        engine's rank plan (policy 1)."""
+        S = np.ascontiguousarray(shapes, dtype=np.uint32)
+        n = S.shape[0]
+        d = _f32(np.ones(n) if density is None else density)
+        v = np.zeros(max(1, n), np.int32)
+        nm = self.norm()
+        check(self._lib.hme_sched_plan_rank(self.engine._h, self._h, n, S.ctypes.data_as(_lib.u32p),
+                                            d.ctypes.data_as(_fp), nm.ctypes.data_as(_fp),
+                                            v.ctypes.data_as(C.POINTER(C.c_int))))
+        return v[:n]
+
 
 def heuristic_choice(F, num_sms: int = 148) -> np.ndarray:
     """The method without the MLP: always the tensor-core GEMM, wide tiles unless
@@ -209,6 +241,24 @@ def autotune_batch(engine, p, m, n, k, count=None, reps: int = 3) -> np.ndarray:
     return ms
 
 
+def rank_batch_count(m, n, k, work: float = 2.0 ** 27, cap: int = 256) -> int:
+    """Jobs of one shape whose ranks the rank autotuner times together: about
+    `work` elimination multiply-adds (m n min(m, n, k)) per batch, 1 .. `cap`."""
+    r = max(1, min(int(m), int(n), int(k)))
+    return int(max(1, min(cap, work // max(1, int(m) * int(n) * r))))
+
+
+def autotune_batch_rank(engine, p, m, n, k, density=1.0, count=None, reps: int = 3) -> np.ndarray:
+    """Per-job marginal device time (ms) of every rank schedule: what `count`
+    products of this shape add to a batch whose rounds run anyway (beside a
+    dense 1024 x 1024 anchor job; hme_autotune_batch_rank)."""
+    ms = np.zeros(N_RANK_VARIANTS, np.float32)
+    c = rank_batch_count(m, n, k) if count is None else int(count)
+    check(_lib.lib().hme_autotune_batch_rank(engine._h, int(p), int(m), int(n), int(k), float(density), c, reps,
+                                             ms.ctypes.data_as(_fp)))
+    return ms
+
+
 def shape_class(p, m, n, k) -> tuple:
     """Quarter-octave class of a product's shape and its limb count (the key of
     the engine's plan table, sched.cu shape_key)."""
@@ -245,19 +295,35 @@ def sample_stream_shapes(n: int, seed: int = 11):
     return np.column_stack([P, S]).astype(np.uint32), dens
 
 
-def collect_batch(engine, n: int, seed: int = 11, reps: int = 3):
+def collect_batch(engine, n: int, seed: int = 11, reps: int = 3, budget_s=None):
     """Time every variant inside batches on n seeded stream shapes: (shapes, density, per-job ms)."""
     shapes, dens = sample_stream_shapes(n, seed)
-    T = np.zeros((n, N_VARIANTS), np.float32)
-    for i, (p, m, nn, k) in enumerate(shapes):
-        T[i] = autotune_batch(engine, p, m, nn, k, reps=reps)
-    return shapes, dens, T
+    return _timed_rows(shapes, dens, N_VARIANTS, lambda i: autotune_batch(engine, *shapes[i], reps=reps), budget_s)
 
 
-def collect(engine, n: int, seed: int = 11, reps: int = 3):
+def _timed_rows(shapes, dens, nv, time_row, budget_s):
+    """Time rows in order until all are done or `budget_s` seconds have passed:
+    (shapes, density, T) of the rows timed."""
+    import time
+
+    T = np.zeros((len(shapes), nv), np.float32)
+    t0, done = time.perf_counter(), 0
+    for i in range(len(shapes)):
+        T[i] = time_row(i)
+        done = i + 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
+    return shapes[:done], dens[:done], T[:done]
+
+
+def collect_batch_rank(engine, n: int, seed: int = 11, reps: int = 3, budget_s=None):
+    """Time every rank schedule inside batches on n seeded stream shapes: (shapes, density, per-job ms)."""
+    shapes, dens = sample_stream_shapes(n, seed)
+    return _timed_rows(shapes, dens, N_RANK_VARIANTS,
+                       lambda i: autotune_batch_rank(engine, *shapes[i], dens[i], reps=reps), budget_s)
+
+
+def collect(engine, n: int, seed: int = 11, reps: int = 3, budget_s=None):
     """Time every variant on n seeded shapes: (shapes, density, times ms)."""
     shapes, dens = sample_shapes(n, seed)
-    T = np.zeros((n, N_VARIANTS), np.float32)
-    for i, (p, m, nn, k) in enumerate(shapes):
-        T[i] = autotune(engine, p, m, nn, k, reps)
-    return shapes, dens, T
+    return _timed_rows(shapes, dens, N_VARIANTS, lambda i: autotune(engine, *shapes[i], reps), budget_s)

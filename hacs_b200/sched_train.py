@@ -13,6 +13,12 @@ hacs_b200/data/sched_timings.npz and hacs_b200/data/sched_mlp.npz.
 per job inside a batch of same-shape jobs (hme_autotune_batch, the cost a job
 adds to a batched call), written to sched_batch_timings.npz and
 sched_batch_mlp.npz; the method without the network is the batch rule.
+
+--rank trains the planner of the batched rank rounds: every rank schedule
+(trailing-update variant x widest last panel) is timed per job inside a
+batch of same-shape products (hme_autotune_batch_rank), written to
+sched_rank_timings.npz and sched_rank_mlp.npz; the method without the network
+is the rank rounds' batch rule (sched.rank_rule).
 """
 import argparse
 import json
@@ -36,10 +42,17 @@ def main():
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--reuse", action="store_true", help="train on the existing timing file")
     ap.add_argument("--batch", action="store_true", help="the batched stream's planner (per-job times in batches)")
+    ap.add_argument("--rank", action="store_true", help="the rank rounds' planner (per-job rank times in batches)")
+    ap.add_argument("--budget-s", type=float, default=None,
+                    help="stop timing shapes after this many seconds and train on the shapes timed so far")
     ap.add_argument("--out-dir", default=None, help="write the timing and weight files here (default: the package)")
     args = ap.parse_args()
-    timings = sched.BATCH_TIMINGS if args.batch else sched.TIMINGS
-    weights = sched.BATCH_WEIGHTS if args.batch else sched.WEIGHTS
+    if args.rank:
+        timings, weights = sched.RANK_TIMINGS, sched.RANK_WEIGHTS
+    else:
+        timings = sched.BATCH_TIMINGS if args.batch else sched.TIMINGS
+        weights = sched.BATCH_WEIGHTS if args.batch else sched.WEIGHTS
+    nv = sched.N_RANK_VARIANTS if args.rank else sched.N_VARIANTS
     if args.out_dir:
         os.makedirs(args.out_dir, exist_ok=True)
         timings = os.path.join(args.out_dir, os.path.basename(timings))
@@ -50,9 +63,9 @@ def main():
         shapes, dens, T = d["shapes"], d["density"], d["ms"]
     else:
         t0 = time.time()
-        collect = sched.collect_batch if args.batch else sched.collect
-        shapes, dens, T = collect(eng, args.shapes, args.seed, args.reps)
-        print(f"timed {len(shapes)} shapes x {sched.N_VARIANTS} variants in {time.time() - t0:.1f} s", flush=True)
+        collect = sched.collect_batch_rank if args.rank else sched.collect_batch if args.batch else sched.collect
+        shapes, dens, T = collect(eng, args.shapes, args.seed, args.reps, budget_s=args.budget_s)
+        print(f"timed {len(shapes)} shapes x {nv} variants in {time.time() - t0:.1f} s", flush=True)
         os.makedirs(os.path.dirname(timings), exist_ok=True)
         np.savez_compressed(timings, shapes=shapes, density=dens, ms=T)
     F = sched.raw_features(shapes[:, 0], shapes[:, 1], shapes[:, 2], shapes[:, 3], dens)
@@ -64,12 +77,15 @@ def main():
     tt = time.time() - t0
     mlp.save(weights)
     ch = mlp.choose(F[cut:])
+    rule = sched.rank_rule(shapes[cut:, 1]) if args.rank else None
     rep = {"train_shapes": cut, "test_shapes": n - cut, "train_loss": loss, "train_s": tt,
            "regret_mlp": sched.regret(T[cut:], ch),
-           "regret_heuristic": (None if args.batch else sched.regret(T[cut:], sched.heuristic_choice(F[cut:]))),
-           "regret_always_wide": sched.regret(T[cut:], np.zeros(n - cut, int)),
-           "variant_share_best": np.bincount(T[cut:].argmin(1), minlength=4).tolist(),
-           "variant_share_mlp": np.bincount(ch, minlength=4).tolist()}
+           "regret_heuristic": (sched.regret(T[cut:], rule) if args.rank else None if args.batch
+                                else sched.regret(T[cut:], sched.heuristic_choice(F[cut:]))),
+           # variant 0: wide tensor-core tiles (GEMM planners); the batch rule (rank planner)
+           "regret_variant0": sched.regret(T[cut:], np.zeros(n - cut, int)),
+           "variant_share_best": np.bincount(T[cut:].argmin(1), minlength=nv).tolist(),
+           "variant_share_mlp": np.bincount(ch, minlength=nv).tolist()}
     print(json.dumps(rep), flush=True)
 
 

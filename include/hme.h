@@ -350,6 +350,27 @@ HME_API int hme_batch_gemm_rank_u32_dev_plan(hme_ctx *ctx, uint32_t njobs, const
 HME_API int hme_batch_rank_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, uint32_t *ranks);
 HME_API int hme_batch_gemm_rank_u32_dev(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, uint32_t *ranks);
 HME_API int hme_gen_jobs_u32_dev(hme_ctx *ctx, uint32_t nmat, const hme_gen_spec *specs);
+/* The rank rounds' schedules (no counterpart in the reference, whose ranks of
+ * p > 127 run on the host, elim::column_rank_profile, DenseElim.h:160-169).
+ * rank_variants[j] picks, for job j's rounds, the trailing-update variant and
+ * the widest last panel (a job whose remaining columns fit it finishes in that
+ * one panel on one CTA; otherwise its rounds take 32 columns):
+ *   0 the grouped tensor-core limb GEMM, last panel up to 128 columns,
+ *   1 the grouped tensor-core limb GEMM, 32-column rounds to the end,
+ *   2 the CUDA-core update (a list of 64 x 64 tiles over a persistent grid,
+ *     exact 96-bit dot products), last panel up to 128 columns,
+ *   3 the CUDA-core update, 32-column rounds to the end,
+ *  -1 the batch rule: 0 for jobs of at most 128 rows, else 1 (a taller job's
+ *     last panel is a long serial chain on one CTA that the round waits for).
+ * rank_variants = NULL takes the context's scheduler (under the learned policy
+ * the rank planner's decision per job's shape class, recorded by
+ * hme_sched_plan_rank; else the batch rule).  No schedule changes a rank.
+ * hme_batch_gemm_rank_u32_dev_sched: the GEMM phase under gemm_variants (as
+ * hme_batch_gemm_u32_dev_plan), then the rank phase under rank_variants. */
+HME_API int hme_batch_rank_u32_dev_sched(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs, const int *rank_variants,
+                                         uint32_t *ranks);
+HME_API int hme_batch_gemm_rank_u32_dev_sched(hme_ctx *ctx, uint32_t njobs, const hme_job *jobs,
+                                              const int *gemm_variants, const int *rank_variants, uint32_t *ranks);
 
 /* ---- scheduler: GEMM variants, exhaustive autotuner, learned MLP planner -------
  * Variants (every one computes the same residues; a schedule changes speed
@@ -386,6 +407,18 @@ HME_API int hme_autotune_gemm(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, 
  * per-job device time of variant v inside a batch. */
 HME_API int hme_autotune_batch(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, uint32_t count, int reps,
                                float *ms);
+/* The exhaustive autotuner of the rank rounds: `count` products C = A B of
+ * one shape (m <= 1024, p prime) built like the stream's jobs (banded sparse
+ * operands when density < 0.5, dense uniform ones otherwise) and one anchor
+ * (a dense 1024 x 1024 product of full rank on the batch rule, whose rounds run
+ * as long as the stream's largest jobs'); the batched rank of fresh copies of
+ * them under each rank schedule in turn (hme_batch_rank_u32_dev_sched), and of
+ * the anchor alone.  ms[v] = (median time with the jobs on schedule v - median
+ * time of the anchor alone) / count: the device time a job on schedule v adds
+ * to a stream whose rounds run anyway (floored at 1 us per batch).  Fails
+ * (HME_EINVAL) if two schedules disagree on a rank. */
+HME_API int hme_autotune_batch_rank(hme_ctx *ctx, uint32_t p, uint32_t m, uint32_t n, uint32_t k, float density,
+                                    uint32_t count, int reps, float *ms);
 HME_API int hme_mlp_param_count(void);
 HME_API int hme_mlp_create(hme_ctx *ctx, uint64_t seed, hme_mlp **out);
 HME_API int hme_mlp_destroy(hme_mlp *mlp);
@@ -397,6 +430,11 @@ HME_API int hme_mlp_train(hme_mlp *mlp, uint32_t n, const float *X, const float 
 HME_API int hme_mlp_predict_bf16(hme_mlp *mlp, uint32_t n, const float *X, float *Y);
 HME_API int hme_sched_plan(hme_ctx *ctx, hme_mlp *mlp, uint32_t n, const uint32_t *shapes, const float *density,
                            const float *norm, int *variants);
+/* The same for the rank rounds: a network trained on hme_autotune_batch_rank
+ * timings picks each job's rank schedule (0..3 above), recorded in the
+ * context's rank plan (used by the batched calls under the learned policy). */
+HME_API int hme_sched_plan_rank(hme_ctx *ctx, hme_mlp *mlp, uint32_t n, const uint32_t *shapes, const float *density,
+                                const float *norm, int *variants);
 
 /* ---- device-resident blocked LU over Z/2^32 and Z/2^64 (ring2k device ops) ----
  * The session behind engine::ring2k::device::Ops (src/ModArithmetic/Binary/

@@ -146,6 +146,11 @@ def test_config4_full_stream_matches_reference(engine):
     engine.gen_jobs_dev(st.specs)
     ranks = engine.batch_gemm_rank_dev(st.jobs)
     assert np.array_equal(ranks, want_rank)
+    # every rank-round schedule at full size: job j on schedule j mod 4
+    engine.gen_jobs_dev(st.specs)
+    ranks = engine.batch_gemm_rank_dev(st.jobs, rank_variants=np.arange(st.n_jobs) % 4)
+    bad = np.nonzero(ranks != want_rank)[0]
+    assert bad.size == 0, f"{bad.size} ranks differ under the mixed rank schedules, first {bad[:5].tolist()}"
 
 
 def test_batch_mixed_with_jobs_taller_than_one_panel_cta(engine):
@@ -224,3 +229,83 @@ def test_batch_autotuner_times_every_variant(engine):
         rc = _lib.lib().hme_autotune_batch(engine._h, p, m, n, k, count, 3, ms.ctypes.data_as(C_.POINTER(C_.c_float)))
         assert rc == 0, _lib.lib().hme_last_error().decode()
         assert np.all(ms > 0) and np.all(np.isfinite(ms))
+
+
+def _planted(rng, m, n, r, p):
+    L = rng.integers(0, p, (m, r), dtype=np.uint64).astype(np.uint32)
+    R = rng.integers(0, p, (r, n), dtype=np.uint64).astype(np.uint32)
+    return O.gemm(p, L, R)
+
+
+def test_batch_rank_schedules_match_oracle(engine):
+    """Every rank-round schedule (trailing update on the grouped tensor-core limb
+    GEMM or on CUDA cores; a last panel of up to 128 columns or 32-column rounds
+    to the end; and -1 the batch rule), mixed
+    in one call over five moduli (one to four limbs, p above 2^31 included), under
+    five rotations of the schedules over the jobs.  The jobs have planted ranks
+    below their sides (a wrong trailing update raises the rank), wide, tall and
+    ragged shapes, trailing blocks both smaller and larger than one 64 x 64
+    CUDA-core tile; every rank equals the oracle's."""
+    import torch
+
+    rng = np.random.default_rng(17)
+    cases = [(100, 300, 40), (64, 700, 64), (200, 150, 150), (129, 200, 60), (390, 390, 200), (700, 500, 300),
+             (33, 1000, 20), (500, 64, 30), (16, 16, 16), (1, 50, 1), (50, 1, 1), (1024, 700, 650), (77, 77, 77)]
+    moduli = [251, 65521, 16777213, 2147483629, 4294967291]
+    mats, want = [], []
+    for t, (m, n, r) in enumerate(cases * 2):
+        p = moduli[t % len(moduli)]
+        A = _planted(rng, m, n, r, p)
+        mats.append((p, A))
+        want.append(len(O.rref(p, A)[1]))
+    for rot in range(5):
+        jobs = [{"p": p, "A": None, "B": None, "C": _dev(A)} for p, A in mats]
+        var = np.array([((t + rot) % 5) - 1 for t in range(len(jobs))], dtype=np.int32)
+        torch.cuda.synchronize()
+        ranks = engine.batch_rank_dev(jobs, rank_variants=var)
+        assert list(ranks) == want, f"rotation {rot}"
+
+
+def test_batch_gemm_rank_sched_config4_sample(engine):
+    """The first 64 config-4 jobs (sides capped at 384) through
+    hme_batch_gemm_rank_u32_dev_sched with both phases' schedules mixed: every
+    GEMM schedule against every rank schedule; ranks equal the oracle's."""
+    import torch
+
+    s, fam, p, sa, sb = gen.job_stream(64)
+    jobs, want = [], []
+    for j in range(64):
+        n = int(min(s[j], 384))
+        jobs.append({"p": int(p[j]), "A": torch.zeros((n, n), dtype=torch.int32, device="cuda"),
+                     "B": torch.zeros((n, n), dtype=torch.int32, device="cuda"),
+                     "C": torch.zeros((n, n), dtype=torch.int32, device="cuda")})
+        Ah = gen.job_matrix(n, n, int(p[j]), int(fam[j]), int(sa[j]))
+        Bh = gen.job_matrix(n, n, int(p[j]), int(fam[j]), int(sb[j]))
+        want.append(len(O.rref(int(p[j]), O.gemm(int(p[j]), Ah, Bh))[1]))
+    engine.gen_jobs_dev([(jb["A"], jb["p"], int(fam[j]), int(sa[j])) for j, jb in enumerate(jobs)] +
+                        [(jb["B"], jb["p"], int(fam[j]), int(sb[j])) for j, jb in enumerate(jobs)])
+    gv = np.array([(j % 5) - 1 for j in range(64)], np.int32)
+    rv = np.array([((j // 5) % 5) - 1 for j in range(64)], np.int32)
+    ranks = engine.batch_gemm_rank_dev(jobs, gemm_variants=gv, rank_variants=rv)
+    assert list(ranks) == want
+
+
+def test_rank_autotuner_times_every_schedule(engine):
+    import ctypes as C_
+
+    from hacs_b200 import _lib, sched
+
+    for (p, m, n, k, dens, count) in [(65521, 48, 48, 48, 1.0, 16), (2147483629, 300, 300, 280, 1.0, 2),
+                                      (65521, 200, 200, 200, 0.05, 2)]:
+        ms = sched.autotune_batch_rank(engine, p, m, n, k, dens, count=count, reps=2)
+        assert ms.shape == (sched.N_RANK_VARIANTS,)
+        assert np.all(ms > 0) and np.all(np.isfinite(ms))
+    L = _lib.lib()
+    ms = np.zeros(4, np.float32)
+    fp = ms.ctypes.data_as(C_.POINTER(C_.c_float))
+    # rows beyond one panel CTA, and a composite modulus, are refused before anything runs
+    assert L.hme_autotune_batch_rank(engine._h, 65521, 1100, 64, 64, 1.0, 1, 1, fp) == _lib.HME_EINVAL
+    assert L.hme_autotune_batch_rank(engine._h, 65536, 64, 64, 64, 1.0, 1, 1, fp) == _lib.HME_EINVAL
+    jobs = [{"p": 65521, "A": None, "B": None, "C": _dev(np.zeros((8, 8), np.uint32))}]
+    with pytest.raises(_lib.HmeError):
+        engine.batch_rank_dev(jobs, rank_variants=[4])

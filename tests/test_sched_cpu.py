@@ -43,3 +43,24 @@ def test_shape_sampler_is_seeded():
     b, db = sched.sample_shapes(50, 3)
     assert np.array_equal(a, b) and np.array_equal(da, db)
     assert a[:, 1:].min() >= 16 and a[:, 1:].max() <= 4096
+
+
+def test_rank_batch_count_and_timing_budget():
+    """The rank autotuner's batch sizes (about 2^27 elimination multiply-adds per
+    batch, 1 .. 256 jobs) and the collection loop's time budget (rows are timed
+    in order; the rows timed so far are kept when the budget runs out)."""
+    assert sched.rank_batch_count(16, 16, 16) == 256
+    assert sched.rank_batch_count(1024, 1024, 1024) == 1
+    assert sched.rank_batch_count(200, 300, 20) == 2 ** 27 // (200 * 300 * 20)
+    shapes, dens = sched.sample_stream_shapes(7, seed=3)
+    calls = []
+
+    def row(i):
+        calls.append(i)
+        return np.full(sched.N_RANK_VARIANTS, i + 1.0)
+
+    s, d, T = sched._timed_rows(shapes, dens, sched.N_RANK_VARIANTS, row, None)
+    assert calls == list(range(7)) and T.shape == (7, 4) and np.array_equal(s, shapes)
+    calls.clear()
+    s, d, T = sched._timed_rows(shapes, dens, sched.N_RANK_VARIANTS, row, -1.0)  # budget spent after row 0
+    assert calls == [0] and len(s) == len(d) == len(T) == 1 and T[0, 0] == 1.0

@@ -103,6 +103,37 @@ def test_learned_plan_routes_gemms_without_changing_values(engine):
     assert np.array_equal(got, O.gemm(p, A, B))
 
 
+def test_learned_rank_plan_routes_rank_rounds_without_changing_ranks(engine):
+    """A rank-planner network whose outputs prefer schedule 2 (the CUDA-core
+    trailing update, last panel up to 128 columns): after hme_sched_plan_rank, policy 1 runs
+    the planned jobs' trailing updates on CUDA cores and no grouped limb GEMM
+    in their rank rounds; the rank is unchanged."""
+    import torch
+
+    mlp = sched.MLP(engine, seed=1)
+    w = np.zeros(mlp.n_params, np.float32)
+    w[-4:] = [1.0, 1.0, 0.0, 1.0]
+    mlp.set_params(w)
+    p, m, n, r = 2147483629, 200, 300, 120
+    assert list(mlp.plan_rank(np.array([[p, m, n, r]], np.uint32))) == [2]
+    rng = np.random.default_rng(8)
+    A = rng.integers(0, p, (m, r), dtype=np.uint64).astype(np.uint32)
+    B = rng.integers(0, p, (r, n), dtype=np.uint64).astype(np.uint32)
+    jobs = [{"p": p, "A": _dev(A), "B": _dev(B), "C": torch.zeros((m, n), dtype=torch.int32, device="cuda")}]
+    L = _lib.lib()
+    try:
+        _lib.check(L.hme_ctx_set_sched_policy(engine._h, 1))
+        engine.set_timing(True)
+        engine.timing_reset()
+        ranks = engine.batch_gemm_rank_dev(jobs)
+        _, simt_launches = engine.kernel_time("batch_simt_update")
+    finally:
+        engine.set_timing(False)
+        _lib.check(L.hme_ctx_set_sched_policy(engine._h, 0))
+    assert simt_launches > 0
+    assert list(ranks) == [len(O.rref(p, O.gemm(p, A, B))[1])] == [r]
+
+
 @pytest.mark.skipif(not os.path.exists(sched.TIMINGS), reason="no measured timing set in the package")
 def test_trained_network_gains_over_the_heuristic(engine):
     """Trained on the GPU from the committed autotuner timings (80 %), the MLP's
@@ -117,4 +148,22 @@ def test_trained_network_gains_over_the_heuristic(engine):
     r_mlp = sched.regret(T[cut:], mlp.choose(F[cut:]))
     r_heur = sched.regret(T[cut:], sched.heuristic_choice(F[cut:]))
     assert r_mlp < r_heur
+    assert r_mlp <= 0.05
+
+
+@pytest.mark.skipif(not os.path.exists(sched.RANK_TIMINGS), reason="no measured rank timing set in the package")
+def test_trained_rank_network_gains_over_the_rank_rule(engine):
+    """The rank rounds' planner: trained on the GPU from the committed marginal
+    rank timings (hme_autotune_batch_rank, 80 %), its BF16 choices on the
+    held-out 20 % have lower regret than the rank rounds' batch rule (the method
+    without it) and stay within 5 % of the autotuner."""
+    d = np.load(sched.RANK_TIMINGS)
+    shapes, dens, T = d["shapes"], d["density"], d["ms"]
+    F = sched.raw_features(shapes[:, 0], shapes[:, 1], shapes[:, 2], shapes[:, 3], dens)
+    cut = int(0.8 * len(F))
+    mlp = sched.MLP(engine, seed=5)
+    mlp.fit(F[:cut], T[:cut], epochs=300, batch=256, lr=2e-3)
+    r_mlp = sched.regret(T[cut:], mlp.choose(F[cut:]))
+    r_rule = sched.regret(T[cut:], sched.rank_rule(shapes[cut:, 1]))
+    assert r_mlp < r_rule
     assert r_mlp <= 0.05
