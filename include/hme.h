@@ -358,7 +358,7 @@ HME_API int hme_gen_jobs_u32_dev(hme_ctx *ctx, uint32_t nmat, const hme_gen_spec
  *   0 the grouped tensor-core limb GEMM, last panel up to 128 columns,
  *   1 the grouped tensor-core limb GEMM, 32-column rounds to the end,
  *   2 the CUDA-core update (a list of 64 x 64 tiles over a persistent grid,
- *     exact 96-bit dot products), last panel up to 128 columns,
+ *     exact dot products), last panel up to 128 columns,
  *   3 the CUDA-core update, 32-column rounds to the end,
  *  -1 the batch rule: 0 for jobs of at most 128 rows, else 1 (a taller job's
  *     last panel is a long serial chain on one CTA that the round waits for).
