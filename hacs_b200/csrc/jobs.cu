@@ -438,8 +438,10 @@ __global__ void batch_gather_l21_kernel(const SolveJob* __restrict__ jobs) {
 // appends its tiles; tile_job[t] = the job, t - simt_base its tile in row-major
 // tile order), taken by a persistent grid, so a large job's tiles spread over
 // the whole GPU and the launch has no idle CTAs for jobs on the other
-// schedule.  A CTA stages the tile's L21 rows and U12 columns in shared
-// memory and gives each thread 4 x 4 outputs (rows ty + 16a, columns tx + 16b,
+// schedule.  A CTA copies the next tile's L21 rows and U12 columns into its
+// second shared-memory buffer (cp.async) while it multiplies the current
+// tile's, loads the current tile's old A22 values before the multiply-adds,
+// and gives each thread 4 x 4 outputs (rows ty + 16a, columns tx + 16b,
 // so a half warp writes 16 consecutive words of a row); each output is an
 // exact dot product reduced once: a 64-bit sum when kRoundBw (p - 1)^2 fits
 // 64 bits (one wide multiply-add per product), else a 96-bit sum
@@ -448,37 +450,68 @@ constexpr int kSimtTile = 64;
 __host__ __device__ inline int simt_tiles(int rows, int cols) {
     return ((rows + kSimtTile - 1) / kSimtTile) * ((cols + kSimtTile - 1) / kSimtTile);
 }
-__global__ void __launch_bounds__(256) batch_simt_update_kernel(const SolveJob* __restrict__ jobs,
-                                                                const int* __restrict__ tile_job,
-                                                                const int* __restrict__ count) {
-    __shared__ uint32_t sL[kSimtTile][kRoundBw + 1];
-    __shared__ uint32_t sU[kRoundBw][kSimtTile];
+__global__ void __launch_bounds__(256, 2) batch_simt_update_kernel(const SolveJob* __restrict__ jobs,
+                                                                   const int* __restrict__ tile_job,
+                                                                   const int* __restrict__ count) {
+    // two operand buffers: tile t's L21 rows / U12 columns are consumed while tile t + gridDim.x's are copied
+    __shared__ uint32_t sL[2][kSimtTile][kRoundBw + 1];
+    __shared__ uint32_t sU[2][kRoundBw][kSimtTile];
     const int total = *count;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {  // t is the same for the whole CTA
+    // the job of tile t and the tile's first row / column in the job's trailing block
+    auto locate = [&](int t, int& i0, int& j0) -> const SolveJob& {
         const SolveJob& J = jobs[tile_job[t]];
+        const int tc = (J.ntrail + kSimtTile - 1) / kSimtTile, local = t - J.simt_base;
+        i0 = (local / tc) * kSimtTile;
+        j0 = (local % tc) * kSimtTile;
+        return J;
+    };
+    // tile t's operands into buffer b as one asynchronous copy group (zero-filled outside the block)
+    auto stage = [&](int t, int b) {
+        int i0, j0;
+        const SolveJob& J = locate(t, i0, j0);
         const int k = J.k, below = J.m - J.r0 - k;
-        const int tc = (J.ntrail + kSimtTile - 1) / kSimtTile;
-        const int local = t - J.simt_base;
-        const int i0 = (local / tc) * kSimtTile, j0 = (local % tc) * kSimtTile;
         const uint32_t* U = J.A + static_cast<size_t>(J.r0) * J.ld + J.c1;
-        uint32_t* A22 = J.A + static_cast<size_t>(J.r0 + k) * J.ld + J.c1;
-        __syncthreads();  // the previous tile's operands are consumed
         for (int idx = threadIdx.x; idx < kSimtTile * k; idx += blockDim.x) {
             const int i = idx / k, s = idx - i * k;
-            sL[i][s] = i0 + i < below ? J.L21[static_cast<size_t>(i0 + i) * k + s] : 0u;
+            const bool v = i0 + i < below;
+            cp_async4(&sL[b][i][s], v ? J.L21 + static_cast<size_t>(i0 + i) * k + s : J.L21, v);
         }
         for (int idx = threadIdx.x; idx < k * kSimtTile; idx += blockDim.x) {
             const int s = idx / kSimtTile, j = idx % kSimtTile;
-            sU[s][j] = j0 + j < J.ntrail ? U[static_cast<size_t>(s) * J.ld + j0 + j] : 0u;
+            const bool v = j0 + j < J.ntrail;
+            cp_async4(&sU[b][s][j], v ? U + static_cast<size_t>(s) * J.ld + j0 + j : U, v);
         }
-        __syncthreads();
-        auto sub = [&](int a, int b, uint32_t d) {  // A22(i, j) -= d mod p
-            const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+        cp_async_commit();
+    };
+    if (static_cast<int>(blockIdx.x) < total) stage(blockIdx.x, 0);
+    int it = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {  // t is the same for the whole CTA
+        const int b = it & 1;
+        // the next tile's copies start now (an empty group when there is none, so the wait below
+        // always leaves exactly the newest group in flight)
+        if (t + static_cast<int>(gridDim.x) < total) stage(t + gridDim.x, b ^ 1);
+        else cp_async_commit();
+        int i0, j0;
+        const SolveJob& J = locate(t, i0, j0);
+        const int k = J.k, below = J.m - J.r0 - k;
+        uint32_t* A22 = J.A + static_cast<size_t>(J.r0 + k) * J.ld + J.c1;
+        // the old A22 values, in flight during the wait and the multiply-adds
+        uint32_t old[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * c;
+                old[a][c] = (i < below && j < J.ntrail) ? A22[static_cast<size_t>(i) * J.ld + j] : 0u;
+            }
+        cp_async_wait<1>();
+        __syncthreads();  // every thread's copies of this tile's operands have landed
+        auto sub = [&](int a, int c, uint32_t d) {  // A22(i, j) = old - d mod p
+            const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * c;
             if (i >= below || j >= J.ntrail) return;
-            uint32_t* c = A22 + static_cast<size_t>(i) * J.ld + j;
-            const uint32_t x = *c;
-            *c = x >= d ? x - d : x + (J.p - d);
+            const uint32_t x = old[a][c];
+            A22[static_cast<size_t>(i) * J.ld + j] = x >= d ? x - d : x + (J.p - d);
         };
         const uint64_t pm1 = J.p - 1u;
         if (pm1 * pm1 <= ~0ull / kRoundBw) {
@@ -487,49 +520,51 @@ __global__ void __launch_bounds__(256) batch_simt_update_kernel(const SolveJob* 
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) acc[a][b] = 0u;
+                for (int c = 0; c < 4; ++c) acc[a][c] = 0u;
             for (int s = 0; s < k; ++s) {
                 uint32_t l[4], u[4];
 #pragma unroll
-                for (int a = 0; a < 4; ++a) l[a] = sL[ty + 16 * a][s];
+                for (int a = 0; a < 4; ++a) l[a] = sL[b][ty + 16 * a][s];
 #pragma unroll
-                for (int b = 0; b < 4; ++b) u[b] = sU[s][tx + 16 * b];
+                for (int c = 0; c < 4; ++c) u[c] = sU[b][s][tx + 16 * c];
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) acc[a][b] += static_cast<uint64_t>(l[a]) * u[b];
+                    for (int c = 0; c < 4; ++c) acc[a][c] += static_cast<uint64_t>(l[a]) * u[c];
             }
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) sub(a, b, reduce_u64(acc[a][b], J.p, J.barrett));
+                for (int c = 0; c < 4; ++c) sub(a, c, reduce_u64(acc[a][c], J.p, J.barrett));
         } else {
             uint32_t a0[4][4], a1[4][4], a2[4][4];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) a0[a][b] = a1[a][b] = a2[a][b] = 0u;
+                for (int c = 0; c < 4; ++c) a0[a][c] = a1[a][c] = a2[a][c] = 0u;
             for (int s = 0; s < k; ++s) {
                 uint32_t l[4], u[4];
 #pragma unroll
-                for (int a = 0; a < 4; ++a) l[a] = sL[ty + 16 * a][s];
+                for (int a = 0; a < 4; ++a) l[a] = sL[b][ty + 16 * a][s];
 #pragma unroll
-                for (int b = 0; b < 4; ++b) u[b] = sU[s][tx + 16 * b];
+                for (int c = 0; c < 4; ++c) u[c] = sU[b][s][tx + 16 * c];
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) mac96(a0[a][b], a1[a][b], a2[a][b], l[a], u[b]);
+                    for (int c = 0; c < 4; ++c) mac96(a0[a][c], a1[a][c], a2[a][c], l[a], u[c]);
             }
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
+                for (int c = 0; c < 4; ++c) {
                     const uint64_t h =
-                        reduce_u64((static_cast<uint64_t>(a2[a][b]) << 32) | a1[a][b], J.p, J.barrett);
-                    sub(a, b, reduce_u64((h << 32) | a0[a][b], J.p, J.barrett));
+                        reduce_u64((static_cast<uint64_t>(a2[a][c]) << 32) | a1[a][c], J.p, J.barrett);
+                    sub(a, c, reduce_u64((h << 32) | a0[a][c], J.p, J.barrett));
                 }
         }
+        __syncthreads();  // buffer b is consumed before the next iteration copies into it
     }
+    cp_async_wait<0>();  // no copy outlives the kernel
 }
 
 size_t a256(size_t x) { return (x + 255) / 256 * 256; }
