@@ -7,9 +7,9 @@ tiles, 1 limb tcgen05 half-width tiles, 2 CUDA-core 32 x 32, 3 CUDA-core
 grouped tcgen05 limb GEMM as the trailing update, 2 / 3 the CUDA-core update;
 0 / 2 finish a job in one last panel of up to 128 columns, 1 / 3 take 32-column
 rounds to the end), each picked by its own network of the same shape, trained
-on its own autotuner's timings.  Every
-variant computes the same residues (and ranks), so neither the MLP nor the
-autotuner can change a value -- only the time.  The MLP (5 -> 3 x 64 -> 4,
+on its own autotuner's timings.  Every variant computes the same residues (and
+ranks), so neither the MLP nor the autotuner can change a value -- only the
+time.  The MLP (5 -> 3 x 64 -> 4,
 hand-written CUDA kernels: FP32 training, BF16 inference) predicts each
 variant's normalised log-time from (log2 m, log2 n, log2 k, log2 p, density);
 the exhaustive autotuner (hme_autotune_gemm) times all variants, supplies the
@@ -31,7 +31,7 @@ TIMINGS = os.path.join(DATA, "sched_timings.npz")
 # the batched stream's planner: trained on per-job times inside batches (hme_autotune_batch)
 BATCH_WEIGHTS = os.path.join(DATA, "sched_batch_mlp.npz")
 BATCH_TIMINGS = os.path.join(DATA, "sched_batch_timings.npz")
-# the rank rounds' planner: trained on per-job rank times inside batches (hme_autotune_batch_rank)
+# the rank rounds' planner: trained on per-job marginal rank times beside an anchor job (hme_autotune_batch_rank)
 RANK_WEIGHTS = os.path.join(DATA, "sched_rank_mlp.npz")
 RANK_TIMINGS = os.path.join(DATA, "sched_rank_timings.npz")
 BATCH_RULE = -1
