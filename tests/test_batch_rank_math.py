@@ -217,3 +217,50 @@ def test_rank_rounds_under_every_schedule_equal_oracle(bw, last_max):
             A = O.gemm(p, L, R) if r else np.zeros((m, n), np.uint32)
             want = len(O.rref(p, A)[1])
             assert _batched_rank(A, p, bw, last_max) == want, (p, m, n, r)
+
+
+def _barrett(x, p):
+    """reduce_u64: x - floor(x * floor(2^64 / p) / 2^64) * p, one correction."""
+    m = (1 << 64) // p
+    r = x - ((x * m) >> 64) * p
+    assert 0 <= r < 2 * p
+    return r - p if r >= p else r
+
+
+@pytest.mark.parametrize("p", [251, 65521, 16777213, 759250125, 759250133, 2147483629, 4294967291])
+def test_cuda_core_update_sums(p):
+    """The CUDA-core update's exact dot products of k <= 32 products: a 64-bit
+    sum when 32 (p - 1)^2 fits 64 bits, else a 96-bit sum (a0, a1, a2 words)
+    reduced as ((a2 2^32 + a1) mod p) 2^32 + a0 mod p; both equal the exact
+    sum mod p, worst case (p - 1)^2 included."""
+    rng = np.random.default_rng(p % 997)
+    narrow = (p - 1) * (p - 1) <= ((1 << 64) - 1) // 32
+    assert narrow == (p <= 759250125)
+    for trial in range(200):
+        k = int(rng.integers(1, 33))
+        if trial < 2:
+            x = [p - 1] * k
+            y = [p - 1] * k
+        else:
+            x = [int(v) for v in rng.integers(0, p, k, dtype=np.uint64)]
+            y = [int(v) for v in rng.integers(0, p, k, dtype=np.uint64)]
+        exact = sum(a * b for a, b in zip(x, y))
+        if narrow:
+            acc = 0
+            for a, b in zip(x, y):
+                acc = (acc + a * b) & ((1 << 64) - 1)
+            assert acc == exact  # no wraparound
+            d = _barrett(acc, p)
+        else:
+            a0 = a1 = a2 = 0
+            for a, b in zip(x, y):  # mad.lo.cc / madc.hi.cc / addc
+                prod = a * b
+                s0 = a0 + (prod & 0xFFFFFFFF)
+                a0, c0 = s0 & 0xFFFFFFFF, s0 >> 32
+                s1 = a1 + (prod >> 32) + c0
+                a1, c1 = s1 & 0xFFFFFFFF, s1 >> 32
+                a2 = (a2 + c1) & 0xFFFFFFFF
+            assert (a2 << 64) | (a1 << 32) | a0 == exact
+            h = _barrett((a2 << 32) | a1, p)
+            d = _barrett((h << 32) | a0, p)
+        assert d == exact % p
