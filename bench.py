@@ -694,12 +694,13 @@ def serve_stream(eng, ms, plan, rank_plan=None, warm: bool = False):
 
 def extra_scheduler(eng, n_stream=50000):
     """Config 5: the 50,000-job mixed stream (stream.MixedStream: config-4 jobs, config-2 rank-deficient
-    products, config-1 products) served end to end through the batched GEMM + rank call under three plans,
-    each a per-job GEMM schedule and a per-job rank-round schedule (trailing-update variant, panel width of
-    the rounds): the learned planners' (two MLPs trained on this engine's batch autotuner timings of the GEMM
-    phase and of the rank rounds, one BF16 inference launch each for the whole stream), the batch rules (the
-    method without the networks) and the exhaustive batch autotuners' best per shape class.  Ranks are
-    checked across plans and against the reference / the construction."""
+    products, config-1 products) served end to end through the batched GEMM + rank call under four plans,
+    each a per-job GEMM schedule and a per-job rank-round schedule (trailing-update variant, widest last
+    panel): the learned planners' (two MLPs trained on this engine's batch autotuner timings of the GEMM
+    phase and of the rank rounds, one BF16 inference launch each for the whole stream), the same networks
+    with the exhaustive autotuner as their fallback in the shape classes where a network is not
+    confident, the batch rules (the method without the networks) and the exhaustive batch autotuners'
+    best per shape class.  Ranks are checked across plans and against the reference / the construction."""
     from hacs_b200 import sched, stream
 
     if not os.path.exists(sched.BATCH_WEIGHTS):
@@ -713,9 +714,14 @@ def extra_scheduler(eng, n_stream=50000):
     t0 = time.perf_counter()
     learned = mlp.plan(shapes, dens)
     t_plan = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    learned_fb, fb_classes = sched.plan_with_fallback(mlp, eng, shapes, dens)
+    t_fb = time.perf_counter() - t0
     mlp.close()
     rule_rank = np.full(ms.n_jobs, sched.BATCH_RULE, np.int32)
-    learned_rank, t_plan_rank = rule_rank, 0.0
+    learned_rank = learned_fb_rank = rule_rank
+    t_plan_rank = t_fb_rank = 0.0
+    fb_classes_rank = 0
     if have_rank:
         mlp_r = sched.MLP(eng)
         mlp_r.load(sched.RANK_WEIGHTS)
@@ -723,6 +729,9 @@ def extra_scheduler(eng, n_stream=50000):
         t0 = time.perf_counter()
         learned_rank = mlp_r.plan_rank(shapes, dens)
         t_plan_rank = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        learned_fb_rank, fb_classes_rank = sched.plan_with_fallback(mlp_r, eng, shapes, dens, rank=True)
+        t_fb_rank = time.perf_counter() - t0
         mlp_r.close()
     # the exhaustive autotuners: every variant timed inside a batch, once per shape class of the stream
     t0 = time.perf_counter()
@@ -740,6 +749,7 @@ def extra_scheduler(eng, n_stream=50000):
     serve_stream(eng, ms, rule, warm=True)  # workspace growth, module load
     res = {}
     for name, plan, rplan in (("heuristic", rule, rule_rank), ("learned", learned, learned_rank),
+                              ("learned_with_fallback", learned_fb, learned_fb_rank),
                               ("autotuner_best", best, best_rank)):
         ts, rk = [], None
         for _ in range(2):
@@ -751,6 +761,7 @@ def extra_scheduler(eng, n_stream=50000):
         res[name] = (min(ts), rk)
     t_h, r_h = res["heuristic"]
     t_l, r_l = res["learned"]
+    t_n, r_n = res["learned_with_fallback"]
     t_b, r_b = res["autotuner_best"]
     per_job = np.array([T[k] for k in keys])  # per-job batch times of every variant, by class
     rows = np.arange(ms.n_jobs)
@@ -758,10 +769,15 @@ def extra_scheduler(eng, n_stream=50000):
                        "rank-deficient products at 2^31-19, config-1 1024^3 products), GEMM + rank per job, "
                        f"served in chunks of {ms.chunk} (config 5)",
            "jobs_per_s_served": {"learned": ms.n_jobs / t_l, "heuristic": ms.n_jobs / t_h,
-                                 "autotuner_best": ms.n_jobs / t_b},
-           "served_s": {"learned": t_l, "heuristic": t_h, "autotuner_best": t_b},
+                                 "learned_with_fallback": ms.n_jobs / t_n, "autotuner_best": ms.n_jobs / t_b},
+           "served_s": {"learned": t_l, "heuristic": t_h, "learned_with_fallback": t_n, "autotuner_best": t_b},
            "regret_served_learned": (t_l - t_b) / t_b, "regret_served_heuristic": (t_h - t_b) / t_b,
+           "regret_served_learned_with_fallback": (t_n - t_b) / t_b,
            "learned_vs_heuristic": t_h / t_l,
+           "fallback": {"margin": 0.03, "gemm_classes": fb_classes, "rank_classes": fb_classes_rank,
+                        "gemm_s": t_fb, "rank_s": t_fb_rank,
+                        "rule": "a class falls back to the exhaustive autotuner when the network's best predicted "
+                                "time is within 3 % of its second best (sched.plan_with_fallback)"},
            "regret_per_job_model_learned": float(np.mean((per_job[rows, learned] - per_job.min(1)) / per_job.min(1))),
            "plan_ms": t_plan * 1e3, "plan_rank_ms": t_plan_rank * 1e3, "autotune_s": t_tune,
            "shape_classes": len(first),
@@ -771,7 +787,8 @@ def extra_scheduler(eng, n_stream=50000):
            "rank_variant_share_learned": np.bincount(np.maximum(learned_rank, 0),
                                                      minlength=sched.N_RANK_VARIANTS).tolist(),
            "rank_variant_share_best": np.bincount(np.maximum(best_rank, 0), minlength=sched.N_RANK_VARIANTS).tolist(),
-           "ranks_equal_across_plans": bool(np.array_equal(r_h, r_l) and np.array_equal(r_h, r_b)),
+           "ranks_equal_across_plans": bool(np.array_equal(r_h, r_l) and np.array_equal(r_h, r_b)
+                                            and np.array_equal(r_h, r_n)),
            "rank_checks": ms.check_ranks(r_l),
            "planner": "MLP 5-64-64-64-4 (hand-written FP32 training / BF16 inference kernels) trained on "
                       "hme_autotune_batch timings (python -m hacs_b200.sched_train --batch); the rank rounds' "

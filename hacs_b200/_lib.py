@@ -116,6 +116,7 @@ PROTOTYPES.update({
                                  C.POINTER(C.c_int)]),
     "hme_sched_plan_rank": (C.c_int, [vp, vp, u32, u32p, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                       C.POINTER(C.c_int)]),
+    "hme_sched_plan_set": (C.c_int, [vp, C.c_int, u32, u32p, C.POINTER(C.c_int)]),
     "hme_batch_gemm_u32_dev_plan": (C.c_int, [vp, u32, C.POINTER(HmeJob), C.POINTER(C.c_int)]),
     "hme_batch_gemm_rank_u32_dev_plan": (C.c_int, [vp, u32, C.POINTER(HmeJob), C.POINTER(C.c_int), u32p]),
     "hme_autotune_batch": (C.c_int, [vp, u32, u32, u32, u32, u32, C.c_int, C.POINTER(C.c_float)]),

@@ -22,12 +22,15 @@
 #include <unordered_map>
 #include <vector>
 
+#include "hme_grouped.h"
 #include "hme_internal.h"
 
 namespace hme {
 namespace {
 
 constexpr int kIn = 5, kH = 64, kOut = kGemmVariants;
+// one network shape serves both planners: its outputs are the GEMM variants or the rank schedules
+static_assert(static_cast<int>(kRankVariants) == kOut, "the rank planner reuses the GEMM planner's network shape");
 constexpr int kOffW1 = 0;
 constexpr int kOffB1 = kOffW1 + kIn * kH;
 constexpr int kOffW2 = kOffB1 + kH;
@@ -386,6 +389,24 @@ int hme_ctx_set_sched_policy(hme_ctx* ctx, int policy) {
         HME_REQUIRE(ctx != nullptr, "null context");
         HME_REQUIRE(policy == 0 || policy == 1, "policy: 0 heuristic, 1 learned plan");
         ctx->sched_policy = policy;
+    });
+}
+
+int hme_sched_plan_set(hme_ctx* ctx, int table, uint32_t n, const uint32_t* shapes, const int* variants) {
+    return guard([&] {
+        HME_REQUIRE(ctx && (n == 0 || (shapes && variants)), "null argument");
+        HME_REQUIRE(table == 0 || table == 1, "plan table: 0 the GEMM plan, 1 the rank plan");
+        const int nv = table == 0 ? static_cast<int>(kGemmVariants) : static_cast<int>(kRankVariants);
+        for (uint32_t t = 0; t < n; ++t)  // every decision checked before any is recorded
+            HME_REQUIRE(variants[t] >= 0 && variants[t] < nv, "plan: unknown schedule");
+        void** tp = table == 0 ? &ctx->sched_table : &ctx->sched_rank_table;
+        if (!*tp) *tp = new PlanTable();
+        PlanTable& tab = *static_cast<PlanTable*>(*tp);
+        for (uint32_t t = 0; t < n; ++t) {
+            const uint32_t* s = shapes + 4 * static_cast<size_t>(t);
+            const uint32_t limbs = s[0] <= 256u ? 1u : s[0] <= 65536u ? 2u : s[0] <= (1u << 24) ? 3u : 4u;  // as make_mod
+            tab[shape_key(s[1], s[2], s[3], limbs)] = variants[t];
+        }
     });
 }
 

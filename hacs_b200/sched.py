@@ -13,7 +13,8 @@ time.  The MLP (5 -> 3 x 64 -> 4,
 hand-written CUDA kernels: FP32 training, BF16 inference) predicts each
 variant's normalised log-time from (log2 m, log2 n, log2 k, log2 p, density);
 the exhaustive autotuner (hme_autotune_gemm) times all variants, supplies the
-training data, and judges the MLP's regret.
+training data, judges the MLP's regret, and is its fallback where the network
+is not confident (plan_with_fallback).
 """
 from __future__ import annotations
 
@@ -160,6 +161,12 @@ class MLP:
                                        v.ctypes.data_as(C.POINTER(C.c_int))))
         return v[:n]
 
+    def predict_ms(self, F) -> np.ndarray:
+        """Predicted per-variant times (ms) for raw features F (n x 5), BF16 inference."""
+        F = np.asarray(F, np.float64)
+        Y = self.predict_normalised((F - self.x_mean) / self.x_std).astype(np.float64)
+        return np.exp(Y * self.y_std + self.y_mean)
+
     def plan_rank(self, shapes, density=None) -> np.ndarray:
         """hme_sched_plan_rank: the same for the rank rounds' schedules (a network
         trained on hme_autotune_batch_rank timings); records the decisions in the
@@ -173,6 +180,52 @@ class MLP:
                                             d.ctypes.data_as(_fp), nm.ctypes.data_as(_fp),
                                             v.ctypes.data_as(C.POINTER(C.c_int))))
         return v[:n]
+
+
+def fallback_classes(shapes, predicted_ms, margin: float):
+    """The shape classes where a network is not confident: its best predicted
+    time is within `margin` (relative) of its second best for some job of the
+    class.  Returns {class: index of its first such job}."""
+    T = np.sort(np.asarray(predicted_ms, np.float64), axis=1)
+    unsure = T[:, 1] <= T[:, 0] * (1.0 + margin)
+    first = {}
+    for t in np.nonzero(unsure)[0]:
+        first.setdefault(shape_class(*shapes[t]), int(t))
+    return first
+
+
+def plan_with_fallback(mlp, engine, shapes, density=None, rank: bool = False, margin: float = 0.03,
+                       autotune_fn=None):
+    """Per-job schedules from a planner network with the exhaustive autotuner as
+    its fallback: the network plans every job (hme_sched_plan / _plan_rank), and
+    in each shape class where it is not confident (fallback_classes) the
+    autotuner times every variant once and its best replaces the network's
+    choice, in the returned array and in the engine's plan (hme_sched_plan_set),
+    so policy 1 follows it too.  Returns (variants, classes that fell back)."""
+    S = np.ascontiguousarray(shapes, dtype=np.uint32)
+    n = S.shape[0]
+    d = np.ones(n) if density is None else np.asarray(density, np.float64)
+    v = (mlp.plan_rank if rank else mlp.plan)(S, d).copy()
+    if n == 0:
+        return v, 0
+    first = fallback_classes(S, mlp.predict_ms(raw_features(S[:, 0], S[:, 1], S[:, 2], S[:, 3], d)), margin)
+    if rank:  # jobs of more than 1024 rows take the single-matrix elimination: no rank schedule to choose
+        first = {key: t for key, t in first.items() if S[t, 1] <= 1024}
+    if not first:
+        return v, 0
+    if autotune_fn is None:
+        autotune_fn = ((lambda p, m, nn, k, dd: autotune_batch_rank(engine, p, m, nn, k, dd)) if rank
+                       else (lambda p, m, nn, k, dd: autotune_batch(engine, p, m, nn, k)))
+    best = {key: int(np.argmin(autotune_fn(*S[t], d[t]))) for key, t in first.items()}
+    for t in range(n):
+        b = best.get(shape_class(*S[t]))
+        if b is not None:
+            v[t] = b
+    rows = np.ascontiguousarray([S[t] for t in first.values()], dtype=np.uint32)
+    vals = np.ascontiguousarray([best[key] for key in first], dtype=np.int32)
+    check(_lib.lib().hme_sched_plan_set(engine._h, 1 if rank else 0, len(vals), rows.ctypes.data_as(_lib.u32p),
+                                        vals.ctypes.data_as(C.POINTER(C.c_int))))
+    return v, len(first)
 
 
 def heuristic_choice(F, num_sms: int = 148) -> np.ndarray:

@@ -430,6 +430,13 @@ HME_API int hme_mlp_train(hme_mlp *mlp, uint32_t n, const float *X, const float 
 HME_API int hme_mlp_predict_bf16(hme_mlp *mlp, uint32_t n, const float *X, float *Y);
 HME_API int hme_sched_plan(hme_ctx *ctx, hme_mlp *mlp, uint32_t n, const uint32_t *shapes, const float *density,
                            const float *norm, int *variants);
+/* Decisions recorded directly in the context's plan (table 0: the GEMM plan,
+ * table 1: the rank plan), one per shape row (p, m, n, k), replacing the
+ * network's for that shape class: the exhaustive autotuner's choice where the
+ * network is not confident (hacs_b200.sched.plan_with_fallback).  HME_EINVAL
+ * (nothing recorded) for a schedule outside 0..3.  No counterpart in the
+ * reference. */
+HME_API int hme_sched_plan_set(hme_ctx *ctx, int table, uint32_t n, const uint32_t *shapes, const int *variants);
 /* The same for the rank rounds: a network trained on hme_autotune_batch_rank
  * timings picks each job's rank schedule (0..3 above), recorded in the
  * context's rank plan (used by the batched calls under the learned policy). */

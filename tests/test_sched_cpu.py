@@ -64,3 +64,19 @@ def test_rank_batch_count_and_timing_budget():
     calls.clear()
     s, d, T = sched._timed_rows(shapes, dens, sched.N_RANK_VARIANTS, row, -1.0)  # budget spent after row 0
     assert calls == [0] and len(s) == len(d) == len(T) == 1 and T[0, 0] == 1.0
+
+
+def test_fallback_classes_pick_unconfident_shapes():
+    """A shape class falls back to the exhaustive autotuner when, for some job of
+    the class, the network's best predicted time is within the margin of its
+    second best; one job per class is timed."""
+    shapes = np.array([[65521, 100, 100, 100], [65521, 101, 101, 101],  # one class (quarter octaves)
+                       [65521, 500, 500, 500], [2147483629, 500, 500, 500]], np.uint32)
+    T = np.array([[1.00, 1.01, 2.0, 3.0],   # within 3 %: unsure
+                  [1.00, 1.50, 2.0, 3.0],   # same class, confident
+                  [1.00, 1.20, 2.0, 3.0],   # confident
+                  [2.00, 2.05, 2.0, 9.0]])  # a tie: unsure
+    first = sched.fallback_classes(shapes, T, 0.03)
+    assert sched.shape_class(*shapes[0]) == sched.shape_class(*shapes[1])
+    assert first == {sched.shape_class(*shapes[0]): 0, sched.shape_class(*shapes[3]): 3}
+    assert sched.fallback_classes(shapes, T, 0.0) == {sched.shape_class(*shapes[3]): 3}

@@ -2,6 +2,7 @@
 gradients against the CPU reference, BF16 inference against the reference's
 bf16 emulation, training, the learned plan routing GEMMs without changing a
 value, and the trained network's gain over the method without it."""
+import ctypes as C
 import os
 
 import numpy as np
@@ -167,3 +168,44 @@ def test_trained_rank_network_gains_over_the_rank_rule(engine):
     r_rule = sched.regret(T[cut:], sched.rank_rule(shapes[cut:, 1]))
     assert r_mlp < r_rule
     assert r_mlp <= 0.05
+
+
+def test_plan_with_fallback_records_the_autotuners_choice(engine):
+    """Where the network is not confident -- here a network whose outputs are all
+    equal, so every class is a tie -- the exhaustive autotuner's best replaces
+    the network's choice, once per shape class, in the returned plan and in the
+    engine's plan (hme_sched_plan_set), which policy 1 then follows; the rank is
+    unchanged.  The autotuner is a stand-in that prefers schedule 2."""
+    import torch
+
+    mlp = sched.MLP(engine, seed=1)
+    mlp.set_params(np.zeros(mlp.n_params, np.float32))
+    p, m, n, r = 2147483629, 200, 300, 120
+    shapes = np.array([[65521, 48, 48, 48], [p, m, n, r], [p, m, n, r]], np.uint32)
+    calls = []
+
+    def tuner(pp, mm, nn, kk, dd):
+        calls.append((int(pp), int(mm)))
+        return np.array([3.0, 2.0, 1.0, 4.0])
+
+    v, nfb = sched.plan_with_fallback(mlp, engine, shapes, rank=True, autotune_fn=tuner)
+    assert nfb == 2 and len(calls) == 2 and list(v) == [2, 2, 2]
+    L = _lib.lib()
+    bad = np.array([4], np.int32)
+    assert L.hme_sched_plan_set(engine._h, 1, 1, shapes[:1].ctypes.data_as(_lib.u32p),
+                                bad.ctypes.data_as(C.POINTER(C.c_int))) == _lib.HME_EINVAL
+    rng = np.random.default_rng(9)
+    A = rng.integers(0, p, (m, r), dtype=np.uint64).astype(np.uint32)
+    B = rng.integers(0, p, (r, n), dtype=np.uint64).astype(np.uint32)
+    jobs = [{"p": p, "A": _dev(A), "B": _dev(B), "C": torch.zeros((m, n), dtype=torch.int32, device="cuda")}]
+    try:
+        _lib.check(L.hme_ctx_set_sched_policy(engine._h, 1))
+        engine.set_timing(True)
+        engine.timing_reset()
+        ranks = engine.batch_gemm_rank_dev(jobs)
+        _, simt_launches = engine.kernel_time("batch_simt_update")
+    finally:
+        engine.set_timing(False)
+        _lib.check(L.hme_ctx_set_sched_policy(engine._h, 0))
+    assert simt_launches > 0  # schedule 2: the CUDA-core update
+    assert list(ranks) == [r]
